@@ -1,0 +1,360 @@
+#!/usr/bin/env python3
+"""Benchmark of the LBM hot path: D3Q19 MLUPS, FP32-shifted vs plain FP64.
+
+Workload (default): D3Q19 channel 256x128x128, nu 0.05 (tau 0.65), no-slip
+walls on y and z, x periodic, body force gx 1e-6, initial velocity at rest
+plus seeded Gaussian noise of std 1e-4 per component (f = feq(1, u0)).  One
+step = one LB step (fused stream + collide kernel) over all nodes.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `value` is FP32-shifted MLUPS with the state
+resident in HBM; `e2e` is the same metric through the fix hooks of the C ABI
+(couplb_fix_post_force / end_of_step, host atom arrays) with the per-step
+status word read back to the host; the accuracy keys compare FP32 / FP16 runs
+with an FP64 run of the same length.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX, NY, NZ = 256, 128, 128
+NU, GX, NOISE, SEED = 0.05, 1e-6, 1e-4, 2
+TAU = 3 * NU + 0.5
+WALL = (0, 0, 1, 1, 1, 1)
+WORKLOAD = "d3q19_channel_256x128x128_walls_yz_gx1e-6"
+BYTES_PER_LU = {"fp64": 2 * 19 * 8, "fp32": 2 * 19 * 4, "fp16": 2 * 19 * 2}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--accuracy-steps", type=int, default=20000,
+                    help="length of the FP32/FP16 vs FP64 accuracy runs (0 = skip)")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="target CPU work of the timed CPU baseline sample")
+    ap.add_argument("--nx", type=int, default=NX)
+    ap.add_argument("--ny", type=int, default=NY)
+    ap.add_argument("--nz", type=int, default=NZ)
+    return ap.parse_args()
+
+
+def initial_populations(nx, ny, nz, seed=SEED):
+    """f = feq(1, u0), u0 ~ N(0, NOISE^2) per component (reference layout,
+    ghosts included; the ghost values are never read)."""
+    E = np.array([[0, 0, 0], [1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1],
+                  [1, 1, 0], [-1, -1, 0], [1, -1, 0], [-1, 1, 0], [1, 0, 1], [-1, 0, -1],
+                  [1, 0, -1], [-1, 0, 1], [0, 1, 1], [0, -1, -1], [0, 1, -1], [0, -1, 1]], float)
+    W = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12)
+    rng = np.random.default_rng(seed)
+    sh = (nz + 2, ny + 2, nx + 2)
+    u = NOISE * rng.standard_normal((3,) + sh)
+    f = np.empty((19,) + sh)
+    uu = (u * u).sum(0)
+    for q in range(19):
+        eu = E[q, 0] * u[0] + E[q, 1] * u[1] + E[q, 2] * u[2]
+        f[q] = W[q] * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * uu)
+    return f
+
+
+# --------------------------------------------------------------------------
+class Clocks:
+    """nvidia-smi sampling of SM clocks / throttle reasons during timing."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except Exception:
+            self.p.kill()
+            return None
+        mhz, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                mhz.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not mhz:
+            return None
+        return {"sm_mhz": float(np.median(mhz)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(mhz)}
+
+
+# --------------------------------------------------------------------------
+def make_lattice(prec, nx, ny, nz, device):
+    from couplb_b200.lattice import Lattice
+    return Lattice(3, nx, ny, nz, tau=TAU, wall=WALL, body_force=True, precision=prec, device=device)
+
+
+def time_lattice(L, steps, warmup, torch, stream):
+    g = (GX, 0.0, 0.0)
+    for _ in range(warmup):
+        L.lbm_step(g)
+    L.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if torch.distributed.is_initialized():
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        L.lbm_step(g)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps   # ms per step (= per fused-kernel launch)
+
+
+def velocity(L):
+    L.macroscopic()
+    _, ux, uy, uz = L.get_macroscopic()
+    return np.stack([ux[1:-1, 1:-1, 1:-1], uy[1:-1, 1:-1, 1:-1], uz[1:-1, 1:-1, 1:-1]])
+
+
+def accuracy_runs(f0, steps, nx, ny, nz, device):
+    """FP64, FP32-shifted, FP16-storage runs of `steps` LB steps from the same
+    state; relative L2 velocity error of the reduced forms vs FP64."""
+    res = {}
+    u = {}
+    for prec in ("fp64", "fp32", "fp16"):
+        L = make_lattice(prec, nx, ny, nz, device)
+        L.set_populations(f0)
+        for _ in range(steps):
+            L.lbm_step((GX, 0.0, 0.0))
+        u[prec] = velocity(L)
+        L.close()
+    ref = u["fp64"]
+    den = math.sqrt(float((ref ** 2).sum()))
+    for prec in ("fp32", "fp16"):
+        res[prec] = math.sqrt(float(((u[prec] - ref) ** 2).sum())) / den
+    res["umax_fp64"] = float(np.abs(ref).max())
+    return res
+
+
+def e2e_fix(steps, warmup, nx, ny, nz, device, torch):
+    """Same metric through the fix hooks of the C ABI: per step one
+    couplb_fix_post_force (host atom arrays; none in this workload) and one
+    couplb_fix_end_of_step, then the device status word (clamp / non-finite
+    counts, 8 bytes) read back as the fix's per-step failure check."""
+    from couplb_b200 import md
+    from couplb_b200.fix import FixCoupLB
+    f0 = initial_populations(nx, ny, nz)
+    fix = FixCoupLB(f"flow all couplb {nx} {ny} {nz} {NU} 1.0 wall_y 1 1 wall_z 1 1 "
+                    f"gravity {GX} 0 0 precision fp32".split(), dimension=3, device=device)
+    fix.init(boxlo=(0, 0, 0), boxhi=(nx, ny, nz), dt=1.0)
+    fix.lattice.set_populations(f0)
+    at = md.empty_atoms().struct()
+    fix.setup(at, 0)
+    for s in range(1, warmup + 1):
+        fix.post_force(at, s)
+        fix.end_of_step(s)
+        fix.lattice.read_status()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s in range(warmup + 1, warmup + steps + 1):
+        fix.post_force(at, s)
+        fix.end_of_step(s)
+        clamps, nonfinite = fix.lattice.read_status()
+        if nonfinite:
+            raise RuntimeError("non-finite density")
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / steps
+    fix.close()
+    return dt
+
+
+def cpu_baseline(nx, ny, nz, seconds):
+    """The reference's CPU path (its own headers, OpenMP, all host threads)
+    on a bounded number of LB steps of the same workload."""
+    from oracle.bindings import OracleFix, available
+    kind = "ref_fast" if available("ref_fast") else ("ref" if available("ref") else "port")
+    from couplb_b200 import abi
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import cases
+    cfg = cases.make_cfg(nx, ny, nz, NU, 1.0, dimension=3, gravity=(GX, 0, 0), wall=WALL)
+    dom = abi.make_domain(3, (0, 0, 0), (nx, ny, nz), 1.0)
+    fix = OracleFix(cfg, dom, kind=kind)
+    fix.grid.set_f(initial_populations(nx, ny, nz))
+    from couplb_b200 import md
+    at = md.empty_atoms().struct()
+    fix.setup(at, 0)
+    t0 = time.perf_counter()
+    fix.post_force(at, 1)
+    t1 = time.perf_counter() - t0
+    steps = max(2, min(200, int(seconds / max(t1, 1e-6))))
+    t0 = time.perf_counter()
+    for s in range(2, steps + 2):
+        fix.post_force(at, s)
+        fix.end_of_step(s)
+    dt = (time.perf_counter() - t0) / steps
+    fix.close()
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    kind_name = "reference" if kind.startswith("ref") else "port"
+    return {"value": nx * ny * nz / dt / 1e6, "unit": "MLUPS", "cores": cores, "kind": kind_name,
+            "sample": f"{steps} LB steps of the {nx}x{ny}x{nz} D3Q19 channel, FP64, "
+                      f"fix post_force + end_of_step ({kind} build)"}
+
+
+def ncu_traffic_estimate():
+    """Per-launch DRAM bytes of the fused kernel from the committed ncu summary,
+    if present."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p))
+        except Exception:
+            return None
+    return None
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    base = cpu_baseline(args.nx, args.ny, args.nz, seconds=max(5.0, 8.0 * args.steps / 20))
+    line = {"metric": "D3Q19 MLUPS: FP32-shifted vs plain FP64 on B200 at <=1e-6 L2 velocity error",
+            "value": base["value"], "unit": "MLUPS", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "impl": "reference",
+            "dtype": "f64", "data": "synthetic", "scaling": "weak",
+            "config": {"workload": WORKLOAD, "nodes": args.nx * args.ny * args.nz},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    from couplb_b200 import build
+    build.build()
+    nx, ny, nz = args.nx, args.ny, args.nz
+    N = nx * ny * nz
+    f0 = initial_populations(nx, ny, nz)
+    stream = torch.cuda.Stream()
+
+    results = {}
+    clocks = Clocks(local)
+    for prec in ("fp64", "fp16", "fp32"):
+        L = make_lattice(prec, nx, ny, nz, local)
+        L.set_stream(stream.cuda_stream)
+        L.set_populations(f0)
+        if prec == "fp32":
+            clocks.start()
+        ms = time_lattice(L, args.steps, args.warmup, torch, stream)
+        if prec == "fp32":
+            clk = clocks.stop()
+        clamps, nonfinite = L.read_status()
+        if nonfinite:
+            raise RuntimeError(f"{prec}: non-finite densities")
+        L.close()
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        results[prec] = ms
+
+    e2e_s = e2e_fix(args.steps, args.warmup, nx, ny, nz, local, torch)
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    acc = accuracy_runs(f0, args.accuracy_steps, nx, ny, nz, local) if args.accuracy_steps else {}
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+
+    ms32 = results["fp32"]
+    mlups = world * N / (ms32 * 1e-3) / 1e6
+    achieved = BYTES_PER_LU["fp32"] * N / (ms32 * 1e-3) / 1e9
+    tr = ncu_traffic_estimate()
+    traffic = None
+    if tr and tr.get("workload") == WORKLOAD and "fp32_bytes_per_launch" in tr:
+        traffic = tr["fp32_bytes_per_launch"]
+    line = {
+        "metric": "D3Q19 MLUPS: FP32-shifted vs plain FP64 on B200 at <=1e-6 L2 velocity error",
+        "value": mlups, "unit": "MLUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "nodes_per_gpu": N, "precision": "fp32-shifted",
+                   "l2_flush": "state 637 MB > 126 MB L2 (inputs larger than L2)",
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "fp64_mlups": world * N / (results["fp64"] * 1e-3) / 1e6,
+        "fp16_mlups": world * N / (results["fp16"] * 1e-3) / 1e6,
+        "speedup_fp32_vs_fp64": results["fp64"] / ms32,
+        "accuracy": ({"steps": args.accuracy_steps, "l2_velocity_err_fp32_vs_fp64": acc["fp32"],
+                      "l2_velocity_err_fp16_vs_fp64": acc["fp16"], "umax": acc["umax_fp64"]}
+                     if acc else None),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                     "bytes_per_lu": BYTES_PER_LU["fp32"],
+                     "fp64_frac": BYTES_PER_LU["fp64"] * N / (results["fp64"] * 1e-3) / 1e9 / peak,
+                     "fp16_frac": BYTES_PER_LU["fp16"] * N / (results["fp16"] * 1e-3) / 1e9 / peak},
+        "e2e": {"value": world * N / e2e_s / 1e6, "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 8},
+        "gpu_launches": args.steps,
+        "clocks": clk,
+    }
+    if rank == 0:
+        try:
+            line["cpu_baseline"] = cpu_baseline(nx, ny, nz, args.cpu_seconds)
+        except Exception as e:   # the checker is optional for the GPU number
+            line["cpu_baseline"] = {"error": str(e)}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

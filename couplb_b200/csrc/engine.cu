@@ -1,0 +1,710 @@
+// engine.cu -- layer 1 of the C ABI (include/couplb_b200.h): one handle per
+// LBM subdomain, all state resident in device memory, kernels on one stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/couplb_b200.h"
+#include "engine_internal.h"
+#include "ibm_kernels.cuh"
+#include "lbm_kernels.cuh"
+
+using namespace couplb;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+int fail(couplb_handle* h, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (h) h->err = buf;
+  else g_create_error = buf;
+  return code;
+}
+
+#define CK(call)                                                                   \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess)                                                         \
+      return fail(h, COUPLB_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+#define CK_LAUNCH()                                                                \
+  do {                                                                             \
+    cudaError_t e_ = cudaGetLastError();                                           \
+    if (e_ != cudaSuccess)                                                         \
+      return fail(h, COUPLB_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e_)); \
+  } while (0)
+
+template <class Fn>
+void with_types(int dim, int prec, Fn&& fn) {
+  if (dim == 3) {
+    if (prec == COUPLB_FP64) fn(D3Q19{}, StoreF64{});
+    else if (prec == COUPLB_FP32_SHIFTED) fn(D3Q19{}, StoreF32S{});
+    else fn(D3Q19{}, StoreF16S{});
+  } else {
+    if (prec == COUPLB_FP64) fn(D2Q9{}, StoreF64{});
+    else if (prec == COUPLB_FP32_SHIFTED) fn(D2Q9{}, StoreF32S{});
+    else fn(D2Q9{}, StoreF16S{});
+  }
+}
+
+size_t elem_bytes_pop(int prec) { return prec == COUPLB_FP64 ? 8 : (prec == COUPLB_FP32_SHIFTED ? 4 : 2); }
+size_t elem_bytes_aux(int prec) { return prec == COUPLB_FP64 ? 8 : 4; }
+
+Geom make_geom(const couplb_handle* h) {
+  Geom g;
+  g.nx = h->p.nx; g.ny = h->p.ny; g.nz = h->p.nz;
+  g.qs = (long long)h->qs;
+  for (int f = 0; f < 6; f++) g.face[f] = h->p.wall[f];
+  if (h->p.dim == 2) g.face[4] = g.face[5] = 0;
+  for (int d = 0; d < 3; d++) g.uw[d] = h->p.wall_vel[d];
+  if (h->p.dim == 2) g.uw[2] = 0.0;
+  g.rho0 = h->p.rho0;
+  return g;
+}
+
+void row_launch(const couplb_handle* h, dim3* grid, dim3* block) {
+  const int bx = std::min(256, ((h->p.nx + 31) / 32) * 32);
+  *block = dim3(bx, 1, 1);
+  *grid = dim3((h->p.nx + bx - 1) / bx, h->p.ny, h->p.nz);
+}
+
+unsigned flat_blocks(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+int dalloc(couplb_handle* h, void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess)
+    return fail(h, COUPLB_ERR_CUDA, "cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+  h->device_bytes += bytes;
+  return COUPLB_OK;
+}
+
+void dfree(void*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+int ensure_macro(couplb_handle* h) {
+  if (h->macro[0]) return COUPLB_OK;
+  const size_t b = h->qs * elem_bytes_aux(h->p.precision);
+  for (int c = 0; c < 4; c++) {
+    int rc = dalloc(h, &h->macro[c], b);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(h->macro[c], 0, b, h->stream));
+  }
+  return COUPLB_OK;
+}
+
+int ensure_staging(couplb_handle* h, size_t bytes) {
+  if (h->staging_bytes >= bytes) return COUPLB_OK;
+  dfree(h->d_staging);
+  h->staging_bytes = 0;
+  int rc = dalloc(h, &h->d_staging, bytes);
+  if (rc) return rc;
+  h->staging_bytes = bytes;
+  return COUPLB_OK;
+}
+
+int ensure_atoms(couplb_handle* h, int n) {
+  if (h->atom_cap >= n) return COUPLB_OK;
+  dfree(h->d_x); dfree(h->d_v); dfree(h->d_m); dfree(h->d_fout); dfree(h->d_active);
+  if (h->h_fout) { cudaFreeHost(h->h_fout); h->h_fout = nullptr; }
+  const int cap = std::max(n, 1024);
+  int rc;
+  if ((rc = dalloc(h, &h->d_x, sizeof(double) * 3 * cap))) return rc;
+  if ((rc = dalloc(h, &h->d_v, sizeof(double) * 3 * cap))) return rc;
+  if ((rc = dalloc(h, &h->d_m, sizeof(double) * cap))) return rc;
+  if ((rc = dalloc(h, &h->d_fout, sizeof(double) * 3 * cap))) return rc;
+  if ((rc = dalloc(h, &h->d_active, sizeof(int) * cap))) return rc;
+  CK(cudaMallocHost(&h->h_fout, sizeof(double) * 3 * cap));
+  h->atom_cap = cap;
+  return COUPLB_OK;
+}
+
+int set_device(couplb_handle* h) {
+  CK(cudaSetDevice(h->p.device));
+  return COUPLB_OK;
+}
+
+// Populations as post-stream state in buffer `cur` (materialise if needed).
+int materialize(couplb_handle* h) {
+  if (h->poststream) return COUPLB_OK;
+  dim3 grid, block;
+  row_launch(h, &grid, &block);
+  const Geom g = make_geom(h);
+  with_types(h->p.dim, h->p.precision, [&](auto l, auto s) {
+    using L = decltype(l);
+    using S = decltype(s);
+    using T = typename S::T;
+    k_materialize<L, S><<<grid, block, 0, h->stream>>>(g, (const T*)h->f[h->cur], (T*)h->f[1 - h->cur]);
+  });
+  CK_LAUNCH();
+  h->cur = 1 - h->cur;
+  h->poststream = 1;
+  return COUPLB_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// internal entry points shared with the fix core and the profile writer
+namespace couplb {
+
+int engine_macro(couplb_handle* h) {
+  int rc = ensure_macro(h);
+  if (rc) return rc;
+  CK(cudaMemsetAsync(h->d_status + kStMacroClamps, 0, sizeof(int), h->stream));
+  dim3 grid, block;
+  row_launch(h, &grid, &block);
+  const Geom g = make_geom(h);
+  const bool pull = !h->poststream;
+  with_types(h->p.dim, h->p.precision, [&](auto l, auto s) {
+    using L = decltype(l);
+    using S = decltype(s);
+    using T = typename S::T;
+    using A = typename S::A;
+    MacroArgs<S> a;
+    a.g = g;
+    a.fin = (const T*)h->f[h->cur];
+    a.rho = (A*)h->macro[0]; a.ux = (A*)h->macro[1]; a.uy = (A*)h->macro[2]; a.uz = (A*)h->macro[3];
+    a.status = h->d_status;
+    if (pull) k_macro<L, S, true><<<grid, block, 0, h->stream>>>(a);
+    else k_macro<L, S, false><<<grid, block, 0, h->stream>>>(a);
+  });
+  CK_LAUNCH();
+  h->macro_valid = 1;
+  if (h->p.body_force) h->rho_state = kRhoCurrent;
+  return COUPLB_OK;
+}
+
+}  // namespace couplb
+
+// ===========================================================================
+extern "C" {
+
+int couplb_version(void) { return COUPLB_ABI_VERSION; }
+
+size_t couplb_struct_size(int which) {
+  switch (which) {
+    case 0: return sizeof(couplb_lattice_params);
+    case 1: return sizeof(couplb_ibm_params);
+    case 2: return sizeof(couplb_diag);
+    case 3: return sizeof(couplb_fix_config);
+    case 4: return sizeof(couplb_domain);
+    case 5: return sizeof(couplb_atoms);
+    default: return 0;
+  }
+}
+
+const char* couplb_last_error(const couplb_handle* h) {
+  return h ? h->err.c_str() : g_create_error.c_str();
+}
+
+int couplb_create(const couplb_lattice_params* p, couplb_handle** out) {
+  couplb_handle* h = nullptr;
+  if (!p || !out) return fail(nullptr, COUPLB_ERR_ARG, "couplb_create: null argument");
+  *out = nullptr;
+  if (p->dim != 2 && p->dim != 3) return fail(nullptr, COUPLB_ERR_ARG, "dim must be 2 or 3");
+  if (p->nx <= 0 || p->ny <= 0 || p->nz <= 0) return fail(nullptr, COUPLB_ERR_ARG, "grid dimensions must be positive");
+  if (p->dim == 2 && p->nz != 1) return fail(nullptr, COUPLB_ERR_ARG, "nz must be 1 for dim 2");
+  if (!(p->tau > 0.5) || !std::isfinite(p->tau)) return fail(nullptr, COUPLB_ERR_ARG, "tau <= 0.5 (unstable)");
+  if (!(p->rho0 > 0.0) || !std::isfinite(p->rho0)) return fail(nullptr, COUPLB_ERR_ARG, "rho0 must be positive");
+  for (int f = 0; f < 6; f++)
+    if (p->wall[f] < 0 || p->wall[f] > 4) return fail(nullptr, COUPLB_ERR_ARG, "wall types must be in [0,4]");
+  if (p->precision < COUPLB_FP64 || p->precision > COUPLB_FP16_SHIFTED)
+    return fail(nullptr, COUPLB_ERR_ARG, "unknown precision %d", p->precision);
+  const long long N = (long long)p->nx * p->ny * p->nz;
+  const int Q = p->dim == 3 ? 19 : 9;
+  if (N * Q >= (1LL << 40)) return fail(nullptr, COUPLB_ERR_ARG, "grid too large");
+
+  h = new couplb_handle();
+  h->p = *p;
+  h->Q = Q;
+  h->N = (size_t)N;
+  h->qs = ((size_t)N + 63) / 64 * 64;
+  {
+    cudaError_t e = cudaSetDevice(p->device);
+    if (e != cudaSuccess) {
+      delete h;
+      return fail(nullptr, COUPLB_ERR_CUDA, "cudaSetDevice(%d) failed: %s", p->device, cudaGetErrorString(e));
+    }
+    e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      delete h;
+      return fail(nullptr, COUPLB_ERR_CUDA, "cudaStreamCreate failed: %s", cudaGetErrorString(e));
+    }
+    h->own_stream = true;
+  }
+  const size_t pb = elem_bytes_pop(p->precision), ab = elem_bytes_aux(p->precision);
+  int rc = COUPLB_OK;
+  for (int b = 0; b < 2 && !rc; b++) rc = dalloc(h, &h->f[b], pb * Q * h->qs);
+  for (int c = 0; c < 3 && !rc; c++) rc = dalloc(h, &h->F[c], ab * h->qs);
+  if (!rc && p->body_force) rc = dalloc(h, &h->rho_field, ab * h->qs);
+  if (!rc) rc = dalloc(h, (void**)&h->d_status, sizeof(int) * 8);
+  if (!rc) rc = dalloc(h, (void**)&h->d_ftot, sizeof(double) * 4);
+  if (!rc && cudaMallocHost(&h->h_small, 4096) != cudaSuccess)
+    rc = fail(h, COUPLB_ERR_CUDA, "cudaMallocHost failed");
+  if (rc) {
+    g_create_error = h->err;
+    couplb_destroy(h);
+    return rc;
+  }
+  for (int c = 0; c < 3 && !rc; c++)
+    if (cudaMemsetAsync(h->F[c], 0, ab * h->qs, h->stream) != cudaSuccess) rc = COUPLB_ERR_CUDA;
+  if (!rc && cudaMemsetAsync(h->d_status, 0, sizeof(int) * 8, h->stream) != cudaSuccess) rc = COUPLB_ERR_CUDA;
+  if (!rc && cudaMemsetAsync(h->d_ftot, 0, sizeof(double) * 4, h->stream) != cudaSuccess) rc = COUPLB_ERR_CUDA;
+  if (!rc) rc = couplb_init_equilibrium(h, p->rho0, 0.0, 0.0, 0.0);
+  if (rc) {
+    g_create_error = h->err.empty() ? "device initialisation failed" : h->err;
+    couplb_destroy(h);
+    return rc ? rc : COUPLB_ERR_CUDA;
+  }
+  *out = h;
+  return COUPLB_OK;
+}
+
+int couplb_destroy(couplb_handle* h) {
+  if (!h) return COUPLB_OK;
+  cudaSetDevice(h->p.device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (int b = 0; b < 2; b++) dfree(h->f[b]);
+  for (int c = 0; c < 3; c++) dfree(h->F[c]);
+  for (int c = 0; c < 4; c++) dfree(h->macro[c]);
+  dfree(h->rho_field);
+  void* p = h->d_status; dfree(p);
+  p = h->d_ftot; dfree(p);
+  dfree(h->d_staging);
+  dfree(h->d_scratch);
+  dfree(h->d_x); dfree(h->d_v); dfree(h->d_m); dfree(h->d_fout); dfree(h->d_active);
+  if (h->h_fout) cudaFreeHost(h->h_fout);
+  if (h->h_small) cudaFreeHost(h->h_small);
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return COUPLB_OK;
+}
+
+int couplb_set_stream(couplb_handle* h, void* s) {
+  if (!h) return COUPLB_ERR_ARG;
+  int rc = set_device(h);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(h->stream));
+  if (h->own_stream) cudaStreamDestroy(h->stream);
+  h->stream = (cudaStream_t)s;
+  h->own_stream = false;
+  return COUPLB_OK;
+}
+
+int couplb_synchronize(couplb_handle* h) {
+  if (!h) return COUPLB_ERR_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  return COUPLB_OK;
+}
+
+size_t couplb_ghost_nodes(const couplb_handle* h) {
+  if (!h) return 0;
+  return (size_t)(h->p.nx + 2) * (h->p.ny + 2) * (h->p.dim == 3 ? h->p.nz + 2 : 1);
+}
+
+size_t couplb_device_bytes(const couplb_handle* h) { return h ? h->device_bytes : 0; }
+
+int couplb_init_equilibrium(couplb_handle* h, double rho, double ux, double uy, double uz) {
+  if (!h) return COUPLB_ERR_ARG;
+  int rc = set_device(h);
+  if (rc) return rc;
+  const Geom g = make_geom(h);
+  const long long N = (long long)h->N;
+  with_types(h->p.dim, h->p.precision, [&](auto l, auto s) {
+    using L = decltype(l);
+    using S = decltype(s);
+    k_init_eq<L, S><<<flat_blocks(N, 256), 256, 0, h->stream>>>(
+        g, (typename S::T*)h->f[0], rho, ux, uy, h->p.dim == 3 ? uz : 0.0,
+        (typename S::A*)h->rho_field);
+  });
+  CK_LAUNCH();
+  h->cur = 0;
+  h->poststream = 1;
+  const size_t ab = elem_bytes_aux(h->p.precision);
+  for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(h->F[c], 0, ab * h->qs, h->stream));
+  h->force_dirty = 0;
+  h->rho_state = h->p.body_force ? kRhoField : kRhoNone;
+  h->macro_valid = 0;
+  return COUPLB_OK;
+}
+
+int couplb_set_populations(couplb_handle* h, const double* f_host) {
+  if (!h || !f_host) return fail(h, COUPLB_ERR_ARG, "null argument");
+  int rc = set_device(h);
+  if (rc) return rc;
+  const size_t G = couplb_ghost_nodes(h);
+  const size_t bytes = sizeof(double) * h->Q * G;
+  if ((rc = ensure_staging(h, bytes))) return rc;
+  CK(cudaMemcpyAsync(h->d_staging, f_host, bytes, cudaMemcpyHostToDevice, h->stream));
+  const Geom g = make_geom(h);
+  with_types(h->p.dim, h->p.precision, [&](auto l, auto s) {
+    using L = decltype(l);
+    using S = decltype(s);
+    k_import_f<L, S><<<flat_blocks((long long)h->N, 256), 256, 0, h->stream>>>(
+        g, (const double*)h->d_staging, (long long)G, (typename S::T*)h->f[0]);
+  });
+  CK_LAUNCH();
+  h->cur = 0;
+  h->poststream = 1;
+  // like IO::read_checkpoint: moments recomputed without the Guo term
+  rc = engine_macro(h);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(h->stream));
+  return COUPLB_OK;
+}
+
+int couplb_get_populations(couplb_handle* h, double* f_host) {
+  if (!h || !f_host) return fail(h, COUPLB_ERR_ARG, "null argument");
+  int rc = set_device(h);
+  if (rc) return rc;
+  if ((rc = materialize(h))) return rc;
+  const size_t G = couplb_ghost_nodes(h);
+  const size_t bytes = sizeof(double) * h->Q * G;
+  if ((rc = ensure_staging(h, bytes))) return rc;
+  const Geom g = make_geom(h);
+  with_types(h->p.dim, h->p.precision, [&](auto l, auto s) {
+    using L = decltype(l);
+    using S = decltype(s);
+    k_export_f<L, S><<<flat_blocks((long long)G, 256), 256, 0, h->stream>>>(
+        g, (const typename S::T*)h->f[h->cur], (long long)G, (double*)h->d_staging);
+  });
+  CK_LAUNCH();
+  CK(cudaMemcpyAsync(f_host, h->d_staging, bytes, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return COUPLB_OK;
+}
+
+int couplb_lbm_step(couplb_handle* h, const double* g_lb) {
+  if (!h) return COUPLB_ERR_ARG;
+  if (g_lb && !h->p.body_force)
+    return fail(h, COUPLB_ERR_STATE, "gravity given to a lattice created with body_force = 0");
+  int rc = set_device(h);
+  if (rc) return rc;
+  const bool g_active = g_lb && !(std::fabs(g_lb[0]) < ZERO_TOL && std::fabs(g_lb[1]) < ZERO_TOL &&
+                                  std::fabs(g_lb[2]) < ZERO_TOL);
+  dim3 grid, block;
+  row_launch(h, &grid, &block);
+  const Geom g = make_geom(h);
+  const bool pull = !h->poststream;
+  const int rho_mode = !g_active ? kRhoNone : (h->rho_state == kRhoCurrent ? kRhoCurrent : kRhoField);
+  with_types(h->p.dim, h->p.precision, [&](auto l, auto s) {
+    using L = decltype(l);
+    using S = decltype(s);
+    using T = typename S::T;
+    using A = typename S::A;
+    LBArgs<S> a;
+    a.g = g;
+    a.fin = (const T*)h->f[h->cur];
+    a.fout = (T*)h->f[1 - h->cur];
+    a.Fx = h->force_dirty ? (const A*)h->F[0] : nullptr;
+    a.Fy = (const A*)h->F[1];
+    a.Fz = (const A*)h->F[2];
+    a.rho_field = (A*)h->rho_field;
+    a.rho_mode = rho_mode;
+    a.write_rho = h->p.body_force ? 1 : 0;
+    for (int d = 0; d < 3; d++) a.grav[d] = g_active ? g_lb[d] : 0.0;
+    a.omega = 1.0 / h->p.tau;
+    a.status = h->d_status;
+    if (pull) k_stream_collide<L, S, true><<<grid, block, 0, h->stream>>>(a);
+    else k_stream_collide<L, S, false><<<grid, block, 0, h->stream>>>(a);
+  });
+  CK_LAUNCH();
+  h->cur = 1 - h->cur;
+  h->poststream = 0;
+  h->lbm_steps++;
+  if (h->force_dirty) {   // clear_forces (couplb_lattice.h:243-247)
+    const size_t ab = elem_bytes_aux(h->p.precision);
+    for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(h->F[c], 0, ab * h->qs, h->stream));
+    h->force_dirty = 0;
+  }
+  h->rho_state = h->p.body_force ? kRhoField : kRhoNone;
+  h->macro_valid = 0;
+  return COUPLB_OK;
+}
+
+int couplb_macroscopic(couplb_handle* h) {
+  if (!h) return COUPLB_ERR_ARG;
+  int rc = set_device(h);
+  if (rc) return rc;
+  return engine_macro(h);
+}
+
+int couplb_get_macroscopic(couplb_handle* h, double* rho, double* ux, double* uy, double* uz) {
+  if (!h) return COUPLB_ERR_ARG;
+  if (!h->macro_valid) return fail(h, COUPLB_ERR_STATE, "moments not computed: call couplb_macroscopic first");
+  int rc = set_device(h);
+  if (rc) return rc;
+  const size_t G = couplb_ghost_nodes(h);
+  if ((rc = ensure_staging(h, sizeof(double) * 4 * G))) return rc;
+  double* st = (double*)h->d_staging;
+  const Geom g = make_geom(h);
+  with_types(h->p.dim, h->p.precision, [&](auto l, auto s) {
+    using S = decltype(s);
+    using A = typename S::A;
+    (void)l;
+    k_export_macro<S><<<flat_blocks((long long)G, 256), 256, 0, h->stream>>>(
+        g, h->p.dim, (const A*)h->macro[0], (const A*)h->macro[1], (const A*)h->macro[2],
+        (const A*)h->macro[3], (long long)G, st, st + G, st + 2 * G, st + 3 * G);
+  });
+  CK_LAUNCH();
+  double* outs[4] = {rho, ux, uy, uz};
+  for (int c = 0; c < 4; c++)
+    if (outs[c]) CK(cudaMemcpyAsync(outs[c], st + c * G, sizeof(double) * G, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return COUPLB_OK;
+}
+
+int couplb_get_force_field(couplb_handle* h, double* fx, double* fy, double* fz) {
+  if (!h || !fx || !fy || !fz) return fail(h, COUPLB_ERR_ARG, "null argument");
+  int rc = set_device(h);
+  if (rc) return rc;
+  const size_t G = couplb_ghost_nodes(h);
+  if ((rc = ensure_staging(h, sizeof(double) * 3 * G))) return rc;
+  double* st = (double*)h->d_staging;
+  const Geom g = make_geom(h);
+  with_types(h->p.dim, h->p.precision, [&](auto l, auto s) {
+    using S = decltype(s);
+    using A = typename S::A;
+    (void)l;
+    k_export_force<S><<<flat_blocks((long long)G, 256), 256, 0, h->stream>>>(
+        g, h->p.dim, (const A*)h->F[0], (const A*)h->F[1], (const A*)h->F[2], (long long)G, st,
+        st + G, st + 2 * G);
+  });
+  CK_LAUNCH();
+  double* outs[3] = {fx, fy, fz};
+  for (int c = 0; c < 3; c++)
+    CK(cudaMemcpyAsync(outs[c], st + c * G, sizeof(double) * G, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return COUPLB_OK;
+}
+
+int couplb_set_force_field(couplb_handle* h, const double* fx, const double* fy, const double* fz) {
+  if (!h || !fx || !fy || !fz) return fail(h, COUPLB_ERR_ARG, "null argument");
+  int rc = set_device(h);
+  if (rc) return rc;
+  const size_t G = couplb_ghost_nodes(h);
+  if ((rc = ensure_staging(h, sizeof(double) * 3 * G))) return rc;
+  double* st = (double*)h->d_staging;
+  const double* ins[3] = {fx, fy, fz};
+  for (int c = 0; c < 3; c++)
+    CK(cudaMemcpyAsync(st + c * G, ins[c], sizeof(double) * G, cudaMemcpyHostToDevice, h->stream));
+  const Geom g = make_geom(h);
+  with_types(h->p.dim, h->p.precision, [&](auto l, auto s) {
+    using S = decltype(s);
+    using A = typename S::A;
+    (void)l;
+    k_import_force<S><<<flat_blocks((long long)h->N, 256), 256, 0, h->stream>>>(
+        g, h->p.dim, st, st + G, st + 2 * G, (A*)h->F[0], (A*)h->F[1], (A*)h->F[2]);
+  });
+  CK_LAUNCH();
+  h->force_dirty = 1;
+  CK(cudaStreamSynchronize(h->stream));
+  return COUPLB_OK;
+}
+
+int couplb_diagnostics(couplb_handle* h, couplb_diag* out) {
+  if (!h || !out) return fail(h, COUPLB_ERR_ARG, "null argument");
+  if (!h->macro_valid) return fail(h, COUPLB_ERR_STATE, "moments not computed: call couplb_macroscopic first");
+  int rc = set_device(h);
+  if (rc) return rc;
+  const int nb = std::min<long long>(1184, std::max<long long>(1, ((long long)h->N + 255) / 256));
+  if (!h->d_scratch || h->scratch_blocks < nb) {
+    dfree(h->d_scratch);
+    if ((rc = dalloc(h, &h->d_scratch, sizeof(double) * (5 * nb + 8)))) return rc;
+    h->scratch_blocks = nb;
+  }
+  double* part = (double*)h->d_scratch;
+  double* res = part + 5 * nb;
+  with_types(h->p.dim, h->p.precision, [&](auto l, auto s) {
+    using S = decltype(s);
+    using A = typename S::A;
+    (void)l;
+    k_diag_partial<S><<<nb, 256, 0, h->stream>>>((long long)h->N, h->p.rho0, (const A*)h->macro[0],
+                                                 (const A*)h->macro[1], (const A*)h->macro[2],
+                                                 (const A*)h->macro[3], part);
+  });
+  CK_LAUNCH();
+  k_reduce_final<<<1, 32, 0, h->stream>>>(nb, part, res);
+  CK_LAUNCH();
+  double* hs = (double*)h->h_small;
+  CK(cudaMemcpyAsync(hs, res, sizeof(double) * 5, cudaMemcpyDeviceToHost, h->stream));
+  int* hi = (int*)(hs + 8);
+  CK(cudaMemcpyAsync(hi, h->d_status, sizeof(int) * 4, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  out->umax = hs[0];
+  out->mass = hs[1];
+  out->mom[0] = hs[2]; out->mom[1] = hs[3]; out->mom[2] = hs[4];
+  out->clamps = hi[kStMacroClamps];
+  out->nonfinite = hi[kStNonfinite];
+  return COUPLB_OK;
+}
+
+int couplb_y_profile(couplb_handle* h, double* ux_sum, double* uy_sum, double* rho_sum) {
+  if (!h || !ux_sum || !uy_sum || !rho_sum) return fail(h, COUPLB_ERR_ARG, "null argument");
+  if (!h->macro_valid) return fail(h, COUPLB_ERR_STATE, "moments not computed: call couplb_macroscopic first");
+  int rc = set_device(h);
+  if (rc) return rc;
+  const int ny = h->p.ny;
+  if ((rc = ensure_staging(h, sizeof(double) * 3 * ny))) return rc;
+  double* st = (double*)h->d_staging;
+  const Geom g = make_geom(h);
+  with_types(h->p.dim, h->p.precision, [&](auto l, auto s) {
+    using S = decltype(s);
+    using A = typename S::A;
+    (void)l;
+    k_y_profile<S><<<ny, 256, 0, h->stream>>>(g, (const A*)h->macro[0], (const A*)h->macro[1],
+                                              (const A*)h->macro[2], st);
+  });
+  CK_LAUNCH();
+  CK(cudaMemcpyAsync(ux_sum, st, sizeof(double) * ny, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(uy_sum, st + ny, sizeof(double) * ny, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(rho_sum, st + 2 * ny, sizeof(double) * ny, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return COUPLB_OK;
+}
+
+int couplb_read_status(couplb_handle* h, int* clamps, int* nonfinite, int reset) {
+  if (!h) return COUPLB_ERR_ARG;
+  int rc = set_device(h);
+  if (rc) return rc;
+  int* hi = (int*)h->h_small;
+  CK(cudaMemcpyAsync(hi, h->d_status, sizeof(int) * 4, cudaMemcpyDeviceToHost, h->stream));
+  if (reset) CK(cudaMemsetAsync(h->d_status, 0, sizeof(int) * 2, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (clamps) *clamps = hi[kStClamps];
+  if (nonfinite) *nonfinite = hi[kStNonfinite];
+  return COUPLB_OK;
+}
+
+int couplb_set_ibm_params(couplb_handle* h, const couplb_ibm_params* ip) {
+  if (!h || !ip) return fail(h, COUPLB_ERR_ARG, "null argument");
+  if (ip->md_per_lb < 1) return fail(h, COUPLB_ERR_ARG, "md_per_lb must be >= 1");
+  if (ip->delta != COUPLB_DELTA_ROMA && ip->delta != COUPLB_DELTA_PESKIN4)
+    return fail(h, COUPLB_ERR_ARG, "unknown delta kernel %d", ip->delta);
+  if (!(ip->dx > 0) || !(ip->dt_lbm > 0) || !(ip->force_scale > 0))
+    return fail(h, COUPLB_ERR_ARG, "dx, dt_lbm and force_scale must be positive");
+  h->ip = *ip;
+  h->ip_set = 1;
+  return COUPLB_OK;
+}
+
+}  // extern "C"
+
+namespace couplb {
+
+// Shared body of the host- and device-array IBM sub-step.
+int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, const double* d_m,
+               const int* d_active, double* d_fout, int accumulate, int refresh) {
+  if (refresh || !h->macro_valid) {
+    int rc = engine_macro(h);
+    if (rc) return rc;
+  }
+  if (n <= 0) return COUPLB_OK;
+  const couplb_ibm_params& ip = h->ip;
+  const double dxp = ip.dx;
+  const double dv = (h->p.dim == 3) ? dxp * dxp * dxp : dxp * dxp;
+  const double cell_vol = dxp * dxp * ((h->p.dim == 3) ? dxp : 1.0);
+  const Geom g = make_geom(h);
+  const int bs = 256;
+  const unsigned nb = (unsigned)(((long long)n * 32 + bs - 1) / bs);
+  with_types(h->p.dim, h->p.precision, [&](auto l, auto s) {
+    using L = decltype(l);
+    using S = decltype(s);
+    using A = typename S::A;
+    IbmArgs<S> a;
+    a.g = g;
+    a.ux = (const A*)h->macro[1]; a.uy = (const A*)h->macro[2]; a.uz = (const A*)h->macro[3];
+    a.Fx = (A*)h->F[0]; a.Fy = (A*)h->F[1]; a.Fz = (A*)h->F[2];
+    a.n = n;
+    a.x = d_x; a.v = d_v; a.m = d_m; a.active = d_active;
+    a.fout = d_fout;
+    a.accumulate = accumulate;
+    a.ftot = h->d_ftot;
+    for (int d = 0; d < 3; d++) { a.lo[d] = ip.domain_lo[d]; a.off[d] = ip.offset[d]; }
+    if (h->p.dim == 2) a.off[2] = 0;
+    a.inv_dx = 1.0 / dxp;
+    a.xi_over_dt = ip.xi_ibm / ip.dt_lbm;
+    a.inv_N = 1.0 / (double)ip.md_per_lb;
+    a.vs = ip.vel_scale;
+    a.fs = ip.force_scale;
+    a.dvr = dv / cell_vol;
+    if (ip.delta == COUPLB_DELTA_ROMA) k_ibm_substep<L, S, 0><<<nb, bs, 0, h->stream>>>(a);
+    else k_ibm_substep<L, S, 1><<<nb, bs, 0, h->stream>>>(a);
+  });
+  CK_LAUNCH();
+  h->force_dirty = 1;
+  return COUPLB_OK;
+}
+
+}  // namespace couplb
+
+extern "C" {
+
+int couplb_ibm_substep(couplb_handle* h, int n, const double* x, const double* v,
+                       const double* mass, const int* active, double* f_add, int refresh,
+                       int* ncoupled) {
+  if (!h) return COUPLB_ERR_ARG;
+  if (!h->ip_set) return fail(h, COUPLB_ERR_STATE, "couplb_set_ibm_params not called");
+  if (n < 0 || (n > 0 && (!x || !v || !mass || !f_add))) return fail(h, COUPLB_ERR_ARG, "bad atom arrays");
+  int rc = set_device(h);
+  if (rc) return rc;
+  int nc = 0;
+  for (int a = 0; a < n; a++) nc += active ? (active[a] != 0) : 1;
+  if (ncoupled) *ncoupled = nc;
+  if ((rc = ensure_atoms(h, n))) return rc;
+  if (n > 0) {
+    CK(cudaMemcpyAsync(h->d_x, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_v, v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_m, mass, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+    if (active) CK(cudaMemcpyAsync(h->d_active, active, sizeof(int) * n, cudaMemcpyHostToDevice, h->stream));
+  }
+  rc = engine_ibm(h, nc > 0 ? n : 0, (const double*)h->d_x, (const double*)h->d_v,
+                  (const double*)h->d_m, active ? (const int*)h->d_active : nullptr,
+                  (double*)h->d_fout, 0, refresh);
+  if (rc) return rc;
+  if (nc > 0) {
+    CK(cudaMemcpyAsync(h->h_fout, h->d_fout, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int a = 0; a < 3 * n; a++) f_add[a] += h->h_fout[a];
+  }
+  return COUPLB_OK;
+}
+
+int couplb_ibm_substep_device(couplb_handle* h, int n, const double* d_x, const double* d_v,
+                              const double* d_mass, const int* d_active, double* d_f_add,
+                              int refresh) {
+  if (!h) return COUPLB_ERR_ARG;
+  if (!h->ip_set) return fail(h, COUPLB_ERR_STATE, "couplb_set_ibm_params not called");
+  if (n < 0 || (n > 0 && (!d_x || !d_v || !d_mass || !d_f_add))) return fail(h, COUPLB_ERR_ARG, "bad atom arrays");
+  int rc = set_device(h);
+  if (rc) return rc;
+  return engine_ibm(h, n, d_x, d_v, d_mass, d_active, d_f_add, 1, refresh);
+}
+
+int couplb_ibm_total_force(couplb_handle* h, double out[3], int reset) {
+  if (!h || !out) return COUPLB_ERR_ARG;
+  int rc = set_device(h);
+  if (rc) return rc;
+  double* hs = (double*)h->h_small;
+  CK(cudaMemcpyAsync(hs, h->d_ftot, sizeof(double) * 3, cudaMemcpyDeviceToHost, h->stream));
+  if (reset) CK(cudaMemsetAsync(h->d_ftot, 0, sizeof(double) * 4, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  out[0] = hs[0]; out[1] = hs[1]; out[2] = hs[2];
+  return COUPLB_OK;
+}
+
+}  // extern "C"

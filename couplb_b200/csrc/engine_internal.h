@@ -1,0 +1,55 @@
+// engine_internal.h -- the lattice handle, shared by engine.cu and the fix
+// core.  Not part of the public ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/couplb_b200.h"
+
+struct couplb_handle {
+  couplb_lattice_params p{};
+  int Q = 0;
+  size_t N = 0;    // interior nodes
+  size_t qs = 0;   // q-plane stride (elements)
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+
+  void* f[2] = {nullptr, nullptr};   // population buffers (A-B)
+  int cur = 0;                       // buffer holding the current state
+  int poststream = 1;                // 1: f[cur] is post-stream S, 0: post-collision P
+  void* F[3] = {nullptr, nullptr, nullptr};   // Eulerian force field
+  int force_dirty = 0;               // F holds nonzero values
+  void* rho_field = nullptr;         // density read by the body force
+  int rho_state = 0;                 // couplb::RhoMode: what the next LB step reads
+  void* macro[4] = {nullptr, nullptr, nullptr, nullptr};   // rho(dev), ux, uy, uz
+  int macro_valid = 0;               // macro[] are the moments of the current state
+  long long lbm_steps = 0;
+
+  int* d_status = nullptr;           // clamp / non-finite counters
+  double* d_ftot = nullptr;          // FP64 sum of the spread IBM force
+  void* h_small = nullptr;           // pinned host scratch for small read-backs
+  void* d_staging = nullptr;         // import / export staging
+  size_t staging_bytes = 0;
+  void* d_scratch = nullptr;         // reduction partials
+  int scratch_blocks = 0;
+
+  couplb_ibm_params ip{};
+  int ip_set = 0;
+  void* d_x = nullptr;
+  void* d_v = nullptr;
+  void* d_m = nullptr;
+  void* d_fout = nullptr;
+  void* d_active = nullptr;
+  double* h_fout = nullptr;
+  int atom_cap = 0;
+
+  size_t device_bytes = 0;
+  std::string err;
+};
+
+namespace couplb {
+int engine_macro(couplb_handle* h);
+int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, const double* d_m,
+               const int* d_active, double* d_fout, int accumulate, int refresh);
+}  // namespace couplb

@@ -1,0 +1,735 @@
+// fix_core.cpp -- layer 2 of the C ABI: the `fix couplb` front end.
+//
+// Keyword parsing, unit conversion and the init / setup / post_force /
+// end_of_step sequencing of FixCoupLB (fix_couplb.cpp), written against plain
+// atom arrays so that a LAMMPS fix (or any MD driver) forwards its hooks
+// here.  The lattice work goes to the layer-1 engine on the GPU; this file does
+// host bookkeeping only.  Error messages are the reference's.
+#include <algorithm>
+#include <cerrno>
+#include <cmath>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/couplb_b200.h"
+
+namespace {
+
+constexpr double kRhoLb = 1.0;   // FixCoupLB::rho_lb (fix_couplb.h:180)
+constexpr double kZeroTol = 1e-15, kMaWarn = 0.3, kMaError = 0.5;
+constexpr uint32_t kCkptMagic = 0x434C424B;   // "CLBK" (couplb_io.h:21)
+constexpr int32_t kCkptVersion = 1;
+
+const char* const kKeywords[] = {"md_per_lb", "xi_ibm",      "gravity", "wall_x",     "wall_y",
+                                 "wall_z",    "wall_vel",    "output",  "check_every", "kernel",
+                                 "vtk",       "vtk_region",  "vtk_solid", "checkpoint", "restart",
+                                 "precision", nullptr};
+
+// is_couplb_keyword (fix_couplb.cpp:22-36), plus the `precision` keyword of
+// this implementation.
+bool is_keyword(const char* s) {
+  for (int i = 0; kKeywords[i]; i++)
+    if (std::strcmp(s, kKeywords[i]) == 0) return true;
+  return false;
+}
+
+struct ParseError {
+  std::string msg;
+};
+
+[[noreturn]] void perr(const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  throw ParseError{buf};
+}
+
+// std::stoi / std::stod semantics: leading number parsed, error when none.
+int to_int(const char* s) {
+  errno = 0;
+  char* end = nullptr;
+  const long v = std::strtol(s, &end, 10);
+  if (end == s) perr("fix couplb: expected an integer, got '%s'", s);
+  if (errno == ERANGE || v > INT32_MAX || v < INT32_MIN) perr("fix couplb: integer out of range: '%s'", s);
+  return (int)v;
+}
+
+double to_double(const char* s) {
+  errno = 0;
+  char* end = nullptr;
+  const double v = std::strtod(s, &end);
+  if (end == s) perr("fix couplb: expected a number, got '%s'", s);
+  return v;
+}
+
+void copy_str(char* dst, const char* src) {
+  std::strncpy(dst, src, COUPLB_PATH_MAX - 1);
+  dst[COUPLB_PATH_MAX - 1] = 0;
+}
+
+}  // namespace
+
+struct couplb_fix {
+  couplb_fix_config cfg{};
+  couplb_handle* h = nullptr;
+  int device = 0;
+  int rank = 0;
+  bool inited = false;
+  bool is3d = true;
+  double dx = 0, inv_dx = 0, dt = 0, dt_LBM = 0, vel_scale = 0, nu_lb = 0, tau = 0,
+         force_scale = 0;
+  double domain_lo[3] = {0, 0, 0}, domain_hi[3] = {0, 0, 0};
+  int nl[3] = {0, 0, 0}, off[3] = {0, 0, 0};
+  int md_sub_count = 0;
+  bool ibm_has_particles = false;
+  long long next_output = 0, next_check = -1, next_vtk = -1, next_checkpoint = -1;
+  long long lbm_step_count = 0;
+  double gvals[3] = {0, 0, 0};
+  couplb_gravity_fn gcb = nullptr;
+  void* gctx = nullptr;
+  couplb_log_fn logcb = nullptr;
+  void* logctx = nullptr;
+  couplb_diag last_diag{};
+  std::string err;
+  std::vector<double> mass_buf;
+  std::vector<int> active_buf;
+  int vtk_region[6] = {0, 0, 0, 0, 0, 0};
+
+  int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    err = buf;
+    return code;
+  }
+  int engine_fail(int rc) {
+    err = couplb_last_error(h);
+    return rc;
+  }
+  void log(const char* fmt, ...) {
+    if (!logcb || rank != 0) return;
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    logcb(logctx, buf);
+  }
+};
+
+namespace {
+
+// FixCoupLB::write_profile (fix_couplb.cpp:903-979) for one rank.
+int write_profile(couplb_fix* F, long long step) {
+  const int ny = F->nl[1];
+  std::vector<double> su(ny), sv(ny), sr(ny);
+  int rc = couplb_y_profile(F->h, su.data(), sv.data(), sr.data());
+  if (rc) return F->engine_fail(rc);
+  if (F->rank != 0) return COUPLB_OK;
+  const int Ny = F->cfg.Ny;
+  const int cxz = F->nl[0] * (F->is3d ? F->nl[2] : 1);
+  std::vector<double> ux(Ny, 0.0), uy(Ny, 0.0), rr(Ny, 0.0);
+  std::vector<int> cnt(Ny, 0);
+  for (int j = 0; j < ny; j++) {
+    const int gy = F->off[1] + j;
+    if (gy < 0 || gy >= Ny) continue;
+    ux[gy] = su[j]; uy[gy] = sv[j]; rr[gy] = sr[j]; cnt[gy] = cxz;
+  }
+  FILE* fp = std::fopen(F->cfg.output_file, "a");
+  if (!fp) {
+    F->log("CoupLB WARNING: cannot open %s\n", F->cfg.output_file);
+    return COUPLB_OK;
+  }
+  std::fprintf(fp, "# step = %lld\n", step);
+  for (int j = 0; j < Ny; j++) {
+    const double inv = (cnt[j] > 0) ? 1.0 / cnt[j] : 0.0;
+    std::fprintf(fp, "%lld %d %.6f %.8f %.10e %.10e\n", step, j, F->domain_lo[1] + (double)j * F->dx,
+                 F->cfg.rho * (rr[j] * inv), F->vel_scale * (ux[j] * inv), F->vel_scale * (uy[j] * inv));
+  }
+  std::fprintf(fp, "\n");
+  std::fclose(fp);
+  return COUPLB_OK;
+}
+
+// IO::write_checkpoint (couplb_io.h:669-719): prefix.<rank>.clbk, header then
+// Q x G doubles of f including ghost nodes.
+int write_checkpoint(couplb_fix* F, long long step) {
+  char fname[COUPLB_PATH_MAX + 32];
+  std::snprintf(fname, sizeof(fname), "%s.%d.clbk", F->cfg.checkpoint_prefix, F->rank);
+  const int Q = F->is3d ? 19 : 9;
+  const size_t G = couplb_ghost_nodes(F->h);
+  std::vector<double> f((size_t)Q * G);
+  int rc = couplb_get_populations(F->h, f.data());
+  if (rc) return F->engine_fail(rc);
+  FILE* fp = std::fopen(fname, "wb");
+  if (!fp) return F->fail(COUPLB_ERR_IO, "CoupLB IO: rank %d cannot open %s for writing", F->rank, fname);
+  const uint32_t magic = kCkptMagic;
+  const int32_t version = kCkptVersion;
+  const int64_t s64 = step;
+  const int32_t D = F->is3d ? 3 : 2, Qi = Q;
+  const int32_t dims[3] = {F->nl[0], F->nl[1], F->is3d ? F->nl[2] : 1};
+  const int32_t offs[3] = {F->off[0], F->off[1], F->is3d ? F->off[2] : 0};
+  const int32_t glob[3] = {F->cfg.Nx, F->cfg.Ny, F->is3d ? F->cfg.Nz : 1};
+  bool ok = std::fwrite(&magic, 4, 1, fp) == 1 && std::fwrite(&version, 4, 1, fp) == 1 &&
+            std::fwrite(&s64, 8, 1, fp) == 1 && std::fwrite(&D, 4, 1, fp) == 1 &&
+            std::fwrite(&Qi, 4, 1, fp) == 1 && std::fwrite(dims, 4, 3, fp) == 3 &&
+            std::fwrite(offs, 4, 3, fp) == 3 && std::fwrite(glob, 4, 3, fp) == 3 &&
+            std::fwrite(f.data(), sizeof(double), f.size(), fp) == f.size();
+  std::fclose(fp);
+  if (!ok) return F->fail(COUPLB_ERR_IO, "CoupLB IO: rank %d write error in %s", F->rank, fname);
+  F->log("CoupLB: checkpoint written at step %lld -> %s.*.clbk\n", step, F->cfg.checkpoint_prefix);
+  return COUPLB_OK;
+}
+
+// IO::read_checkpoint (couplb_io.h:721-829): every header field validated.
+int read_checkpoint(couplb_fix* F, long long* step_out) {
+  char fname[COUPLB_PATH_MAX + 32];
+  std::snprintf(fname, sizeof(fname), "%s.%d.clbk", F->cfg.restart_prefix, F->rank);
+  FILE* fp = std::fopen(fname, "rb");
+  if (!fp) return F->fail(COUPLB_ERR_IO, "CoupLB IO: rank %d cannot open %s for reading", F->rank, fname);
+  struct Closer { FILE* f; ~Closer() { std::fclose(f); } } closer{fp};
+  uint32_t magic = 0;
+  if (std::fread(&magic, 4, 1, fp) != 1 || magic != kCkptMagic)
+    return F->fail(COUPLB_ERR_IO, "CoupLB IO: rank %d bad magic in %s", F->rank, fname);
+  int32_t version = 0;
+  if (std::fread(&version, 4, 1, fp) != 1 || version != kCkptVersion)
+    return F->fail(COUPLB_ERR_IO, "CoupLB IO: rank %d unsupported version %d in %s", F->rank, version, fname);
+  int64_t s64 = 0;
+  if (std::fread(&s64, 8, 1, fp) != 1)
+    return F->fail(COUPLB_ERR_IO, "CoupLB IO: rank %d truncated header (step) in %s", F->rank, fname);
+  int32_t D = 0, Q = 0;
+  if (std::fread(&D, 4, 1, fp) != 1 || std::fread(&Q, 4, 1, fp) != 1)
+    return F->fail(COUPLB_ERR_IO, "CoupLB IO: rank %d truncated header (D/Q) in %s", F->rank, fname);
+  const int eD = F->is3d ? 3 : 2, eQ = F->is3d ? 19 : 9;
+  if (D != eD || Q != eQ)
+    return F->fail(COUPLB_ERR_IO,
+                   "CoupLB IO: rank %d D/Q mismatch in %s (file: D=%d Q=%d, expected: D=%d Q=%d)",
+                   F->rank, fname, D, Q, eD, eQ);
+  int32_t dims[3], offs[3], glob[3];
+  if (std::fread(dims, 4, 3, fp) != 3 || std::fread(offs, 4, 3, fp) != 3 || std::fread(glob, 4, 3, fp) != 3)
+    return F->fail(COUPLB_ERR_IO, "CoupLB IO: rank %d truncated header (dims) in %s", F->rank, fname);
+  const int nz = F->is3d ? F->nl[2] : 1;
+  if (dims[0] != F->nl[0] || dims[1] != F->nl[1] || dims[2] != nz)
+    return F->fail(COUPLB_ERR_IO,
+                   "CoupLB IO: rank %d local grid mismatch in %s (file: %dx%dx%d, current: %dx%dx%d)",
+                   F->rank, fname, dims[0], dims[1], dims[2], F->nl[0], F->nl[1], nz);
+  const int oz = F->is3d ? F->off[2] : 0;
+  if (offs[0] != F->off[0] || offs[1] != F->off[1] || offs[2] != oz)
+    return F->fail(COUPLB_ERR_IO,
+                   "CoupLB IO: rank %d offset mismatch in %s (file: %d,%d,%d, current: %d,%d,%d)",
+                   F->rank, fname, offs[0], offs[1], offs[2], F->off[0], F->off[1], oz);
+  const int gz = F->is3d ? F->cfg.Nz : 1;
+  if (glob[0] != F->cfg.Nx || glob[1] != F->cfg.Ny || glob[2] != gz)
+    return F->fail(COUPLB_ERR_IO, "CoupLB IO: rank %d global grid mismatch in %s", F->rank, fname);
+  const size_t nf = (size_t)Q * couplb_ghost_nodes(F->h);
+  std::vector<double> f(nf);
+  const size_t nread = std::fread(f.data(), sizeof(double), nf, fp);
+  if (nread != nf)
+    return F->fail(COUPLB_ERR_IO, "CoupLB IO: rank %d short read in %s (%zu/%zu doubles)", F->rank,
+                   fname, nread, nf);
+  int rc = couplb_set_populations(F->h, f.data());
+  if (rc) return F->engine_fail(rc);
+  *step_out = s64;
+  F->log("CoupLB: checkpoint loaded from step %lld <- %s.*.clbk\n", (long long)s64, F->cfg.restart_prefix);
+  F->log("CoupLB WARNING: LAMMPS timestep is NOT updated by checkpoint.\n"
+         "  Use 'reset_timestep %lld' in your input script if needed.\n", (long long)s64);
+  return COUPLB_OK;
+}
+
+// FixCoupLB::do_ibm_sub_coupling (fix_couplb.cpp:730-798).
+int ibm_sub_coupling(couplb_fix* F, const couplb_atoms* at) {
+  const bool first = (F->md_sub_count == 0);
+  const int nl = at ? at->nlocal : 0;
+  F->active_buf.resize(nl > 0 ? nl : 1);
+  F->mass_buf.resize(nl > 0 ? nl : 1);
+  int ng = 0;
+  for (int i = 0; i < nl; i++) {
+    const int act = at->mask ? ((at->mask[i] & at->groupbit) != 0) : 1;
+    F->active_buf[i] = act;
+    ng += act;
+    F->mass_buf[i] = at->rmass ? at->rmass[i] : (at->mass ? at->mass[at->type[i]] : 1.0);
+  }
+  if (ng == 0) {
+    F->ibm_has_particles = false;
+    return COUPLB_OK;
+  }
+  const int refresh = (first || !F->ibm_has_particles) ? 1 : 0;
+  F->ibm_has_particles = true;
+  int nc = 0;
+  const int rc = couplb_ibm_substep(F->h, nl, at->x, at->v, F->mass_buf.data(), F->active_buf.data(),
+                                    at->f, refresh, &nc);
+  if (rc) return F->engine_fail(rc);
+  return COUPLB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int couplb_fix_setmask(void) { return COUPLB_MASK_POST_FORCE | COUPLB_MASK_END_OF_STEP; }
+
+// FixCoupLB::FixCoupLB (fix_couplb.cpp:71-238)
+int couplb_fix_parse(int narg, const char* const* arg, int dimension, couplb_fix_config* cfg,
+                     char* err, int errlen) {
+  if (!cfg || !arg) return COUPLB_ERR_ARG;
+  couplb_fix_config c;
+  std::memset(&c, 0, sizeof(c));
+  try {
+    if (narg < 8) perr("Illegal fix couplb command: need Nx Ny Nz nu rho");
+    c.Nx = to_int(arg[3]); c.Ny = to_int(arg[4]); c.Nz = to_int(arg[5]);
+    c.nu = to_double(arg[6]); c.rho = to_double(arg[7]);
+    if (c.Nx <= 0 || c.Ny <= 0 || c.Nz <= 0) perr("fix couplb: Nx, Ny, and Nz must be positive");
+    if (c.nu <= 0.0 || !std::isfinite(c.nu)) perr("fix couplb: viscosity must be positive and finite");
+    if (c.rho <= 0.0 || !std::isfinite(c.rho)) perr("fix couplb: density must be positive and finite");
+    c.md_per_lb = 1;
+    c.xi_ibm = 1.0;
+    copy_str(c.output_file, "couplb_profile.dat");
+    copy_str(c.vtk_prefix, "couplb_vtk");
+    copy_str(c.checkpoint_prefix, "couplb_ckpt");
+    c.delta = COUPLB_DELTA_ROMA;
+    c.precision = COUPLB_FP64;
+    int iarg = 8;
+    while (iarg < narg) {
+      const char* kw = arg[iarg];
+      if (!is_keyword(kw)) perr("Unknown fix couplb keyword: %s", kw);
+      if (!std::strcmp(kw, "md_per_lb")) {
+        if (iarg + 2 > narg) perr("fix couplb md_per_lb: need 1 value");
+        c.md_per_lb = to_int(arg[iarg + 1]);
+        if (c.md_per_lb < 1) perr("fix couplb: md_per_lb must be >= 1");
+        iarg += 2;
+      } else if (!std::strcmp(kw, "xi_ibm")) {
+        if (iarg + 2 > narg) perr("fix couplb xi_ibm: need 1 value");
+        c.xi_ibm = to_double(arg[iarg + 1]);
+        if (c.xi_ibm <= 0.0 || c.xi_ibm > 1.0 || !std::isfinite(c.xi_ibm))
+          perr("fix couplb: xi_ibm must satisfy 0 < xi_ibm <= 1");
+        iarg += 2;
+      } else if (!std::strcmp(kw, "gravity")) {
+        if (iarg + 4 > narg) perr("fix couplb gravity: need 3 values");
+        for (int d = 0; d < 3; d++) {
+          const char* a = arg[iarg + 1 + d];
+          if (std::strstr(a, "v_") == a) {
+            std::strncpy(c.gvar[d], a + 2, 63);
+            c.gvar[d][63] = 0;
+            c.gstyle[d] = COUPLB_G_EQUAL;
+          } else {
+            c.gconst[d] = to_double(a);
+            c.gstyle[d] = COUPLB_G_CONSTANT;
+          }
+        }
+        iarg += 4;
+      } else if (!std::strcmp(kw, "wall_x") || !std::strcmp(kw, "wall_y") || !std::strcmp(kw, "wall_z")) {
+        const int d = kw[5] - 'x';
+        if (iarg + 3 > narg) perr("fix couplb %s: need 2 values", kw);
+        const int lo = to_int(arg[iarg + 1]), hi = to_int(arg[iarg + 2]);
+        c.wall[2 * d] = lo;
+        c.wall[2 * d + 1] = hi;
+        if (lo < 0 || lo > 4 || hi < 0 || hi > 4) perr("fix couplb: %s types must be in [0,4]", kw);
+        iarg += 3;
+      } else if (!std::strcmp(kw, "wall_vel")) {
+        if (iarg + 4 > narg) perr("fix couplb wall_vel: need 3 values");
+        for (int d = 0; d < 3; d++) c.wall_vel[d] = to_double(arg[iarg + 1 + d]);
+        iarg += 4;
+      } else if (!std::strcmp(kw, "output")) {
+        if (iarg + 3 > narg) perr("fix couplb output: need 2 values");
+        c.output_every = to_int(arg[iarg + 1]);
+        copy_str(c.output_file, arg[iarg + 2]);
+        if (c.output_every < 0) perr("fix couplb: output frequency cannot be negative");
+        iarg += 3;
+      } else if (!std::strcmp(kw, "check_every")) {
+        if (iarg + 2 > narg) perr("fix couplb check_every: need 1 value");
+        c.check_every = to_int(arg[iarg + 1]);
+        if (c.check_every < 0) perr("fix couplb: check_every cannot be negative");
+        iarg += 2;
+      } else if (!std::strcmp(kw, "kernel")) {
+        if (iarg + 2 > narg) perr("fix couplb kernel: need 1 value");
+        if (!std::strcmp(arg[iarg + 1], "roma")) c.delta = COUPLB_DELTA_ROMA;
+        else if (!std::strcmp(arg[iarg + 1], "peskin4")) c.delta = COUPLB_DELTA_PESKIN4;
+        else perr("fix couplb kernel: use roma or peskin4");
+        iarg += 2;
+      } else if (!std::strcmp(kw, "vtk")) {
+        if (iarg + 3 > narg) perr("fix couplb vtk: need N prefix");
+        c.vtk_every = to_int(arg[iarg + 1]);
+        copy_str(c.vtk_prefix, arg[iarg + 2]);
+        if (c.vtk_every < 0) perr("fix couplb: vtk frequency cannot be negative");
+        iarg += 3;
+      } else if (!std::strcmp(kw, "vtk_region")) {
+        iarg++;
+        int nreg = 0;
+        while (iarg + nreg < narg && !is_keyword(arg[iarg + nreg])) nreg++;
+        if (nreg != 4 && nreg != 6)
+          perr("fix couplb vtk_region: need 4 values (2D: xlo xhi ylo yhi) or 6 values (3D: xlo xhi ylo yhi zlo zhi)");
+        c.vtk_rlo[0] = to_double(arg[iarg]); c.vtk_rhi[0] = to_double(arg[iarg + 1]);
+        c.vtk_rlo[1] = to_double(arg[iarg + 2]); c.vtk_rhi[1] = to_double(arg[iarg + 3]);
+        if (nreg == 6) { c.vtk_rlo[2] = to_double(arg[iarg + 4]); c.vtk_rhi[2] = to_double(arg[iarg + 5]); }
+        else { c.vtk_rlo[2] = -1e30; c.vtk_rhi[2] = 1e30; }
+        c.has_vtk_region = 1;
+        c.vtk_region_n = nreg;
+        iarg += nreg;
+      } else if (!std::strcmp(kw, "vtk_solid")) {
+        if (c.vtk_solid_nattr) perr("fix couplb vtk_solid: keyword specified more than once");
+        iarg++;
+        int na = 0;
+        while (iarg < narg && !is_keyword(arg[iarg])) { na++; iarg++; }
+        if (na == 0) perr("fix couplb vtk_solid: need at least one attribute");
+        c.vtk_solid_nattr = na;
+      } else if (!std::strcmp(kw, "checkpoint")) {
+        if (iarg + 3 > narg) perr("fix couplb checkpoint: need N prefix");
+        c.checkpoint_every = to_int(arg[iarg + 1]);
+        copy_str(c.checkpoint_prefix, arg[iarg + 2]);
+        if (c.checkpoint_every < 0) perr("fix couplb: checkpoint frequency cannot be negative");
+        iarg += 3;
+      } else if (!std::strcmp(kw, "restart")) {
+        if (iarg + 2 > narg) perr("fix couplb restart: need prefix");
+        copy_str(c.restart_prefix, arg[iarg + 1]);
+        c.do_restart = 1;
+        iarg += 2;
+      } else if (!std::strcmp(kw, "precision")) {
+        if (iarg + 2 > narg) perr("fix couplb precision: need 1 value");
+        if (!std::strcmp(arg[iarg + 1], "fp64")) c.precision = COUPLB_FP64;
+        else if (!std::strcmp(arg[iarg + 1], "fp32")) c.precision = COUPLB_FP32_SHIFTED;
+        else if (!std::strcmp(arg[iarg + 1], "fp16")) c.precision = COUPLB_FP16_SHIFTED;
+        else perr("fix couplb precision: use fp64, fp32 or fp16");
+        iarg += 2;
+      }
+    }
+    c.dimension = dimension;
+    if (dimension != 3 && c.Nz != 1) perr("fix couplb: Nz must be 1 for 2D");
+  } catch (const ParseError& e) {
+    if (err && errlen > 0) {
+      std::strncpy(err, e.msg.c_str(), errlen - 1);
+      err[errlen - 1] = 0;
+    }
+    return COUPLB_ERR_PARSE;
+  }
+  *cfg = c;
+  return COUPLB_OK;
+}
+
+int couplb_fix_create(const couplb_fix_config* cfg, couplb_fix** out) {
+  if (!cfg || !out) return COUPLB_ERR_ARG;
+  couplb_fix* F = new couplb_fix();
+  F->cfg = *cfg;
+  *out = F;
+  return COUPLB_OK;
+}
+
+int couplb_fix_destroy(couplb_fix* F) {
+  if (!F) return COUPLB_OK;
+  if (F->h) couplb_destroy(F->h);
+  delete F;
+  return COUPLB_OK;
+}
+
+const char* couplb_fix_last_error(const couplb_fix* F) { return F ? F->err.c_str() : ""; }
+
+int couplb_fix_set_gravity_callback(couplb_fix* F, couplb_gravity_fn fn, void* ctx) {
+  if (!F) return COUPLB_ERR_ARG;
+  F->gcb = fn;
+  F->gctx = ctx;
+  return COUPLB_OK;
+}
+
+int couplb_fix_set_log_callback(couplb_fix* F, couplb_log_fn fn, void* ctx) {
+  if (!F) return COUPLB_ERR_ARG;
+  F->logcb = fn;
+  F->logctx = ctx;
+  return COUPLB_OK;
+}
+
+int couplb_fix_set_gravity_values(couplb_fix* F, const double g[3]) {
+  if (!F || !g) return COUPLB_ERR_ARG;
+  for (int d = 0; d < 3; d++) F->gvals[d] = g[d];
+  return COUPLB_OK;
+}
+
+int couplb_fix_set_device(couplb_fix* F, int device) {
+  if (!F) return COUPLB_ERR_ARG;
+  if (F->h) return F->fail(COUPLB_ERR_STATE, "couplb_fix_set_device must precede couplb_fix_init");
+  F->device = device;
+  return COUPLB_OK;
+}
+
+couplb_handle* couplb_fix_handle(couplb_fix* F) { return F ? F->h : nullptr; }
+
+int couplb_fix_scales(const couplb_fix* F, double out[6]) {
+  if (!F || !out) return COUPLB_ERR_ARG;
+  out[0] = F->dx; out[1] = F->dt_LBM; out[2] = F->vel_scale;
+  out[3] = F->force_scale; out[4] = F->nu_lb; out[5] = F->tau;
+  return COUPLB_OK;
+}
+
+int couplb_fix_last_diag(const couplb_fix* F, couplb_diag* out) {
+  if (!F || !out) return COUPLB_ERR_ARG;
+  *out = F->last_diag;
+  return COUPLB_OK;
+}
+
+long long couplb_fix_lbm_steps(const couplb_fix* F) { return F ? F->lbm_step_count : 0; }
+
+// FixCoupLB::init (fix_couplb.cpp:256-482) for one rank.
+int couplb_fix_init(couplb_fix* F, const couplb_domain* dom) {
+  if (!F || !dom) return COUPLB_ERR_ARG;
+  const couplb_fix_config& c = F->cfg;
+  if (c.md_per_lb < 1) return F->fail(COUPLB_ERR_ARG, "fix couplb: md_per_lb must be >= 1");
+  if (c.xi_ibm <= 0.0 || c.xi_ibm > 1.0 || !std::isfinite(c.xi_ibm))
+    return F->fail(COUPLB_ERR_ARG, "fix couplb: xi_ibm must satisfy 0 < xi_ibm <= 1");
+  F->is3d = (dom->dimension == 3);
+  for (int d = 0; d < 3; d++) { F->domain_lo[d] = dom->boxlo[d]; F->domain_hi[d] = dom->boxhi[d]; }
+  const double dx_x = (F->domain_hi[0] - F->domain_lo[0]) / c.Nx;
+  const double dx_y = (F->domain_hi[1] - F->domain_lo[1]) / c.Ny;
+  if (std::fabs(dx_x - dx_y) > 1e-10 * dx_x)
+    return F->fail(COUPLB_ERR_ARG,
+                   "fix couplb: non-cubic grid cells (Lx/Nx=%.6e != Ly/Ny=%.6e). Adjust Nx, Ny, or domain size.",
+                   dx_x, dx_y);
+  if (F->is3d) {
+    const double dx_z = (F->domain_hi[2] - F->domain_lo[2]) / c.Nz;
+    if (std::fabs(dx_x - dx_z) > 1e-10 * dx_x)
+      return F->fail(COUPLB_ERR_ARG,
+                     "fix couplb: non-cubic grid cells (Lx/Nx=%.6e != Lz/Nz=%.6e). Adjust Nx, Nz, or domain size.",
+                     dx_x, dx_z);
+  }
+  F->dx = dx_x;
+  F->inv_dx = 1.0 / F->dx;
+  F->dt = dom->dt;
+  F->dt_LBM = dom->dt * c.md_per_lb;
+  F->vel_scale = F->dx / F->dt_LBM;
+  F->nu_lb = c.nu * F->dt_LBM / (F->dx * F->dx);
+  F->tau = F->nu_lb / (1.0 / 3.0) + 0.5;
+  if (F->tau <= 0.5) return F->fail(COUPLB_ERR_ARG, "fix couplb: tau <= 0.5 (unstable)");
+  if (F->tau < 0.505) F->log("WARNING: fix couplb: tau very close to 0.5\n");
+  const int dim = F->is3d ? 3 : 2;
+  double dp = 1.0;
+  for (int d = 0; d < dim + 1; d++) dp *= F->dx;
+  F->force_scale = c.rho * dp / (F->dt_LBM * F->dt_LBM);
+  if (F->force_scale <= 0.0 || !std::isfinite(F->force_scale))
+    return F->fail(COUPLB_ERR_ARG,
+                   "fix couplb: force_scale is non-positive or non-finite (check rho, dx, dt_LBM)");
+  const double inv_vel = 1.0 / F->vel_scale;
+  const double wv_lb[3] = {c.wall_vel[0] * inv_vel, c.wall_vel[1] * inv_vel, c.wall_vel[2] * inv_vel};
+  const double cs = std::sqrt(1.0 / 3.0);
+  const double uw = std::sqrt(wv_lb[0] * wv_lb[0] + wv_lb[1] * wv_lb[1] + wv_lb[2] * wv_lb[2]);
+  if (uw > kMaError * cs) return F->fail(COUPLB_ERR_ARG, "fix couplb: wall Ma > 0.5");
+  if (uw > kMaWarn * cs) F->log("CoupLB WARNING: wall Ma=%.3f > 0.3\n", uw / cs);
+  if (c.gstyle[0] == COUPLB_G_CONSTANT && c.gstyle[1] == COUPLB_G_CONSTANT &&
+      c.gstyle[2] == COUPLB_G_CONSTANT) {
+    const double ac = F->dt_LBM * F->dt_LBM / F->dx;
+    const double gx = c.gconst[0] * ac, gy = c.gconst[1] * ac, gz = c.gconst[2] * ac;
+    const double gm = std::sqrt(gx * gx + gy * gy + gz * gz);
+    if (gm > kZeroTol) {
+      const int H = (c.wall[2] > 0 && c.wall[3] > 0) ? c.Ny : (c.wall[4] > 0 && c.wall[5] > 0) ? c.Nz : 0;
+      if (H > 0) {
+        const double ue = gm * H * H / (8.0 * F->nu_lb);
+        if (ue / cs > kMaError) return F->fail(COUPLB_ERR_ARG, "fix couplb: estimated Poiseuille Ma > 0.5");
+        if (ue / cs > kMaWarn) F->log("CoupLB WARNING: estimated Poiseuille Ma=%.3f\n", ue / cs);
+      }
+    }
+  }
+  if (c.output_every > 0) F->next_output = dom->ntimestep + c.output_every;
+  F->next_check = (c.check_every > 0) ? dom->ntimestep + c.check_every : -1;
+  F->next_vtk = (c.vtk_every > 0) ? dom->ntimestep + c.vtk_every : -1;
+  F->next_checkpoint = (c.checkpoint_every > 0) ? dom->ntimestep + c.checkpoint_every : -1;
+  F->lbm_step_count = 0;
+  F->md_sub_count = 0;
+
+  // setup_grid (fix_couplb.cpp:484-520)
+  const double eps = 1e-12;
+  int lo[3], hi[3];
+  for (int d = 0; d < 3; d++) {
+    lo[d] = (int)std::floor((dom->sublo[d] - F->domain_lo[d]) / F->dx + eps);
+    hi[d] = (int)std::floor((dom->subhi[d] - F->domain_lo[d]) / F->dx + eps);
+    F->nl[d] = hi[d] - lo[d];
+    F->off[d] = lo[d];
+  }
+  if (!F->is3d) { F->nl[2] = 1; F->off[2] = 0; }
+  if (F->nl[0] <= 0 || F->nl[1] <= 0 || (F->is3d && F->nl[2] <= 0))
+    return F->fail(COUPLB_ERR_ARG, "fix couplb: local grid empty");
+  if (F->h) { couplb_destroy(F->h); F->h = nullptr; }
+  couplb_lattice_params lp;
+  std::memset(&lp, 0, sizeof(lp));
+  lp.dim = dim;
+  lp.nx = F->nl[0]; lp.ny = F->nl[1]; lp.nz = F->nl[2];
+  lp.tau = F->tau;
+  lp.rho0 = kRhoLb;
+  // setup_boundaries (fix_couplb.cpp:522-539): in 2D only x and y walls
+  for (int f = 0; f < (F->is3d ? 6 : 4); f++) lp.wall[f] = c.wall[f];
+  for (int d = 0; d < 3; d++) lp.wall_vel[d] = wv_lb[d];
+  if (!F->is3d) lp.wall_vel[2] = 0.0;
+  lp.body_force = (c.gstyle[0] != COUPLB_G_NONE || c.gstyle[1] != COUPLB_G_NONE ||
+                   c.gstyle[2] != COUPLB_G_NONE);
+  lp.precision = c.precision;
+  lp.device = F->device;
+  int rc = couplb_create(&lp, &F->h);
+  if (rc) return F->fail(rc, "%s", couplb_last_error(nullptr));
+  couplb_ibm_params ip;
+  std::memset(&ip, 0, sizeof(ip));
+  ip.delta = c.delta;
+  ip.md_per_lb = c.md_per_lb;
+  ip.xi_ibm = c.xi_ibm;
+  ip.dt_lbm = F->dt_LBM;
+  ip.dx = F->dx;
+  ip.vel_scale = F->vel_scale;
+  ip.force_scale = F->force_scale;
+  for (int d = 0; d < 3; d++) { ip.domain_lo[d] = F->domain_lo[d]; ip.offset[d] = F->off[d]; }
+  if ((rc = couplb_set_ibm_params(F->h, &ip))) return F->engine_fail(rc);
+
+  if (c.do_restart) {
+    long long ck = 0;
+    if ((rc = read_checkpoint(F, &ck))) {
+      const std::string why = F->err;
+      return F->fail(rc, "fix couplb: failed to read checkpoint (%s)", why.c_str());
+    }
+    F->log("CoupLB: restarted from checkpoint step %lld\n", ck);
+    F->cfg.do_restart = 0;
+  }
+  if (c.vtk_solid_nattr > 0) {
+    if (c.vtk_every <= 0)
+      return F->fail(COUPLB_ERR_ARG, "fix couplb vtk_solid requires vtk keyword to set output frequency");
+    F->log("CoupLB: vtk_solid with %d attributes\n", c.vtk_solid_nattr);
+  }
+  if (c.has_vtk_region) {
+    // clamp, convert to node indices and validate (fix_couplb.cpp:386-426)
+    double rlo[3], rhi[3];
+    for (int d = 0; d < 3; d++) {
+      rlo[d] = std::max(c.vtk_rlo[d], F->domain_lo[d]);
+      rhi[d] = std::min(c.vtk_rhi[d], F->domain_hi[d]);
+    }
+    int* r = F->vtk_region;
+    r[0] = (int)std::floor((rlo[0] - F->domain_lo[0]) / F->dx);
+    r[1] = (int)std::ceil((rhi[0] - F->domain_lo[0]) / F->dx);
+    r[2] = (int)std::floor((rlo[1] - F->domain_lo[1]) / F->dx);
+    r[3] = (int)std::ceil((rhi[1] - F->domain_lo[1]) / F->dx);
+    if (F->is3d) {
+      r[4] = (int)std::floor((rlo[2] - F->domain_lo[2]) / F->dx);
+      r[5] = (int)std::ceil((rhi[2] - F->domain_lo[2]) / F->dx);
+    } else { r[4] = 0; r[5] = 1; }
+    const int Nn[3] = {c.Nx, c.Ny, c.Nz};
+    for (int d = 0; d < (F->is3d ? 3 : 2); d++)
+      for (int s = 0; s < 2; s++) r[2 * d + s] = std::max(0, std::min(r[2 * d + s], Nn[d]));
+    if (r[1] <= r[0] || r[3] <= r[2] || r[5] <= r[4])
+      return F->fail(COUPLB_ERR_ARG,
+                     "fix couplb vtk_region: empty or inverted region ([%d,%d]x[%d,%d]x[%d,%d]). Check that xlo<xhi, ylo<yhi%s",
+                     r[0], r[1], r[2], r[3], r[4], r[5], F->is3d ? ", zlo<zhi" : "");
+  }
+  if (c.vtk_every > 0)
+    F->log("CoupLB WARNING: vtk output is not written by the GPU build (keyword accepted, ignored)\n");
+  F->log("CoupLB: %dD grid %dx%dx%d tau=%.6f nu=%.6f rho=%.4f\n", dim, c.Nx, c.Ny, c.Nz, F->tau, c.nu, c.rho);
+  F->log("CoupLB: nu=%.4e -> nu_lb=%.6f\n", c.nu, F->nu_lb);
+  F->log("CoupLB: dx=%.4e dt_LBM=%.4e vel_scale=%.4e force_scale=%.4e\n", F->dx, F->dt_LBM, F->vel_scale,
+         F->force_scale);
+  F->log("CoupLB: kernel=%s xi_ibm=%.4f\n", c.delta == COUPLB_DELTA_ROMA ? "roma" : "peskin4", c.xi_ibm);
+  F->log("CoupLB: precision=%s device memory %.1f MB\n",
+         c.precision == COUPLB_FP64 ? "fp64" : (c.precision == COUPLB_FP32_SHIFTED ? "fp32" : "fp16"),
+         couplb_device_bytes(F->h) / 1048576.0);
+  F->inited = true;
+  return COUPLB_OK;
+}
+
+// FixCoupLB::setup (fix_couplb.cpp:551-638): spread the first forces without
+// advancing the fluid, then the step-0 profile.
+int couplb_fix_setup(couplb_fix* F, const couplb_atoms* at, long long ntimestep) {
+  if (!F || !F->inited) return F ? F->fail(COUPLB_ERR_STATE, "couplb_fix_init not called") : COUPLB_ERR_ARG;
+  F->md_sub_count = 0;
+  int rc = ibm_sub_coupling(F, at);
+  if (rc) return rc;
+  F->md_sub_count = 0;
+  const couplb_fix_config& c = F->cfg;
+  const bool need_macro = (c.output_every > 0 || c.vtk_every > 0);
+  if (need_macro && (rc = couplb_macroscopic(F->h))) return F->engine_fail(rc);
+  if (c.output_every > 0) {
+    if (F->rank == 0) {
+      FILE* fp = std::fopen(c.output_file, ntimestep == 0 ? "w" : "a");
+      if (fp) {
+        if (ntimestep == 0) {
+          std::fprintf(fp, "# H=Ny=%d tau=%.6f nu=%.4e nu_lb=%.6f rho=%.4f kernel=%s\n", c.Ny, F->tau, c.nu,
+                       F->nu_lb, c.rho, c.delta == COUPLB_DELTA_ROMA ? "roma" : "peskin4");
+          std::fprintf(fp, "# CoupLB velocity profile\n# Columns: step j y rho ux uy\n#\n");
+        }
+        std::fclose(fp);
+      }
+    }
+    if ((rc = write_profile(F, ntimestep))) return rc;
+  }
+  return COUPLB_OK;
+}
+
+// FixCoupLB::post_force + lbm_step + apply_external_force's gravity
+// (fix_couplb.cpp:640-651, 671-695).
+int couplb_fix_post_force(couplb_fix* F, const couplb_atoms* at, long long ntimestep) {
+  (void)ntimestep;
+  if (!F || !F->inited) return F ? F->fail(COUPLB_ERR_STATE, "couplb_fix_init not called") : COUPLB_ERR_ARG;
+  const couplb_fix_config& c = F->cfg;
+  int rc;
+  if (F->md_sub_count == 0) {
+    const bool none = c.gstyle[0] == COUPLB_G_NONE && c.gstyle[1] == COUPLB_G_NONE &&
+                      c.gstyle[2] == COUPLB_G_NONE;
+    if (none) {
+      rc = couplb_lbm_step(F->h, nullptr);
+    } else {
+      double gv[3];
+      for (int d = 0; d < 3; d++) {
+        if (c.gstyle[d] == COUPLB_G_EQUAL) {
+          if (F->gcb) {
+            if (F->gcb(F->gctx, d, &gv[d]) != 0)
+              return F->fail(COUPLB_ERR_ARG, "Variable %s for gravity in fix couplb could not be evaluated",
+                             c.gvar[d]);
+          } else {
+            gv[d] = F->gvals[d];
+          }
+        } else {
+          gv[d] = c.gconst[d];
+        }
+      }
+      const double ac = F->dt_LBM * F->dt_LBM / F->dx;
+      const double gl[3] = {gv[0] * ac, gv[1] * ac, gv[2] * ac};
+      rc = couplb_lbm_step(F->h, gl);
+    }
+    if (rc) return F->engine_fail(rc);
+    F->lbm_step_count++;
+  }
+  rc = ibm_sub_coupling(F, at);
+  if (rc) return rc;
+  F->md_sub_count = (F->md_sub_count + 1) % c.md_per_lb;
+  return COUPLB_OK;
+}
+
+// FixCoupLB::end_of_step (fix_couplb.cpp:846-901) with
+// check_stability_precomputed (:818-844).
+int couplb_fix_end_of_step(couplb_fix* F, long long step) {
+  if (!F || !F->inited) return F ? F->fail(COUPLB_ERR_STATE, "couplb_fix_init not called") : COUPLB_ERR_ARG;
+  const couplb_fix_config& c = F->cfg;
+  bool chk = false, out = false, vtk = false, ckpt = false;
+  if (c.check_every > 0 && step >= F->next_check) { chk = true; F->next_check = step + c.check_every; }
+  if (c.output_every > 0 && step >= F->next_output) { out = true; chk = true; F->next_output += c.output_every; }
+  if (c.vtk_every > 0 && step >= F->next_vtk) { vtk = true; F->next_vtk = step + c.vtk_every; }
+  if (c.checkpoint_every > 0 && step >= F->next_checkpoint) { ckpt = true; F->next_checkpoint = step + c.checkpoint_every; }
+  if (!chk && !out && !vtk && !ckpt) return COUPLB_OK;
+  int rc;
+  if (chk || out || vtk) {
+    if ((rc = couplb_macroscopic(F->h))) return F->engine_fail(rc);
+  }
+  if (chk) {
+    couplb_diag d;
+    if ((rc = couplb_diagnostics(F->h, &d))) return F->engine_fail(rc);
+    F->last_diag = d;
+    const double ma = d.umax / std::sqrt(1.0 / 3.0);
+    if (ma > kMaError) return F->fail(COUPLB_ERR_NUMERIC, "fix couplb: Ma>0.5, simulation invalid");
+    if (ma > kMaWarn) F->log("CoupLB WARNING: Ma=%.4f at step %lld\n", ma, step);
+    F->log("CoupLB step %lld: Ma=%.4f mass=%.8e mom=(%.4e,%.4e,%.4e)\n", step, ma, d.mass, d.mom[0], d.mom[1],
+           d.mom[2]);
+    if (d.clamps > 0) F->log("CoupLB WARNING: %d nodes had density clamped at step %lld\n", d.clamps, step);
+  }
+  if (out && (rc = write_profile(F, step))) return rc;
+  if (ckpt && (rc = write_checkpoint(F, step))) return rc;
+  return COUPLB_OK;
+}
+
+}  // extern "C"

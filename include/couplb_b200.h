@@ -1,0 +1,311 @@
+/*
+ * couplb_b200.h -- C ABI of the B200 (sm_100a) CoupLB hot path.
+ *
+ * Two layers, both plain C (no CUDA or torch types in any signature):
+ *
+ *   1. The lattice engine (couplb_*): one handle owns the device state of one
+ *      LBM subdomain (populations, force field, moments) and runs the
+ *      per-step kernels on one CUDA stream.  It replaces the member calls that
+ *      FixCoupLB makes on CoupLB::Grid / BGK / Streaming / IBM.
+ *
+ *   2. The fix core (couplb_fix_*): the `fix couplb` keyword parser, unit
+ *      conversion and the init / setup / post_force / end_of_step sequencing of
+ *      FixCoupLB, written against plain atom arrays so that a LAMMPS FixCoupLB
+ *      (or any MD code) forwards its hooks here.
+ *
+ * Every function returns an int status: COUPLB_OK (0) on success, a negative
+ * COUPLB_ERR_* code on failure.  Nothing aborts the process; the message of the
+ * last failure is available from couplb_last_error / couplb_fix_last_error.
+ * A handle is used from one host thread at a time.
+ *
+ * Reference interfaces each entry point replaces are cited as
+ * <file>:<line> relative to the CoupLB source tree.
+ */
+#ifndef COUPLB_B200_H
+#define COUPLB_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define COUPLB_ABI_VERSION 1
+
+/* ---- status codes ---------------------------------------------------- */
+#define COUPLB_OK               0
+#define COUPLB_ERR_ARG         -1  /* invalid argument / size                */
+#define COUPLB_ERR_CUDA        -2  /* a CUDA runtime call failed              */
+#define COUPLB_ERR_STATE       -3  /* call out of order / handle not ready    */
+#define COUPLB_ERR_NUMERIC     -4  /* non-finite density or Mach > 0.5        */
+#define COUPLB_ERR_IO          -5  /* checkpoint / profile file error         */
+#define COUPLB_ERR_PARSE       -6  /* `fix couplb` argument error             */
+#define COUPLB_ERR_UNSUPPORTED -7  /* feature outside this build              */
+
+/* ---- enumerations ---------------------------------------------------- */
+/* storage / arithmetic precision of the populations */
+#define COUPLB_FP64          0  /* plain f in FP64, FP64 arithmetic            */
+#define COUPLB_FP32_SHIFTED  1  /* h = f - w*rho0 stored and computed in FP32  */
+#define COUPLB_FP16_SHIFTED  2  /* h stored as scaled IEEE half, FP32 compute  */
+
+/* IBM delta kernel (couplb_ibm.h:37) */
+#define COUPLB_DELTA_ROMA    0
+#define COUPLB_DELTA_PESKIN4 1
+
+/* wall types (fix_couplb.cpp:56-58) */
+#define COUPLB_WALL_PERIODIC 0
+#define COUPLB_WALL_NOSLIP   1
+#define COUPLB_WALL_MOVING   2
+#define COUPLB_WALL_FREESLIP 3
+#define COUPLB_WALL_OPEN     4
+
+/* gravity component styles (fix_couplb.h:172) */
+#define COUPLB_G_NONE     0
+#define COUPLB_G_CONSTANT 1
+#define COUPLB_G_EQUAL    2
+
+/* ======================================================================
+ * Layer 1: lattice engine
+ * ==================================================================== */
+
+/* Lattice of one subdomain, in lattice units (dx = dt = 1). */
+typedef struct couplb_lattice_params {
+  int    dim;          /* 2 -> D2Q9, 3 -> D3Q19                               */
+  int    nx, ny, nz;   /* interior nodes; nz must be 1 when dim == 2          */
+  double tau;          /* BGK relaxation time, > 0.5                          */
+  double rho0;         /* lattice reference density (FixCoupLB uses 1.0)      */
+  int    wall[6];      /* xlo xhi ylo yhi zlo zhi wall types, 0..4            */
+  double wall_vel[3];  /* velocity of type-2 walls, lattice units             */
+  int    body_force;   /* 1 if a gravity style is set: keeps the density field
+                          that apply_external_force reads (fix_couplb.cpp:706) */
+  int    precision;    /* COUPLB_FP64 / COUPLB_FP32_SHIFTED / COUPLB_FP16_SHIFTED */
+  int    device;       /* CUDA device ordinal                                 */
+} couplb_lattice_params;
+
+/* IBM coupling constants (fix_couplb.cpp:286-317, 763-769). */
+typedef struct couplb_ibm_params {
+  int    delta;          /* COUPLB_DELTA_ROMA / COUPLB_DELTA_PESKIN4          */
+  int    md_per_lb;      /* MD sub-steps per LB step, >= 1                    */
+  double xi_ibm;         /* penalty relaxation factor, 0 < xi <= 1            */
+  double dt_lbm;         /* LB time step, MD units                           */
+  double dx;             /* lattice spacing, MD units                         */
+  double vel_scale;      /* dx / dt_lbm                                       */
+  double force_scale;    /* rho * dx^(D+1) / dt_lbm^2                         */
+  double domain_lo[3];   /* box lower corner, MD units                        */
+  int    offset[3];      /* global index of this subdomain's first node       */
+} couplb_ibm_params;
+
+/* Reductions of a20 (couplb_lattice.h:203-242, fix_couplb.cpp:818-844). */
+typedef struct couplb_diag {
+  double umax;       /* max |u| over fluid nodes, lattice units               */
+  double mass;       /* sum rho over fluid nodes (FP64 on the device)         */
+  double mom[3];     /* sum rho*u over fluid nodes (FP64 on the device)       */
+  int    clamps;     /* density clamps of the last moment pass                */
+  int    nonfinite;  /* non-finite densities seen by any kernel since reset   */
+} couplb_diag;
+
+typedef struct couplb_handle couplb_handle;
+
+/* Create / destroy.  Replaces Grid::allocate + init_equilibrium(rho0,0,0,0)
+ * (couplb_lattice.h:105-154), BGK::set_tau (couplb_collision.h:15),
+ * Boundary::set_walls_x/y/z + set_wall_velocity (couplb_boundary.h:12-38) and
+ * Streaming::precompute_wall_flags (couplb_streaming.h:74-80), as called from
+ * FixCoupLB::setup_grid / setup_boundaries (fix_couplb.cpp:484-539). */
+int  couplb_create(const couplb_lattice_params* p, couplb_handle** out);
+int  couplb_destroy(couplb_handle* h);
+const char* couplb_last_error(const couplb_handle* h);  /* h may be NULL */
+int  couplb_version(void);
+/* sizeof of the ABI structs, for bindings to check their layouts:
+ * 0 lattice_params, 1 ibm_params, 2 diag, 3 fix_config, 4 domain, 5 atoms.
+ * No counterpart in the reference (binding support only). */
+size_t couplb_struct_size(int which);
+
+/* Run on a caller-owned stream (a cudaStream_t passed as void*). */
+int  couplb_set_stream(couplb_handle* h, void* cuda_stream);
+int  couplb_synchronize(couplb_handle* h);
+
+/* Grid::init_equilibrium (couplb_lattice.h:145-154). */
+int  couplb_init_equilibrium(couplb_handle* h, double rho, double ux,
+                             double uy, double uz);
+
+/* Populations in the reference layout: double f[q*G + n], G = gx*gy*gz
+ * ghost-inclusive nodes, n = i + gx*(j + gy*k) (couplb_lattice.h:82-129).
+ * set: like IO::read_checkpoint (couplb_io.h:802-817) -- f and f_buf take the
+ * values, then the moments are recomputed without the Guo term.  Only interior
+ * values are used.  get: interior values are the post-stream state; ghost
+ * values are the periodic images (non-wall faces) or w_q*rho0 (wall faces). */
+int  couplb_set_populations(couplb_handle* h, const double* f_host);
+int  couplb_get_populations(couplb_handle* h, double* f_host);
+size_t couplb_ghost_nodes(const couplb_handle* h);   /* G */
+
+/* One LB step: FixCoupLB::do_lbm_step (fix_couplb.cpp:659-669) =
+ * apply_external_force (:680-708) + compute_macroscopic(true) + collide +
+ * exchange + stream + enforce_wall_ghost_fields + clear_forces, fused.
+ * g_lb: body-force acceleration in lattice units, or NULL when no gravity
+ * style is set (fix_couplb.cpp:686). */
+int  couplb_lbm_step(couplb_handle* h, const double* g_lb);
+
+/* Grid::compute_macroscopic(false) (couplb_lattice.h:155-202) followed by
+ * Streaming::exchange_velocity (couplb_streaming.h:140-143). */
+int  couplb_macroscopic(couplb_handle* h);
+
+/* Ghost-inclusive (G-node) copies of rho, u after the last couplb_macroscopic;
+ * wall ghost nodes carry the values of enforce_wall_ghost_fields
+ * (fix_couplb.cpp:800-809).  Any pointer may be NULL. */
+int  couplb_get_macroscopic(couplb_handle* h, double* rho, double* ux,
+                            double* uy, double* uz);
+
+/* The Eulerian force field (Grid::fx/fy/fz), G-node layout; ghost values 0.
+ * set is for tests and restarts: the values act as already folded forces. */
+int  couplb_get_force_field(couplb_handle* h, double* fx, double* fy, double* fz);
+int  couplb_set_force_field(couplb_handle* h, const double* fx,
+                            const double* fy, const double* fz);
+
+/* Grid::max_velocity + compute_diagnostics + rho_clamp_count over the moments
+ * of the last couplb_macroscopic (couplb_lattice.h:203-242). */
+int  couplb_diagnostics(couplb_handle* h, couplb_diag* out);
+
+/* Per-j sums over i and k of ux, uy and rho after the last couplb_macroscopic
+ * (each output holds ny doubles): the local sums of FixCoupLB::write_profile
+ * (fix_couplb.cpp:906-910). */
+int  couplb_y_profile(couplb_handle* h, double* ux_sum, double* uy_sum,
+                      double* rho_sum);
+
+/* IBM: constants, then one MD sub-step of FixCoupLB::do_ibm_sub_coupling
+ * (fix_couplb.cpp:730-798): interpolate (couplb_ibm.h:57-90), penalty force
+ * (fix_couplb.cpp:777-785), spread (couplb_ibm.h:92-133) and the reverse
+ * force fold (couplb_streaming.h:155-158).
+ *   host arrays:   x, v: n*3 doubles (MD units), mass: n doubles,
+ *                  active: n ints (nonzero = atom is in the fix group) or NULL,
+ *                  f_add: n*3 doubles; the IBM force is ADDED to it.
+ *   refresh:       nonzero on the first sub-step of an LB cycle (or when atoms
+ *                  reappear): recompute the fluid velocity (fix_couplb.cpp:757).
+ * Returns the number of coupled atoms through *ncoupled (may be NULL). */
+int  couplb_set_ibm_params(couplb_handle* h, const couplb_ibm_params* ip);
+int  couplb_ibm_substep(couplb_handle* h, int n, const double* x,
+                        const double* v, const double* mass, const int* active,
+                        double* f_add, int refresh, int* ncoupled);
+/* Same with device-resident atom arrays (device pointers, same shapes). */
+int  couplb_ibm_substep_device(couplb_handle* h, int n, const double* d_x,
+                               const double* d_v, const double* d_mass,
+                               const int* d_active, double* d_f_add,
+                               int refresh);
+
+/* FP64 sum over all spread markers of the force given to the grid (lattice
+ * units), accumulated on the device since the last reset: the fluid side of the
+ * momentum balance of docs/theory.md (sub-stepped coupling).  No counterpart
+ * function in the reference, which conserves this sum implicitly. */
+int  couplb_ibm_total_force(couplb_handle* h, double out[3], int reset);
+
+/* Device status word: counts of density clamps / non-finite densities seen by
+ * the stepping kernels since the last reset.  Reading synchronises. */
+int  couplb_read_status(couplb_handle* h, int* clamps, int* nonfinite, int reset);
+
+/* Bytes of device memory held by the handle. */
+size_t couplb_device_bytes(const couplb_handle* h);
+
+/* ======================================================================
+ * Layer 2: fix core (`fix ID group couplb Nx Ny Nz nu rho [keywords]`)
+ * ==================================================================== */
+
+#define COUPLB_PATH_MAX 256
+
+/* Parsed arguments of `fix couplb` (fix_couplb.cpp:71-238). */
+typedef struct couplb_fix_config {
+  int    Nx, Ny, Nz;
+  double nu, rho;
+  int    md_per_lb;
+  double xi_ibm;
+  int    gstyle[3];                 /* COUPLB_G_*                          */
+  double gconst[3];                 /* constant components, MD units       */
+  char   gvar[3][64];               /* variable names of v_ components     */
+  int    wall[6];
+  double wall_vel[3];
+  int    output_every;
+  char   output_file[COUPLB_PATH_MAX];
+  int    check_every;
+  int    delta;                     /* COUPLB_DELTA_*                      */
+  int    vtk_every;
+  char   vtk_prefix[COUPLB_PATH_MAX];
+  int    has_vtk_region;
+  int    vtk_region_n;              /* 4 or 6 values given                 */
+  double vtk_rlo[3], vtk_rhi[3];
+  int    vtk_solid_nattr;           /* 0 = off                             */
+  int    checkpoint_every;
+  char   checkpoint_prefix[COUPLB_PATH_MAX];
+  int    do_restart;
+  char   restart_prefix[COUPLB_PATH_MAX];
+  int    precision;                 /* `precision fp64|fp32|fp16`, default fp64 */
+  int    dimension;                 /* domain->dimension                   */
+} couplb_fix_config;
+
+/* The MD side of one subdomain (LAMMPS: domain, update). */
+typedef struct couplb_domain {
+  int       dimension;
+  double    boxlo[3], boxhi[3];
+  double    sublo[3], subhi[3];   /* = box for one rank                     */
+  int       periodicity[3];
+  double    dt;                   /* MD time step                           */
+  long long ntimestep;
+} couplb_domain;
+
+/* Atom arrays of one subdomain (LAMMPS: atom->x[0], v[0], f[0], ...). */
+typedef struct couplb_atoms {
+  int           nlocal;
+  const double* x;           /* nlocal*3                                     */
+  const double* v;           /* nlocal*3                                     */
+  double*       f;           /* nlocal*3, IBM force added                    */
+  const int*    mask;        /* nlocal, or NULL = every atom in the group    */
+  int           groupbit;
+  const double* rmass;       /* nlocal per-atom masses, or NULL              */
+  const double* mass;        /* per-type masses indexed by type, if !rmass   */
+  const int*    type;        /* nlocal, used with mass                       */
+} couplb_atoms;
+
+typedef struct couplb_fix couplb_fix;
+
+/* Gravity callback for v_ components: fills *value (MD units) for component
+ * comp (0..2); called once per LB step, like update_gravity_variables
+ * (fix_couplb.cpp:671-678).  Return 0 on success. */
+typedef int  (*couplb_gravity_fn)(void* ctx, int comp, double* value);
+/* Screen/log sink for rank-0 messages (fix_couplb.cpp:452-481). */
+typedef void (*couplb_log_fn)(void* ctx, const char* line);
+
+/* FixCoupLB::FixCoupLB argument parsing (fix_couplb.cpp:71-238); arg[0..2] are
+ * ID, group, "couplb" as in LAMMPS.  On failure err holds the reference's
+ * message. */
+int  couplb_fix_parse(int narg, const char* const* arg, int dimension,
+                      couplb_fix_config* cfg, char* err, int errlen);
+int  couplb_fix_create(const couplb_fix_config* cfg, couplb_fix** out);
+int  couplb_fix_destroy(couplb_fix* fx);
+const char* couplb_fix_last_error(const couplb_fix* fx);
+int  couplb_fix_set_gravity_callback(couplb_fix* fx, couplb_gravity_fn fn, void* ctx);
+int  couplb_fix_set_log_callback(couplb_fix* fx, couplb_log_fn fn, void* ctx);
+/* Values for v_ gravity components when no callback is set (MD units). */
+int  couplb_fix_set_gravity_values(couplb_fix* fx, const double g[3]);
+int  couplb_fix_set_device(couplb_fix* fx, int device);
+
+/* FixCoupLB::setmask: POST_FORCE | END_OF_STEP (fix_couplb.cpp:248-254). */
+#define COUPLB_MASK_POST_FORCE  1
+#define COUPLB_MASK_END_OF_STEP 2
+int  couplb_fix_setmask(void);
+
+/* Hooks (fix_couplb.h:26-30). */
+int  couplb_fix_init(couplb_fix* fx, const couplb_domain* dom);       /* :256-482 */
+int  couplb_fix_setup(couplb_fix* fx, const couplb_atoms* at,
+                      long long ntimestep);                           /* :551-638 */
+int  couplb_fix_post_force(couplb_fix* fx, const couplb_atoms* at,
+                           long long ntimestep);                      /* :640-651 */
+int  couplb_fix_end_of_step(couplb_fix* fx, long long ntimestep);     /* :846-901 */
+
+/* Accessors for drivers and tests. */
+couplb_handle* couplb_fix_handle(couplb_fix* fx);
+int  couplb_fix_scales(const couplb_fix* fx, double out[6]);  /* dx dt_LBM vel_scale force_scale nu_lb tau */
+int  couplb_fix_last_diag(const couplb_fix* fx, couplb_diag* out);
+long long couplb_fix_lbm_steps(const couplb_fix* fx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* COUPLB_B200_H */

@@ -1,0 +1,619 @@
+/*
+ * couplb_oracle.c -- plain-C restatement of CoupLB's per-timestep LBM + IBM
+ * path, used ONLY as the checker of the CUDA implementation (tests/,
+ * __graft_entry__.smoke(), bench.py's CPU-baseline leg).  It is never linked
+ * into or called by the product library.
+ *
+ * Each function names the reference code it follows (paths relative to the
+ * CoupLB source tree).  Arithmetic is kept in the reference's operation order
+ * so that, compiled without FMA contraction, it reproduces the reference
+ * bit for bit; tests/test_oracle_pin.py checks this against the reference's
+ * own headers (oracle/_ref) and against committed golden vectors.
+ *
+ * One subdomain = the whole box (one MPI rank in the reference).  With one
+ * rank every non-wall face exchanges with itself, so the MPI ghost exchange
+ * (couplb_streaming.h:136-245) becomes the face copies below.
+ */
+#include "couplb_oracle.h"
+
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ---- constants (couplb_lattice.h:13-20) ----------------------------- */
+#define RHO_MIN        1e-10
+#define DELTA_TOL      1e-12
+#define ZERO_TOL       1e-15
+#define RHO_CLAMP_FRAC 0.1
+#define MA_WARN        0.3
+#define MA_ERROR       0.5
+
+/* ---- lattice descriptors (couplb_lattice.h:24-75) ------------------- */
+static const int E9[9][3] = {{0,0,0},{1,0,0},{-1,0,0},{0,1,0},{0,-1,0},
+                             {1,1,0},{-1,-1,0},{1,-1,0},{-1,1,0}};
+static const double W9[9] = {4.0/9.0, 1.0/9.0, 1.0/9.0, 1.0/9.0, 1.0/9.0,
+                             1.0/36.0, 1.0/36.0, 1.0/36.0, 1.0/36.0};
+static const int OPP9[9] = {0,2,1,4,3,6,5,8,7};
+static const int REFL9[3][9] = {{0,2,1,3,4,8,7,6,5},
+                                {0,1,2,4,3,7,8,5,6},
+                                {0,1,2,3,4,5,6,7,8}};
+static const int E19[19][3] = {{0,0,0},{1,0,0},{-1,0,0},{0,1,0},{0,-1,0},
+                               {0,0,1},{0,0,-1},{1,1,0},{-1,-1,0},{1,-1,0},
+                               {-1,1,0},{1,0,1},{-1,0,-1},{1,0,-1},{-1,0,1},
+                               {0,1,1},{0,-1,-1},{0,1,-1},{0,-1,1}};
+static const double W19[19] = {1.0/3.0, 1.0/18.0, 1.0/18.0, 1.0/18.0,
+                               1.0/18.0, 1.0/18.0, 1.0/18.0, 1.0/36.0,
+                               1.0/36.0, 1.0/36.0, 1.0/36.0, 1.0/36.0,
+                               1.0/36.0, 1.0/36.0, 1.0/36.0, 1.0/36.0,
+                               1.0/36.0, 1.0/36.0, 1.0/36.0};
+static const int OPP19[19] = {0,2,1,4,3,6,5,8,7,10,9,12,11,14,13,16,15,18,17};
+static const int REFL19[3][19] = {
+  {0,2,1,3,4,5,6,10,9,8,7,14,13,12,11,15,16,17,18},
+  {0,1,2,4,3,5,6,9,10,7,8,11,12,13,14,18,17,16,15},
+  {0,1,2,3,4,6,5,7,8,9,10,13,14,11,12,17,18,15,16}};
+static const double CS2 = 1.0 / 3.0;
+
+typedef struct orc_grid {
+  int D, Q;
+  const int (*e)[3];
+  const double* w;
+  const int* opp;
+  const int* refl;      /* refl[d*Q + q] */
+  int nx, ny, nz, gx, gy, gz, ntotal;
+  double *f, *f_buf, *rho, *ux, *uy, *uz, *fx, *fy, *fz;
+  double *bc_ux, *bc_uy, *bc_uz;
+  int *type, *wall_dim;
+  int rho_clamp_count;
+  double tau, omega, rho0;
+  int wall_face[3][2];
+} orc_grid;
+
+static inline int gidx(const orc_grid* g, int i, int j, int k) {
+  return i + g->gx * (j + g->gy * k);
+}
+#define FI(g, q, n)   ((g)->f[(size_t)(q) * (g)->ntotal + (n)])
+#define FB(g, q, n)   ((g)->f_buf[(size_t)(q) * (g)->ntotal + (n)])
+
+/* Grid::feq (couplb_lattice.h:137-144) */
+static double feq(const orc_grid* g, int q, double r, double u0, double u1,
+                  double u2) {
+  const double eu = g->e[q][0]*u0 + g->e[q][1]*u1 + g->e[q][2]*u2;
+  const double uu = u0*u0 + u1*u1 + u2*u2;
+  const double cs4 = CS2 * CS2;
+  return g->w[q] * r * (1.0 + eu/CS2 + 0.5*eu*eu/cs4 - 0.5*uu/CS2);
+}
+
+/* Grid::init_equilibrium (couplb_lattice.h:145-154) */
+void ORC_FN(grid_init_equilibrium)(void* gp, double r0, double ux0, double uy0,
+                                   double uz0) {
+  orc_grid* g = (orc_grid*)gp;
+  for (int n = 0; n < g->ntotal; n++) {
+    g->rho[n] = r0;
+    g->ux[n] = ux0; g->uy[n] = uy0; g->uz[n] = uz0;
+    g->fx[n] = g->fy[n] = g->fz[n] = 0.0;
+    for (int q = 0; q < g->Q; q++) FI(g, q, n) = feq(g, q, r0, ux0, uy0, uz0);
+  }
+  memcpy(g->f_buf, g->f, sizeof(double) * (size_t)g->Q * g->ntotal);
+}
+
+/* Boundary::set_walls_x/y/z (couplb_boundary.h:12-35) */
+static void set_walls(orc_grid* g, int d, int lo, int hi, int tlo, int thi) {
+  const int ext[3] = {g->gx, g->gy, g->gz};
+  for (int side = 0; side < 2; side++) {
+    if (!(side ? hi : lo)) continue;
+    const int pos = side ? ext[d] - 1 : 0;
+    for (int k = 0; k < g->gz; k++)
+      for (int j = 0; j < g->gy; j++)
+        for (int i = 0; i < g->gx; i++) {
+          const int c[3] = {i, j, k};
+          if (c[d] != pos) continue;
+          const int n = gidx(g, i, j, k);
+          g->type[n] = side ? thi : tlo;
+          g->wall_dim[n] = d;
+        }
+  }
+}
+
+/* Streaming::has_wall_on_face (couplb_streaming.h:163-169) */
+static int has_wall_on_face(const orc_grid* g, int d, int pos) {
+  for (int k = 0; k < g->gz; k++)
+    for (int j = 0; j < g->gy; j++)
+      for (int i = 0; i < g->gx; i++) {
+        const int c[3] = {i, j, k};
+        if (c[d] != pos) continue;
+        if (g->type[gidx(g, i, j, k)] == 0) return 0;
+      }
+  return 1;
+}
+
+/* Grid::allocate + init_equilibrium(rho0) + BGK::set_tau + setup_boundaries
+ * + precompute_wall_flags (couplb_lattice.h:105-123, fix_couplb.cpp:501-539,
+ * couplb_streaming.h:74-80).  In 2D only x and y walls are applied
+ * (fix_couplb.cpp:533-537). */
+void* ORC_FN(grid_create)(int dim, int nx, int ny, int nz, double tau,
+                          double rho0, const int wall[6],
+                          const double wall_vel[3]) {
+  orc_grid* g = (orc_grid*)calloc(1, sizeof(orc_grid));
+  g->D = dim;
+  if (dim == 3) { g->Q = 19; g->e = E19; g->w = W19; g->opp = OPP19; g->refl = &REFL19[0][0]; }
+  else          { g->Q = 9;  g->e = E9;  g->w = W9;  g->opp = OPP9;  g->refl = &REFL9[0][0]; }
+  g->nx = nx; g->ny = ny; g->nz = nz;
+  g->gx = nx + 2; g->gy = ny + 2; g->gz = (dim == 3) ? nz + 2 : 1;
+  g->ntotal = g->gx * g->gy * g->gz;
+  const size_t G = (size_t)g->ntotal, QG = (size_t)g->Q * G;
+  g->f = (double*)calloc(QG, sizeof(double));
+  g->f_buf = (double*)calloc(QG, sizeof(double));
+  g->rho = (double*)calloc(G, sizeof(double));
+  g->ux = (double*)calloc(G, sizeof(double));
+  g->uy = (double*)calloc(G, sizeof(double));
+  g->uz = (double*)calloc(G, sizeof(double));
+  g->fx = (double*)calloc(G, sizeof(double));
+  g->fy = (double*)calloc(G, sizeof(double));
+  g->fz = (double*)calloc(G, sizeof(double));
+  g->bc_ux = (double*)calloc(G, sizeof(double));
+  g->bc_uy = (double*)calloc(G, sizeof(double));
+  g->bc_uz = (double*)calloc(G, sizeof(double));
+  g->type = (int*)calloc(G, sizeof(int));
+  g->wall_dim = (int*)malloc(G * sizeof(int));
+  for (size_t n = 0; n < G; n++) { g->rho[n] = 1.0; g->wall_dim[n] = -1; }
+  g->rho0 = rho0;
+  ORC_FN(grid_init_equilibrium)(g, rho0, 0, 0, 0);
+  g->tau = tau; g->omega = 1.0 / tau;
+  const int nd = (dim == 3) ? 3 : 2;
+  for (int d = 0; d < nd; d++) {
+    const int tlo = wall[2*d], thi = wall[2*d + 1];
+    if (tlo || thi) set_walls(g, d, tlo > 0, thi > 0, tlo, thi);
+  }
+  const double wv[3] = {wall_vel[0], wall_vel[1], dim == 3 ? wall_vel[2] : 0.0};
+  for (int n = 0; n < g->ntotal; n++)
+    if (g->type[n] == 2) { g->bc_ux[n] = wv[0]; g->bc_uy[n] = wv[1]; g->bc_uz[n] = wv[2]; }
+  for (int d = 0; d < 3; d++) g->wall_face[d][0] = g->wall_face[d][1] = 0;
+  for (int d = 0; d < nd; d++) {
+    const int ext = d == 0 ? g->gx : d == 1 ? g->gy : g->gz;
+    g->wall_face[d][0] = has_wall_on_face(g, d, 0);
+    g->wall_face[d][1] = has_wall_on_face(g, d, ext - 1);
+  }
+  return g;
+}
+
+void ORC_FN(grid_destroy)(void* gp) {
+  orc_grid* g = (orc_grid*)gp;
+  if (!g) return;
+  free(g->f); free(g->f_buf); free(g->rho); free(g->ux); free(g->uy); free(g->uz);
+  free(g->fx); free(g->fy); free(g->fz); free(g->bc_ux); free(g->bc_uy);
+  free(g->bc_uz); free(g->type); free(g->wall_dim); free(g);
+}
+
+long ORC_FN(grid_ntotal)(void* gp) { return ((orc_grid*)gp)->ntotal; }
+
+/* Grid::compute_macroscopic (couplb_lattice.h:155-202) */
+void ORC_FN(grid_macroscopic)(void* gp, int guo) {
+  orc_grid* g = (orc_grid*)gp;
+  const int klo = (g->D == 3) ? 1 : 0, khi = (g->D == 3) ? g->gz - 2 : 0;
+  int clamps = 0;
+#pragma omp parallel for collapse(2) schedule(static) reduction(+:clamps)
+  for (int k = klo; k <= khi; k++)
+    for (int j = 1; j <= g->gy - 2; j++)
+      for (int i = 1; i <= g->gx - 2; i++) {
+        const int n = gidx(g, i, j, k);
+        if (g->type[n] != 0) continue;
+        double r = 0.0, su = 0.0, sv = 0.0, sw = 0.0;
+        for (int q = 0; q < g->Q; q++) {
+          const double fv = FI(g, q, n);
+          r  += fv;
+          su += g->e[q][0] * fv;
+          sv += g->e[q][1] * fv;
+          sw += g->e[q][2] * fv;
+        }
+        if (r <= RHO_MIN) { r = RHO_MIN; clamps++; }
+        if (!isfinite(r)) { r = RHO_MIN; clamps++; }
+        g->rho[n] = r;
+        const double inv_r = 1.0 / r;
+        if (guo) {
+          g->ux[n] = (su + 0.5 * g->fx[n]) * inv_r;
+          g->uy[n] = (sv + 0.5 * g->fy[n]) * inv_r;
+          g->uz[n] = (sw + 0.5 * g->fz[n]) * inv_r;
+        } else {
+          g->ux[n] = su * inv_r;
+          g->uy[n] = sv * inv_r;
+          g->uz[n] = sw * inv_r;
+        }
+      }
+  g->rho_clamp_count = clamps;
+}
+
+/* BGK::collide (couplb_collision.h:18-62) */
+static void collide(orc_grid* g) {
+  const double cs4 = CS2 * CS2;
+  const double om = g->omega, half_om = 1.0 - 0.5 * om;
+  const int klo = (g->D == 3) ? 1 : 0, khi = (g->D == 3) ? g->gz - 2 : 0;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int k = klo; k <= khi; k++)
+    for (int j = 1; j <= g->gy - 2; j++)
+      for (int i = 1; i <= g->gx - 2; i++) {
+        const int n = gidx(g, i, j, k);
+        if (g->type[n] != 0) continue;
+        const double r = g->rho[n];
+        const double u0 = g->ux[n], u1 = g->uy[n], u2 = g->uz[n];
+        const double f0 = g->fx[n], f1 = g->fy[n], f2 = g->fz[n];
+        const double uu = u0*u0 + u1*u1 + u2*u2;
+        const double uf = u0*f0 + u1*f1 + u2*f2;
+        for (int q = 0; q < g->Q; q++) {
+          const double cx = g->e[q][0], cy = g->e[q][1], cz = g->e[q][2];
+          const double w = g->w[q];
+          const double eu = cx*u0 + cy*u1 + cz*u2;
+          const double ef = cx*f0 + cy*f1 + cz*f2;
+          const double fe = w * r * (1.0 + eu/CS2 + 0.5*eu*eu/cs4 - 0.5*uu/CS2);
+          const double Si = w * half_om * ((ef - uf)/CS2 + eu*ef/cs4);
+          FI(g, q, n) += -om * (FI(g, q, n) - fe) + Si;
+        }
+      }
+}
+
+/* Face iteration over the full ghost-inclusive extent of the other dims
+ * (couplb_streaming.h:281-293): calls fn(src, dst) for every node of plane
+ * s -> plane t along dim d. */
+#define FACE_LOOP(g, d, s, t, BODY)                                            \
+  do {                                                                         \
+    if ((d) == 0) { for (int k_ = 0; k_ < (g)->gz; k_++) for (int j_ = 0; j_ < (g)->gy; j_++) { \
+        const int sn = gidx(g, s, j_, k_), dn = gidx(g, t, j_, k_); BODY; } } \
+    else if ((d) == 1) { for (int k_ = 0; k_ < (g)->gz; k_++) for (int i_ = 0; i_ < (g)->gx; i_++) { \
+        const int sn = gidx(g, i_, s, k_), dn = gidx(g, i_, t, k_); BODY; } } \
+    else { for (int j_ = 0; j_ < (g)->gy; j_++) for (int i_ = 0; i_ < (g)->gx; i_++) { \
+        const int sn = gidx(g, i_, j_, s), dn = gidx(g, i_, j_, t); BODY; } } \
+  } while (0)
+
+static int dim_ext(const orc_grid* g, int d) {
+  return d == 0 ? g->gx : d == 1 ? g->gy : g->gz;
+}
+
+/* Streaming::exchange with one rank (couplb_streaming.h:136-139, 176-194):
+ * ghost_lo <- interior hi face, ghost_hi <- interior lo face, unless the
+ * ghost face is all wall. */
+static void exchange_f(orc_grid* g) {
+  const int nd = (g->D == 3) ? 3 : 2;
+  for (int d = 0; d < nd; d++) {
+    const int ds = dim_ext(g, d), lf = 1, hf = ds - 2, gl = 0, gh = ds - 1;
+    if (!g->wall_face[d][0])
+      FACE_LOOP(g, d, hf, gl, for (int q = 0; q < g->Q; q++) FI(g, q, dn) = FI(g, q, sn));
+    if (!g->wall_face[d][1])
+      FACE_LOOP(g, d, lf, gh, for (int q = 0; q < g->Q; q++) FI(g, q, dn) = FI(g, q, sn));
+  }
+}
+
+/* Streaming::exchange_velocity with one rank (couplb_streaming.h:140-143,
+ * 196-214). */
+void ORC_FN(grid_exchange_velocity)(void* gp) {
+  orc_grid* g = (orc_grid*)gp;
+  const int nd = (g->D == 3) ? 3 : 2;
+  for (int d = 0; d < nd; d++) {
+    const int ds = dim_ext(g, d), lf = 1, hf = ds - 2, gl = 0, gh = ds - 1;
+    if (!g->wall_face[d][0])
+      FACE_LOOP(g, d, hf, gl, { g->rho[dn] = g->rho[sn]; g->ux[dn] = g->ux[sn];
+                                g->uy[dn] = g->uy[sn]; g->uz[dn] = g->uz[sn]; });
+    if (!g->wall_face[d][1])
+      FACE_LOOP(g, d, lf, gh, { g->rho[dn] = g->rho[sn]; g->ux[dn] = g->ux[sn];
+                                g->uy[dn] = g->uy[sn]; g->uz[dn] = g->uz[sn]; });
+  }
+}
+
+/* Streaming::exchange_forces with one rank (couplb_streaming.h:155-158,
+ * 217-245): ghost_lo forces are added onto the interior hi face and ghost_hi
+ * onto the interior lo face, x then y then z. */
+static void exchange_forces(orc_grid* g) {
+  const int nd = (g->D == 3) ? 3 : 2;
+  for (int d = 0; d < nd; d++) {
+    const int ds = dim_ext(g, d), lf = 1, hf = ds - 2, gl = 0, gh = ds - 1;
+    FACE_LOOP(g, d, gl, hf, { g->fx[dn] += g->fx[sn]; g->fy[dn] += g->fy[sn];
+                              g->fz[dn] += g->fz[sn]; });
+    FACE_LOOP(g, d, gh, lf, { g->fx[dn] += g->fx[sn]; g->fy[dn] += g->fy[sn];
+                              g->fz[dn] += g->fz[sn]; });
+  }
+}
+
+/* Streaming::stream (couplb_streaming.h:82-134): pull from x - e_q with the
+ * rule of the source node's type, then swap f and f_buf. */
+static void stream(orc_grid* g) {
+  const double a = RHO_CLAMP_FRAC * g->rho0;
+  const double rho_floor = (a < RHO_MIN) ? RHO_MIN : a;     /* std::max */
+  const int klo = (g->D == 3) ? 1 : 0, khi = (g->D == 3) ? g->gz - 2 : 0;
+  const int Q = g->Q;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int k = klo; k <= khi; k++)
+    for (int j = 1; j <= g->gy - 2; j++)
+      for (int i = 1; i <= g->gx - 2; i++) {
+        const int n = gidx(g, i, j, k);
+        if (g->type[n] != 0) continue;
+        for (int q = 0; q < Q; q++) {
+          const int si = i - g->e[q][0], sj = j - g->e[q][1], sk = k - g->e[q][2];
+          if (si < 0 || si >= g->gx || sj < 0 || sj >= g->gy ||
+              (g->D == 3 && (sk < 0 || sk >= g->gz))) {
+            FB(g, q, n) = FI(g, q, n);
+            continue;
+          }
+          const int sn = gidx(g, si, sj, sk);
+          const int st = g->type[sn];
+          if (st == 0) {
+            FB(g, q, n) = FI(g, q, sn);
+          } else if (st == 1) {
+            FB(g, q, n) = FI(g, g->opp[q], n);
+          } else if (st == 2) {
+            const int qo = g->opp[q];
+            const double eu = g->e[q][0]*g->bc_ux[sn] + g->e[q][1]*g->bc_uy[sn]
+                            + g->e[q][2]*g->bc_uz[sn];
+            const double rn = g->rho[n];
+            const double rw = (rn < rho_floor) ? rho_floor : rn;   /* std::max */
+            FB(g, q, n) = FI(g, qo, n) + 2.0*g->w[qo]*rw*eu/CS2;
+          } else if (st == 3) {
+            FB(g, q, n) = FI(g, g->refl[g->wall_dim[sn] * Q + q], n);
+          } else if (st == 4) {
+            FB(g, q, n) = FI(g, q, n);
+          }
+        }
+      }
+  double* t = g->f; g->f = g->f_buf; g->f_buf = t;
+}
+
+/* FixCoupLB::enforce_wall_ghost_fields (fix_couplb.cpp:800-809), rho_lb = 1 */
+static void enforce_wall_ghost_fields(orc_grid* g) {
+  for (int n = 0; n < g->ntotal; n++) {
+    if (g->type[n] == 1) { g->rho[n] = 1.0; g->ux[n] = g->uy[n] = g->uz[n] = 0; }
+    else if (g->type[n] == 2) { g->rho[n] = 1.0; g->ux[n] = g->bc_ux[n];
+                                g->uy[n] = g->bc_uy[n]; g->uz[n] = g->bc_uz[n]; }
+    else if (g->type[n] == 3) { g->rho[n] = 1.0; g->ux[n] = g->uy[n] = g->uz[n] = 0; }
+  }
+}
+
+/* Grid::clear_forces (couplb_lattice.h:243-247) */
+static void clear_forces(orc_grid* g) {
+  memset(g->fx, 0, sizeof(double) * g->ntotal);
+  memset(g->fy, 0, sizeof(double) * g->ntotal);
+  memset(g->fz, 0, sizeof(double) * g->ntotal);
+}
+
+/* The grid part of FixCoupLB::apply_external_force (fix_couplb.cpp:693-707):
+ * g_lb already in lattice units; skipped when every |g| < ZERO_TOL.  It reads
+ * rho[] as left by the last compute_macroscopic. */
+static void apply_external_force(orc_grid* g, const double* gl) {
+  if (!gl) return;
+  if (fabs(gl[0]) < ZERO_TOL && fabs(gl[1]) < ZERO_TOL && fabs(gl[2]) < ZERO_TOL)
+    return;
+  const int klo = (g->D == 3) ? 1 : 0, khi = (g->D == 3) ? g->gz - 2 : 0;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int k = klo; k <= khi; k++)
+    for (int j = 1; j <= g->gy - 2; j++)
+      for (int i = 1; i <= g->gx - 2; i++) {
+        const int n = gidx(g, i, j, k);
+        if (g->type[n] != 0) continue;
+        g->fx[n] += gl[0] * g->rho[n];
+        g->fy[n] += gl[1] * g->rho[n];
+        g->fz[n] += gl[2] * g->rho[n];
+      }
+}
+
+/* FixCoupLB::do_lbm_step (fix_couplb.cpp:659-669) */
+void ORC_FN(grid_lbm_step)(void* gp, const double* g_lb) {
+  orc_grid* g = (orc_grid*)gp;
+  apply_external_force(g, g_lb);
+  ORC_FN(grid_macroscopic)(g, 1);
+  collide(g);
+  exchange_f(g);
+  stream(g);
+  enforce_wall_ghost_fields(g);
+  clear_forces(g);
+}
+
+void ORC_FN(grid_set_f)(void* gp, const double* f) {
+  orc_grid* g = (orc_grid*)gp;
+  const size_t QG = (size_t)g->Q * g->ntotal;
+  memcpy(g->f, f, QG * sizeof(double));
+  memcpy(g->f_buf, f, QG * sizeof(double));      /* couplb_io.h:814 */
+  ORC_FN(grid_macroscopic)(g, 0);                /* couplb_io.h:817 */
+}
+
+void ORC_FN(grid_get_f)(void* gp, double* f) {
+  orc_grid* g = (orc_grid*)gp;
+  memcpy(f, g->f, sizeof(double) * (size_t)g->Q * g->ntotal);
+}
+
+void ORC_FN(grid_get_macro)(void* gp, double* rho, double* ux, double* uy,
+                            double* uz) {
+  orc_grid* g = (orc_grid*)gp;
+  const size_t b = sizeof(double) * g->ntotal;
+  if (rho) memcpy(rho, g->rho, b);
+  if (ux) memcpy(ux, g->ux, b);
+  if (uy) memcpy(uy, g->uy, b);
+  if (uz) memcpy(uz, g->uz, b);
+}
+
+void ORC_FN(grid_set_force)(void* gp, const double* fx, const double* fy,
+                            const double* fz) {
+  orc_grid* g = (orc_grid*)gp;
+  const size_t b = sizeof(double) * g->ntotal;
+  memcpy(g->fx, fx, b); memcpy(g->fy, fy, b); memcpy(g->fz, fz, b);
+}
+
+void ORC_FN(grid_get_force)(void* gp, double* fx, double* fy, double* fz) {
+  orc_grid* g = (orc_grid*)gp;
+  const size_t b = sizeof(double) * g->ntotal;
+  memcpy(fx, g->fx, b); memcpy(fy, g->fy, b); memcpy(fz, g->fz, b);
+}
+
+/* Grid::max_velocity + compute_diagnostics + rho_clamp_count
+ * (couplb_lattice.h:203-242, 100) */
+void ORC_FN(grid_diagnostics)(void* gp, double out[5], int* clamps) {
+  orc_grid* g = (orc_grid*)gp;
+  const int klo = (g->D == 3) ? 1 : 0, khi = (g->D == 3) ? g->gz - 2 : 0;
+  double umax2 = 0.0, mass = 0.0, px = 0.0, py = 0.0, pz = 0.0;
+  for (int k = klo; k <= khi; k++)
+    for (int j = 1; j <= g->gy - 2; j++)
+      for (int i = 1; i <= g->gx - 2; i++) {
+        const int n = gidx(g, i, j, k);
+        if (g->type[n] != 0) continue;
+        const double u2 = g->ux[n]*g->ux[n] + g->uy[n]*g->uy[n] + g->uz[n]*g->uz[n];
+        if (u2 > umax2) umax2 = u2;
+        mass += g->rho[n];
+        px += g->rho[n] * g->ux[n];
+        py += g->rho[n] * g->uy[n];
+        pz += g->rho[n] * g->uz[n];
+      }
+  out[0] = sqrt(umax2); out[1] = mass; out[2] = px; out[3] = py; out[4] = pz;
+  if (clamps) *clamps = g->rho_clamp_count;
+}
+
+/* ---- IBM (couplb_ibm.h) --------------------------------------------- */
+
+/* delta_roma (couplb_ibm.h:11-22) */
+static double delta_roma(double r) {
+  const double ar = fabs(r);
+  if (ar <= 0.5) {
+    const double a = 1.0 - 3.0*r*r;
+    return (1.0 + sqrt(a > 0.0 ? a : 0.0)) / 3.0;
+  }
+  if (ar <= 1.5) {
+    const double a = -2.0 + 6.0*ar - 3.0*r*r;
+    return (5.0 - 3.0*ar - sqrt(a > 0.0 ? a : 0.0)) / 6.0;
+  }
+  return 0.0;
+}
+
+/* delta_peskin4 (couplb_ibm.h:24-35) */
+static double delta_peskin4(double r) {
+  const double ar = fabs(r);
+  if (ar <= 1.0) {
+    const double a = 1.0 + 4.0*ar - 4.0*ar*ar;
+    return (3.0 - 2.0*ar + sqrt(a > 0.0 ? a : 0.0)) / 8.0;
+  }
+  if (ar <= 2.0) {
+    const double a = -7.0 + 12.0*ar - 4.0*ar*ar;
+    return (5.0 - 2.0*ar - sqrt(a > 0.0 ? a : 0.0)) / 8.0;
+  }
+  return 0.0;
+}
+
+/* IBM::delta_product (couplb_ibm.h:42-45) */
+static double delta_product(const orc_grid* g, int kern, double rx, double ry,
+                            double rz) {
+  double (*d)(double) = (kern == COUPLB_DELTA_ROMA) ? delta_roma : delta_peskin4;
+  return d(rx) * d(ry) * ((g->D == 3) ? d(rz) : 1.0);
+}
+
+/* IBM::phys_to_local (couplb_ibm.h:49-55) */
+static void phys_to_local(const orc_grid* g, const couplb_ibm_params* ip,
+                          double inv_dx, double xp, double yp, double zp,
+                          double* lx, double* ly, double* lz) {
+  *lx = (xp - ip->domain_lo[0]) * inv_dx - ip->offset[0] + 1.0;
+  *ly = (yp - ip->domain_lo[1]) * inv_dx - ip->offset[1] + 1.0;
+  *lz = (g->D == 3) ? ((zp - ip->domain_lo[2]) * inv_dx - ip->offset[2] + 1.0) : 0.0;
+}
+
+/* IBM::interpolate (couplb_ibm.h:57-90) */
+static void interpolate(const orc_grid* g, const couplb_ibm_params* ip,
+                        double inv_dx, double xp, double yp, double zp,
+                        double out[3]) {
+  double lx, ly, lz;
+  phys_to_local(g, ip, inv_dx, xp, yp, zp, &lx, &ly, &lz);
+  const int i0 = (int)floor(lx), j0 = (int)floor(ly);
+  const int k0 = (g->D == 3) ? (int)floor(lz) : 0;
+  double ui = 0, vi = 0, wi = 0, ws = 0;
+  for (int k = (g->D == 3 ? k0 - 1 : 0); k <= (g->D == 3 ? k0 + 2 : 0); k++) {
+    if (g->D == 3 && (k < 0 || k >= g->gz)) continue;
+    for (int j = j0 - 1; j <= j0 + 2; j++) {
+      if (j < 0 || j >= g->gy) continue;
+      for (int i = i0 - 1; i <= i0 + 2; i++) {
+        if (i < 0 || i >= g->gx) continue;
+        const int n = gidx(g, i, j, k);
+        const int nt = g->type[n];
+        const double d = delta_product(g, ip->delta, lx - i, ly - j, lz - k);
+        if (nt == 0) { ui += g->ux[n]*d; vi += g->uy[n]*d; wi += g->uz[n]*d; ws += d; }
+        else if (nt == 1) { ws += d; }
+        else if (nt == 2) { ui += g->bc_ux[n]*d; vi += g->bc_uy[n]*d; wi += g->bc_uz[n]*d; ws += d; }
+        else if (nt == 3) { ws += d; }
+      }
+    }
+  }
+  if (ws > DELTA_TOL) {
+    const double iw = 1.0 / ws;
+    out[0] = ui*iw; out[1] = vi*iw; out[2] = wi*iw;
+  } else {
+    out[0] = out[1] = out[2] = 0.0;
+  }
+}
+
+/* IBM::spread (couplb_ibm.h:92-133) */
+static void spread(orc_grid* g, const couplb_ibm_params* ip, double inv_dx,
+                   double xp, double yp, double zp, double fxl, double fyl,
+                   double fzl, double dvl) {
+  double lx, ly, lz;
+  phys_to_local(g, ip, inv_dx, xp, yp, zp, &lx, &ly, &lz);
+  const int i0 = (int)floor(lx), j0 = (int)floor(ly);
+  const int k0 = (g->D == 3) ? (int)floor(lz) : 0;
+  const double dxp = ip->dx;
+  const double cell_vol = dxp * dxp * ((g->D == 3) ? dxp : 1.0);
+  const double dvr = dvl / cell_vol;
+  double ws = 0.0, dcache[64];
+  int ncache[64], nc = 0;
+  for (int k = (g->D == 3 ? k0 - 1 : 0); k <= (g->D == 3 ? k0 + 2 : 0); k++) {
+    if (g->D == 3 && (k < 0 || k >= g->gz)) continue;
+    for (int j = j0 - 1; j <= j0 + 2; j++) {
+      if (j < 0 || j >= g->gy) continue;
+      for (int i = i0 - 1; i <= i0 + 2; i++) {
+        if (i < 0 || i >= g->gx) continue;
+        const int n = gidx(g, i, j, k);
+        if (g->type[n] != 0) continue;
+        const double d = delta_product(g, ip->delta, lx - i, ly - j, lz - k);
+        dcache[nc] = d; ncache[nc] = n; nc++;
+        ws += d;
+      }
+    }
+  }
+  if (ws < DELTA_TOL) return;
+  const double sc = dvr / ws;
+  for (int c = 0; c < nc; c++) {
+    const double w = dcache[c] * sc;
+    g->fx[ncache[c]] += fxl * w;
+    g->fy[ncache[c]] += fyl * w;
+    g->fz[ncache[c]] += fzl * w;
+  }
+}
+
+/* The per-atom part of FixCoupLB::do_ibm_sub_coupling (fix_couplb.cpp:
+ * 755-797).  refresh: macroscopic(false) + exchange_velocity (:757-760);
+ * fold: exchange_forces (:795-797).  Returns the number of coupled atoms. */
+int ORC_FN(grid_ibm_substep)(void* gp, const couplb_ibm_params* ip, int n,
+                             const double* x, const double* v,
+                             const double* mass, const int* active,
+                             double* f_add, int refresh, int fold) {
+  orc_grid* g = (orc_grid*)gp;
+  if (refresh) {
+    ORC_FN(grid_macroscopic)(g, 0);
+    ORC_FN(grid_exchange_velocity)(g);
+  }
+  const double inv_dx = 1.0 / ip->dx;
+  const double xi_over_dtLBM = ip->xi_ibm / ip->dt_lbm;
+  const double inv_N = 1.0 / (double)ip->md_per_lb;
+  const double dv = (g->D == 3) ? (ip->dx * ip->dx * ip->dx) : (ip->dx * ip->dx);
+  const double vs = ip->vel_scale, fs = ip->force_scale;
+  int nc = 0;
+  for (int a = 0; a < n; a++) {
+    if (active && !active[a]) continue;
+    nc++;
+    double uf[3];
+    interpolate(g, ip, inv_dx, x[3*a], x[3*a+1], x[3*a+2], uf);
+    const double m = mass[a];
+    const double fxi = m * xi_over_dtLBM * (uf[0]*vs - v[3*a]);
+    const double fyi = m * xi_over_dtLBM * (uf[1]*vs - v[3*a+1]);
+    const double fzi = m * xi_over_dtLBM * (uf[2]*vs - v[3*a+2]);
+    f_add[3*a] += fxi; f_add[3*a+1] += fyi; f_add[3*a+2] += fzi;
+    spread(g, ip, inv_dx, x[3*a], x[3*a+1], x[3*a+2],
+           -fxi * inv_N / fs, -fyi * inv_N / fs, -fzi * inv_N / fs, dv);
+  }
+  if (fold) exchange_forces(g);
+  return nc;
+}
+
+/* Streaming::exchange_forces as an entry point for the fix layer. */
+void ORC_FN(grid_fold_forces)(void* gp) { exchange_forces((orc_grid*)gp); }
+
+#include "oracle_fix.inc"

@@ -1,0 +1,103 @@
+"""GPU immersed-boundary sub-step against the oracle and golden vectors.
+
+Tolerances (north star): per-atom IBM forces within 1e-11 relative, Eulerian
+force field within 1e-12 relative, FP64.  The FP32 path is bounded loosely.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import cases
+from couplb_b200.lattice import Lattice
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def golden(name):
+    return dict(np.load(os.path.join(GOLDEN, f"ibm_{name}.npz")))
+
+
+@pytest.mark.parametrize("name", sorted(cases.IBM_CASES))
+def test_fp64_forces_match_reference(cuda_lib, name):
+    out = cases.run_ibm_case_gpu(cases.IBM_CASES[name], "fp64")
+    ref = golden(name)
+    assert rel(out["fatom"], ref["fatom"]) <= 1e-11, rel(out["fatom"], ref["fatom"])
+    for k in ("fx", "fy", "fz"):
+        assert rel(out[k], ref[k]) <= 1e-12, (k, rel(out[k], ref[k]))
+
+
+@pytest.mark.parametrize("name", sorted(cases.IBM_CASES))
+def test_fp32_forces_close(cuda_lib, name):
+    out = cases.run_ibm_case_gpu(cases.IBM_CASES[name], "fp32")
+    ref = golden(name)
+    assert rel(out["fatom"], ref["fatom"]) <= 1e-5
+    for k in ("fx", "fy", "fz"):
+        assert rel(out[k], ref[k]) <= 1e-5
+
+
+def test_device_arrays_match_host_arrays(cuda_lib):
+    import torch
+    case = cases.IBM_CASES["d3_peskin_periodic"]
+    x, v, m, active, _ = cases.ibm_atoms(case)
+    res = []
+    for dev in (False, True):
+        L = Lattice(3, *case["n"], tau=case["tau"])
+        L.set_populations(cases.initial_populations(3, case["n"], case["seed"]))
+        L.set_ibm_params(delta="peskin4", md_per_lb=2, xi_ibm=0.7)
+        if dev:
+            t = {k: torch.from_numpy(a).cuda() for k, a in dict(x=x, v=v, m=m).items()}
+            ta = torch.from_numpy(active).cuda()
+            tf = torch.zeros((x.shape[0], 3), dtype=torch.float64, device="cuda")
+            torch.cuda.synchronize()
+            L.ibm_substep_device(x.shape[0], t["x"].data_ptr(), t["v"].data_ptr(), t["m"].data_ptr(),
+                                 tf.data_ptr(), ta.data_ptr(), refresh=True)
+            L.synchronize()
+            fa = tf.cpu().numpy()
+        else:
+            fa = np.zeros_like(x)
+            L.ibm_substep(x, v, m, fa, active=active, refresh=True)
+        res.append((fa, L.get_force_field()))
+        L.close()
+    assert rel(res[1][0], res[0][0]) <= 1e-14
+    for a, b in zip(res[1][1], res[0][1]):
+        assert rel(a, b) <= 1e-12
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("fp32", 2e-5)])
+def test_momentum_conservation_per_lb_interval(cuda_lib, prec, tol):
+    """Periodic box, markers coupled with md_per_lb sub-steps: over one LB
+    interval the fluid gains exactly the momentum the markers lose,
+    dP_fluid = -(1/N) sum_sub sum_i F_i (docs/theory.md:44-60)."""
+    n = (40, 36, 32)
+    rng = np.random.default_rng(3)
+    na, N = 400, 4
+    L = Lattice(3, *n, tau=0.8, precision=prec)
+    L.set_populations(cases.initial_populations(3, n, 8))
+    L.set_ibm_params(delta="peskin4", md_per_lb=N, xi_ibm=1.0, dt_lbm=1.0)
+    x = rng.uniform(0, 1, (na, 3)) * np.array(n)
+    v = 0.01 * rng.standard_normal((na, 3))
+    m = np.ones(na)
+    for cycle in range(3):
+        L.lbm_step()
+        L.macroscopic()
+        p0 = np.array(L.diagnostics().mom)
+        fsum = np.zeros(3)
+        for s in range(N):
+            fa = np.zeros((na, 3))
+            L.ibm_substep(np.ascontiguousarray(x + 0.01 * s), v, m, fa, refresh=(s == 0))
+            fsum += fa.sum(0)
+        L.lbm_step()
+        L.macroscopic()
+        p1 = np.array(L.diagnostics().mom)
+        dp = p1 - p0
+        expect = -fsum / N
+        assert np.abs(dp - expect).max() <= tol * np.abs(expect).max() + 1e-14, (cycle, dp, expect)
+        # the FP64 device accumulator of the spread force agrees as well
+        tot = L.ibm_total_force(reset=True)
+        assert np.abs(tot - expect).max() <= 1e-12 * np.abs(expect).max()

@@ -1,0 +1,133 @@
+"""GPU lattice kernels against the CPU oracle and the reference's golden vectors.
+
+Tolerances (north star): the FP64 GPU path matches the oracle's fields within
+1e-12 relative (max |a-b| / max |b| over the field); the FP32-shifted path is
+checked by its relative L2 velocity error against FP64; FP16 storage is
+reported with a loose bound.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import cases
+from couplb_b200.lattice import Lattice
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+TOL_FP64 = 1e-12
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def l2(a, b):
+    return np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-300))
+
+
+def golden(prefix, name):
+    return dict(np.load(os.path.join(GOLDEN, f"{prefix}_{name}.npz")))
+
+
+@pytest.mark.parametrize("name", sorted(cases.LB_CASES))
+def test_fp64_matches_reference_golden(cuda_lib, name):
+    out = cases.run_lb_case_gpu(cases.LB_CASES[name], "fp64")
+    ref = golden("lb", name)
+    for k in ref:
+        assert rel(out[k], ref[k]) <= TOL_FP64, (k, rel(out[k], ref[k]))
+
+
+@pytest.mark.parametrize("name", ["d3q19_mixed", "d2q9_mixed"])
+def test_fp64_matches_port_oracle(cuda_lib, name):
+    case = cases.LB_CASES[name]
+    out = cases.run_lb_case_gpu(case, "fp64")
+    ref = cases.run_lb_case_oracle(case, "port")
+    for k in ref:
+        assert rel(out[k], ref[k]) <= TOL_FP64, (k, rel(out[k], ref[k]))
+
+
+@pytest.mark.parametrize("prec,tol_f,tol_u", [("fp32", 1e-6, 1e-5), ("fp16", 2e-3, 5e-2)])
+@pytest.mark.parametrize("name", sorted(cases.LB_CASES))
+def test_reduced_precision_close_to_fp64(cuda_lib, name, prec, tol_f, tol_u):
+    out = cases.run_lb_case_gpu(cases.LB_CASES[name], prec)
+    ref = golden("lb", name)
+    assert rel(out["f"], ref["f"]) <= tol_f
+    u = np.stack([out["ux"], out["uy"], out["uz"]])
+    ur = np.stack([ref["ux"], ref["uy"], ref["uz"]])
+    assert l2(u, ur) <= tol_u, l2(u, ur)
+
+
+def test_init_equilibrium_matches_reference_feq(cuda_lib):
+    from oracle.bindings import OracleGrid
+    G = OracleGrid(3, 6, 5, 4, tau=0.8, wall=(0, 0, 1, 1, 0, 0))
+    G.init_equilibrium(1.02, 0.01, -0.02, 0.005)
+    L = Lattice(3, 6, 5, 4, tau=0.8, wall=(0, 0, 1, 1, 0, 0))
+    L.init_equilibrium(1.02, 0.01, -0.02, 0.005)
+    a = cases.interior(L.get_populations(), 3)
+    b = cases.interior(G.get_f(), 3)
+    assert rel(a, b) <= 1e-15
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 0.0), ("fp32", 1e-7), ("fp16", 2e-4)])
+def test_population_round_trip(cuda_lib, prec, tol):
+    f0 = cases.initial_populations(3, (7, 5, 6), 7)
+    L = Lattice(3, 7, 5, 6, tau=0.7, precision=prec)
+    L.set_populations(f0)
+    f1 = L.get_populations()
+    assert np.abs(cases.interior(f1, 3) - cases.interior(f0, 3)).max() <= tol
+
+
+def test_larger_grid_matches_oracle(cuda_lib):
+    """64x32x24 channel with moving and free-slip walls, 15 steps, FP64."""
+    case = dict(dim=3, n=(64, 32, 24), tau=0.62, wall=(0, 0, 2, 1, 3, 3), wall_vel=(0.03, 0, 0),
+                gravity=(2e-6, 0, 0), steps=15, seed=5, noise=1.0, force=True, refresh_every=6)
+    out = cases.run_lb_case_gpu(case, "fp64")
+    ref = cases.run_lb_case_oracle(case, "port")
+    for k in ref:
+        assert rel(out[k], ref[k]) <= TOL_FP64, (k, rel(out[k], ref[k]))
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-13), ("fp32", 1e-9)])
+def test_mass_conservation_periodic(cuda_lib, prec, tol):
+    """Fully periodic box without forcing: sum rho is invariant (FP64 sums)."""
+    L = Lattice(3, 96, 64, 48, tau=0.7, precision=prec)
+    L.set_populations(cases.initial_populations(3, (96, 64, 48), 9))
+    m0 = L.diagnostics().mass
+    for _ in range(50):
+        L.lbm_step()
+    L.macroscopic()
+    m1 = L.diagnostics().mass
+    assert abs(m1 - m0) / m0 <= tol, (m0, m1)
+
+
+def test_momentum_gain_equals_body_force(cuda_lib):
+    """Periodic box with gravity: each LB step adds g * sum(rho_prev) of momentum
+    (Guo forcing, fix_couplb.cpp:706 and couplb_collision.h:55)."""
+    n = (32, 24, 16)
+    g = (3e-6, -1e-6, 2e-6)
+    L = Lattice(3, *n, tau=0.8, body_force=True)
+    L.set_populations(cases.initial_populations(3, n, 4))
+    L.macroscopic()
+    d0 = L.diagnostics()
+    p0 = np.array(d0.mom)
+    L.lbm_step(g)
+    L.macroscopic()
+    d1 = L.diagnostics()
+    dp = np.array(d1.mom) - p0
+    np.testing.assert_allclose(dp, np.array(g) * d0.mass, rtol=1e-9)
+
+
+def test_nonfinite_density_is_reported_not_trapped(cuda_lib):
+    """A NaN population: the kernel clamps the density like the reference
+    (couplb_lattice.h:178-186) and counts it in the status word."""
+    f0 = cases.initial_populations(3, (8, 6, 5), 3)
+    f0[4, 3, 3, 3] = np.nan
+    L = Lattice(3, 8, 6, 5, tau=0.8)
+    L.set_populations(f0)
+    L.lbm_step()
+    clamps, nonfinite = L.read_status(reset=True)
+    assert clamps >= 1 and nonfinite >= 1
+    L.set_populations(cases.initial_populations(3, (8, 6, 5), 3))
+    L.lbm_step()
+    assert L.read_status() == (0, 0)

@@ -1,0 +1,79 @@
+"""`fix couplb` argument parsing (fix_couplb.cpp:71-238): values, defaults and
+the reference's error messages.  Host-only: needs no GPU."""
+import pytest
+
+from couplb_b200 import abi
+from couplb_b200.fix import parse_args
+from couplb_b200.lib import CoupLBError
+
+
+def P(cmd, dim=3):
+    return parse_args(cmd.split(), dimension=dim)
+
+
+def test_defaults(cuda_lib):
+    c = P("f all couplb 8 32 4 0.1 1.0")
+    assert (c.Nx, c.Ny, c.Nz, c.nu, c.rho) == (8, 32, 4, 0.1, 1.0)
+    assert c.md_per_lb == 1 and c.xi_ibm == 1.0 and c.delta == abi.DELTA_ROMA
+    assert list(c.wall) == [0] * 6 and list(c.gstyle) == [0, 0, 0]
+    assert c.output_file == b"couplb_profile.dat" and c.checkpoint_prefix == b"couplb_ckpt"
+    assert c.precision == abi.FP64
+
+
+def test_all_keywords(cuda_lib):
+    c = P("f all couplb 64 48 32 0.1 1.26 md_per_lb 10 xi_ibm 0.1 wall_y 1 1 wall_z 2 3 "
+          "wall_vel 0.1 0 0 gravity v_Gx 0.0 -2e-3 kernel peskin4 vtk 5000 flow_vtk "
+          "vtk_region 0 10 0 5 0 3 vtk_solid x v checkpoint 10000 ckpt/fluid check_every 1000 "
+          "output 100 prof.dat restart old precision fp32")
+    assert c.md_per_lb == 10 and c.xi_ibm == 0.1
+    assert list(c.wall) == [0, 0, 1, 1, 2, 3]
+    assert list(c.wall_vel) == [0.1, 0, 0]
+    assert list(c.gstyle) == [abi.G_EQUAL, abi.G_CONSTANT, abi.G_CONSTANT]
+    assert c.gvar[0].value == b"Gx" and c.gconst[2] == -2e-3
+    assert c.delta == abi.DELTA_PESKIN4
+    assert c.vtk_every == 5000 and c.vtk_prefix == b"flow_vtk"
+    assert c.has_vtk_region == 1 and c.vtk_region_n == 6 and list(c.vtk_rhi) == [10, 5, 3]
+    assert c.vtk_solid_nattr == 2
+    assert c.checkpoint_every == 10000 and c.checkpoint_prefix == b"ckpt/fluid"
+    assert c.check_every == 1000 and c.output_every == 100 and c.output_file == b"prof.dat"
+    assert c.do_restart == 1 and c.restart_prefix == b"old"
+    assert c.precision == abi.FP32_SHIFTED
+
+
+@pytest.mark.parametrize("cmd,dim,msg", [
+    ("f all couplb 8 32 1 0.1", 2, "Illegal fix couplb command: need Nx Ny Nz nu rho"),
+    ("f all couplb 0 32 1 0.1 1.0", 2, "fix couplb: Nx, Ny, and Nz must be positive"),
+    ("f all couplb 8 32 1 -0.1 1.0", 2, "fix couplb: viscosity must be positive and finite"),
+    ("f all couplb 8 32 1 0.1 0", 2, "fix couplb: density must be positive and finite"),
+    ("f all couplb 8 32 1 0.1 1.0 bogus 1", 2, "Unknown fix couplb keyword: bogus"),
+    ("f all couplb 8 32 1 0.1 1.0 md_per_lb 0", 2, "fix couplb: md_per_lb must be >= 1"),
+    ("f all couplb 8 32 1 0.1 1.0 md_per_lb", 2, "fix couplb md_per_lb: need 1 value"),
+    ("f all couplb 8 32 1 0.1 1.0 xi_ibm 5.0", 2, "fix couplb: xi_ibm must satisfy 0 < xi_ibm <= 1"),
+    ("f all couplb 8 32 1 0.1 1.0 gravity 1 2", 2, "fix couplb gravity: need 3 values"),
+    ("f all couplb 8 32 1 0.1 1.0 wall_y 1 5", 2, "fix couplb: wall_y types must be in [0,4]"),
+    ("f all couplb 8 32 1 0.1 1.0 wall_x 1", 2, "fix couplb wall_x: need 2 values"),
+    ("f all couplb 8 32 1 0.1 1.0 output -1 a", 2, "fix couplb: output frequency cannot be negative"),
+    ("f all couplb 8 32 1 0.1 1.0 check_every -2", 2, "fix couplb: check_every cannot be negative"),
+    ("f all couplb 8 32 1 0.1 1.0 kernel cubic", 2, "fix couplb kernel: use roma or peskin4"),
+    ("f all couplb 8 32 1 0.1 1.0 vtk_region 0 1 2", 2,
+     "fix couplb vtk_region: need 4 values (2D: xlo xhi ylo yhi) or 6 values (3D: xlo xhi ylo yhi zlo zhi)"),
+    ("f all couplb 8 32 1 0.1 1.0 vtk_solid", 2, "fix couplb vtk_solid: need at least one attribute"),
+    ("f all couplb 8 32 1 0.1 1.0 vtk_solid x vtk_solid v", 2,
+     "fix couplb vtk_solid: keyword specified more than once"),
+    ("f all couplb 8 32 1 0.1 1.0 checkpoint -5 p", 2, "fix couplb: checkpoint frequency cannot be negative"),
+    ("f all couplb 8 32 1 0.1 1.0 restart", 2, "fix couplb restart: need prefix"),
+    ("f all couplb 8 32 2 0.1 1.0", 2, "fix couplb: Nz must be 1 for 2D"),
+    ("f all couplb 8 32 2 0.1 1.0 precision fp8", 3, "fix couplb precision: use fp64, fp32 or fp16"),
+])
+def test_errors(cuda_lib, cmd, dim, msg):
+    with pytest.raises(CoupLBError) as e:
+        P(cmd, dim)
+    assert e.value.msg == msg
+    assert e.value.code == abi.ERR_PARSE
+
+
+def test_swimmer_deck_is_rejected_like_the_reference(cuda_lib):
+    """examples/swimming/in.swim:49 passes `xi_ibm 5.0`, which the reference
+    parser rejects (fix_couplb.cpp:119-120)."""
+    with pytest.raises(CoupLBError):
+        P("lb all couplb 64 64 1 0.1 1.0 xi_ibm 5.0", 2)
