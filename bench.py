@@ -45,6 +45,8 @@ def parse():
                     help="length of the FP32/FP16 vs FP64 accuracy runs (0 = skip)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU work of the timed CPU baseline sample")
+    ap.add_argument("--only", choices=["fp64", "fp32", "fp16"], default=None,
+                    help="time the fused kernel of one precision only (profiling runs)")
     ap.add_argument("--nx", type=int, default=NX)
     ap.add_argument("--ny", type=int, default=NY)
     ap.add_argument("--nz", type=int, default=NZ)
@@ -278,6 +280,17 @@ def main():
     N = nx * ny * nz
     f0 = initial_populations(nx, ny, nz)
     stream = torch.cuda.Stream()
+
+    if args.only:
+        L = make_lattice(args.only, nx, ny, nz, local)
+        L.set_stream(stream.cuda_stream)
+        L.set_populations(f0)
+        ms = time_lattice(L, args.steps, args.warmup, torch, stream)
+        print(json.dumps({"only": args.only, "ms_per_step": ms, "mlups": N / (ms * 1e-3) / 1e6,
+                          "gbs": BYTES_PER_LU[args.only] * N / (ms * 1e-3) / 1e9,
+                          "status": L.read_status()}), flush=True)
+        L.close()
+        return
 
     results = {}
     clocks = Clocks(local)

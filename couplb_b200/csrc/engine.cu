@@ -147,7 +147,9 @@ int materialize(couplb_handle* h) {
     using L = decltype(l);
     using S = decltype(s);
     using T = typename S::T;
-    k_materialize<L, S><<<grid, block, 0, h->stream>>>(g, (const T*)h->f[h->cur], (T*)h->f[1 - h->cur]);
+    k_materialize<L, S><<<grid, block, 0, h->stream>>>(g, (const T*)h->f[h->cur],
+                                                       (const typename S::A*)h->rho_field,
+                                                       (T*)h->f[1 - h->cur]);
   });
   CK_LAUNCH();
   h->cur = 1 - h->cur;
@@ -177,6 +179,7 @@ int engine_macro(couplb_handle* h) {
     MacroArgs<S> a;
     a.g = g;
     a.fin = (const T*)h->f[h->cur];
+    a.rho_field = (const A*)h->rho_field;
     a.rho = (A*)h->macro[0]; a.ux = (A*)h->macro[1]; a.uy = (A*)h->macro[2]; a.uz = (A*)h->macro[3];
     a.status = h->d_status;
     if (pull) k_macro<L, S, true><<<grid, block, 0, h->stream>>>(a);
@@ -250,7 +253,10 @@ int couplb_create(const couplb_lattice_params* p, couplb_handle** out) {
   int rc = COUPLB_OK;
   for (int b = 0; b < 2 && !rc; b++) rc = dalloc(h, &h->f[b], pb * Q * h->qs);
   for (int c = 0; c < 3 && !rc; c++) rc = dalloc(h, &h->F[c], ab * h->qs);
-  if (!rc && p->body_force) rc = dalloc(h, &h->rho_field, ab * h->qs);
+  h->moving_walls = false;
+  for (int f = 0; f < (p->dim == 3 ? 6 : 4); f++) h->moving_walls |= (p->wall[f] == 2);
+  if (!rc && (p->body_force || h->moving_walls)) rc = dalloc(h, &h->rho_field, ab * h->qs);
+  h->idx32 = ((unsigned long long)Q * h->qs < (1ULL << 32));
   if (!rc) rc = dalloc(h, (void**)&h->d_status, sizeof(int) * 8);
   if (!rc) rc = dalloc(h, (void**)&h->d_ftot, sizeof(double) * 4);
   if (!rc && cudaMallocHost(&h->h_small, 4096) != cudaSuccess)
@@ -415,12 +421,17 @@ int couplb_lbm_step(couplb_handle* h, const double* g_lb) {
     a.Fz = (const A*)h->F[2];
     a.rho_field = (A*)h->rho_field;
     a.rho_mode = rho_mode;
-    a.write_rho = h->p.body_force ? 1 : 0;
+    a.write_rho = h->p.body_force ? 2 : (h->moving_walls ? 1 : 0);
     for (int d = 0; d < 3; d++) a.grav[d] = g_active ? g_lb[d] : 0.0;
     a.omega = 1.0 / h->p.tau;
     a.status = h->d_status;
-    if (pull) k_stream_collide<L, S, true><<<grid, block, 0, h->stream>>>(a);
-    else k_stream_collide<L, S, false><<<grid, block, 0, h->stream>>>(a);
+    if (h->idx32) {
+      if (pull) k_stream_collide<L, S, unsigned, true><<<grid, block, 0, h->stream>>>(a);
+      else k_stream_collide<L, S, unsigned, false><<<grid, block, 0, h->stream>>>(a);
+    } else {
+      if (pull) k_stream_collide<L, S, size_t, true><<<grid, block, 0, h->stream>>>(a);
+      else k_stream_collide<L, S, size_t, false><<<grid, block, 0, h->stream>>>(a);
+    }
   });
   CK_LAUNCH();
   h->cur = 1 - h->cur;

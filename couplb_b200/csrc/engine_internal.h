@@ -20,7 +20,9 @@ struct couplb_handle {
   int poststream = 1;                // 1: f[cur] is post-stream S, 0: post-collision P
   void* F[3] = {nullptr, nullptr, nullptr};   // Eulerian force field
   int force_dirty = 0;               // F holds nonzero values
-  void* rho_field = nullptr;         // density read by the body force
+  void* rho_field = nullptr;         // density of the last fused launch (body force, moving walls)
+  bool moving_walls = false;         // a face of type 2
+  bool idx32 = true;                 // Q * qs fits 32-bit element indices
   int rho_state = 0;                 // couplb::RhoMode: what the next LB step reads
   void* macro[4] = {nullptr, nullptr, nullptr, nullptr};   // rho(dev), ux, uy, uz
   int macro_valid = 0;               // macro[] are the moments of the current state

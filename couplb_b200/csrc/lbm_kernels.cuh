@@ -70,21 +70,25 @@ __device__ __forceinline__ Cf clamp_rho(Cf r, int* status, int slot) {
   return r;
 }
 
-// Density of the receiving node that the moving-wall rule uses: in the
-// reference it is rho[n] of the last compute_macroscopic(true), i.e. the
-// density of the state this node collided from, which equals the sum of its
-// post-collision populations (BGK + Guo conserve mass).
-template <class L, class S>
-__device__ __forceinline__ typename S::C moving_wall_rho(const typename S::T* fin, long long qs,
-                                                         long long n, double rho0) {
+// Density the moving-wall rule uses for the receiving node n
+// (couplb_streaming.h:86,112-118): rho[n] of the last compute_macroscopic(true),
+// i.e. the clamped density the previous fused launch computed at n, which it
+// stored in the density field; floored at RHO_CLAMP_FRAC * rho0.
+template <class S>
+__device__ __forceinline__ typename S::C moving_wall_rho(const typename S::A* rho_field, size_t n,
+                                                         double rho0) {
   using C = typename S::C;
-  C s = C(0);
-#pragma unroll
-  for (int q = 0; q < L::Q; q++) s += S::ld(fin + q * qs + n);
-  C r = S::kShift ? C(rho0) + s : s;
-  if (r <= C(RHO_MIN) || !isfinite(r)) r = C(RHO_MIN);
+  const C r = S::kShift ? C(rho0) + C(rho_field[n]) : C(rho_field[n]);
   const C fl = C(RHO_CLAMP_FRAC * rho0 < RHO_MIN ? RHO_MIN : RHO_CLAMP_FRAC * rho0);
   return (r < fl) ? fl : r;
+}
+
+template <class L>
+__device__ __forceinline__ bool near_moving_wall(const Geom& g, int i, int j, int k) {
+  bool m = (g.face[0] == 2 && i == 0) || (g.face[1] == 2 && i == g.nx - 1) ||
+           (g.face[2] == 2 && j == 0) || (g.face[3] == 2 && j == g.ny - 1);
+  if (L::D == 3) m = m || (g.face[4] == 2 && k == 0) || (g.face[5] == 2 && k == g.nz - 1);
+  return m;
 }
 
 // Pull of all Q populations of node (i,j,k) with the reference's boundary
@@ -92,17 +96,15 @@ __device__ __forceinline__ typename S::C moving_wall_rho(const typename S::T* fi
 // is either interior, or on one or more ghost planes; on a ghost node the wall
 // set last (x, then y, then z: couplb_boundary.h, fix_couplb.cpp:529-531)
 // decides the rule, and a ghost node without wall is a periodic image.
-template <class L, class S>
+template <class L, class S, class I>
 __device__ __forceinline__ void pull_general(const Geom& g, const typename S::T* __restrict__ fin,
-                                             int i, int j, int k, long long n,
-                                             typename S::C (&f)[L::Q]) {
+                                             const typename S::A* __restrict__ rho_field, int i,
+                                             int j, int k, I n, typename S::C (&f)[L::Q]) {
   using C = typename S::C;
-  const long long sxy = (long long)g.nx * g.ny;
-  bool near_moving = (g.face[0] == 2 && i == 0) || (g.face[1] == 2 && i == g.nx - 1) ||
-                     (g.face[2] == 2 && j == 0) || (g.face[3] == 2 && j == g.ny - 1);
-  if (L::D == 3) near_moving |= (g.face[4] == 2 && k == 0) || (g.face[5] == 2 && k == g.nz - 1);
+  const I qs = (I)g.qs;
+  const I sx = (I)g.nx, sxy = (I)g.nx * (I)g.ny;
   C rw = C(0);
-  if (near_moving) rw = moving_wall_rho<L, S>(fin, g.qs, n, g.rho0);
+  if (near_moving_wall<L>(g, i, j, k)) rw = moving_wall_rho<S>(rho_field, n, g.rho0);
 #pragma unroll
   for (int q = 0; q < L::Q; q++) {
     const int ex = L::ex(q), ey = L::ey(q), ez = L::ez(q);
@@ -111,7 +113,7 @@ __device__ __forceinline__ void pull_general(const Geom& g, const typename S::T*
     const bool oy = sj < 0 || sj >= g.ny;
     const bool oz = (L::D == 3) && (sk < 0 || sk >= g.nz);
     if (!(ox || oy || oz)) {
-      f[q] = S::ld(fin + q * g.qs + (n - ex - (long long)ey * g.nx - (long long)ez * sxy));
+      f[q] = S::ld(fin + (q * qs + (I)(si + (I)sj * sx + (I)sk * sxy)));
       continue;
     }
     int t = 0, wd = 0;
@@ -122,35 +124,37 @@ __device__ __forceinline__ void pull_general(const Geom& g, const typename S::T*
       si = si < 0 ? si + g.nx : (si >= g.nx ? si - g.nx : si);
       sj = sj < 0 ? sj + g.ny : (sj >= g.ny ? sj - g.ny : sj);
       if (L::D == 3) sk = sk < 0 ? sk + g.nz : (sk >= g.nz ? sk - g.nz : sk);
-      f[q] = S::ld(fin + q * g.qs + (si + (long long)g.nx * sj + sxy * sk));
+      f[q] = S::ld(fin + (q * qs + (I)si + (I)sj * sx + (I)sk * sxy));
     } else if (t == 1) {
-      f[q] = S::ld(fin + L::opp(q) * g.qs + n);
+      f[q] = S::ld(fin + (L::opp(q) * qs + n));
     } else if (t == 2) {
       const C eu = C(ex * g.uw[0] + ey * g.uw[1] + ez * g.uw[2]);
-      f[q] = S::ld(fin + L::opp(q) * g.qs + n) + C(2.0 * L::w(L::opp(q)) * 3.0) * rw * eu;
+      f[q] = S::ld(fin + (L::opp(q) * qs + n)) + C(2.0 * L::w(L::opp(q)) * 3.0) * rw * eu;
     } else if (t == 3) {
       const int qr = wd == 0 ? L::refl(0, q) : (wd == 1 ? L::refl(1, q) : L::refl(2, q));
-      f[q] = S::ld(fin + qr * g.qs + n);
+      f[q] = S::ld(fin + (qr * qs + n));
     } else {
-      f[q] = S::ld(fin + q * g.qs + n);
+      f[q] = S::ld(fin + (q * qs + n));
     }
   }
 }
 
 // Pull for rows that touch no wall: only x can wrap, handled by selecting the
 // wrapped column; y/z offsets are constants of q.
-template <class L, class S>
+template <class L, class S, class I>
 __device__ __forceinline__ void pull_interior(const Geom& g, const typename S::T* __restrict__ fin,
                                               int i, int j, int k, typename S::C (&f)[L::Q]) {
-  const int im = (i == 0) ? g.nx - 1 : i - 1;
-  const int ip = (i == g.nx - 1) ? 0 : i + 1;
-  const long long row = (long long)g.nx * (j + (long long)g.ny * k);
-  const long long sxy = (long long)g.nx * g.ny;
+  const I qs = (I)g.qs;
+  const I sx = (I)g.nx, sxy = (I)g.nx * (I)g.ny;
+  const I row = (I)j * sx + (I)k * sxy;
+  const I im = (i == 0) ? g.nx - 1 : i - 1;
+  const I ip = (i == g.nx - 1) ? 0 : i + 1;
 #pragma unroll
   for (int q = 0; q < L::Q; q++) {
     const int ex = L::ex(q), ey = L::ey(q), ez = L::ez(q);
-    const int xs = ex == 1 ? im : (ex == -1 ? ip : i);
-    f[q] = S::ld(fin + q * g.qs + (row - (long long)ey * g.nx - (long long)ez * sxy + xs));
+    const I xs = ex == 1 ? im : (ex == -1 ? ip : (I)i);
+    const I ro = row - (I)(ey * g.nx) - (I)ez * sxy;   // unsigned wrap-around is exact
+    f[q] = S::ld(fin + (q * qs + ro + xs));
   }
 }
 
@@ -163,17 +167,18 @@ __device__ __forceinline__ bool row_is_interior(const Geom& g, int j, int k) {
   return yin && zin && g.face[0] == 0 && g.face[1] == 0;
 }
 
-template <class L, class S, bool kPull>
+template <class L, class S, class I, bool kPull>
 __device__ __forceinline__ void load_node(const Geom& g, const typename S::T* __restrict__ fin,
-                                          int i, int j, int k, long long n,
-                                          typename S::C (&f)[L::Q]) {
+                                          const typename S::A* __restrict__ rho_field, int i,
+                                          int j, int k, I n, typename S::C (&f)[L::Q]) {
   if (!kPull) {
+    const I qs = (I)g.qs;
 #pragma unroll
-    for (int q = 0; q < L::Q; q++) f[q] = S::ld(fin + q * g.qs + n);
+    for (int q = 0; q < L::Q; q++) f[q] = S::ld(fin + (q * qs + n));
   } else if (row_is_interior<L>(g, j, k)) {
-    pull_interior<L, S>(g, fin, i, j, k, f);
+    pull_interior<L, S, I>(g, fin, i, j, k, f);
   } else {
-    pull_general<L, S>(g, fin, i, j, k, n, f);
+    pull_general<L, S, I>(g, fin, rho_field, i, j, k, n, f);
   }
 }
 
@@ -191,20 +196,127 @@ __device__ __forceinline__ void moments(const C (&f)[L::Q], C& r, C& jx, C& jy, 
   }
 }
 
+// BGK + Guo collision of one node (couplb_collision.h:35-57) written over
+// the pairs (q, opp(q)) = (2p+1, 2p+2), e_{2p+2} = -e_{2p+1}: the even part
+// of the equilibrium and source is shared by the pair, the odd part flips sign.
+// 1/cs2 = 3, 1/cs4 = 9.  Produces the post-collision increment d_q:
+//   d_q = -omega (f_q - feq_q) + S_q.
+// r is rho (plain) or its deviation (shifted), rho the full density.
+template <class L, class C>
+__device__ __forceinline__ void collision_increment(const C (&f)[L::Q], C r, C rho, C ux, C uy,
+                                                    C uz, C Fx, C Fy, C Fz, C om, bool shifted,
+                                                    C (&d)[L::Q]) {
+  const C hom = C(1) - C(0.5) * om;
+  const C uu15 = C(1.5) * (ux * ux + uy * uy + uz * uz);
+  const C uf3 = C(3) * (ux * Fx + uy * Fy + uz * Fz);
+  {
+    const C w = C(L::w(0));
+    const C fe = shifted ? w * (r - rho * uu15) : w * rho * (C(1) - uu15);
+    d[0] = -om * (f[0] - fe) + w * hom * (-uf3);
+  }
+#pragma unroll
+  for (int q = 1; q < L::Q; q += 2) {
+    const C cx = C(L::ex(q)), cy = C(L::ey(q)), cz = C(L::ez(q));
+    const C w = C(L::w(q));
+    const C eu = cx * ux + cy * uy + cz * uz;
+    const C ef = cx * Fx + cy * Fy + cz * Fz;
+    const C even = C(4.5) * eu * eu - uu15;
+    const C odd = C(3) * eu;
+    C fp, fm;
+    if (shifted) {
+      const C a = r + rho * even, b = rho * odd;
+      fp = w * (a + b); fm = w * (a - b);
+    } else {
+      const C wr = w * rho;
+      fp = wr * (C(1) + even + odd); fm = wr * (C(1) + even - odd);
+    }
+    const C se = w * hom * (C(9) * eu * ef - uf3);
+    const C so = w * hom * (C(3) * ef);
+    d[q] = -om * (f[q] - fp) + (se + so);
+    d[q + 1] = -om * (f[q + 1] - fm) + (se - so);
+  }
+}
+
+// Exact conservation of the FP32 increment: in exact arithmetic the BGK + Guo
+// increment carries no mass and exactly the momentum F; FP32 rounding of the
+// equilibrium leaves residuals of ~1e-11 per node and step that do not
+// decorrelate from step to step in slowly varying flows and act as a spurious
+// body force.  The residuals are summed in FP64 and removed from the rest
+// population (mass) and from the three axis pairs (momentum), which leaves
+// the second-order moments untouched.
+//
+// The shifted (FP32-arithmetic) collision with the conservation correction of
+// conserve_fp32 folded in: increments are produced pair by pair, their FP64
+// mass / momentum residuals accumulated, the 12 (D3Q19) or 4 (D2Q9) diagonal
+// populations stored at once, and only the rest and axis increments kept for
+// the correction -- fewer live registers than holding all Q increments.
+template <class L, class S, class I>
+__device__ __forceinline__ void collide_store_conserved(const float (&f)[L::Q], float r, float rho,
+                                                        float ux, float uy, float uz, float Fx,
+                                                        float Fy, float Fz, float om,
+                                                        typename S::T* __restrict__ fout, I qs,
+                                                        I n) {
+  const float hom = 1.0f - 0.5f * om;
+  const float uu15 = 1.5f * (ux * ux + uy * uy + uz * uz);
+  const float uf3 = 3.0f * (ux * Fx + uy * Fy + uz * Fz);
+  double m = 0, px = -double(Fx), py = -double(Fy), pz = -double(Fz);
+  float d0, da[2 * L::D];
+  {
+    const float w = float(L::w(0));
+    d0 = -om * (f[0] - w * (r - rho * uu15)) + w * hom * (-uf3);
+    m += double(d0);
+  }
+#pragma unroll
+  for (int q = 1; q < L::Q; q += 2) {
+    const float cx = float(L::ex(q)), cy = float(L::ey(q)), cz = float(L::ez(q));
+    const float w = float(L::w(q));
+    const float eu = cx * ux + cy * uy + cz * uz;
+    const float ef = cx * Fx + cy * Fy + cz * Fz;
+    const float aa = r + rho * (4.5f * eu * eu - uu15), bb = rho * (3.0f * eu);
+    const float se = w * hom * (9.0f * eu * ef - uf3);
+    const float so = w * hom * (3.0f * ef);
+    const float dp = -om * (f[q] - w * (aa + bb)) + (se + so);
+    const float dm = -om * (f[q + 1] - w * (aa - bb)) + (se - so);
+    const double sdp = double(dp), sdm = double(dm), dd = sdp - sdm;
+    m += sdp + sdm;
+    if (L::ex(q) != 0) px += L::ex(q) * dd;
+    if (L::ey(q) != 0) py += L::ey(q) * dd;
+    if (L::D == 3 && L::ez(q) != 0) pz += L::ez(q) * dd;
+    if (q < 2 * L::D) {
+      da[q - 1] = dp;
+      da[q] = dm;
+    } else {
+      S::st(fout + (q * qs + n), f[q] + dp);
+      S::st(fout + ((q + 1) * qs + n), f[q + 1] + dm);
+    }
+  }
+  // remove the residuals: mass from the rest population, momentum from the
+  // axis pairs (q = 1,2 along x; 3,4 along y; 5,6 along z)
+  S::st(fout + n, f[0] + float(double(d0) - m));
+  const double pr[3] = {px, py, pz};
+#pragma unroll
+  for (int a = 0; a < L::D; a++) {
+    S::st(fout + ((2 * a + 1) * qs + n), f[2 * a + 1] + float(double(da[2 * a]) - 0.5 * pr[a]));
+    S::st(fout + ((2 * a + 2) * qs + n), f[2 * a + 2] + float(double(da[2 * a + 1]) + 0.5 * pr[a]));
+  }
+}
+
 // ---------------------------------------------------------------------------
 // K1: fused stream (step k-1) + external force + moments + BGK/Guo collision
 // (step k).  One thread per node, threads along x.
-template <class L, class S, bool kPull>
+//   write_rho: 0 none, 1 only nodes next to a moving wall, 2 every node.
+template <class L, class S, class I, bool kPull>
 __global__ void __launch_bounds__(256) k_stream_collide(const LBArgs<S> a) {
   using C = typename S::C;
   const Geom& g = a.g;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y, k = blockIdx.z;
   if (i >= g.nx) return;
-  const long long n = i + (long long)g.nx * (j + (long long)g.ny * k);
+  const I n = (I)i + (I)g.nx * ((I)j + (I)g.ny * (I)k);
+  const I qs = (I)g.qs;
 
   C f[L::Q];
-  load_node<L, S, kPull>(g, a.fin, i, j, k, n, f);
+  load_node<L, S, I, kPull>(g, a.fin, a.rho_field, i, j, k, n, f);
 
   C r, jx, jy, jz;
   moments<L, C>(f, r, jx, jy, jz);
@@ -225,7 +337,8 @@ __global__ void __launch_bounds__(256) k_stream_collide(const LBArgs<S> a) {
     Fy += C(a.grav[1]) * rp;
     Fz += C(a.grav[2]) * rp;
   }
-  if (a.write_rho) a.rho_field[n] = typename S::A(S::kShift ? r : rho);
+  if (a.write_rho == 2 || (a.write_rho == 1 && near_moving_wall<L>(g, i, j, k)))
+    a.rho_field[n] = typename S::A(S::kShift ? r : rho);
 
   // compute_macroscopic(true): u = (sum e f + F/2) / rho
   const C inv_r = C(1) / rho;
@@ -233,21 +346,13 @@ __global__ void __launch_bounds__(256) k_stream_collide(const LBArgs<S> a) {
   const C uy = (jy + C(0.5) * Fy) * inv_r;
   const C uz = (jz + C(0.5) * Fz) * inv_r;
 
-  // BGK + Guo (couplb_collision.h:35-57), with 1/cs2 = 3, 1/cs4 = 9
-  const C om = C(a.omega);
-  const C half_om = C(1) - C(0.5) * om;
-  const C uu = ux * ux + uy * uy + uz * uz;
-  const C uf = ux * Fx + uy * Fy + uz * Fz;
+  if constexpr (S::kShift) {
+    collide_store_conserved<L, S, I>(f, r, rho, ux, uy, uz, Fx, Fy, Fz, float(a.omega), a.fout, qs, n);
+  } else {
+    C d[L::Q];
+    collision_increment<L, C>(f, r, rho, ux, uy, uz, Fx, Fy, Fz, C(a.omega), false, d);
 #pragma unroll
-  for (int q = 0; q < L::Q; q++) {
-    const C cx = C(L::ex(q)), cy = C(L::ey(q)), cz = C(L::ez(q));
-    const C w = C(L::w(q));
-    const C eu = cx * ux + cy * uy + cz * uz;
-    const C ef = cx * Fx + cy * Fy + cz * Fz;
-    const C poly = C(3) * eu + C(4.5) * eu * eu - C(1.5) * uu;
-    const C fe = S::kShift ? w * (r + rho * poly) : w * rho * (C(1) + poly);
-    const C si = w * half_om * (C(3) * (ef - uf) + C(9) * eu * ef);
-    S::st(a.fout + q * g.qs + n, f[q] + (-om * (f[q] - fe) + si));
+    for (int q = 0; q < L::Q; q++) S::st(a.fout + (q * qs + n), f[q] + d[q]);
   }
 }
 
@@ -259,6 +364,7 @@ template <class S>
 struct MacroArgs {
   Geom g;
   const typename S::T* __restrict__ fin;
+  const typename S::A* __restrict__ rho_field;
   typename S::A* __restrict__ rho;
   typename S::A* __restrict__ ux;
   typename S::A* __restrict__ uy;
@@ -269,13 +375,14 @@ struct MacroArgs {
 template <class L, class S, bool kPull>
 __global__ void __launch_bounds__(256) k_macro(const MacroArgs<S> a) {
   using C = typename S::C;
+  using I = size_t;
   const Geom& g = a.g;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y, k = blockIdx.z;
   if (i >= g.nx) return;
-  const long long n = i + (long long)g.nx * (j + (long long)g.ny * k);
+  const I n = (I)i + (I)g.nx * ((I)j + (I)g.ny * (I)k);
   C f[L::Q];
-  load_node<L, S, kPull>(g, a.fin, i, j, k, n, f);
+  load_node<L, S, I, kPull>(g, a.fin, a.rho_field, i, j, k, n, f);
   C r, jx, jy, jz;
   moments<L, C>(f, r, jx, jy, jz);
   C rho = S::kShift ? C(g.rho0) + r : r;
@@ -292,16 +399,18 @@ __global__ void __launch_bounds__(256) k_macro(const MacroArgs<S> a) {
 // (streaming alone), so it can be exported or restarted from.
 template <class L, class S>
 __global__ void __launch_bounds__(256) k_materialize(Geom g, const typename S::T* __restrict__ fin,
+                                                     const typename S::A* __restrict__ rho_field,
                                                      typename S::T* __restrict__ fout) {
   using C = typename S::C;
+  using I = size_t;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y, k = blockIdx.z;
   if (i >= g.nx) return;
-  const long long n = i + (long long)g.nx * (j + (long long)g.ny * k);
+  const I n = (I)i + (I)g.nx * ((I)j + (I)g.ny * (I)k);
   C f[L::Q];
-  load_node<L, S, true>(g, fin, i, j, k, n, f);
+  load_node<L, S, I, true>(g, fin, rho_field, i, j, k, n, f);
 #pragma unroll
-  for (int q = 0; q < L::Q; q++) S::st(fout + q * g.qs + n, f[q]);
+  for (int q = 0; q < L::Q; q++) S::st(fout + (q * (I)g.qs + n), f[q]);
 }
 
 // Equilibrium initial state (Grid::init_equilibrium, couplb_lattice.h:137-154).
