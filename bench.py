@@ -45,6 +45,8 @@ def parse():
                     help="length of the FP32/FP16 vs FP64 accuracy runs (0 = skip)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU work of the timed CPU baseline sample")
+    ap.add_argument("--kernel", type=int, default=-1,
+                    help="fused-kernel variant: -1 auto, 0 plain, 1 staged, 2 packed")
     ap.add_argument("--only", choices=["fp64", "fp32", "fp16"], default=None,
                     help="time the fused kernel of one precision only (profiling runs)")
     ap.add_argument("--nx", type=int, default=NX)
@@ -121,9 +123,14 @@ class Clocks:
 
 
 # --------------------------------------------------------------------------
+KERNEL = -1
+
+
 def make_lattice(prec, nx, ny, nz, device):
     from couplb_b200.lattice import Lattice
-    return Lattice(3, nx, ny, nz, tau=TAU, wall=WALL, body_force=True, precision=prec, device=device)
+    L = Lattice(3, nx, ny, nz, tau=TAU, wall=WALL, body_force=True, precision=prec, device=device)
+    L.set_option("kernel", KERNEL)
+    return L
 
 
 def time_lattice(L, steps, warmup, torch, stream):
@@ -263,7 +270,9 @@ def run_reference(args):
 
 
 def main():
+    global KERNEL
     args = parse()
+    KERNEL = args.kernel
     if args.impl == "reference":
         return run_reference(args)
     import torch
@@ -288,7 +297,8 @@ def main():
         ms = time_lattice(L, args.steps, args.warmup, torch, stream)
         print(json.dumps({"only": args.only, "ms_per_step": ms, "mlups": N / (ms * 1e-3) / 1e6,
                           "gbs": BYTES_PER_LU[args.only] * N / (ms * 1e-3) / 1e9,
-                          "status": L.read_status()}), flush=True)
+                          "status": L.read_status(), "kernel": L.get_option("last_kernel")}),
+              flush=True)
         L.close()
         return
 

@@ -14,6 +14,7 @@
 #include "engine_internal.h"
 #include "ibm_kernels.cuh"
 #include "lbm_kernels.cuh"
+#include "lbm_packed.cuh"
 
 using namespace couplb;
 
@@ -135,6 +136,38 @@ int ensure_atoms(couplb_handle* h, int n) {
 int set_device(couplb_handle* h) {
   CK(cudaSetDevice(h->p.device));
   return COUPLB_OK;
+}
+
+// Launch of the bulk-copy staged fused kernel: returns false (nothing
+// launched) when the row layout does not meet the copy alignment rules or the
+// stages do not fit in shared memory, so the caller uses the plain kernel.
+template <class L, class S, int STAGES>
+bool launch_staged(couplb_handle* h, const LBArgs<S>& a) {
+  using T = typename S::T;
+  const size_t row_bytes = (size_t)h->p.nx * sizeof(T);
+  if (row_bytes % 16 != 0 || (h->qs * sizeof(T)) % 16 != 0) return false;
+  if (h->p.wall[0] != 0 || h->p.wall[1] != 0) return false;   // no interior rows
+  const size_t smem = (size_t)STAGES * L::Q * row_bytes;
+  if (smem > 200 * 1024) return false;
+  static bool configured = false;   // per template instance
+  auto kern = k_stream_collide_tma<L, S, STAGES>;
+  if (!configured) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+      return false;
+    configured = true;
+  } else {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  }
+  const int threads = std::min(256, ((h->p.nx + 31) / 32) * 32);
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1)
+    return false;
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->p.device);
+  const long long rows = (long long)h->p.ny * h->p.nz;
+  const int grid = (int)std::min<long long>(rows, (long long)sms * per_sm);
+  kern<<<grid, threads, smem, h->stream>>>(a);
+  return true;
 }
 
 // Populations as post-stream state in buffer `cur` (materialise if needed).
@@ -425,13 +458,35 @@ int couplb_lbm_step(couplb_handle* h, const double* g_lb) {
     for (int d = 0; d < 3; d++) a.grav[d] = g_active ? g_lb[d] : 0.0;
     a.omega = 1.0 / h->p.tau;
     a.status = h->d_status;
-    if (h->idx32) {
-      if (pull) k_stream_collide<L, S, unsigned, true><<<grid, block, 0, h->stream>>>(a);
-      else k_stream_collide<L, S, unsigned, false><<<grid, block, 0, h->stream>>>(a);
-    } else {
-      if (pull) k_stream_collide<L, S, size_t, true><<<grid, block, 0, h->stream>>>(a);
-      else k_stream_collide<L, S, size_t, false><<<grid, block, 0, h->stream>>>(a);
+    // kernel choice: packed (shifted formats, pull, even nx, 32-bit indices),
+    // else staged (when asked for), else plain
+    int used = kKernelPlain;
+    int want = h->kernel;
+    if (want == kKernelAuto) want = S::kShift ? kKernelPacked : kKernelPlain;
+    if constexpr (S::kShift) {
+      if (want == kKernelPacked && pull && h->idx32 && h->p.nx % 2 == 0) {
+        const int pairs = h->p.nx / 2;
+        const dim3 pg((pairs + 127) / 128, h->p.ny, h->p.nz);
+        k_stream_collide_x2<L, S><<<pg, 128, 0, h->stream>>>(a);
+        used = kKernelPacked;
+      }
     }
+    if (used == kKernelPlain && want == kKernelStaged && pull) {
+      bool ok;
+      if constexpr (sizeof(typename S::T) == 8) ok = launch_staged<L, S, 2>(h, a);
+      else ok = launch_staged<L, S, 3>(h, a);
+      if (ok) used = kKernelStaged;
+    }
+    if (used == kKernelPlain) {
+      if (h->idx32) {
+        if (pull) k_stream_collide<L, S, unsigned, true><<<grid, block, 0, h->stream>>>(a);
+        else k_stream_collide<L, S, unsigned, false><<<grid, block, 0, h->stream>>>(a);
+      } else {
+        if (pull) k_stream_collide<L, S, size_t, true><<<grid, block, 0, h->stream>>>(a);
+        else k_stream_collide<L, S, size_t, false><<<grid, block, 0, h->stream>>>(a);
+      }
+    }
+    h->last_kernel = used;
   });
   CK_LAUNCH();
   h->cur = 1 - h->cur;
@@ -599,6 +654,33 @@ int couplb_read_status(couplb_handle* h, int* clamps, int* nonfinite, int reset)
   if (clamps) *clamps = hi[kStClamps];
   if (nonfinite) *nonfinite = hi[kStNonfinite];
   return COUPLB_OK;
+}
+
+int couplb_set_option(couplb_handle* h, const char* name, long long value) {
+  if (!h || !name) return COUPLB_ERR_ARG;
+  if (!std::strcmp(name, "kernel")) {
+    if (value < kKernelAuto || value > kKernelPacked)
+      return fail(h, COUPLB_ERR_ARG, "kernel must be -1 (auto), 0 (plain), 1 (staged) or 2 (packed)");
+    h->kernel = (int)value;
+    return COUPLB_OK;
+  }
+  return fail(h, COUPLB_ERR_ARG, "unknown or read-only option '%s'", name);
+}
+
+int couplb_get_option(couplb_handle* h, const char* name, long long* value) {
+  if (!h || !name || !value) return COUPLB_ERR_ARG;
+  if (!std::strcmp(name, "kernel")) { *value = h->kernel; return COUPLB_OK; }
+  if (!std::strcmp(name, "last_kernel")) { *value = h->last_kernel; return COUPLB_OK; }
+  if (!std::strcmp(name, "timeouts")) {
+    int rc = set_device(h);
+    if (rc) return rc;
+    int* hi = (int*)h->h_small;
+    CK(cudaMemcpyAsync(hi, h->d_status, sizeof(int) * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    *value = hi[kStTimeout];
+    return COUPLB_OK;
+  }
+  return fail(h, COUPLB_ERR_ARG, "unknown option '%s'", name);
 }
 
 int couplb_set_ibm_params(couplb_handle* h, const couplb_ibm_params* ip) {

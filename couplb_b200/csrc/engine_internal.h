@@ -23,6 +23,8 @@ struct couplb_handle {
   void* rho_field = nullptr;         // density of the last fused launch (body force, moving walls)
   bool moving_walls = false;         // a face of type 2
   bool idx32 = true;                 // Q * qs fits 32-bit element indices
+  int kernel = -1;                   // fused-kernel choice (couplb::KernelKind), -1 auto
+  int last_kernel = 0;               // the variant the last LB step ran
   int rho_state = 0;                 // couplb::RhoMode: what the next LB step reads
   void* macro[4] = {nullptr, nullptr, nullptr, nullptr};   // rho(dev), ux, uy, uz
   int macro_valid = 0;               // macro[] are the moments of the current state

@@ -27,6 +27,8 @@ namespace couplb {
 
 enum RhoMode : int { kRhoNone = 0, kRhoField = 1, kRhoCurrent = 2 };
 enum StatusSlot : int { kStClamps = 0, kStNonfinite = 1, kStMacroClamps = 2 };
+// variants of the fused LB kernel (the "kernel" option of a handle)
+enum KernelKind : int { kKernelAuto = -1, kKernelPlain = 0, kKernelStaged = 1, kKernelPacked = 2 };
 
 // Geometry + boundary description shared by all lattice kernels.
 struct Geom {
@@ -241,9 +243,9 @@ __device__ __forceinline__ void collision_increment(const C (&f)[L::Q], C r, C r
 // increment carries no mass and exactly the momentum F; FP32 rounding of the
 // equilibrium leaves residuals of ~1e-11 per node and step that do not
 // decorrelate from step to step in slowly varying flows and act as a spurious
-// body force.  The residuals are summed in FP64 and removed from the rest
-// population (mass) and from the three axis pairs (momentum), which leaves
-// the second-order moments untouched.
+// body force.  The residuals are summed and removed from the rest population
+// (mass) and from the three axis pairs (momentum), which leaves the
+// second-order moments untouched.
 //
 // The shifted (FP32-arithmetic) collision with the conservation correction of
 // conserve_fp32 folded in: increments are produced pair by pair, their FP64
@@ -259,12 +261,14 @@ __device__ __forceinline__ void collide_store_conserved(const float (&f)[L::Q], 
   const float hom = 1.0f - 0.5f * om;
   const float uu15 = 1.5f * (ux * ux + uy * uy + uz * uz);
   const float uf3 = 3.0f * (ux * Fx + uy * Fy + uz * Fz);
-  double m = 0, px = -double(Fx), py = -double(Fy), pz = -double(Fz);
+  // residual sums in FP32: their own rounding (~1e-13 on increments of ~1e-6)
+  // is two orders below the residuals they remove and does not correlate in time
+  float m = 0.0f, px = -Fx, py = -Fy, pz = -Fz;
   float d0, da[2 * L::D];
   {
     const float w = float(L::w(0));
     d0 = -om * (f[0] - w * (r - rho * uu15)) + w * hom * (-uf3);
-    m += double(d0);
+    m += d0;
   }
 #pragma unroll
   for (int q = 1; q < L::Q; q += 2) {
@@ -277,11 +281,11 @@ __device__ __forceinline__ void collide_store_conserved(const float (&f)[L::Q], 
     const float so = w * hom * (3.0f * ef);
     const float dp = -om * (f[q] - w * (aa + bb)) + (se + so);
     const float dm = -om * (f[q + 1] - w * (aa - bb)) + (se - so);
-    const double sdp = double(dp), sdm = double(dm), dd = sdp - sdm;
-    m += sdp + sdm;
-    if (L::ex(q) != 0) px += L::ex(q) * dd;
-    if (L::ey(q) != 0) py += L::ey(q) * dd;
-    if (L::D == 3 && L::ez(q) != 0) pz += L::ez(q) * dd;
+    const float dd = dp - dm;
+    m += dp + dm;
+    if (L::ex(q) == 1) px += dd; else if (L::ex(q) == -1) px -= dd;
+    if (L::ey(q) == 1) py += dd; else if (L::ey(q) == -1) py -= dd;
+    if (L::D == 3) { if (L::ez(q) == 1) pz += dd; else if (L::ez(q) == -1) pz -= dd; }
     if (q < 2 * L::D) {
       da[q - 1] = dp;
       da[q] = dm;
@@ -292,12 +296,12 @@ __device__ __forceinline__ void collide_store_conserved(const float (&f)[L::Q], 
   }
   // remove the residuals: mass from the rest population, momentum from the
   // axis pairs (q = 1,2 along x; 3,4 along y; 5,6 along z)
-  S::st(fout + n, f[0] + float(double(d0) - m));
-  const double pr[3] = {px, py, pz};
+  S::st(fout + n, f[0] + (d0 - m));
+  const float pr[3] = {0.5f * px, 0.5f * py, 0.5f * pz};
 #pragma unroll
   for (int a = 0; a < L::D; a++) {
-    S::st(fout + ((2 * a + 1) * qs + n), f[2 * a + 1] + float(double(da[2 * a]) - 0.5 * pr[a]));
-    S::st(fout + ((2 * a + 2) * qs + n), f[2 * a + 2] + float(double(da[2 * a + 1]) + 0.5 * pr[a]));
+    S::st(fout + ((2 * a + 1) * qs + n), f[2 * a + 1] + (da[2 * a] - pr[a]));
+    S::st(fout + ((2 * a + 2) * qs + n), f[2 * a + 2] + (da[2 * a + 1] + pr[a]));
   }
 }
 
@@ -305,19 +309,14 @@ __device__ __forceinline__ void collide_store_conserved(const float (&f)[L::Q], 
 // K1: fused stream (step k-1) + external force + moments + BGK/Guo collision
 // (step k).  One thread per node, threads along x.
 //   write_rho: 0 none, 1 only nodes next to a moving wall, 2 every node.
-template <class L, class S, class I, bool kPull>
-__global__ void __launch_bounds__(256) k_stream_collide(const LBArgs<S> a) {
+// Everything after the pull, for node (i,j,k) = n with its post-stream
+// populations in f.
+template <class L, class S, class I>
+__device__ __forceinline__ void node_update(const LBArgs<S>& a, typename S::C (&f)[L::Q], int i,
+                                            int j, int k, I n) {
   using C = typename S::C;
   const Geom& g = a.g;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y, k = blockIdx.z;
-  if (i >= g.nx) return;
-  const I n = (I)i + (I)g.nx * ((I)j + (I)g.ny * (I)k);
   const I qs = (I)g.qs;
-
-  C f[L::Q];
-  load_node<L, S, I, kPull>(g, a.fin, a.rho_field, i, j, k, n, f);
-
   C r, jx, jy, jz;
   moments<L, C>(f, r, jx, jy, jz);
   // r is rho (plain) or the density deviation (shifted)
@@ -353,6 +352,180 @@ __global__ void __launch_bounds__(256) k_stream_collide(const LBArgs<S> a) {
     collision_increment<L, C>(f, r, rho, ux, uy, uz, Fx, Fy, Fz, C(a.omega), false, d);
 #pragma unroll
     for (int q = 0; q < L::Q; q++) S::st(a.fout + (q * qs + n), f[q] + d[q]);
+  }
+}
+
+template <class L, class S, class I, bool kPull>
+__global__ void __launch_bounds__(256) k_stream_collide(const LBArgs<S> a) {
+  using C = typename S::C;
+  const Geom& g = a.g;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y, k = blockIdx.z;
+  if (i >= g.nx) return;
+  const I n = (I)i + (I)g.nx * ((I)j + (I)g.ny * (I)k);
+  C f[L::Q];
+  load_node<L, S, I, kPull>(g, a.fin, a.rho_field, i, j, k, n, f);
+  node_update<L, S, I>(a, f, i, j, k, n);
+}
+
+// ---------------------------------------------------------------------------
+// K1 with bulk-copy staging (the pull form for rows that touch no wall).
+//
+// A persistent CTA walks x-rows r = blockIdx.x + t * gridDim.x.  For an
+// interior row (j, k) the Q source rows (j - ey_q, k - ez_q) of the pull are
+// whole, contiguous rows of the q planes; one thread copies them into a
+// shared-memory stage with cp.async.bulk, completing on an mbarrier, STAGES
+// rows ahead of the row being computed.  Threads then read f_q(i - ex_q) from
+// shared memory, which also makes the periodic x wrap an index wrap.  Rows next
+// to a wall take the general pull from global memory.  The copies keep
+// Q * nx * sizeof(T) * STAGES bytes per CTA in flight without registers.
+//
+// Every wait on an mbarrier is bounded: after kMaxSpin failed polls the CTA
+// counts a timeout in status[kStTimeout], waits (bounded again) for its own
+// copies still in flight and returns.
+enum : int { kStTimeout = 3 };
+constexpr unsigned kMaxSpin = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  for (unsigned it = 0; it < kMaxSpin; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+// 1D bulk copy global -> shared; both addresses 16-byte aligned, bytes % 16 == 0.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes,
+                                              uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+template <class L>
+struct TmaRow {
+  // rows are numbered r = j + ny * k
+  __device__ __forceinline__ static void jk(const Geom& g, long long r, int& j, int& k) {
+    j = (int)(r % g.ny);
+    k = (int)(r / g.ny);
+  }
+};
+
+// Issue the Q row copies of row r into stage buffer `buf` (thread 0 only).
+template <class L, class S>
+__device__ __forceinline__ void stage_row(const LBArgs<S>& a, long long r, typename S::T* buf,
+                                          uint64_t* bar) {
+  using T = typename S::T;
+  const Geom& g = a.g;
+  int j, k;
+  TmaRow<L>::jk(g, r, j, k);
+  if (!row_is_interior<L>(g, j, k)) {
+    mbar_arrive(bar);   // nothing to copy: complete the phase
+    return;
+  }
+  const uint32_t rb = (uint32_t)(g.nx * sizeof(T));
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  mbar_arrive_expect_tx(bar, rb * L::Q);
+  const size_t sxy = (size_t)g.nx * g.ny;
+#pragma unroll
+  for (int q = 0; q < L::Q; q++) {
+    const size_t src = (size_t)q * g.qs + (size_t)g.nx * (j - L::ey(q)) + sxy * (k - L::ez(q));
+    bulk_copy_g2s(buf + (size_t)q * g.nx, a.fin + src, rb, bar);
+  }
+}
+
+template <class L, class S, int STAGES>
+__global__ void __launch_bounds__(256, sizeof(typename S::T) == 8 ? 2 : 3)
+    k_stream_collide_tma(const LBArgs<S> a) {
+  using C = typename S::C;
+  using T = typename S::T;
+  using I = size_t;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bars[STAGES];
+  const Geom& g = a.g;
+  const long long nrows = (long long)g.ny * g.nz;
+  T* stage0 = reinterpret_cast<T*>(smem_raw);
+  const size_t stage_elems = (size_t)L::Q * g.nx;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) mbar_init(&bars[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      const long long r = blockIdx.x + (long long)s * gridDim.x;
+      if (r < nrows) stage_row<L, S>(a, r, stage0 + s * stage_elems, &bars[s]);
+    }
+  }
+  long long t_fail = -1;
+  for (long long t = 0;; ++t) {
+    const long long r = blockIdx.x + t * gridDim.x;
+    if (r >= nrows) break;
+    const int s = (int)(t % STAGES);
+    const uint32_t parity = (uint32_t)((t / STAGES) & 1);
+    const bool ok = mbar_wait_bounded(&bars[s], parity);
+    if (__syncthreads_or(!ok)) {   // CTA-uniform decision
+      t_fail = t;
+      break;
+    }
+    int j, k;
+    TmaRow<L>::jk(g, r, j, k);
+    const bool interior = row_is_interior<L>(g, j, k);
+    const T* buf = stage0 + s * stage_elems;
+    for (int i = threadIdx.x; i < g.nx; i += blockDim.x) {
+      const I n = (I)i + (I)g.nx * ((I)j + (I)g.ny * (I)k);
+      C f[L::Q];
+      if (interior) {
+        const int im = (i == 0) ? g.nx - 1 : i - 1;
+        const int ip = (i == g.nx - 1) ? 0 : i + 1;
+#pragma unroll
+        for (int q = 0; q < L::Q; q++) {
+          const int xs = L::ex(q) == 1 ? im : (L::ex(q) == -1 ? ip : i);
+          f[q] = S::ld_shared(buf + q * g.nx + xs);
+        }
+      } else {
+        pull_general<L, S, I>(g, a.fin, a.rho_field, i, j, k, n, f);
+      }
+      node_update<L, S, I>(a, f, i, j, k, n);
+    }
+    __syncthreads();   // stage s fully consumed
+    if (threadIdx.x == 0) {
+      const long long rn = r + (long long)STAGES * gridDim.x;
+      if (rn < nrows) stage_row<L, S>(a, rn, stage0 + s * stage_elems, &bars[s]);
+    }
+  }
+  if (t_fail >= 0 && threadIdx.x == 0) {
+    atomicAdd(a.status + kStTimeout, 1);
+    // Rows t_fail .. t_fail + STAGES - 1 were issued and not consumed: let
+    // their copies land (bounded) before the CTA's shared memory is released.
+    for (long long t = t_fail; t < t_fail + STAGES; ++t) {
+      if (blockIdx.x + t * gridDim.x >= nrows) break;
+      (void)mbar_wait_bounded(&bars[t % STAGES], (uint32_t)((t / STAGES) & 1));
+    }
   }
 }
 

@@ -23,6 +23,7 @@ struct StoreF64 {
   using A = double;  // auxiliary fields (force, density, moments)
   static constexpr bool kShift = false;
   __device__ __forceinline__ static C ld(const T* p) { return __ldg(p); }
+  __device__ __forceinline__ static C ld_shared(const T* p) { return *p; }
   __device__ __forceinline__ static void st(T* p, C v) { *p = v; }
 };
 
@@ -32,6 +33,7 @@ struct StoreF32S {
   using A = float;
   static constexpr bool kShift = true;
   __device__ __forceinline__ static C ld(const T* p) { return __ldg(p); }
+  __device__ __forceinline__ static C ld_shared(const T* p) { return *p; }
   __device__ __forceinline__ static void st(T* p, C v) { *p = v; }
 };
 
@@ -45,6 +47,7 @@ struct StoreF16S {
   __device__ __forceinline__ static C ld(const T* p) {
     return __half2float(__ldg(p)) * kInvScale;
   }
+  __device__ __forceinline__ static C ld_shared(const T* p) { return __half2float(*p) * kInvScale; }
   __device__ __forceinline__ static void st(T* p, C v) {
     *p = __float2half_rn(v * kScale);
   }

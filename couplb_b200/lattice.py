@@ -121,6 +121,14 @@ class Lattice:
     def device_bytes(self):
         return int(self.L.couplb_device_bytes(self.h))
 
+    def set_option(self, name, value):
+        self._ck(self.L.couplb_set_option(self.h, name.encode(), int(value)))
+
+    def get_option(self, name):
+        v = C.c_longlong(0)
+        self._ck(self.L.couplb_get_option(self.h, name.encode(), C.byref(v)))
+        return v.value
+
     # -- IBM ----------------------------------------------------------------
     def set_ibm_params(self, delta="roma", md_per_lb=1, xi_ibm=1.0, dt_lbm=1.0, dx=1.0,
                        vel_scale=1.0, force_scale=1.0, domain_lo=(0.0, 0.0, 0.0),

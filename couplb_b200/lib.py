@@ -44,6 +44,8 @@ SIGNATURES = {
     "couplb_ibm_total_force": (C.c_int, [_H, _D, C.c_int]),
     "couplb_read_status": (C.c_int, [_H, _I, _I, C.c_int]),
     "couplb_device_bytes": (C.c_size_t, [_H]),
+    "couplb_set_option": (C.c_int, [_H, C.c_char_p, C.c_longlong]),
+    "couplb_get_option": (C.c_int, [_H, C.c_char_p, C.POINTER(C.c_longlong)]),
     "couplb_fix_parse": (C.c_int, [C.c_int, C.POINTER(C.c_char_p), C.c_int,
                                    C.POINTER(abi.FixConfig), C.c_char_p, C.c_int]),
     "couplb_fix_create": (C.c_int, [C.POINTER(abi.FixConfig), C.POINTER(_H)]),

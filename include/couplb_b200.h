@@ -202,6 +202,18 @@ int  couplb_ibm_total_force(couplb_handle* h, double out[3], int reset);
  * the stepping kernels since the last reset.  Reading synchronises. */
 int  couplb_read_status(couplb_handle* h, int* clamps, int* nonfinite, int reset);
 
+/* Runtime options of a handle (no counterpart in the reference):
+ *   "kernel"      variant of the fused LB kernel: -1 auto (default: packed for
+ *                 the shifted formats, plain for FP64), 0 plain (one node per
+ *                 thread), 1 staged (interior rows copied to shared memory with
+ *                 bulk copies; same arithmetic as plain), 2 packed (two nodes
+ *                 per thread in paired FP32 arithmetic; shifted formats, even
+ *                 nx).  A variant that does not apply falls back to plain.
+ *   "last_kernel" read-only: the variant the last LB step ran.
+ *   "timeouts"    read-only: bounded device waits that gave up (synchronises). */
+int  couplb_set_option(couplb_handle* h, const char* name, long long value);
+int  couplb_get_option(couplb_handle* h, const char* name, long long* value);
+
 /* Bytes of device memory held by the handle. */
 size_t couplb_device_bytes(const couplb_handle* h);
 
