@@ -15,6 +15,7 @@ ERR_NUMERIC = -4
 ERR_IO = -5
 ERR_PARSE = -6
 ERR_UNSUPPORTED = -7
+ERR_TOO_LARGE = -8
 
 FP64 = 0
 FP32_SHIFTED = 1

@@ -37,6 +37,9 @@ SIGNATURES = {
     "couplb_set_force_field": (C.c_int, [_H, _D, _D, _D]),
     "couplb_diagnostics": (C.c_int, [_H, C.POINTER(abi.Diag)]),
     "couplb_y_profile": (C.c_int, [_H, _D, _D, _D]),
+    "couplb_diagnostics_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_longlong, C.c_int, C.c_double, C.c_void_p,
+                                             C.c_void_p]),
     "couplb_set_ibm_params": (C.c_int, [_H, C.POINTER(abi.IbmParams)]),
     "couplb_ibm_substep": (C.c_int, [_H, C.c_int, _D, _D, _D, _I, _D, C.c_int, _I]),
     "couplb_ibm_substep_device": (C.c_int, [_H, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,

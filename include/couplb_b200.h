@@ -42,6 +42,7 @@ extern "C" {
 #define COUPLB_ERR_IO          -5  /* checkpoint / profile file error         */
 #define COUPLB_ERR_PARSE       -6  /* `fix couplb` argument error             */
 #define COUPLB_ERR_UNSUPPORTED -7  /* feature outside this build              */
+#define COUPLB_ERR_TOO_LARGE   -8  /* input above a fixed capacity            */
 
 /* ---- enumerations ---------------------------------------------------- */
 /* storage / arithmetic precision of the populations */
@@ -165,6 +166,34 @@ int  couplb_set_force_field(couplb_handle* h, const double* fx,
 /* Grid::max_velocity + compute_diagnostics + rho_clamp_count over the moments
  * of the last couplb_macroscopic (couplb_lattice.h:203-242). */
 int  couplb_diagnostics(couplb_handle* h, couplb_diag* out);
+
+/* couplb_diagnostics_noalloc -- the reductions of couplb_diagnostics (max |u|,
+ * total mass, total momentum) for callers that cannot let a library allocate
+ * device memory: an MD code that owns all device memory through its own pool
+ * (a foreign cudaMalloc fragments the pool, and cudaFree synchronises the
+ * whole device) or a time loop that must not stall on such a synchronisation.
+ * No counterpart in the reference; nothing here calls cudaMalloc or cudaFree.
+ *   d_rho, d_ux, d_uy, d_uz: caller-owned device arrays of n moments --
+ *       double for COUPLB_FP64 (rho absolute), float for the shifted formats
+ *       (rho stored as its deviation from rho0, like the lattice's moments);
+ *   d_out: caller-owned device array of 5 doubles receiving
+ *       {max |u|, sum rho, sum rho*ux, sum rho*uy, sum rho*uz};
+ *   stream: cudaStream_t (as void*) the two kernels are queued on; no sync.
+ * Scratch lives in a fixed array of COUPLB_NOALLOC_MAX_PARTIALS * 5 doubles
+ * (1.25 MiB) in device global memory that every GPU loading this library keeps
+ * until exit; n above COUPLB_NOALLOC_MAX_NODES returns COUPLB_ERR_TOO_LARGE.
+ * The first call on a device looks up that array's device address (with the
+ * device current), so make that first call before any stream capture.  All
+ * calls share the array and it keeps the last call's contents; nothing in it
+ * needs to start at zero, but calls whose kernels overlap on the GPU race on
+ * it and must be serialised by the caller. */
+#define COUPLB_NOALLOC_CHUNK        2048        /* nodes reduced per block      */
+#define COUPLB_NOALLOC_MAX_PARTIALS 32768       /* scratch slots                */
+#define COUPLB_NOALLOC_MAX_NODES    (COUPLB_NOALLOC_CHUNK * (long long)COUPLB_NOALLOC_MAX_PARTIALS)
+int  couplb_diagnostics_noalloc(const void* d_rho, const void* d_ux,
+                                const void* d_uy, const void* d_uz, long long n,
+                                int precision, double rho0, double* d_out,
+                                void* stream);
 
 /* Per-j sums over i and k of ux, uy and rho after the last couplb_macroscopic
  * (each output holds ny doubles): the local sums of FixCoupLB::write_profile
