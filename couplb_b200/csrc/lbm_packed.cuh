@@ -50,8 +50,8 @@ struct Pair<StoreF16S> {
   }
 };
 
-template <class L, class S>
-__global__ void __launch_bounds__(128) k_stream_collide_x2(const LBArgs<S> a) {
+template <class L, class S, int MINB = 5>
+__global__ void __launch_bounds__(128, MINB) k_stream_collide_x2(const LBArgs<S> a) {
   using T = typename S::T;
   using I = unsigned;
   const Geom& g = a.g;
