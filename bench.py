@@ -45,6 +45,8 @@ def parse():
                     help="length of the FP32/FP16 vs FP64 accuracy runs (0 = skip)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU work of the timed CPU baseline sample")
+    ap.add_argument("--ibm-cycles", type=int, default=50,
+                    help="LB cycles of the 256^3 IBM point-marker workload (0 = skip)")
     ap.add_argument("--kernel", type=int, default=-1,
                     help="fused-kernel variant: -1 auto, 0 plain, 1 staged, 2 packed")
     ap.add_argument("--only", choices=["fp64", "fp32", "fp16"], default=None,
@@ -209,6 +211,81 @@ def e2e_fix(steps, warmup, nx, ny, nz, device, torch):
     return dt
 
 
+def ibm_bench(torch, device, prec, cycles, warmup, n=256, natoms=20000, md_per_lb=4, seed=3):
+    """LBM + IBM on the D3Q19 256^3 periodic box with point markers (nu 0.1,
+    uniform random positions, v ~ N(0, 0.01^2), m 1, xi 1, Peskin4,
+    md_per_lb 4).  Markers stay on the device; a velocity-Verlet stand-in for
+    the MD side runs on the same stream.  Timed: the library's own calls (one
+    LB step + md_per_lb IBM sub-steps per LB cycle), CUDA events around them.
+    Also checks momentum conservation per LB interval in FP64."""
+    from couplb_b200.lattice import Lattice
+    L = Lattice(3, n, n, n, tau=3 * 0.1 + 0.5, precision=prec, device=device)
+    stream = torch.cuda.current_stream()
+    L.set_stream(stream.cuda_stream)
+    L.init_equilibrium(1.0)
+    dt = 1.0 / md_per_lb
+    L.set_ibm_params(delta="peskin4", md_per_lb=md_per_lb, xi_ibm=1.0, dt_lbm=1.0, dx=1.0)
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    x = (torch.rand((natoms, 3), generator=g, dtype=torch.float64) * n).cuda()
+    v = (0.01 * torch.randn((natoms, 3), generator=g, dtype=torch.float64)).cuda()
+    m = torch.ones(natoms, dtype=torch.float64, device="cuda")
+    f = torch.zeros((natoms, 3), dtype=torch.float64, device="cuda")
+    evs = []
+
+    def cycle(timed):
+        for s in range(md_per_lb):
+            v.add_(f, alpha=0.5 * dt)
+            x.add_(v, alpha=dt).remainder_(n)
+            f.zero_()
+            if timed:
+                e0 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            if s == 0:
+                L.lbm_step()
+            L.ibm_substep_device(natoms, x.data_ptr(), v.data_ptr(), m.data_ptr(), f.data_ptr(),
+                                 0, refresh=(s == 0))
+            if timed:
+                e1 = torch.cuda.Event(enable_timing=True)
+                e1.record(stream)
+                evs.append((e0, e1))
+            v.add_(f, alpha=0.5 * dt)
+
+    for _ in range(warmup):
+        cycle(False)
+    torch.cuda.synchronize()
+    for _ in range(cycles):
+        cycle(True)
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in evs) / cycles
+    # momentum balance of one LB interval: the fluid gains what the markers lose
+    L.lbm_step()   # consume the forces still pending from the timed cycles
+    L.macroscopic()
+    p0 = np.array(L.diagnostics().mom)
+    L.ibm_total_force(reset=True)
+    fsum = torch.zeros(3, dtype=torch.float64, device="cuda")
+    for s in range(md_per_lb):
+        f.zero_()
+        L.ibm_substep_device(natoms, x.data_ptr(), v.data_ptr(), m.data_ptr(), f.data_ptr(), 0,
+                             refresh=(s == 0))
+        fsum += f.sum(0)
+    L.lbm_step()
+    L.macroscopic()
+    dp = np.array(L.diagnostics().mom) - p0
+    expect = -(fsum.cpu().numpy()) / md_per_lb
+    err = float(np.abs(dp - expect).max() / max(np.abs(expect).max(), 1e-300))
+    clamps, nonfinite = L.read_status()
+    L.close()
+    nodes = n ** 3
+    mu = natoms * md_per_lb / (ms * 1e-3)
+    b_lu = BYTES_PER_LU[prec] + 3 * (8 if prec == "fp64" else 4)
+    b_mk = 64 * (3 * (8 if prec == "fp64" else 4) * 3) + 72
+    return {"workload": f"d3q19_periodic_{n}^3_{natoms}_markers_peskin4_md_per_lb{md_per_lb}",
+            "precision": prec, "ms_per_lb_cycle": ms, "mlups": nodes / (ms * 1e-3) / 1e6,
+            "marker_updates_per_s": mu,
+            "roofline_frac": (nodes * b_lu + natoms * md_per_lb * b_mk) / (ms * 1e-3) / 1e9 / 6460.5,
+            "momentum_rel_err_per_lb_interval": err, "nonfinite": nonfinite}
+
+
 def cpu_baseline(nx, ny, nz, seconds):
     """The reference's CPU path (its own headers, OpenMP, all host threads)
     on a bounded number of LB steps of the same workload."""
@@ -325,6 +402,9 @@ def main():
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_s = float(t.item())
     acc = accuracy_runs(f0, args.accuracy_steps, nx, ny, nz, local) if args.accuracy_steps else {}
+    ibm = None
+    if args.ibm_cycles > 0:
+        ibm = {p: ibm_bench(torch, local, p, args.ibm_cycles, 3) for p in ("fp32", "fp64")}
 
     peaks = {}
     try:
@@ -360,6 +440,7 @@ def main():
         "e2e": {"value": world * N / e2e_s / 1e6, "unit": "MLUPS", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 8},
         "gpu_launches": args.steps,
+        "ibm": ibm,
         "clocks": clk,
     }
     if rank == 0:

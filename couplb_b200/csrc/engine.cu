@@ -117,6 +117,33 @@ int ensure_staging(couplb_handle* h, size_t bytes) {
   return COUPLB_OK;
 }
 
+// Stencil velocity records of the IBM sub-step, one per marker slot
+// (StencilKey + 64 x 3 values).  Keys start with epoch 0xffffffff, which
+// cur_epoch never takes, so a fresh record never hits.
+int ensure_stencil_cache(couplb_handle* h, int n) {
+  if (h->stencil_cap >= n) return COUPLB_OK;
+  dfree(h->sbuf);
+  void* k = h->skey;
+  dfree(k);
+  h->skey = nullptr;
+  h->stencil_cap = 0;
+  const int cap = std::max(n, 1024);
+  int rc;
+  if ((rc = dalloc(h, &h->sbuf, elem_bytes_aux(h->p.precision) * 64 * 3 * (size_t)cap))) return rc;
+  if ((rc = dalloc(h, (void**)&h->skey, sizeof(couplb::StencilKey) * (size_t)cap))) return rc;
+  CK(cudaMemsetAsync(h->skey, 0xff, sizeof(couplb::StencilKey) * (size_t)cap, h->stream));
+  h->stencil_cap = cap;
+  return COUPLB_OK;
+}
+
+// The population state changed: every cached stencil velocity is stale.
+void bump_epoch(couplb_handle* h) {
+  if (++h->cur_epoch == 0xffffffffu) {
+    h->cur_epoch = 0;
+    if (h->skey) cudaMemsetAsync(h->skey, 0xff, sizeof(couplb::StencilKey) * (size_t)h->stencil_cap, h->stream);
+  }
+}
+
 int ensure_atoms(couplb_handle* h, int n) {
   if (h->atom_cap >= n) return COUPLB_OK;
   dfree(h->d_x); dfree(h->d_v); dfree(h->d_m); dfree(h->d_fout); dfree(h->d_active);
@@ -285,13 +312,14 @@ int couplb_create(const couplb_lattice_params* p, couplb_handle** out) {
   const size_t pb = elem_bytes_pop(p->precision), ab = elem_bytes_aux(p->precision);
   int rc = COUPLB_OK;
   for (int b = 0; b < 2 && !rc; b++) rc = dalloc(h, &h->f[b], pb * Q * h->qs);
-  for (int c = 0; c < 3 && !rc; c++) rc = dalloc(h, &h->F[c], ab * h->qs);
+  if (!rc) rc = dalloc(h, &h->F, 4 * ab * h->qs);
   h->moving_walls = false;
   for (int f = 0; f < (p->dim == 3 ? 6 : 4); f++) h->moving_walls |= (p->wall[f] == 2);
   if (!rc && (p->body_force || h->moving_walls)) rc = dalloc(h, &h->rho_field, ab * h->qs);
   h->idx32 = ((unsigned long long)Q * h->qs < (1ULL << 32));
   if (!rc) rc = dalloc(h, (void**)&h->d_status, sizeof(int) * 8);
   if (!rc) rc = dalloc(h, (void**)&h->d_ftot, sizeof(double) * 4);
+  if (!rc) rc = dalloc(h, (void**)&h->row_force, (size_t)p->ny * p->nz);
   if (!rc && cudaMallocHost(&h->h_small, 4096) != cudaSuccess)
     rc = fail(h, COUPLB_ERR_CUDA, "cudaMallocHost failed");
   if (rc) {
@@ -299,8 +327,7 @@ int couplb_create(const couplb_lattice_params* p, couplb_handle** out) {
     couplb_destroy(h);
     return rc;
   }
-  for (int c = 0; c < 3 && !rc; c++)
-    if (cudaMemsetAsync(h->F[c], 0, ab * h->qs, h->stream) != cudaSuccess) rc = COUPLB_ERR_CUDA;
+  if (!rc && cudaMemsetAsync(h->F, 0, 4 * ab * h->qs, h->stream) != cudaSuccess) rc = COUPLB_ERR_CUDA;
   if (!rc && cudaMemsetAsync(h->d_status, 0, sizeof(int) * 8, h->stream) != cudaSuccess) rc = COUPLB_ERR_CUDA;
   if (!rc && cudaMemsetAsync(h->d_ftot, 0, sizeof(double) * 4, h->stream) != cudaSuccess) rc = COUPLB_ERR_CUDA;
   if (!rc) rc = couplb_init_equilibrium(h, p->rho0, 0.0, 0.0, 0.0);
@@ -318,10 +345,13 @@ int couplb_destroy(couplb_handle* h) {
   cudaSetDevice(h->p.device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (int b = 0; b < 2; b++) dfree(h->f[b]);
-  for (int c = 0; c < 3; c++) dfree(h->F[c]);
+  dfree(h->F);
   for (int c = 0; c < 4; c++) dfree(h->macro[c]);
   dfree(h->rho_field);
   void* p = h->d_status; dfree(p);
+  p = h->row_force; dfree(p);
+  p = h->skey; dfree(p);
+  dfree(h->sbuf);
   p = h->d_ftot; dfree(p);
   dfree(h->d_staging);
   dfree(h->d_scratch);
@@ -374,10 +404,13 @@ int couplb_init_equilibrium(couplb_handle* h, double rho, double ux, double uy, 
   h->cur = 0;
   h->poststream = 1;
   const size_t ab = elem_bytes_aux(h->p.precision);
-  for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(h->F[c], 0, ab * h->qs, h->stream));
+  CK(cudaMemsetAsync(h->F, 0, 4 * ab * h->qs, h->stream));
+  CK(cudaMemsetAsync(h->row_force, 0, (size_t)h->p.ny * h->p.nz, h->stream));
   h->force_dirty = 0;
+  h->force_rows_all = 0;
   h->rho_state = h->p.body_force ? kRhoField : kRhoNone;
   h->macro_valid = 0;
+  bump_epoch(h);
   return COUPLB_OK;
 }
 
@@ -399,6 +432,7 @@ int couplb_set_populations(couplb_handle* h, const double* f_host) {
   CK_LAUNCH();
   h->cur = 0;
   h->poststream = 1;
+  bump_epoch(h);
   // like IO::read_checkpoint: moments recomputed without the Guo term
   rc = engine_macro(h);
   if (rc) return rc;
@@ -449,9 +483,8 @@ int couplb_lbm_step(couplb_handle* h, const double* g_lb) {
     a.g = g;
     a.fin = (const T*)h->f[h->cur];
     a.fout = (T*)h->f[1 - h->cur];
-    a.Fx = h->force_dirty ? (const A*)h->F[0] : nullptr;
-    a.Fy = (const A*)h->F[1];
-    a.Fz = (const A*)h->F[2];
+    a.F = h->force_dirty ? (A*)h->F : nullptr;
+    a.row_force = h->force_rows_all ? nullptr : h->row_force;
     a.rho_field = (A*)h->rho_field;
     a.rho_mode = rho_mode;
     a.write_rho = h->p.body_force ? 2 : (h->moving_walls ? 1 : 0);
@@ -492,13 +525,15 @@ int couplb_lbm_step(couplb_handle* h, const double* g_lb) {
   h->cur = 1 - h->cur;
   h->poststream = 0;
   h->lbm_steps++;
-  if (h->force_dirty) {   // clear_forces (couplb_lattice.h:243-247)
-    const size_t ab = elem_bytes_aux(h->p.precision);
-    for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(h->F[c], 0, ab * h->qs, h->stream));
+  if (h->force_dirty) {
+    // the kernel zeroed every force it read (clear_forces); reset the row flags
+    CK(cudaMemsetAsync(h->row_force, 0, (size_t)h->p.ny * h->p.nz, h->stream));
     h->force_dirty = 0;
+    h->force_rows_all = 0;
   }
   h->rho_state = h->p.body_force ? kRhoField : kRhoNone;
   h->macro_valid = 0;
+  bump_epoch(h);
   return COUPLB_OK;
 }
 
@@ -547,7 +582,7 @@ int couplb_get_force_field(couplb_handle* h, double* fx, double* fy, double* fz)
     using A = typename S::A;
     (void)l;
     k_export_force<S><<<flat_blocks((long long)G, 256), 256, 0, h->stream>>>(
-        g, h->p.dim, (const A*)h->F[0], (const A*)h->F[1], (const A*)h->F[2], (long long)G, st,
+        g, h->p.dim, (const A*)h->F, (long long)G, st,
         st + G, st + 2 * G);
   });
   CK_LAUNCH();
@@ -574,10 +609,11 @@ int couplb_set_force_field(couplb_handle* h, const double* fx, const double* fy,
     using A = typename S::A;
     (void)l;
     k_import_force<S><<<flat_blocks((long long)h->N, 256), 256, 0, h->stream>>>(
-        g, h->p.dim, st, st + G, st + 2 * G, (A*)h->F[0], (A*)h->F[1], (A*)h->F[2]);
+        g, h->p.dim, st, st + G, st + 2 * G, (A*)h->F);
   });
   CK_LAUNCH();
   h->force_dirty = 1;
+  h->force_rows_all = 1;   // the row flags know nothing of these forces
   CK(cudaStreamSynchronize(h->stream));
   return COUPLB_OK;
 }
@@ -702,11 +738,15 @@ namespace couplb {
 // Shared body of the host- and device-array IBM sub-step.
 int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, const double* d_m,
                const int* d_active, double* d_fout, int accumulate, int refresh) {
-  if (refresh || !h->macro_valid) {
-    int rc = engine_macro(h);
-    if (rc) return rc;
-  }
+  // no coupled atoms: the reference returns before refreshing the moments
+  // (fix_couplb.cpp:750-753)
   if (n <= 0) return COUPLB_OK;
+  // The refresh of compute_macroscopic(false) (fix_couplb.cpp:757-760): the
+  // velocities are computed on demand by the kernel; the density it would
+  // store is what the next LB step's body force reads.
+  if (refresh && h->p.body_force) h->rho_state = kRhoCurrent;
+  int rc = ensure_stencil_cache(h, n);
+  if (rc) return rc;
   const couplb_ibm_params& ip = h->ip;
   const double dxp = ip.dx;
   const double dv = (h->p.dim == 3) ? dxp * dxp * dxp : dxp * dxp;
@@ -720,8 +760,16 @@ int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, co
     using A = typename S::A;
     IbmArgs<S> a;
     a.g = g;
-    a.ux = (const A*)h->macro[1]; a.uy = (const A*)h->macro[2]; a.uz = (const A*)h->macro[3];
-    a.Fx = (A*)h->F[0]; a.Fy = (A*)h->F[1]; a.Fz = (A*)h->F[2];
+    a.fin = (const typename S::T*)h->f[h->cur];
+    a.rho_field = (const A*)h->rho_field;
+    a.pull = h->poststream ? 0 : 1;
+    a.cux = (const A*)h->macro[1]; a.cuy = (const A*)h->macro[2]; a.cuz = (const A*)h->macro[3];
+    a.all_valid = h->macro_valid;
+    a.sbuf = (A*)h->sbuf;
+    a.skey = h->skey;
+    a.cur_epoch = h->cur_epoch;
+    a.F = (A*)h->F;
+    a.row_force = h->row_force;
     a.n = n;
     a.x = d_x; a.v = d_v; a.m = d_m; a.active = d_active;
     a.fout = d_fout;
@@ -735,6 +783,7 @@ int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, co
     a.vs = ip.vel_scale;
     a.fs = ip.force_scale;
     a.dvr = dv / cell_vol;
+    if (refresh && !a.all_valid) k_ibm_prefetch<L, S><<<nb, bs, 0, h->stream>>>(a);
     if (ip.delta == COUPLB_DELTA_ROMA) k_ibm_substep<L, S, 0><<<nb, bs, 0, h->stream>>>(a);
     else k_ibm_substep<L, S, 1><<<nb, bs, 0, h->stream>>>(a);
   });

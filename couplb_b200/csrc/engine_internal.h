@@ -7,6 +7,10 @@
 
 #include "../../include/couplb_b200.h"
 
+namespace couplb {
+struct StencilKey;
+}
+
 struct couplb_handle {
   couplb_lattice_params p{};
   int Q = 0;
@@ -18,8 +22,14 @@ struct couplb_handle {
   void* f[2] = {nullptr, nullptr};   // population buffers (A-B)
   int cur = 0;                       // buffer holding the current state
   int poststream = 1;                // 1: f[cur] is post-stream S, 0: post-collision P
-  void* F[3] = {nullptr, nullptr, nullptr};   // Eulerian force field
+  void* F = nullptr;                 // Eulerian force field {fx, fy, fz, 0} per node
   int force_dirty = 0;               // F holds nonzero values
+  int force_rows_all = 0;            // F was set from outside: the row flags do not cover it
+  unsigned char* row_force = nullptr;   // per (j,k) row: IBM force spread there
+  unsigned cur_epoch = 0;            // epoch of the current population state
+  void* sbuf = nullptr;              // IBM stencil velocity records (64 x 3 per marker slot)
+  couplb::StencilKey* skey = nullptr;   // their keys
+  int stencil_cap = 0;
   void* rho_field = nullptr;         // density of the last fused launch (body force, moving walls)
   bool moving_walls = false;         // a face of type 2
   bool idx32 = true;                 // Q * qs fits 32-bit element indices

@@ -8,6 +8,15 @@
 // IBM::interpolate / IBM::spread (couplb_ibm.h:57-133); a periodic ghost node
 // of the window reads and receives through its interior image, which is what
 // exchange_velocity / exchange_forces do on one rank.
+//
+// Fluid velocities are not computed for the whole grid.  The reference
+// refreshes the moments of every node once per LB cycle
+// (compute_macroscopic(false), fix_couplb.cpp:757-760); the populations do
+// not change within the cycle, so the velocity of a node is a pure function of
+// them.  At the refresh, k_ibm_prefetch computes (arithmetic of k_macro) the
+// velocities of each marker's stencil into a contiguous per-marker record;
+// the sub-steps of the cycle read the record and compute directly only the
+// stencils of markers that moved to another cell.
 #pragma once
 #include "lbm_kernels.cuh"
 
@@ -48,15 +57,30 @@ __device__ __forceinline__ R delta1(R r) {
   return DELTA == 0 ? delta_roma<R>(r) : delta_peskin4<R>(r);
 }
 
+// Key of a stencil velocity record (see k_ibm_prefetch).
+struct StencilKey {
+  int i0, j0, k0;
+  unsigned epoch;
+};
+
 template <class S>
 struct IbmArgs {
   Geom g;
-  const typename S::A* __restrict__ ux;   // moments of the post-stream state
-  const typename S::A* __restrict__ uy;
-  const typename S::A* __restrict__ uz;
-  typename S::A* Fx;                      // Eulerian force field (accumulated)
-  typename S::A* Fy;
-  typename S::A* Fz;
+  // populations of the current state and how to read them
+  const typename S::T* __restrict__ fin;
+  const typename S::A* __restrict__ rho_field;
+  int pull;                               // 1: post-collision store (pull), 0: post-stream
+  // dense moment arrays, used when they hold this state everywhere
+  const typename S::A* cux;
+  const typename S::A* cuy;
+  const typename S::A* cuz;
+  int all_valid;
+  // stencil velocity records, one per marker slot (64 x 3 values each)
+  typename S::A* sbuf;
+  StencilKey* skey;
+  unsigned cur_epoch;
+  typename S::A* F;                       // Eulerian force field {fx,fy,fz,0} per node
+  unsigned char* row_force;               // per (j,k) row: a force was spread there
   int n;
   const double* __restrict__ x;           // n*3, MD units
   const double* __restrict__ v;           // n*3
@@ -69,6 +93,121 @@ struct IbmArgs {
   int off[3];
   double inv_dx, xi_over_dt, inv_N, vs, fs, dvr;
 };
+
+// Add a spread force to one node of the interleaved force field: one vector
+// atomic (16 B, sm_90+) for FP32; three FP64 atomics otherwise.
+__device__ __forceinline__ void spread_add(float* p, double a, double b, double c) {
+  atomicAdd(reinterpret_cast<float4*>(p), make_float4(float(a), float(b), float(c), 0.f));
+}
+__device__ __forceinline__ void spread_add(double* p, double a, double b, double c) {
+  atomicAdd(p, a);
+  atomicAdd(p + 1, b);
+  atomicAdd(p + 2, c);
+}
+
+// Ghost-inclusive node (ig, jg, kg) -> -1 and the interior coordinates of the
+// node or of its periodic image, or the wall type (1..4).
+__device__ __forceinline__ int classify_node(const Geom& g, int D, int ig, int jg, int kg, int& i,
+                                             int& j, int& k) {
+  const int gx = g.nx + 2, gy = g.ny + 2, gz = (D == 3) ? g.nz + 2 : 1;
+  int t = 0;
+  const bool ox = ig == 0 || ig == gx - 1;
+  const bool oy = jg == 0 || jg == gy - 1;
+  const bool oz = (D == 3) && (kg == 0 || kg == gz - 1);
+  if (ox) { const int ft = ig == 0 ? g.face[0] : g.face[1]; if (ft) t = ft; }
+  if (oy) { const int ft = jg == 0 ? g.face[2] : g.face[3]; if (ft) t = ft; }
+  if (oz) { const int ft = kg == 0 ? g.face[4] : g.face[5]; if (ft) t = ft; }
+  if (t) return t;
+  i = ig - 1; j = jg - 1; k = (D == 3) ? kg - 1 : 0;
+  i = i < 0 ? g.nx - 1 : (i >= g.nx ? 0 : i);
+  j = j < 0 ? g.ny - 1 : (j >= g.ny ? 0 : j);
+  if (D == 3) k = k < 0 ? g.nz - 1 : (k >= g.nz ? 0 : k);
+  return -1;
+}
+
+// Velocity of interior node (i,j,k) = n of the post-stream state, with the
+// arithmetic of k_macro (compute_macroscopic(false), couplb_lattice.h:155-202).
+template <class L, class S>
+__device__ __forceinline__ void compute_velocity(const IbmArgs<S>& a, int i, int j, int k, size_t n,
+                                                 typename S::A& v0, typename S::A& v1,
+                                                 typename S::A& v2) {
+  using C = typename S::C;
+  C f[L::Q];
+  if (a.pull) load_node<L, S, size_t, true>(a.g, a.fin, a.rho_field, i, j, k, n, f);
+  else load_node<L, S, size_t, false>(a.g, a.fin, a.rho_field, i, j, k, n, f);
+  C r, jx, jy, jz;
+  moments<L, C>(f, r, jx, jy, jz);
+  C rho = S::kShift ? C(a.g.rho0) + r : r;
+  if (rho <= C(RHO_MIN) || !isfinite(rho)) rho = C(RHO_MIN);
+  const C inv_r = C(1) / rho;
+  v0 = typename S::A(jx * inv_r);
+  v1 = typename S::A(jy * inv_r);
+  v2 = typename S::A(jz * inv_r);
+}
+
+// Stencil velocity cache: one record per marker slot holding the velocities of
+// the 4^D nodes of a stencil whose base cell is (i0, j0, k0), valid for one
+// population state (epoch).  The velocities depend only on the base cell and
+// the state, so a record serves any marker whose stencil has that base; a
+// marker that moved to another cell since the refresh (or a slot filled by a
+// different atom) misses and computes its nodes directly.  Records are
+// contiguous (64 x 3 values), so a sub-step reads its marker's stencil as a
+// few full cache lines that stay in L2 across the sub-steps of a cycle.
+template <class S>
+__device__ __forceinline__ typename S::A* stencil_record(const IbmArgs<S>& a, int mk) {
+  return a.sbuf + (size_t)mk * (64 * 3);
+}
+
+// Refresh prefetch: one warp per active marker fills its slot's record.
+template <class L, class S>
+__global__ void __launch_bounds__(256) k_ibm_prefetch(const IbmArgs<S> a) {
+  const int mk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (mk >= a.n) return;
+  if (a.active && !a.active[mk]) return;
+  const Geom& g = a.g;
+  const double lx = (a.x[3 * mk] - a.lo[0]) * a.inv_dx - a.off[0] + 1.0;
+  const double ly = (a.x[3 * mk + 1] - a.lo[1]) * a.inv_dx - a.off[1] + 1.0;
+  const double lz = (L::D == 3) ? ((a.x[3 * mk + 2] - a.lo[2]) * a.inv_dx - a.off[2] + 1.0) : 0.0;
+  const int i0 = (int)floor(lx), j0 = (int)floor(ly);
+  const int k0 = (L::D == 3) ? (int)floor(lz) : 0;
+  const int gx = g.nx + 2, gy = g.ny + 2, gz = (L::D == 3) ? g.nz + 2 : 1;
+  constexpr int NS = (L::D == 3) ? 64 : 16;
+  typename S::A* rec = stencil_record(a, mk);
+#pragma unroll
+  for (int rep = 0; rep < 2; rep++) {
+    const int s = lane + 32 * rep;
+    if (s >= NS) break;
+    const int ig = i0 - 1 + (s & 3);
+    const int jg = j0 - 1 + ((s >> 2) & 3);
+    const int kg = (L::D == 3) ? k0 - 1 + (s >> 4) : 0;
+    typename S::A v0 = 0, v1 = 0, v2 = 0;
+    int ii = 0, jj = 0, kk = 0;
+    if (ig >= 0 && ig < gx && jg >= 0 && jg < gy && kg >= 0 && kg < gz &&
+        classify_node(g, L::D, ig, jg, kg, ii, jj, kk) < 0) {
+      const size_t n = (size_t)ii + (size_t)g.nx * ((size_t)jj + (size_t)g.ny * kk);
+      compute_velocity<L, S>(a, ii, jj, kk, n, v0, v1, v2);
+    }
+    rec[s] = v0; rec[64 + s] = v1; rec[128 + s] = v2;
+  }
+  if (lane == 0) a.skey[mk] = StencilKey{i0, j0, k0, a.cur_epoch};
+}
+
+// Velocity of stencil slot s of marker mk (node (i,j,k) = n).
+template <class L, class S>
+__device__ __forceinline__ void node_velocity(const IbmArgs<S>& a, bool hit,
+                                              const typename S::A* rec, int s, int i, int j,
+                                              int k, size_t n, double& u0, double& u1, double& u2) {
+  if (a.all_valid) {
+    u0 = double(a.cux[n]); u1 = double(a.cuy[n]); u2 = double(a.cuz[n]);
+  } else if (hit) {
+    u0 = double(rec[s]); u1 = double(rec[64 + s]); u2 = double(rec[128 + s]);
+  } else {
+    typename S::A v0, v1, v2;
+    compute_velocity<L, S>(a, i, j, k, n, v0, v1, v2);
+    u0 = double(v0); u1 = double(v1); u2 = double(v2);
+  }
+}
 
 // Weight arithmetic in the storage's compute type: FP64 for the parity form,
 // FP32 for the shifted forms.  Sums are carried in FP64 either way.
@@ -96,6 +235,10 @@ __global__ void __launch_bounds__(256) k_ibm_substep(const IbmArgs<S> a) {
   double ui = 0, vi = 0, wi = 0, ws = 0, wss = 0;
   long long sn0 = -1, sn1 = -1;   // fluid nodes of this lane (interior index)
   double sd0 = 0, sd1 = 0;
+  int row0 = 0, row1 = 0;
+  const StencilKey key = a.skey[mk];
+  const bool hit = key.epoch == a.cur_epoch && key.i0 == i0 && key.j0 == j0 && key.k0 == k0;
+  const typename S::A* rec = stencil_record(a, mk);
 #pragma unroll
   for (int rep = 0; rep < 2; rep++) {
     const int s = lane + 32 * rep;
@@ -106,16 +249,20 @@ __global__ void __launch_bounds__(256) k_ibm_substep(const IbmArgs<S> a) {
     if (ig < 0 || ig >= gx || jg < 0 || jg >= gy || kg < 0 || kg >= gz) continue;
     R d = delta1<DELTA, R>(R(lx - ig)) * delta1<DELTA, R>(R(ly - jg));
     if (L::D == 3) d *= delta1<DELTA, R>(R(lz - kg));
-    long long src = 0;
-    const int t = classify_ghost(g, L::D, ig, jg, kg, &src);
+    int ii = 0, jj = 0, kk = 0;
+    const int t = classify_node(g, L::D, ig, jg, kg, ii, jj, kk);
     const double dd = double(d);
     if (t < 0) {
-      ui += double(a.ux[src]) * dd;
-      vi += double(a.uy[src]) * dd;
-      wi += double(a.uz[src]) * dd;
+      const size_t src = (size_t)ii + (size_t)g.nx * ((size_t)jj + (size_t)g.ny * kk);
+      double u0, u1, u2;
+      node_velocity<L, S>(a, hit, rec, s, ii, jj, kk, src, u0, u1, u2);
+      ui += u0 * dd;
+      vi += u1 * dd;
+      wi += u2 * dd;
       ws += dd;
       wss += dd;
-      if (rep == 0) { sn0 = src; sd0 = dd; } else { sn1 = src; sd1 = dd; }
+      if (rep == 0) { sn0 = (long long)src; sd0 = dd; row0 = jj + g.ny * kk; }
+      else { sn1 = (long long)src; sd1 = dd; row1 = jj + g.ny * kk; }
     } else if (t == 1 || t == 3) {
       ws += dd;
     } else if (t == 2) {
@@ -155,16 +302,14 @@ __global__ void __launch_bounds__(256) k_ibm_substep(const IbmArgs<S> a) {
   const double sc = a.dvr / wss;
   const double fl0 = -F0 * a.inv_N / a.fs, fl1 = -F1 * a.inv_N / a.fs, fl2 = -F2 * a.inv_N / a.fs;
   if (sn0 >= 0) {
-    const double w = sd0 * sc;
-    atomicAdd(a.Fx + sn0, typename S::A(fl0 * w));
-    atomicAdd(a.Fy + sn0, typename S::A(fl1 * w));
-    atomicAdd(a.Fz + sn0, typename S::A(fl2 * w));
+    const double w = sd0 * sc;   // couplb_ibm.h:128
+    spread_add(a.F + 4 * sn0, fl0 * w, fl1 * w, fl2 * w);
+    if (a.row_force) a.row_force[row0] = 1;
   }
   if (sn1 >= 0) {
     const double w = sd1 * sc;
-    atomicAdd(a.Fx + sn1, typename S::A(fl0 * w));
-    atomicAdd(a.Fy + sn1, typename S::A(fl1 * w));
-    atomicAdd(a.Fz + sn1, typename S::A(fl2 * w));
+    spread_add(a.F + 4 * sn1, fl0 * w, fl1 * w, fl2 * w);
+    if (a.row_force) a.row_force[row1] = 1;
   }
   if (lane == 0 && a.ftot) {
     atomicAdd(a.ftot, fl0 * a.dvr);

@@ -44,9 +44,11 @@ struct LBArgs {
   Geom g;
   const typename S::T* __restrict__ fin;
   typename S::T* __restrict__ fout;
-  const typename S::A* __restrict__ Fx;   // IBM force field, or null
-  const typename S::A* __restrict__ Fy;
-  const typename S::A* __restrict__ Fz;
+  // IBM force field {fx, fy, fz, 0} per node (F[4n + c]), or null; the step
+  // reads it and leaves it zero (clear_forces, couplb_lattice.h:243-247) by
+  // zeroing the nonzero entries
+  typename S::A* __restrict__ F;
+  const unsigned char* __restrict__ row_force;  // per (j,k) row: force present, or null = all
   typename S::A* __restrict__ rho_field;  // stale density (see RhoMode)
   int rho_mode;
   int write_rho;
@@ -327,7 +329,13 @@ __device__ __forceinline__ void node_update(const LBArgs<S>& a, typename S::C (&
   // apply_external_force (fix_couplb.cpp:693-707): F += g * rho[n], rho[n]
   // being the density the last moment pass stored.
   C Fx = C(0), Fy = C(0), Fz = C(0);
-  if (a.Fx) { Fx = C(a.Fx[n]); Fy = C(a.Fy[n]); Fz = C(a.Fz[n]); }
+  if (a.F && (!a.row_force || a.row_force[j + g.ny * k])) {
+    using A = typename S::A;
+    A* p = a.F + 4 * (size_t)n;
+    const A fx = p[0], fy = p[1], fz = p[2];
+    Fx = C(fx); Fy = C(fy); Fz = C(fz);
+    if (fx != A(0) || fy != A(0) || fz != A(0)) { p[0] = A(0); p[1] = A(0); p[2] = A(0); }
+  }
   if (a.rho_mode != kRhoNone) {
     C rp;
     if (a.rho_mode == kRhoField) rp = S::kShift ? C(g.rho0) + C(a.rho_field[n]) : C(a.rho_field[n]);
@@ -699,11 +707,10 @@ __global__ void k_export_macro(Geom g, int D, const typename S::A* __restrict__ 
   if (duz) duz[gn] = c;
 }
 
-// Force field export (interior values, ghosts zero) and import.
+// Force field export (interior values, ghosts zero) and import; the device
+// field is interleaved, F[4n + c].
 template <class S>
-__global__ void k_export_force(Geom g, int D, const typename S::A* __restrict__ Fx,
-                               const typename S::A* __restrict__ Fy,
-                               const typename S::A* __restrict__ Fz, long long G,
+__global__ void k_export_force(Geom g, int D, const typename S::A* __restrict__ F, long long G,
                                double* __restrict__ dx, double* __restrict__ dy,
                                double* __restrict__ dz) {
   const long long gn = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -715,7 +722,7 @@ __global__ void k_export_force(Geom g, int D, const typename S::A* __restrict__ 
   double a = 0, b = 0, c = 0;
   if (inside) {
     const long long n = (ig - 1) + (long long)g.nx * ((jg - 1) + (long long)g.ny * (D == 3 ? kg - 1 : 0));
-    a = double(Fx[n]); b = double(Fy[n]); c = double(Fz[n]);
+    a = double(F[4 * n]); b = double(F[4 * n + 1]); c = double(F[4 * n + 2]);
   }
   dx[gn] = a; dy[gn] = b; dz[gn] = c;
 }
@@ -723,17 +730,17 @@ __global__ void k_export_force(Geom g, int D, const typename S::A* __restrict__ 
 template <class S>
 __global__ void k_import_force(Geom g, int D, const double* __restrict__ sx,
                                const double* __restrict__ sy, const double* __restrict__ sz,
-                               typename S::A* __restrict__ Fx, typename S::A* __restrict__ Fy,
-                               typename S::A* __restrict__ Fz) {
+                               typename S::A* __restrict__ F) {
   const long long N = (long long)g.nx * g.ny * g.nz;
   const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
   const int i = n % g.nx, j = (n / g.nx) % g.ny, k = n / ((long long)g.nx * g.ny);
   const int gx = g.nx + 2, gy = g.ny + 2;
   const long long gn = (i + 1) + (long long)gx * ((j + 1) + (long long)gy * (D == 3 ? k + 1 : 0));
-  Fx[n] = typename S::A(sx[gn]);
-  Fy[n] = typename S::A(sy[gn]);
-  Fz[n] = typename S::A(sz[gn]);
+  F[4 * n] = typename S::A(sx[gn]);
+  F[4 * n + 1] = typename S::A(sy[gn]);
+  F[4 * n + 2] = typename S::A(sz[gn]);
+  F[4 * n + 3] = typename S::A(0);
 }
 
 // ---------------------------------------------------------------------------

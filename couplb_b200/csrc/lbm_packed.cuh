@@ -108,10 +108,15 @@ __global__ void __launch_bounds__(128, MINB) k_stream_collide_x2(const LBArgs<S>
 
   // apply_external_force (fix_couplb.cpp:693-707)
   float2 Fx = f2(0.f), Fy = f2(0.f), Fz = f2(0.f);
-  if (a.Fx) {
-    Fx = *reinterpret_cast<const float2*>(a.Fx + n0);
-    Fy = *reinterpret_cast<const float2*>(a.Fy + n0);
-    Fz = *reinterpret_cast<const float2*>(a.Fz + n0);
+  if (a.F && (!a.row_force || a.row_force[j + g.ny * k])) {
+    float4* p = reinterpret_cast<float4*>(a.F + 4 * (size_t)n0);
+    const float4 fa = p[0], fb = p[1];
+    Fx = make_float2(fa.x, fb.x);
+    Fy = make_float2(fa.y, fb.y);
+    Fz = make_float2(fa.z, fb.z);
+    // clear_forces: leave the field zero where it was read nonzero
+    if (fa.x != 0.f || fa.y != 0.f || fa.z != 0.f) p[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (fb.x != 0.f || fb.y != 0.f || fb.z != 0.f) p[1] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
   if (a.rho_mode != kRhoNone) {
     float2 rp = rho;
