@@ -318,8 +318,9 @@ int couplb_create(const couplb_lattice_params* p, couplb_handle** out) {
   if (!rc && (p->body_force || h->moving_walls)) rc = dalloc(h, &h->rho_field, ab * h->qs);
   h->idx32 = ((unsigned long long)Q * h->qs < (1ULL << 32));
   if (!rc) rc = dalloc(h, (void**)&h->d_status, sizeof(int) * 8);
-  if (!rc) rc = dalloc(h, (void**)&h->d_ftot, sizeof(double) * 4);
+  if (!rc) rc = dalloc(h, (void**)&h->d_ftot, sizeof(double) * 4 * kFtotSlots);
   if (!rc) rc = dalloc(h, (void**)&h->row_force, (size_t)p->ny * p->nz);
+  static_assert(sizeof(double) * 4 * kFtotSlots <= 4096, "h_small holds the force accumulators");
   if (!rc && cudaMallocHost(&h->h_small, 4096) != cudaSuccess)
     rc = fail(h, COUPLB_ERR_CUDA, "cudaMallocHost failed");
   if (rc) {
@@ -329,7 +330,8 @@ int couplb_create(const couplb_lattice_params* p, couplb_handle** out) {
   }
   if (!rc && cudaMemsetAsync(h->F, 0, 4 * ab * h->qs, h->stream) != cudaSuccess) rc = COUPLB_ERR_CUDA;
   if (!rc && cudaMemsetAsync(h->d_status, 0, sizeof(int) * 8, h->stream) != cudaSuccess) rc = COUPLB_ERR_CUDA;
-  if (!rc && cudaMemsetAsync(h->d_ftot, 0, sizeof(double) * 4, h->stream) != cudaSuccess) rc = COUPLB_ERR_CUDA;
+  if (!rc && cudaMemsetAsync(h->d_ftot, 0, sizeof(double) * 4 * kFtotSlots, h->stream) != cudaSuccess)
+    rc = COUPLB_ERR_CUDA;
   if (!rc) rc = couplb_init_equilibrium(h, p->rho0, 0.0, 0.0, 0.0);
   if (rc) {
     g_create_error = h->err.empty() ? "device initialisation failed" : h->err;
@@ -842,10 +844,12 @@ int couplb_ibm_total_force(couplb_handle* h, double out[3], int reset) {
   int rc = set_device(h);
   if (rc) return rc;
   double* hs = (double*)h->h_small;
-  CK(cudaMemcpyAsync(hs, h->d_ftot, sizeof(double) * 3, cudaMemcpyDeviceToHost, h->stream));
-  if (reset) CK(cudaMemsetAsync(h->d_ftot, 0, sizeof(double) * 4, h->stream));
+  CK(cudaMemcpyAsync(hs, h->d_ftot, sizeof(double) * 4 * kFtotSlots, cudaMemcpyDeviceToHost, h->stream));
+  if (reset) CK(cudaMemsetAsync(h->d_ftot, 0, sizeof(double) * 4 * kFtotSlots, h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  out[0] = hs[0]; out[1] = hs[1]; out[2] = hs[2];
+  out[0] = out[1] = out[2] = 0.0;
+  for (int s = 0; s < kFtotSlots; s++)
+    for (int c = 0; c < 3; c++) out[c] += hs[4 * s + c];
   return COUPLB_OK;
 }
 

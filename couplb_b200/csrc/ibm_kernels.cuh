@@ -57,6 +57,9 @@ __device__ __forceinline__ R delta1(R r) {
   return DELTA == 0 ? delta_roma<R>(r) : delta_peskin4<R>(r);
 }
 
+// Accumulators of the total spread force, each 4 doubles (32 B) apart.
+constexpr int kFtotSlots = 64;
+
 // Key of a stencil velocity record (see k_ibm_prefetch).
 struct StencilKey {
   int i0, j0, k0;
@@ -88,7 +91,7 @@ struct IbmArgs {
   const int* __restrict__ active;         // n or null
   double* fout;                           // n*3 marker forces
   int accumulate;                         // 1: fout += F, 0: fout = F (0 for inactive)
-  double* ftot;                           // [3] FP64 sum of the spread grid force
+  double* ftot;                           // [kFtotSlots][4] FP64 sums of the spread grid force
   double lo[3];
   int off[3];
   double inv_dx, xi_over_dt, inv_N, vs, fs, dvr;
@@ -312,9 +315,12 @@ __global__ void __launch_bounds__(256) k_ibm_substep(const IbmArgs<S> a) {
     if (a.row_force) a.row_force[row1] = 1;
   }
   if (lane == 0 && a.ftot) {
-    atomicAdd(a.ftot, fl0 * a.dvr);
-    atomicAdd(a.ftot + 1, fl1 * a.dvr);
-    atomicAdd(a.ftot + 2, fl2 * a.dvr);
+    // one of kFtotSlots accumulators (32 B apart) by marker index: the
+    // same-address FP64 atomics of all markers would serialise in L2
+    double* t = a.ftot + 4 * (mk & (kFtotSlots - 1));
+    atomicAdd(t, fl0 * a.dvr);
+    atomicAdd(t + 1, fl1 * a.dvr);
+    atomicAdd(t + 2, fl2 * a.dvr);
   }
 }
 
