@@ -77,6 +77,16 @@ def load(kind="port"):
         "fix_scales": (None, [_V, _D]),
         "fix_last_error": (C.c_char_p, [_V]),
     }
+    if kind == "port":
+        # project definitions without a reference counterpart
+        sig.update({
+            "grid_ibm_substep_method": (C.c_int, [_V, C.POINTER(abi.IbmParams), C.c_int, _D, _D, _D,
+                                                  _I, _D, C.c_int, C.c_int, C.c_int, C.c_int,
+                                                  C.c_double, _D, C.c_double, C.c_double, _D, _D,
+                                                  _D]),
+            "mlp_forward": (None, [_D, C.c_double, C.c_double, C.c_int, _D, C.c_int, _D]),
+            "mlp_loss_grad": (C.c_double, [_D, C.c_double, C.c_double, C.c_int, _D, _D]),
+        })
     fns = {}
     for name, (res, args) in sig.items():
         fn = getattr(lib, pre + name)
@@ -174,6 +184,51 @@ class OracleGrid:
         n = x.shape[0]
         return self.L["grid_ibm_substep"](self.h, C.byref(ip), n, _d(x), _d(v), _d(mass),
                                           abi.iptr(active), _d(f_add), int(refresh), int(fold))
+
+
+    def ibm_substep_method(self, ip, x, v, mass, f_add, method, passes, slip_tol=0.0,
+                           mlp=None, g_lb=(0.0, 0.0, 0.0), active=None, refresh=True, fold=True,
+                           rows=False):
+        """One sub-step with a forcing method (1 iterative, 2 learned; port
+        oracle only).  mlp: (weights float64[MLP_NPARAM], s_in, s_out).
+        Returns (coupled, stats[6], rows or None)."""
+        n = x.shape[0]
+        st = np.zeros(6)
+        rw = np.zeros((n, MLP_ROW)) if rows else None
+        w, s_in, s_out = mlp if mlp is not None else (None, 1.0, 1.0)
+        wv = None if w is None else np.ascontiguousarray(w, dtype=np.float64)
+        gl = np.asarray(g_lb, dtype=np.float64)
+        nc = self.L["grid_ibm_substep_method"](
+            self.h, C.byref(ip), n, _d(x), _d(v), _d(mass), abi.iptr(active), _d(f_add),
+            int(refresh), int(fold), int(method), int(passes), float(slip_tol),
+            _D() if wv is None else _d(wv), float(s_in), float(s_out), _d(gl), _d(st),
+            _D() if rw is None else _d(rw))
+        return nc, st, rw
+
+
+MLP_IN, MLP_HID, MLP_OUT, MLP_ROW = 84, 64, 3, 88
+MLP_NPARAM = MLP_HID * MLP_IN + MLP_HID + MLP_HID * MLP_HID + MLP_HID + MLP_OUT * MLP_HID + MLP_OUT
+
+
+def mlp_forward(w, s_in, s_out, x):
+    """FP64 network output for inputs x (n x 84, or rows n x 88)."""
+    L = load("port")
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    n, stride = x.shape
+    y = np.empty((n, MLP_OUT))
+    L["mlp_forward"](_d(np.ascontiguousarray(w, dtype=np.float64)), s_in, s_out, n, _d(x),
+                     stride, _d(y))
+    return y
+
+
+def mlp_loss_grad(w, s_in, s_out, rows):
+    """FP64 loss and gradient over sample rows (n x 88)."""
+    L = load("port")
+    rows = np.ascontiguousarray(rows, dtype=np.float64)
+    g = np.empty(MLP_NPARAM)
+    loss = L["mlp_loss_grad"](_d(np.ascontiguousarray(w, dtype=np.float64)), s_in, s_out,
+                              rows.shape[0], _d(rows), _d(g))
+    return loss, g
 
 
 class OracleFix:

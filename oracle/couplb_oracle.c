@@ -617,3 +617,306 @@ int ORC_FN(grid_ibm_substep)(void* gp, const couplb_ibm_params* ip, int n,
 void ORC_FN(grid_fold_forces)(void* gp) { exchange_forces((orc_grid*)gp); }
 
 #include "oracle_fix.inc"
+
+/* ---- IBM forcing methods and the correction network ------------------
+ * No counterpart in the reference: the reference applies the single penalty
+ * pass above.  These restate the project's own definitions (multi-direct
+ * forcing after Wang, Fan & Luo, J. Comput. Phys. 227 (2008), written with the
+ * reference's penalty law; and the 84-64-64-3 correction network), so that the
+ * CUDA forms have a CPU checker.  Definitions:
+ *   u_corr(x) = u0(x) + (G(x)/rho(x) + g_lb)/2  at fluid nodes, u0 and rho from
+ *               the refresh, G the IBM force field so far, g_lb the body force;
+ *   U_i       = the reference's interpolation of u_corr at marker i;
+ *   dF_i      = m xi/dt (U_i vs - v_i), added to the atom and spread as
+ *               -dF_i/(N fs) (Jacobi: all dF_i of a pass before any spread);
+ *   slip_i    = |U_i vs - v_i| after the last pass.
+ * Network: x = (u0 at the 27 Roma nodes round(l)-1..round(l)+1, node-major
+ * dz,dy,dx, then v/vs), all lattice velocities; h1 = relu(W1 s_in x + b1),
+ * h2 = relu(W2 h1 + b2), y = W3 h2 + b3; correction dF = m xi/dt vs y/s_out. */
+
+#define MLP_IN 84
+#define MLP_HID 64
+#define MLP_OUT 3
+#define MLP_ROW 88
+#define MLP_NPARAM (MLP_HID * MLP_IN + MLP_HID + MLP_HID * MLP_HID + MLP_HID + MLP_OUT * MLP_HID + MLP_OUT)
+
+void ORC_FN(mlp_forward)(const double* w, double s_in, double s_out, int n,
+                         const double* rows, int stride, double* y) {
+  const double *W1 = w, *b1 = W1 + MLP_HID * MLP_IN, *W2 = b1 + MLP_HID;
+  const double *b2 = W2 + MLP_HID * MLP_HID, *W3 = b2 + MLP_HID, *b3 = W3 + MLP_OUT * MLP_HID;
+  for (int s = 0; s < n; s++) {
+    const double* x = rows + (size_t)s * stride;
+    double h1[MLP_HID], h2[MLP_HID];
+    for (int j = 0; j < MLP_HID; j++) {
+      double a = b1[j];
+      for (int k = 0; k < MLP_IN; k++) a += W1[j * MLP_IN + k] * (x[k] * s_in);
+      h1[j] = a > 0.0 ? a : 0.0;
+    }
+    for (int j = 0; j < MLP_HID; j++) {
+      double a = b2[j];
+      for (int k = 0; k < MLP_HID; k++) a += W2[j * MLP_HID + k] * h1[k];
+      h2[j] = a > 0.0 ? a : 0.0;
+    }
+    for (int c = 0; c < MLP_OUT; c++) {
+      double a = b3[c];
+      for (int k = 0; k < MLP_HID; k++) a += W3[c * MLP_HID + k] * h2[k];
+      y[(size_t)s * MLP_OUT + c] = a / s_out;
+    }
+  }
+}
+
+/* Loss L = sum over rows and outputs of (y_norm - s_out t)^2 / (3 n) with
+ * t = rows[84..86]; returns L and writes dL/dw (MLP_NPARAM) to grad. */
+double ORC_FN(mlp_loss_grad)(const double* w, double s_in, double s_out, int n,
+                             const double* rows, double* grad) {
+  const double *W1 = w, *b1 = W1 + MLP_HID * MLP_IN, *W2 = b1 + MLP_HID;
+  const double *b2 = W2 + MLP_HID * MLP_HID, *W3 = b2 + MLP_HID, *b3 = W3 + MLP_OUT * MLP_HID;
+  double *gW1 = grad, *gb1 = gW1 + MLP_HID * MLP_IN, *gW2 = gb1 + MLP_HID;
+  double *gb2 = gW2 + MLP_HID * MLP_HID, *gW3 = gb2 + MLP_HID, *gb3 = gW3 + MLP_OUT * MLP_HID;
+  memset(grad, 0, sizeof(double) * MLP_NPARAM);
+  double loss = 0.0;
+  const double inv = 1.0 / (3.0 * (double)n);
+  for (int s = 0; s < n; s++) {
+    const double* r = rows + (size_t)s * MLP_ROW;
+    double x[MLP_IN], h1[MLP_HID], h2[MLP_HID], d2[MLP_HID], d1[MLP_HID], dy[MLP_OUT];
+    for (int k = 0; k < MLP_IN; k++) x[k] = r[k] * s_in;
+    for (int j = 0; j < MLP_HID; j++) {
+      double a = b1[j];
+      for (int k = 0; k < MLP_IN; k++) a += W1[j * MLP_IN + k] * x[k];
+      h1[j] = a > 0.0 ? a : 0.0;
+    }
+    for (int j = 0; j < MLP_HID; j++) {
+      double a = b2[j];
+      for (int k = 0; k < MLP_HID; k++) a += W2[j * MLP_HID + k] * h1[k];
+      h2[j] = a > 0.0 ? a : 0.0;
+    }
+    for (int c = 0; c < MLP_OUT; c++) {
+      double a = b3[c];
+      for (int k = 0; k < MLP_HID; k++) a += W3[c * MLP_HID + k] * h2[k];
+      const double e = a - s_out * r[MLP_IN + c];
+      loss += e * e * inv;
+      dy[c] = 2.0 * e * inv;
+    }
+    for (int c = 0; c < MLP_OUT; c++) {
+      gb3[c] += dy[c];
+      for (int k = 0; k < MLP_HID; k++) gW3[c * MLP_HID + k] += dy[c] * h2[k];
+    }
+    for (int k = 0; k < MLP_HID; k++) {
+      double a = 0.0;
+      for (int c = 0; c < MLP_OUT; c++) a += W3[c * MLP_HID + k] * dy[c];
+      d2[k] = h2[k] > 0.0 ? a : 0.0;
+    }
+    for (int j = 0; j < MLP_HID; j++) {
+      gb2[j] += d2[j];
+      for (int k = 0; k < MLP_HID; k++) gW2[j * MLP_HID + k] += d2[j] * h1[k];
+    }
+    for (int k = 0; k < MLP_HID; k++) {
+      double a = 0.0;
+      for (int j = 0; j < MLP_HID; j++) a += W2[j * MLP_HID + k] * d2[j];
+      d1[k] = h1[k] > 0.0 ? a : 0.0;
+    }
+    for (int j = 0; j < MLP_HID; j++) {
+      gb1[j] += d1[j];
+      for (int k = 0; k < MLP_IN; k++) gW1[j * MLP_IN + k] += d1[j] * x[k];
+    }
+  }
+  return loss;
+}
+
+/* Sum of the force field over all ghost-inclusive aliases of a fluid node
+ * (spreads that landed on periodic ghosts are not folded until the last
+ * sub-step). */
+static void force_over_aliases(const orc_grid* g, int i, int j, int k, double out[3]) {
+  const int nn[3] = {g->nx, g->ny, g->nz};
+  const int c[3] = {i, j, k};
+  int al[3][3], na[3];
+  const int nd = (g->D == 3) ? 3 : 2;
+  for (int d = 0; d < 3; d++) {
+    if (d >= nd) { al[d][0] = c[d]; na[d] = 1; continue; }
+    int ii = c[d];
+    if (ii < 1) ii += nn[d];
+    else if (ii > nn[d]) ii -= nn[d];
+    na[d] = 0;
+    al[d][na[d]++] = ii;
+    if (ii == nn[d] && !g->wall_face[d][0]) al[d][na[d]++] = 0;
+    if (ii == 1 && !g->wall_face[d][1]) al[d][na[d]++] = nn[d] + 1;
+  }
+  out[0] = out[1] = out[2] = 0.0;
+  for (int a = 0; a < na[2]; a++)
+    for (int b = 0; b < na[1]; b++)
+      for (int e = 0; e < na[0]; e++) {
+        const int n = gidx(g, al[0][e], al[1][b], al[2][a]);
+        out[0] += g->fx[n]; out[1] += g->fy[n]; out[2] += g->fz[n];
+      }
+}
+
+/* The reference's interpolation (couplb_ibm.h:57-90) of u_corr. */
+static void interpolate_corr(const orc_grid* g, const couplb_ibm_params* ip, double inv_dx,
+                             const double* xp, const double g_lb[3], double out[3]) {
+  double lx, ly, lz;
+  phys_to_local(g, ip, inv_dx, xp[0], xp[1], xp[2], &lx, &ly, &lz);
+  const int i0 = (int)floor(lx), j0 = (int)floor(ly);
+  const int k0 = (g->D == 3) ? (int)floor(lz) : 0;
+  double ui = 0, vi = 0, wi = 0, ws = 0;
+  for (int k = (g->D == 3 ? k0 - 1 : 0); k <= (g->D == 3 ? k0 + 2 : 0); k++) {
+    if (g->D == 3 && (k < 0 || k >= g->gz)) continue;
+    for (int j = j0 - 1; j <= j0 + 2; j++) {
+      if (j < 0 || j >= g->gy) continue;
+      for (int i = i0 - 1; i <= i0 + 2; i++) {
+        if (i < 0 || i >= g->gx) continue;
+        const int n = gidx(g, i, j, k);
+        const int nt = g->type[n];
+        const double d = delta_product(g, ip->delta, lx - i, ly - j, lz - k);
+        if (nt == 0) {
+          double G[3];
+          force_over_aliases(g, i, j, k, G);
+          const double ir = 1.0 / g->rho[n];
+          const double c0 = g->ux[n] + 0.5 * (G[0] * ir + g_lb[0]);
+          const double c1 = g->uy[n] + 0.5 * (G[1] * ir + g_lb[1]);
+          const double c2 = g->uz[n] + 0.5 * (G[2] * ir + (g->D == 3 ? g_lb[2] : 0.0));
+          ui += c0 * d; vi += c1 * d; wi += c2 * d; ws += d;
+        } else if (nt == 1 || nt == 3) {
+          ws += d;
+        } else if (nt == 2) {
+          ui += g->bc_ux[n] * d; vi += g->bc_uy[n] * d; wi += g->bc_uz[n] * d; ws += d;
+        }
+      }
+    }
+  }
+  if (ws > DELTA_TOL) {
+    const double iw = 1.0 / ws;
+    out[0] = ui * iw; out[1] = vi * iw; out[2] = wi * iw;
+  } else {
+    out[0] = out[1] = out[2] = 0.0;
+  }
+}
+
+/* Network input of one marker: u0 at the 27 Roma nodes and v / vs. */
+static void mlp_input(const orc_grid* g, const couplb_ibm_params* ip, double inv_dx,
+                      const double* xp, const double* vp, double* x) {
+  double l[3];
+  phys_to_local(g, ip, inv_dx, xp[0], xp[1], xp[2], &l[0], &l[1], &l[2]);
+  int s[3];
+  for (int d = 0; d < 3; d++) {
+    const int f = (int)floor(l[d]);
+    s[d] = f - 1 + ((l[d] - f) >= 0.5 ? 1 : 0);
+  }
+  for (int p = 0; p < 27; p++) {
+    const int i = s[0] + p % 3, j = s[1] + (p / 3) % 3, k = s[2] + p / 9;
+    double u[3] = {0.0, 0.0, 0.0};
+    if (i >= 0 && i < g->gx && j >= 0 && j < g->gy && k >= 0 && k < g->gz) {
+      const int n = gidx(g, i, j, k);
+      if (g->type[n] == 0) { u[0] = g->ux[n]; u[1] = g->uy[n]; u[2] = g->uz[n]; }
+      else if (g->type[n] == 2) { u[0] = g->bc_ux[n]; u[1] = g->bc_uy[n]; u[2] = g->bc_uz[n]; }
+    }
+    x[3 * p] = u[0]; x[3 * p + 1] = u[1]; x[3 * p + 2] = u[2];
+  }
+  for (int c = 0; c < 3; c++) x[81 + c] = vp[c] / ip->vel_scale;
+}
+
+static void slip_stats(const orc_grid* g, const couplb_ibm_params* ip, double inv_dx, int n,
+                       const double* x, const double* v, const int* active,
+                       const double g_lb[3], int nc, double* rms, double* mx) {
+  double s2 = 0.0, m = 0.0;
+  for (int a = 0; a < n; a++) {
+    if (active && !active[a]) continue;
+    double U[3];
+    interpolate_corr(g, ip, inv_dx, x + 3*a, g_lb, U);
+    double e2 = 0.0;
+    for (int c = 0; c < 3; c++) { const double e = U[c] * ip->vel_scale - v[3*a+c]; e2 += e * e; }
+    s2 += e2;
+    if (sqrt(e2) > m) m = sqrt(e2);
+  }
+  *rms = nc ? sqrt(s2 / nc) : 0.0;
+  *mx = m;
+}
+
+/* One sub-step with a forcing method.  method 1: iterative with `passes`
+ * passes (1 = the reference pass plus a slip measurement); method 2: the
+ * reference pass plus the network correction (mlp_w, bf16-valued weights),
+ * then the slip check; above slip_tol the passes-1 iterative corrections run.
+ * stats: [rms slip of the method-2 check, its max, rms slip at the end, its
+ * max, 1 if the fallback ran, coupled markers].  rows (n x 88, may be NULL):
+ * network input, total correction beyond the reference pass / (m xi vs / dt)
+ * in lattice velocity units, 0. */
+int ORC_FN(grid_ibm_substep_method)(void* gp, const couplb_ibm_params* ip, int n,
+                                    const double* x, const double* v, const double* mass,
+                                    const int* active, double* f_add, int refresh, int fold,
+                                    int method, int passes, double slip_tol,
+                                    const double* mlp_w, double s_in, double s_out,
+                                    const double g_lb[3], double* stats, double* rows) {
+  orc_grid* g = (orc_grid*)gp;
+  if (refresh) {
+    ORC_FN(grid_macroscopic)(g, 0);
+    ORC_FN(grid_exchange_velocity)(g);
+  }
+  const double inv_dx = 1.0 / ip->dx;
+  const double xo = ip->xi_ibm / ip->dt_lbm;
+  const double inv_N = 1.0 / (double)ip->md_per_lb;
+  const double dv = (g->D == 3) ? (ip->dx * ip->dx * ip->dx) : (ip->dx * ip->dx);
+  const double vs = ip->vel_scale, fs = ip->force_scale;
+  double* dF = (double*)calloc((size_t)3 * (n > 0 ? n : 1), sizeof(double));
+  double* corr = (double*)calloc((size_t)3 * (n > 0 ? n : 1), sizeof(double));
+  int nc = 0;
+  /* pass 0: the reference pass (+ the network correction) */
+  for (int a = 0; a < n; a++) {
+    if (active && !active[a]) continue;
+    nc++;
+    double uf[3];
+    interpolate(g, ip, inv_dx, x[3*a], x[3*a+1], x[3*a+2], uf);
+    const double m = mass[a];
+    double F[3];
+    for (int c = 0; c < 3; c++) F[c] = m * xo * (uf[c] * vs - v[3*a+c]);
+    if (method == 2) {
+      double in[MLP_IN], y[3];
+      mlp_input(g, ip, inv_dx, x + 3*a, v + 3*a, in);
+      ORC_FN(mlp_forward)(mlp_w, s_in, s_out, 1, in, MLP_IN, y);
+      for (int c = 0; c < 3; c++) { corr[3*a+c] = m * xo * vs * y[c]; F[c] += corr[3*a+c]; }
+    }
+    for (int c = 0; c < 3; c++) f_add[3*a+c] += F[c];
+    spread(g, ip, inv_dx, x[3*a], x[3*a+1], x[3*a+2],
+           -F[0] * inv_N / fs, -F[1] * inv_N / fs, -F[2] * inv_N / fs, dv);
+  }
+  double rms0 = 0.0, max0 = 0.0, rms1 = 0.0, max1 = 0.0;
+  int fallback = 0, run = 1;
+  if (method == 2) {
+    slip_stats(g, ip, inv_dx, n, x, v, active, g_lb, nc, &rms0, &max0);
+    run = rms0 > slip_tol;
+    fallback = run;
+    if (!run) { rms1 = rms0; max1 = max0; }
+  }
+  if (run) {
+    for (int it = 0; it < passes - 1; it++) {
+      for (int a = 0; a < n; a++) {
+        if (active && !active[a]) continue;
+        double U[3];
+        interpolate_corr(g, ip, inv_dx, x + 3*a, g_lb, U);
+        for (int c = 0; c < 3; c++) dF[3*a+c] = mass[a] * xo * (U[c] * vs - v[3*a+c]);
+      }
+      for (int a = 0; a < n; a++) {
+        if (active && !active[a]) continue;
+        for (int c = 0; c < 3; c++) { f_add[3*a+c] += dF[3*a+c]; corr[3*a+c] += dF[3*a+c]; }
+        spread(g, ip, inv_dx, x[3*a], x[3*a+1], x[3*a+2],
+               -dF[3*a] * inv_N / fs, -dF[3*a+1] * inv_N / fs, -dF[3*a+2] * inv_N / fs, dv);
+      }
+    }
+    slip_stats(g, ip, inv_dx, n, x, v, active, g_lb, nc, &rms1, &max1);
+  }
+  if (stats) {
+    stats[0] = rms0; stats[1] = max0; stats[2] = rms1; stats[3] = max1;
+    stats[4] = fallback; stats[5] = nc;
+  }
+  if (rows) {
+    for (int a = 0; a < n; a++) {
+      double* r = rows + (size_t)a * MLP_ROW;
+      if (active && !active[a]) { memset(r, 0, sizeof(double) * MLP_ROW); continue; }
+      mlp_input(g, ip, inv_dx, x + 3*a, v + 3*a, r);
+      for (int c = 0; c < 3; c++) r[MLP_IN + c] = corr[3*a+c] / (mass[a] * xo * vs);
+      r[MLP_ROW - 1] = 0.0;
+    }
+  }
+  free(dF);
+  free(corr);
+  if (fold) exchange_forces(g);
+  return nc;
+}

@@ -52,6 +52,21 @@ int    ORC_FN(grid_ibm_substep)(void* g, const couplb_ibm_params* ip, int n,
                                 const double* mass, const int* active,
                                 double* f_add, int refresh, int fold);
 
+/* IBM forcing methods and the correction network (project definitions, no
+ * reference counterpart; port library only) */
+int    ORC_FN(grid_ibm_substep_method)(void* g, const couplb_ibm_params* ip, int n,
+                                       const double* x, const double* v,
+                                       const double* mass, const int* active,
+                                       double* f_add, int refresh, int fold,
+                                       int method, int passes, double slip_tol,
+                                       const double* mlp_w, double s_in, double s_out,
+                                       const double g_lb[3], double* stats,
+                                       double* rows);
+void   ORC_FN(mlp_forward)(const double* w, double s_in, double s_out, int n,
+                           const double* rows, int stride, double* y);
+double ORC_FN(mlp_loss_grad)(const double* w, double s_in, double s_out, int n,
+                             const double* rows, double* grad);
+
 /* fix layer (FixCoupLB hooks) */
 void*  ORC_FN(fix_create)(const couplb_fix_config* cfg, const couplb_domain* dom,
                           char* err, int errlen);
