@@ -25,6 +25,13 @@ PRECISIONS = {"fp64": FP64, "fp32": FP32_SHIFTED, "fp16": FP16_SHIFTED}
 DELTA_ROMA = 0
 DELTA_PESKIN4 = 1
 
+IBM_SINGLE = 0
+IBM_ITERATIVE = 1
+IBM_LEARNED = 2
+IBM_METHODS = {"single": IBM_SINGLE, "iterative": IBM_ITERATIVE, "learned": IBM_LEARNED}
+
+MLP_IN, MLP_HID, MLP_OUT, MLP_ROW, MLP_NPARAM = 84, 64, 3, 88, 9795
+
 G_NONE = 0
 G_CONSTANT = 1
 G_EQUAL = 2
@@ -55,6 +62,29 @@ class IbmParams(C.Structure):
         ("force_scale", C.c_double),
         ("domain_lo", C.c_double * 3),
         ("offset", C.c_int * 3),
+    ]
+
+
+class IbmMethod(C.Structure):
+    _fields_ = [
+        ("method", C.c_int),
+        ("passes", C.c_int),
+        ("slip_tol", C.c_double),
+        ("model", C.c_void_p),
+    ]
+
+
+class MlpTrainParams(C.Structure):
+    _fields_ = [
+        ("epochs", C.c_int),
+        ("batch", C.c_int),
+        ("lr", C.c_double),
+        ("lr_final", C.c_double),
+        ("beta1", C.c_double),
+        ("beta2", C.c_double),
+        ("eps", C.c_double),
+        ("seed", C.c_ulonglong),
+        ("n_val", C.c_longlong),
     ]
 
 

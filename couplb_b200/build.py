@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 LIB = os.path.join(HERE, "libcouplb_b200.so")
-SOURCES = ["engine.cu", "fix_core.cpp", "noalloc.cu"]
+SOURCES = ["engine.cu", "fix_core.cpp", "noalloc.cu", "mlp.cu"]
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo",
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -43,15 +43,32 @@ def nvcc():
 
 
 def build(force=False, verbose=False):
+    """Compile every source to an object in parallel (couplb_b200/_build),
+    then link the shared library."""
     if not force and not needs_build():
         return LIB
-    tmp = LIB + ".tmp"
-    cmd = [nvcc()] + NVCC_FLAGS + ["-o", tmp] + [os.path.join(CSRC, s) for s in SOURCES]
-    if verbose:
-        print(" ".join(cmd), flush=True)
+    obj_dir = os.path.join(HERE, "_build")
+    os.makedirs(obj_dir, exist_ok=True)
     env = dict(os.environ)
     env.pop("CC", None)
     env.pop("CXX", None)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    procs = []
+    objs = []
+    for src in SOURCES:
+        obj = os.path.join(obj_dir, os.path.splitext(src)[0] + ".o")
+        objs.append(obj)
+        cmd = [nvcc()] + compile_flags + ["-c", "-o", obj, os.path.join(CSRC, src)]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        procs.append((cmd, subprocess.Popen(cmd, cwd=CSRC, env=env)))
+    failed = [cmd for cmd, p in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
+    tmp = LIB + ".tmp"
+    cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp] + objs
+    if verbose:
+        print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True, cwd=CSRC, env=env)
     os.replace(tmp, LIB)
     return LIB

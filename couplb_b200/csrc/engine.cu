@@ -13,8 +13,10 @@
 #include "../../include/couplb_b200.h"
 #include "engine_internal.h"
 #include "ibm_kernels.cuh"
+#include "ibm_methods.cuh"
 #include "lbm_kernels.cuh"
 #include "lbm_packed.cuh"
+#include "mlp_internal.h"
 
 using namespace couplb;
 
@@ -118,7 +120,7 @@ int ensure_staging(couplb_handle* h, size_t bytes) {
 }
 
 // Stencil velocity records of the IBM sub-step, one per marker slot
-// (StencilKey + 64 x 3 values).  Keys start with epoch 0xffffffff, which
+// (StencilKey + 64 x {ux, uy, uz, rho}).  Keys start with epoch 0xffffffff, which
 // cur_epoch never takes, so a fresh record never hits.
 int ensure_stencil_cache(couplb_handle* h, int n) {
   if (h->stencil_cap >= n) return COUPLB_OK;
@@ -129,7 +131,7 @@ int ensure_stencil_cache(couplb_handle* h, int n) {
   h->stencil_cap = 0;
   const int cap = std::max(n, 1024);
   int rc;
-  if ((rc = dalloc(h, &h->sbuf, elem_bytes_aux(h->p.precision) * 64 * 3 * (size_t)cap))) return rc;
+  if ((rc = dalloc(h, &h->sbuf, elem_bytes_aux(h->p.precision) * kRecStride * (size_t)cap))) return rc;
   if ((rc = dalloc(h, (void**)&h->skey, sizeof(couplb::StencilKey) * (size_t)cap))) return rc;
   CK(cudaMemsetAsync(h->skey, 0xff, sizeof(couplb::StencilKey) * (size_t)cap, h->stream));
   h->stencil_cap = cap;
@@ -142,6 +144,25 @@ void bump_epoch(couplb_handle* h) {
     h->cur_epoch = 0;
     if (h->skey) cudaMemsetAsync(h->skey, 0xff, sizeof(couplb::StencilKey) * (size_t)h->stencil_cap, h->stream);
   }
+}
+
+// Per-marker buffers of the correction passes and their state block.
+int ensure_method_buffers(couplb_handle* h, int n) {
+  if (!h->d_pass) {
+    int rc = dalloc(h, &h->d_pass, sizeof(PassState));
+    if (rc) return rc;
+    CK(cudaMemsetAsync(h->d_pass, 0, sizeof(PassState), h->stream));
+  }
+  if (h->method_cap >= n) return COUPLB_OK;
+  void* p = h->d_corr; dfree(p); h->d_corr = nullptr;
+  p = h->d_dF; dfree(p); h->d_dF = nullptr;
+  h->method_cap = 0;
+  const int cap = std::max(n, 1024);
+  int rc;
+  if ((rc = dalloc(h, (void**)&h->d_corr, sizeof(double) * 3 * cap))) return rc;
+  if ((rc = dalloc(h, (void**)&h->d_dF, sizeof(double) * 3 * cap))) return rc;
+  h->method_cap = cap;
+  return COUPLB_OK;
 }
 
 int ensure_atoms(couplb_handle* h, int n) {
@@ -266,6 +287,8 @@ size_t couplb_struct_size(int which) {
     case 3: return sizeof(couplb_fix_config);
     case 4: return sizeof(couplb_domain);
     case 5: return sizeof(couplb_atoms);
+    case 6: return sizeof(couplb_ibm_method);
+    case 7: return sizeof(couplb_mlp_train_params);
     default: return 0;
   }
 }
@@ -355,6 +378,9 @@ int couplb_destroy(couplb_handle* h) {
   p = h->skey; dfree(p);
   dfree(h->sbuf);
   p = h->d_ftot; dfree(p);
+  p = h->d_corr; dfree(p);
+  p = h->d_dF; dfree(p);
+  dfree(h->d_pass);
   dfree(h->d_staging);
   dfree(h->d_scratch);
   dfree(h->d_x); dfree(h->d_v); dfree(h->d_m); dfree(h->d_fout); dfree(h->d_active);
@@ -491,6 +517,7 @@ int couplb_lbm_step(couplb_handle* h, const double* g_lb) {
     a.rho_mode = rho_mode;
     a.write_rho = h->p.body_force ? 2 : (h->moving_walls ? 1 : 0);
     for (int d = 0; d < 3; d++) a.grav[d] = g_active ? g_lb[d] : 0.0;
+    for (int d = 0; d < 3; d++) h->g_lb[d] = a.grav[d];
     a.omega = 1.0 / h->p.tau;
     a.status = h->d_status;
     // kernel choice: packed (shifted formats, pull, even nx, 32-bit indices),
@@ -738,24 +765,59 @@ int couplb_set_ibm_params(couplb_handle* h, const couplb_ibm_params* ip) {
 namespace couplb {
 
 // Shared body of the host- and device-array IBM sub-step.
+// Cooperative launch of the correction passes (all blocks resident at once,
+// which their grid barrier needs).
+template <class L, class S>
+int launch_passes(couplb_handle* h, PassArgs<S>& P, int delta, int n) {
+  void (*kern)(const PassArgs<S>) =
+      delta == COUPLB_DELTA_ROMA ? k_ibm_passes<L, S, 0> : k_ibm_passes<L, S, 1>;
+  int& resident = h->coop_blocks[delta == COUPLB_DELTA_ROMA ? 0 : 1][h->p.precision];
+  if (resident == 0) {
+    int coop = 0, sms = 0, per_sm = 0;
+    CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, h->p.device));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->p.device));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0));
+    if (!coop || per_sm < 1)
+      return fail(h, COUPLB_ERR_UNSUPPORTED, "the device cannot run the cooperative pass kernel");
+    resident = per_sm * sms;
+  }
+  const long long want = ((long long)n * 32 + 255) / 256;
+  const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(want, resident));
+  void* args[] = {&P};
+  CK(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(256), args, 0, h->stream));
+  return COUPLB_OK;
+}
+
 int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, const double* d_m,
                const int* d_active, double* d_fout, int accumulate, int refresh) {
   // no coupled atoms: the reference returns before refreshing the moments
   // (fix_couplb.cpp:750-753)
   if (n <= 0) return COUPLB_OK;
+  const couplb_ibm_params& ip = h->ip;
+  const int method = h->ibm_method;
+  if (method == COUPLB_IBM_LEARNED && (ip.delta != COUPLB_DELTA_ROMA || h->p.dim != 3 || !h->mlp))
+    return fail(h, COUPLB_ERR_UNSUPPORTED, "the learned correction needs D3Q19, the Roma kernel and a network");
   // The refresh of compute_macroscopic(false) (fix_couplb.cpp:757-760): the
   // velocities are computed on demand by the kernel; the density it would
   // store is what the next LB step's body force reads.
   if (refresh && h->p.body_force) h->rho_state = kRhoCurrent;
   int rc = ensure_stencil_cache(h, n);
   if (rc) return rc;
-  const couplb_ibm_params& ip = h->ip;
+  bool record = false;
+  if (method != COUPLB_IBM_SINGLE) {
+    if ((rc = ensure_method_buffers(h, n))) return rc;
+    if (h->rec_rows) {
+      if (d_active) return fail(h, COUPLB_ERR_STATE, "sample capture needs every atom coupled");
+      record = h->rec_count + n <= h->rec_cap;
+    }
+  }
   const double dxp = ip.dx;
   const double dv = (h->p.dim == 3) ? dxp * dxp * dxp : dxp * dxp;
   const double cell_vol = dxp * dxp * ((h->p.dim == 3) ? dxp : 1.0);
   const Geom g = make_geom(h);
   const int bs = 256;
   const unsigned nb = (unsigned)(((long long)n * 32 + bs - 1) / bs);
+  int lrc = COUPLB_OK;
   with_types(h->p.dim, h->p.precision, [&](auto l, auto s) {
     using L = decltype(l);
     using S = decltype(s);
@@ -767,6 +829,7 @@ int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, co
     a.pull = h->poststream ? 0 : 1;
     a.cux = (const A*)h->macro[1]; a.cuy = (const A*)h->macro[2]; a.cuz = (const A*)h->macro[3];
     a.all_valid = h->macro_valid;
+    a.crho = (const A*)h->macro[0];
     a.sbuf = (A*)h->sbuf;
     a.skey = h->skey;
     a.cur_epoch = h->cur_epoch;
@@ -785,11 +848,37 @@ int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, co
     a.vs = ip.vel_scale;
     a.fs = ip.force_scale;
     a.dvr = dv / cell_vol;
+    a.corr = method != COUPLB_IBM_SINGLE ? h->d_corr : nullptr;
+    a.mlp = (method == COUPLB_IBM_LEARNED) ? h->mlp->pack : nullptr;
     if (refresh && !a.all_valid) k_ibm_prefetch<L, S><<<nb, bs, 0, h->stream>>>(a);
-    if (ip.delta == COUPLB_DELTA_ROMA) k_ibm_substep<L, S, 0><<<nb, bs, 0, h->stream>>>(a);
-    else k_ibm_substep<L, S, 1><<<nb, bs, 0, h->stream>>>(a);
+    if (method == COUPLB_IBM_LEARNED) {
+      if constexpr (L::D == 3) k_ibm_substep_learned<L, S><<<nb, bs, kLearnedSmem, h->stream>>>(a);
+    } else if (ip.delta == COUPLB_DELTA_ROMA) {
+      k_ibm_substep<L, S, 0><<<nb, bs, 0, h->stream>>>(a);
+    } else {
+      k_ibm_substep<L, S, 1><<<nb, bs, 0, h->stream>>>(a);
+    }
+    if (method != COUPLB_IBM_SINGLE) {
+      if (cudaMemsetAsync(h->d_pass, 0, sizeof(PassState), h->stream) != cudaSuccess) {
+        lrc = fail(h, COUPLB_ERR_CUDA, "cudaMemsetAsync of the pass state failed");
+        return;
+      }
+      PassArgs<S> P;
+      P.a = a;
+      P.dF = h->d_dF;
+      P.ps = (PassState*)h->d_pass;
+      P.status = h->d_status;
+      P.ncorr = h->ibm_passes - 1;
+      P.check_first = method == COUPLB_IBM_LEARNED;
+      P.slip_tol = h->slip_tol;
+      for (int d = 0; d < 3; d++) P.g_lb[d] = h->g_lb[d];
+      P.rows = record ? h->rec_rows + h->rec_count * kMlpRow : nullptr;
+      lrc = launch_passes<L, S>(h, P, ip.delta, n);
+    }
   });
+  if (lrc) return lrc;
   CK_LAUNCH();
+  if (record) h->rec_count += n;
   h->force_dirty = 1;
   return COUPLB_OK;
 }
@@ -837,6 +926,78 @@ int couplb_ibm_substep_device(couplb_handle* h, int n, const double* d_x, const 
   int rc = set_device(h);
   if (rc) return rc;
   return engine_ibm(h, n, d_x, d_v, d_mass, d_active, d_f_add, 1, refresh);
+}
+
+int couplb_set_ibm_method(couplb_handle* h, const couplb_ibm_method* m) {
+  if (!h || !m) return COUPLB_ERR_ARG;
+  if (m->method < COUPLB_IBM_SINGLE || m->method > COUPLB_IBM_LEARNED)
+    return fail(h, COUPLB_ERR_ARG, "unknown IBM method %d", m->method);
+  if (m->passes < 1 || m->passes > 64) return fail(h, COUPLB_ERR_ARG, "passes must be 1..64");
+  if (m->method == COUPLB_IBM_LEARNED) {
+    if (!m->model) return fail(h, COUPLB_ERR_ARG, "the learned method needs a network");
+    if (h->p.dim != 3) return fail(h, COUPLB_ERR_UNSUPPORTED, "the learned correction is defined for D3Q19");
+    if (m->model->device != h->p.device)
+      return fail(h, COUPLB_ERR_ARG, "the network lives on device %d, the lattice on %d", m->model->device,
+                  h->p.device);
+    if (!(m->slip_tol >= 0.0)) return fail(h, COUPLB_ERR_ARG, "slip_tol must be >= 0");
+  }
+  h->ibm_method = m->method;
+  h->ibm_passes = m->passes;
+  h->slip_tol = m->slip_tol;
+  h->mlp = m->method == COUPLB_IBM_LEARNED ? m->model : nullptr;
+  return COUPLB_OK;
+}
+
+int couplb_ibm_slip(couplb_handle* h, double out[8], int reset) {
+  if (!h || !out) return COUPLB_ERR_ARG;
+  int rc = set_device(h);
+  if (rc) return rc;
+  for (int i = 0; i < 8; i++) out[i] = 0.0;
+  unsigned char* hs = (unsigned char*)h->h_small;
+  static_assert(sizeof(PassState) + 8 * sizeof(int) <= 4096, "h_small holds the pass state");
+  if (h->d_pass) CK(cudaMemcpyAsync(hs, h->d_pass, sizeof(PassState), cudaMemcpyDeviceToHost, h->stream));
+  else std::memset(hs, 0, sizeof(PassState));
+  int* st = (int*)(hs + sizeof(PassState));
+  CK(cudaMemcpyAsync(st, h->d_status, sizeof(int) * 8, cudaMemcpyDeviceToHost, h->stream));
+  if (reset) CK(cudaMemsetAsync(h->d_status + kStSlipChecks, 0, sizeof(int) * 2, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  PassState ps;
+  std::memcpy(&ps, hs, sizeof ps);
+  auto rms = [&](int r) {
+    double s = 0.0;
+    for (int i = 0; i < kSlipSlots; i++) s += ps.s2[r][i];
+    return ps.count[r] > 0 ? std::sqrt(s / ps.count[r]) : 0.0;
+  };
+  auto mx = [&](int r) {
+    double v;
+    std::memcpy(&v, &ps.max_bits[r], sizeof v);
+    return v;
+  };
+  const int r = (ps.checked && !ps.fell_back) ? 0 : 1;
+  out[0] = rms(r);
+  out[1] = mx(r);
+  out[2] = ps.checked ? rms(0) : 0.0;
+  out[3] = ps.checked ? mx(0) : 0.0;
+  out[4] = ps.count[r];
+  out[5] = ps.fell_back;
+  out[6] = st[kStSlipChecks];
+  out[7] = st[kStFallbacks];
+  return COUPLB_OK;
+}
+
+int couplb_ibm_record(couplb_handle* h, float* d_rows, long long capacity) {
+  if (!h) return COUPLB_ERR_ARG;
+  if (d_rows && capacity < 0) return fail(h, COUPLB_ERR_ARG, "negative capacity");
+  h->rec_rows = d_rows;
+  h->rec_cap = d_rows ? capacity : 0;
+  h->rec_count = 0;
+  return COUPLB_OK;
+}
+
+int couplb_ibm_record_count(couplb_handle* h, long long* rows) {
+  if (!h || !rows) return COUPLB_ERR_ARG;
+  *rows = h->rec_count;
+  return COUPLB_OK;
 }
 
 int couplb_ibm_total_force(couplb_handle* h, double out[3], int reset) {

@@ -58,6 +58,20 @@ struct couplb_handle {
   double* h_fout = nullptr;
   int atom_cap = 0;
 
+  // IBM forcing method (couplb_set_ibm_method)
+  int ibm_method = 0;                // COUPLB_IBM_*
+  int ibm_passes = 1;
+  double slip_tol = 0.0;
+  const couplb_mlp* mlp = nullptr;
+  double* d_corr = nullptr;          // per marker: correction beyond the penalty pass
+  double* d_dF = nullptr;            // per marker: increment of the current pass
+  int method_cap = 0;
+  void* d_pass = nullptr;            // couplb::PassState of the last sub-step
+  int coop_blocks[2][3] = {{0, 0, 0}, {0, 0, 0}};   // resident blocks of k_ibm_passes [delta][prec]
+  double g_lb[3] = {0.0, 0.0, 0.0};  // body force of the last LB step
+  float* rec_rows = nullptr;         // training-sample capture
+  long long rec_cap = 0, rec_count = 0;
+
   size_t device_bytes = 0;
   std::string err;
 };

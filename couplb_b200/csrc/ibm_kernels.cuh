@@ -19,6 +19,7 @@
 // stencils of markers that moved to another cell.
 #pragma once
 #include "lbm_kernels.cuh"
+#include "mlp_kernels.cuh"
 
 namespace couplb {
 
@@ -78,7 +79,8 @@ struct IbmArgs {
   const typename S::A* cuy;
   const typename S::A* cuz;
   int all_valid;
-  // stencil velocity records, one per marker slot (64 x 3 values each)
+  const typename S::A* crho;              // with all_valid: density (deviation if shifted)
+  // stencil velocity records, one per marker slot (64 x {ux, uy, uz, rho})
   typename S::A* sbuf;
   StencilKey* skey;
   unsigned cur_epoch;
@@ -95,6 +97,9 @@ struct IbmArgs {
   double lo[3];
   int off[3];
   double inv_dx, xi_over_dt, inv_N, vs, fs, dvr;
+  // forcing methods beyond the single pass (null / unused otherwise)
+  double* corr;                           // n*3: correction beyond the penalty pass
+  const MlpPacked* mlp;                   // learned correction network
 };
 
 // Add a spread force to one node of the interleaved force field: one vector
@@ -133,7 +138,7 @@ __device__ __forceinline__ int classify_node(const Geom& g, int D, int ig, int j
 template <class L, class S>
 __device__ __forceinline__ void compute_velocity(const IbmArgs<S>& a, int i, int j, int k, size_t n,
                                                  typename S::A& v0, typename S::A& v1,
-                                                 typename S::A& v2) {
+                                                 typename S::A& v2, typename S::A& vr) {
   using C = typename S::C;
   C f[L::Q];
   if (a.pull) load_node<L, S, size_t, true>(a.g, a.fin, a.rho_field, i, j, k, n, f);
@@ -146,6 +151,7 @@ __device__ __forceinline__ void compute_velocity(const IbmArgs<S>& a, int i, int
   v0 = typename S::A(jx * inv_r);
   v1 = typename S::A(jy * inv_r);
   v2 = typename S::A(jz * inv_r);
+  vr = typename S::A(rho);
 }
 
 // Stencil velocity cache: one record per marker slot holding the velocities of
@@ -155,10 +161,13 @@ __device__ __forceinline__ void compute_velocity(const IbmArgs<S>& a, int i, int
 // marker that moved to another cell since the refresh (or a slot filled by a
 // different atom) misses and computes its nodes directly.  Records are
 // contiguous (64 x 3 values), so a sub-step reads its marker's stencil as a
-// few full cache lines that stay in L2 across the sub-steps of a cycle.
+// few full cache lines that stay in L2 across the sub-steps of a cycle.  The
+// density (kept for the corrected velocity of the iterative passes) follows
+// the three velocity components.
+constexpr int kRecStride = 64 * 4;
 template <class S>
 __device__ __forceinline__ typename S::A* stencil_record(const IbmArgs<S>& a, int mk) {
-  return a.sbuf + (size_t)mk * (64 * 3);
+  return a.sbuf + (size_t)mk * kRecStride;
 }
 
 // Refresh prefetch: one warp per active marker fills its slot's record.
@@ -184,14 +193,14 @@ __global__ void __launch_bounds__(256) k_ibm_prefetch(const IbmArgs<S> a) {
     const int ig = i0 - 1 + (s & 3);
     const int jg = j0 - 1 + ((s >> 2) & 3);
     const int kg = (L::D == 3) ? k0 - 1 + (s >> 4) : 0;
-    typename S::A v0 = 0, v1 = 0, v2 = 0;
+    typename S::A v0 = 0, v1 = 0, v2 = 0, vr = 1;
     int ii = 0, jj = 0, kk = 0;
     if (ig >= 0 && ig < gx && jg >= 0 && jg < gy && kg >= 0 && kg < gz &&
         classify_node(g, L::D, ig, jg, kg, ii, jj, kk) < 0) {
       const size_t n = (size_t)ii + (size_t)g.nx * ((size_t)jj + (size_t)g.ny * kk);
-      compute_velocity<L, S>(a, ii, jj, kk, n, v0, v1, v2);
+      compute_velocity<L, S>(a, ii, jj, kk, n, v0, v1, v2, vr);
     }
-    rec[s] = v0; rec[64 + s] = v1; rec[128 + s] = v2;
+    rec[s] = v0; rec[64 + s] = v1; rec[128 + s] = v2; rec[192 + s] = vr;
   }
   if (lane == 0) a.skey[mk] = StencilKey{i0, j0, k0, a.cur_epoch};
 }
@@ -206,16 +215,40 @@ __device__ __forceinline__ void node_velocity(const IbmArgs<S>& a, bool hit,
   } else if (hit) {
     u0 = double(rec[s]); u1 = double(rec[64 + s]); u2 = double(rec[128 + s]);
   } else {
-    typename S::A v0, v1, v2;
-    compute_velocity<L, S>(a, i, j, k, n, v0, v1, v2);
+    typename S::A v0, v1, v2, vr;
+    compute_velocity<L, S>(a, i, j, k, n, v0, v1, v2, vr);
     u0 = double(v0); u1 = double(v1); u2 = double(v2);
+  }
+}
+
+// Velocity and density of stencil slot s (the iterative passes).
+template <class L, class S>
+__device__ __forceinline__ void node_state(const IbmArgs<S>& a, bool hit, const typename S::A* rec,
+                                           int s, int i, int j, int k, size_t n, double& u0,
+                                           double& u1, double& u2, double& rho) {
+  if (a.all_valid) {
+    u0 = double(a.cux[n]); u1 = double(a.cuy[n]); u2 = double(a.cuz[n]);
+    rho = S::kShift ? a.g.rho0 + double(a.crho[n]) : double(a.crho[n]);
+  } else if (hit) {
+    u0 = double(rec[s]); u1 = double(rec[64 + s]); u2 = double(rec[128 + s]);
+    rho = double(rec[192 + s]);
+  } else {
+    typename S::A v0, v1, v2, vr;
+    compute_velocity<L, S>(a, i, j, k, n, v0, v1, v2, vr);
+    u0 = double(v0); u1 = double(v1); u2 = double(v2); rho = double(vr);
   }
 }
 
 // Weight arithmetic in the storage's compute type: FP64 for the parity form,
 // FP32 for the shifted forms.  Sums are carried in FP64 either way.
-template <class L, class S, int DELTA>
-__global__ void __launch_bounds__(256) k_ibm_substep(const IbmArgs<S> a) {
+//
+// LEARNED (D3Q19, Roma): the lanes also gather the network input (u0 at the 27
+// nodes round(l)-1..round(l)+1 of each axis, then v / vel_scale) into the
+// warp's shared scratch xs, the warp runs the correction network, and the
+// marker force F = F_penalty + m xi/dt vs y is returned and spread.
+template <class L, class S, int DELTA, bool LEARNED>
+__device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, const MlpPacked* P,
+                                                 float* xs, float* hs) {
   using R = typename S::C;
   const int mk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -234,6 +267,15 @@ __global__ void __launch_bounds__(256) k_ibm_substep(const IbmArgs<S> a) {
   const int k0 = (L::D == 3) ? (int)floor(lz) : 0;
   const int gx = g.nx + 2, gy = g.ny + 2, gz = (L::D == 3) ? g.nz + 2 : 1;
   constexpr int NS = (L::D == 3) ? 64 : 16;
+  // first node of the 27-node network window, in window coordinates
+  int ox = 0, oy = 0, oz = 0;
+  if (LEARNED) {
+    ox = (lx - i0) >= 0.5 ? 1 : 0;
+    oy = (ly - j0) >= 0.5 ? 1 : 0;
+    oz = (lz - k0) >= 0.5 ? 1 : 0;
+    for (int t = lane; t < kMlpIn; t += 32) xs[t] = 0.f;
+    __syncwarp();
+  }
 
   double ui = 0, vi = 0, wi = 0, ws = 0, wss = 0;
   long long sn0 = -1, sn1 = -1;   // fluid nodes of this lane (interior index)
@@ -255,6 +297,12 @@ __global__ void __launch_bounds__(256) k_ibm_substep(const IbmArgs<S> a) {
     int ii = 0, jj = 0, kk = 0;
     const int t = classify_node(g, L::D, ig, jg, kg, ii, jj, kk);
     const double dd = double(d);
+    // slot of this node in the network input, or -1
+    int p = -1;
+    if (LEARNED) {
+      const int rx = (s & 3) - ox, ry = ((s >> 2) & 3) - oy, rz = (s >> 4) - oz;
+      if (rx >= 0 && rx < 3 && ry >= 0 && ry < 3 && rz >= 0 && rz < 3) p = rx + 3 * ry + 9 * rz;
+    }
     if (t < 0) {
       const size_t src = (size_t)ii + (size_t)g.nx * ((size_t)jj + (size_t)g.ny * kk);
       double u0, u1, u2;
@@ -266,6 +314,7 @@ __global__ void __launch_bounds__(256) k_ibm_substep(const IbmArgs<S> a) {
       wss += dd;
       if (rep == 0) { sn0 = (long long)src; sd0 = dd; row0 = jj + g.ny * kk; }
       else { sn1 = (long long)src; sd1 = dd; row1 = jj + g.ny * kk; }
+      if (LEARNED && p >= 0) { xs[3 * p] = float(u0); xs[3 * p + 1] = float(u1); xs[3 * p + 2] = float(u2); }
     } else if (t == 1 || t == 3) {
       ws += dd;
     } else if (t == 2) {
@@ -273,6 +322,9 @@ __global__ void __launch_bounds__(256) k_ibm_substep(const IbmArgs<S> a) {
       vi += g.uw[1] * dd;
       wi += (L::D == 3 ? g.uw[2] : 0.0) * dd;
       ws += dd;
+      if (LEARNED && p >= 0) {
+        xs[3 * p] = float(g.uw[0]); xs[3 * p + 1] = float(g.uw[1]); xs[3 * p + 2] = float(g.uw[2]);
+      }
     }
   }
 #pragma unroll
@@ -290,9 +342,21 @@ __global__ void __launch_bounds__(256) k_ibm_substep(const IbmArgs<S> a) {
   }
   // penalty force (fix_couplb.cpp:777-781)
   const double mass = a.m[mk];
-  const double F0 = mass * a.xi_over_dt * (u0 * a.vs - a.v[3 * mk]);
-  const double F1 = mass * a.xi_over_dt * (u1 * a.vs - a.v[3 * mk + 1]);
-  const double F2 = mass * a.xi_over_dt * (u2 * a.vs - a.v[3 * mk + 2]);
+  double F0 = mass * a.xi_over_dt * (u0 * a.vs - a.v[3 * mk]);
+  double F1 = mass * a.xi_over_dt * (u1 * a.vs - a.v[3 * mk + 1]);
+  double F2 = mass * a.xi_over_dt * (u2 * a.vs - a.v[3 * mk + 2]);
+  if (LEARNED) {
+    if (lane < 3) xs[81 + lane] = float(a.v[3 * mk + lane] / a.vs);
+    __syncwarp();
+    float y[3];
+    mlp_warp_forward(*P, xs, hs, lane, y);
+    const double sc = mass * a.xi_over_dt * a.vs;
+    const double c0 = sc * double(y[0]), c1 = sc * double(y[1]), c2 = sc * double(y[2]);
+    F0 += c0; F1 += c1; F2 += c2;
+    if (lane == 0 && a.corr) { a.corr[3 * mk] = c0; a.corr[3 * mk + 1] = c1; a.corr[3 * mk + 2] = c2; }
+  } else if (lane == 0 && a.corr) {
+    a.corr[3 * mk] = 0.0; a.corr[3 * mk + 1] = 0.0; a.corr[3 * mk + 2] = 0.0;
+  }
   if (lane == 0) {
     if (a.accumulate) {
       a.fout[3 * mk] += F0; a.fout[3 * mk + 1] += F1; a.fout[3 * mk + 2] += F2;
@@ -322,6 +386,28 @@ __global__ void __launch_bounds__(256) k_ibm_substep(const IbmArgs<S> a) {
     atomicAdd(t + 1, fl1 * a.dvr);
     atomicAdd(t + 2, fl2 * a.dvr);
   }
+}
+
+template <class L, class S, int DELTA>
+__global__ void __launch_bounds__(256) k_ibm_substep(const IbmArgs<S> a) {
+  ibm_substep_body<L, S, DELTA, false>(a, nullptr, nullptr, nullptr);
+}
+
+// Per-warp shared scratch of the learned sub-step: 84 inputs + 64 hidden.
+constexpr int kMlpWarpScratch = kMlpIn + kMlpHid;
+constexpr size_t kLearnedSmem = sizeof(MlpPacked) + 8 * kMlpWarpScratch * sizeof(float);
+
+// The reference pass with the fused network correction (D3Q19, Roma; blocks
+// of 256 threads, dynamic shared memory kLearnedSmem).
+template <class L, class S>
+__global__ void __launch_bounds__(256) k_ibm_substep_learned(const IbmArgs<S> a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  MlpPacked* P = reinterpret_cast<MlpPacked*>(smem);
+  float* scratch = reinterpret_cast<float*>(smem + sizeof(MlpPacked));
+  mlp_stage(P, a.mlp);
+  __syncthreads();
+  float* xs = scratch + (threadIdx.x >> 5) * kMlpWarpScratch;
+  ibm_substep_body<L, S, 0, true>(a, P, xs, xs + kMlpIn);
 }
 
 }  // namespace couplb

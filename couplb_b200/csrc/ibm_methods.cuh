@@ -1,0 +1,349 @@
+// ibm_methods.cuh -- IBM forcing beyond the single penalty pass: the
+// iterative (multi-direct forcing) corrections, the slip residual that judges
+// the learned correction, and the training-sample capture.
+//
+// No counterpart in the reference, which applies one penalty pass.  The
+// definitions (restated on the CPU by the oracle):
+//   u_corr(x) = u0(x) + (G(x)/rho(x) + g_lb)/2 at fluid nodes: u0 and rho of
+//               the refresh, G the IBM force field so far, g_lb the body force;
+//   U_i       = the reference's interpolation of u_corr (couplb_ibm.h:57-90);
+//   dF_i      = m xi/dt (U_i vs - v_i), added to the atom and spread as
+//               -dF_i/(N fs) with the reference's spread weights; all dF_i of
+//               a pass are formed before any is spread (Jacobi);
+//   slip_i    = |U_i vs - v_i| after the last pass.
+//
+// One cooperative launch runs every pass of a sub-step: warps loop over the
+// markers, and a grid-wide barrier (bounded wait, error flag on timeout)
+// separates "form all dF" from "spread all dF".  The learned method measures
+// the slip first and runs the corrections only when its RMS exceeds the
+// tolerance, so the fallback costs nothing when the network is good enough.
+#pragma once
+#include "ibm_kernels.cuh"
+
+namespace couplb {
+
+constexpr int kSlipSlots = 32;
+// status words (cumulative until reset): slip checks made, fallbacks taken
+enum : int { kStSlipChecks = 4, kStFallbacks = 5 };
+constexpr long long kBarrierSpin = 1LL << 21;   // x ~100 ns sleeps
+
+// Zeroed before every launch of k_ibm_passes.
+struct PassState {
+  unsigned bar_count, bar_gen;
+  int fell_back;                    // the learned method ran the corrections
+  int checked;                      // a slip check ran
+  unsigned long long max_bits[2];   // max slip (non-negative double bits): [0] check, [1] final
+  int count[2];
+  double s2[2][kSlipSlots];         // slip^2 sums, striped by marker index
+};
+
+template <class S>
+struct PassArgs {
+  IbmArgs<S> a;
+  double* dF;           // n*3: the increment of the current pass
+  PassState* ps;
+  int* status;
+  int ncorr;            // iterative corrections (passes - 1)
+  int check_first;      // learned: slip check first, corrections only above tol
+  double slip_tol;      // MD velocity units
+  double g_lb[3];       // body force of the LB steps, lattice units
+  float* rows;          // n x kMlpRow training rows, or null
+};
+
+// Grid-wide barrier of a cooperative launch.  Returns false (and counts a
+// timeout) if the other blocks did not arrive within the spin limit.
+__device__ __forceinline__ bool grid_barrier(PassState* ps, int* status) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = &ps->bar_gen;
+    const unsigned g0 = *gen;
+    __threadfence();
+    int good = 1;
+    if (atomicAdd(&ps->bar_count, 1u) + 1 == gridDim.x) {
+      atomicExch(&ps->bar_count, 0u);
+      __threadfence();
+      atomicAdd(&ps->bar_gen, 1u);
+    } else {
+      long long it = 0;
+      while (*gen == g0) {
+        if (++it > kBarrierSpin) {
+          good = 0;
+          if (status) atomicAdd(status + kStTimeout, 1);
+          break;
+        }
+        __nanosleep(100);
+      }
+    }
+    __threadfence();
+    ok = good;
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+__device__ __forceinline__ void load_force(const float* F, size_t n, double G[3]) {
+  const float4 v = __ldcg(reinterpret_cast<const float4*>(F + 4 * n));
+  G[0] = v.x; G[1] = v.y; G[2] = v.z;
+}
+__device__ __forceinline__ void load_force(const double* F, size_t n, double G[3]) {
+  G[0] = __ldcg(F + 4 * n); G[1] = __ldcg(F + 4 * n + 1); G[2] = __ldcg(F + 4 * n + 2);
+}
+
+// Marker window of the reference (couplb_ibm.h:62-86).
+struct MarkerWindow {
+  double lx, ly, lz;
+  int i0, j0, k0;
+};
+
+template <class L, class S>
+__device__ __forceinline__ MarkerWindow marker_window(const IbmArgs<S>& a, int mk) {
+  MarkerWindow w;
+  w.lx = (a.x[3 * mk] - a.lo[0]) * a.inv_dx - a.off[0] + 1.0;
+  w.ly = (a.x[3 * mk + 1] - a.lo[1]) * a.inv_dx - a.off[1] + 1.0;
+  w.lz = (L::D == 3) ? ((a.x[3 * mk + 2] - a.lo[2]) * a.inv_dx - a.off[2] + 1.0) : 0.0;
+  w.i0 = (int)floor(w.lx);
+  w.j0 = (int)floor(w.ly);
+  w.k0 = (L::D == 3) ? (int)floor(w.lz) : 0;
+  return w;
+}
+
+// Interpolated u_corr of marker mk (every lane returns it).
+template <class L, class S, int DELTA>
+__device__ __forceinline__ void interp_corr(const PassArgs<S>& P, int mk, int lane, double U[3]) {
+  using R = typename S::C;
+  const IbmArgs<S>& a = P.a;
+  const Geom& g = a.g;
+  const MarkerWindow w = marker_window<L, S>(a, mk);
+  const int gx = g.nx + 2, gy = g.ny + 2, gz = (L::D == 3) ? g.nz + 2 : 1;
+  constexpr int NS = (L::D == 3) ? 64 : 16;
+  const StencilKey key = a.skey[mk];
+  const bool hit = key.epoch == a.cur_epoch && key.i0 == w.i0 && key.j0 == w.j0 && key.k0 == w.k0;
+  const typename S::A* rec = stencil_record(a, mk);
+  double ui = 0, vi = 0, wi = 0, ws = 0;
+#pragma unroll
+  for (int rep = 0; rep < 2; rep++) {
+    const int s = lane + 32 * rep;
+    if (s >= NS) break;
+    const int ig = w.i0 - 1 + (s & 3);
+    const int jg = w.j0 - 1 + ((s >> 2) & 3);
+    const int kg = (L::D == 3) ? w.k0 - 1 + (s >> 4) : 0;
+    if (ig < 0 || ig >= gx || jg < 0 || jg >= gy || kg < 0 || kg >= gz) continue;
+    R d = delta1<DELTA, R>(R(w.lx - ig)) * delta1<DELTA, R>(R(w.ly - jg));
+    if (L::D == 3) d *= delta1<DELTA, R>(R(w.lz - kg));
+    const double dd = double(d);
+    int ii = 0, jj = 0, kk = 0;
+    const int t = classify_node(g, L::D, ig, jg, kg, ii, jj, kk);
+    if (t < 0) {
+      const size_t n = (size_t)ii + (size_t)g.nx * ((size_t)jj + (size_t)g.ny * kk);
+      double u0, u1, u2, rho;
+      node_state<L, S>(a, hit, rec, s, ii, jj, kk, n, u0, u1, u2, rho);
+      double G[3];
+      load_force(a.F, n, G);
+      const double ir = 1.0 / rho;
+      u0 = u0 + 0.5 * (G[0] * ir + P.g_lb[0]);
+      u1 = u1 + 0.5 * (G[1] * ir + P.g_lb[1]);
+      u2 = u2 + 0.5 * (G[2] * ir + (L::D == 3 ? P.g_lb[2] : 0.0));
+      ui += u0 * dd; vi += u1 * dd; wi += u2 * dd; ws += dd;
+    } else if (t == 1 || t == 3) {
+      ws += dd;
+    } else if (t == 2) {
+      ui += g.uw[0] * dd; vi += g.uw[1] * dd; wi += (L::D == 3 ? g.uw[2] : 0.0) * dd; ws += dd;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ui += __shfl_xor_sync(0xffffffffu, ui, o);
+    vi += __shfl_xor_sync(0xffffffffu, vi, o);
+    wi += __shfl_xor_sync(0xffffffffu, wi, o);
+    ws += __shfl_xor_sync(0xffffffffu, ws, o);
+  }
+  if (ws > DELTA_TOL) {
+    const double iw = 1.0 / ws;
+    U[0] = ui * iw; U[1] = vi * iw; U[2] = wi * iw;
+  } else {
+    U[0] = U[1] = U[2] = 0.0;
+  }
+}
+
+// Spread -dF/(N fs) of marker mk with the reference's weights
+// (couplb_ibm.h:92-133).
+template <class L, class S, int DELTA>
+__device__ __forceinline__ void spread_marker(const IbmArgs<S>& a, int mk, int lane,
+                                              const double dF[3]) {
+  using R = typename S::C;
+  const Geom& g = a.g;
+  const MarkerWindow w = marker_window<L, S>(a, mk);
+  const int gx = g.nx + 2, gy = g.ny + 2, gz = (L::D == 3) ? g.nz + 2 : 1;
+  constexpr int NS = (L::D == 3) ? 64 : 16;
+  long long sn0 = -1, sn1 = -1;
+  double sd0 = 0.0, sd1 = 0.0;
+  int row0 = 0, row1 = 0;
+  double wss = 0.0;
+#pragma unroll
+  for (int rep = 0; rep < 2; rep++) {
+    const int s = lane + 32 * rep;
+    if (s >= NS) break;
+    const int ig = w.i0 - 1 + (s & 3);
+    const int jg = w.j0 - 1 + ((s >> 2) & 3);
+    const int kg = (L::D == 3) ? w.k0 - 1 + (s >> 4) : 0;
+    if (ig < 0 || ig >= gx || jg < 0 || jg >= gy || kg < 0 || kg >= gz) continue;
+    int ii = 0, jj = 0, kk = 0;
+    if (classify_node(g, L::D, ig, jg, kg, ii, jj, kk) >= 0) continue;
+    R d = delta1<DELTA, R>(R(w.lx - ig)) * delta1<DELTA, R>(R(w.ly - jg));
+    if (L::D == 3) d *= delta1<DELTA, R>(R(w.lz - kg));
+    const double dd = double(d);
+    wss += dd;
+    const long long nn = (long long)((size_t)ii + (size_t)g.nx * ((size_t)jj + (size_t)g.ny * kk));
+    if (rep == 0) { sn0 = nn; sd0 = dd; row0 = jj + g.ny * kk; }
+    else { sn1 = nn; sd1 = dd; row1 = jj + g.ny * kk; }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) wss += __shfl_xor_sync(0xffffffffu, wss, o);
+  if (wss < DELTA_TOL) return;
+  const double sc = a.dvr / wss;
+  const double fl0 = -dF[0] * a.inv_N / a.fs, fl1 = -dF[1] * a.inv_N / a.fs;
+  const double fl2 = -dF[2] * a.inv_N / a.fs;
+  if (sn0 >= 0) {
+    const double wgt = sd0 * sc;
+    spread_add(a.F + 4 * sn0, fl0 * wgt, fl1 * wgt, fl2 * wgt);
+    if (a.row_force) a.row_force[row0] = 1;
+  }
+  if (sn1 >= 0) {
+    const double wgt = sd1 * sc;
+    spread_add(a.F + 4 * sn1, fl0 * wgt, fl1 * wgt, fl2 * wgt);
+    if (a.row_force) a.row_force[row1] = 1;
+  }
+  if (lane == 0 && a.ftot) {
+    double* t = a.ftot + 4 * (mk & (kFtotSlots - 1));
+    atomicAdd(t, fl0 * a.dvr);
+    atomicAdd(t + 1, fl1 * a.dvr);
+    atomicAdd(t + 2, fl2 * a.dvr);
+  }
+}
+
+// Slip of marker mk into residual r of the pass state.
+template <class L, class S, int DELTA>
+__device__ __forceinline__ void measure_marker(const PassArgs<S>& P, int mk, int lane, int r) {
+  double U[3];
+  interp_corr<L, S, DELTA>(P, mk, lane, U);
+  if (lane == 0) {
+    const IbmArgs<S>& a = P.a;
+    double e2 = 0.0;
+    for (int c = 0; c < 3; c++) {
+      const double e = U[c] * a.vs - a.v[3 * mk + c];
+      e2 += e * e;
+    }
+    atomicAdd(&P.ps->s2[r][mk & (kSlipSlots - 1)], e2);
+    atomicMax(&P.ps->max_bits[r], (unsigned long long)__double_as_longlong(sqrt(e2)));
+    atomicAdd(&P.ps->count[r], 1);
+  }
+}
+
+__device__ __forceinline__ double slip_rms(const PassState* ps, int r) {
+  double s = 0.0;
+  for (int i = 0; i < kSlipSlots; i++) s += __ldcg(&ps->s2[r][i]);
+  const int c = __ldcg(&ps->count[r]);
+  return c > 0 ? sqrt(s / c) : 0.0;
+}
+
+// Training row of marker mk: network input, then the correction beyond the
+// penalty pass over (m xi vs / dt), lattice velocity units, then 0.
+template <class L, class S>
+__device__ __forceinline__ void record_marker(const PassArgs<S>& P, int mk, int lane) {
+  const IbmArgs<S>& a = P.a;
+  const Geom& g = a.g;
+  float* row = P.rows + (size_t)mk * kMlpRow;
+  for (int t = lane; t < kMlpRow; t += 32) row[t] = 0.f;
+  __syncwarp();
+  if (L::D != 3) return;
+  const MarkerWindow w = marker_window<L, S>(a, mk);
+  const int ox = (w.lx - w.i0) >= 0.5 ? 1 : 0, oy = (w.ly - w.j0) >= 0.5 ? 1 : 0;
+  const int oz = (w.lz - w.k0) >= 0.5 ? 1 : 0;
+  const int gx = g.nx + 2, gy = g.ny + 2, gz = g.nz + 2;
+  const StencilKey key = a.skey[mk];
+  const bool hit = key.epoch == a.cur_epoch && key.i0 == w.i0 && key.j0 == w.j0 && key.k0 == w.k0;
+  const typename S::A* rec = stencil_record(a, mk);
+  if (lane < 27) {
+    const int rx = lane % 3, ry = (lane / 3) % 3, rz = lane / 9;
+    const int s = (rx + ox) + 4 * (ry + oy) + 16 * (rz + oz);   // window slot
+    const int ig = w.i0 - 1 + rx + ox, jg = w.j0 - 1 + ry + oy, kg = w.k0 - 1 + rz + oz;
+    if (ig >= 0 && ig < gx && jg >= 0 && jg < gy && kg >= 0 && kg < gz) {
+      int ii = 0, jj = 0, kk = 0;
+      const int t = classify_node(g, 3, ig, jg, kg, ii, jj, kk);
+      if (t < 0) {
+        const size_t n = (size_t)ii + (size_t)g.nx * ((size_t)jj + (size_t)g.ny * kk);
+        double u0, u1, u2;
+        node_velocity<L, S>(a, hit, rec, s, ii, jj, kk, n, u0, u1, u2);
+        row[3 * lane] = float(u0); row[3 * lane + 1] = float(u1); row[3 * lane + 2] = float(u2);
+      } else if (t == 2) {
+        row[3 * lane] = float(g.uw[0]); row[3 * lane + 1] = float(g.uw[1]);
+        row[3 * lane + 2] = float(g.uw[2]);
+      }
+    }
+  } else if (lane < 30) {
+    const int c = lane - 27;
+    row[81 + c] = float(a.v[3 * mk + c] / a.vs);
+    row[kMlpIn + c] = float(a.corr[3 * mk + c] / (a.m[mk] * a.xi_over_dt * a.vs));
+  }
+}
+
+// All passes after the first of one sub-step (cooperative launch, blocks of
+// 256 threads, at most as many blocks as fit on the device at once).
+template <class L, class S, int DELTA>
+__global__ void __launch_bounds__(256) k_ibm_passes(const PassArgs<S> P) {
+  const IbmArgs<S>& a = P.a;
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  if (P.check_first) {
+    for (int mk = gw; mk < a.n; mk += nw)
+      if (!a.active || a.active[mk]) measure_marker<L, S, DELTA>(P, mk, lane, 0);
+    if (!grid_barrier(P.ps, P.status)) return;
+    const bool fall = slip_rms(P.ps, 0) > P.slip_tol;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      P.ps->checked = 1;
+      if (P.status) atomicAdd(P.status + kStSlipChecks, 1);
+      if (fall) {
+        P.ps->fell_back = 1;
+        if (P.status) atomicAdd(P.status + kStFallbacks, 1);
+      }
+    }
+    if (!fall) {
+      if (P.rows)
+        for (int mk = gw; mk < a.n; mk += nw) record_marker<L, S>(P, mk, lane);
+      return;
+    }
+  }
+  for (int it = 0; it < P.ncorr; it++) {
+    for (int mk = gw; mk < a.n; mk += nw) {
+      if (a.active && !a.active[mk]) continue;
+      double U[3];
+      interp_corr<L, S, DELTA>(P, mk, lane, U);
+      if (lane == 0) {
+        const double c = a.m[mk] * a.xi_over_dt;
+        for (int d = 0; d < 3; d++) {
+          const double dF = c * (U[d] * a.vs - a.v[3 * mk + d]);
+          P.dF[3 * mk + d] = dF;
+          a.fout[3 * mk + d] += dF;
+          a.corr[3 * mk + d] += dF;
+        }
+      }
+    }
+    if (!grid_barrier(P.ps, P.status)) return;
+    for (int mk = gw; mk < a.n; mk += nw) {
+      if (a.active && !a.active[mk]) continue;
+      const double dF[3] = {__ldcg(P.dF + 3 * mk), __ldcg(P.dF + 3 * mk + 1),
+                            __ldcg(P.dF + 3 * mk + 2)};
+      spread_marker<L, S, DELTA>(a, mk, lane, dF);
+    }
+    if (!grid_barrier(P.ps, P.status)) return;
+  }
+  for (int mk = gw; mk < a.n; mk += nw) {
+    if (a.active && !a.active[mk]) continue;
+    measure_marker<L, S, DELTA>(P, mk, lane, 1);
+    if (P.rows) record_marker<L, S>(P, mk, lane);
+  }
+}
+
+}  // namespace couplb

@@ -160,6 +160,34 @@ class Lattice:
                                                   C.c_void_p(m_ptr), C.c_void_p(active_ptr or None),
                                                   C.c_void_p(f_ptr), int(refresh)))
 
+    def set_ibm_method(self, method="single", passes=1, slip_tol=0.0, model=None):
+        """IBM forcing method: "single" (the reference's pass), "iterative"
+        (passes-1 correction passes) or "learned" (network correction with the
+        iterative fallback above slip_tol); model: a CorrectionNet."""
+        m = abi.IbmMethod()
+        m.method = abi.IBM_METHODS[method] if isinstance(method, str) else int(method)
+        m.passes, m.slip_tol = int(passes), float(slip_tol)
+        m.model = model.h if model is not None else None
+        self._ck(self.L.couplb_set_ibm_method(self.h, C.byref(m)))
+        self._model = model
+
+    def ibm_slip(self, reset=False):
+        """dict of the last slip measurement (synchronises)."""
+        out = np.zeros(8)
+        self._ck(self.L.couplb_ibm_slip(self.h, abi.dptr(out), int(reset)))
+        keys = ["rms", "max", "check_rms", "check_max", "markers", "fell_back", "checks",
+                "fallbacks"]
+        return dict(zip(keys, out.tolist()))
+
+    def ibm_record(self, rows_ptr, capacity):
+        """Capture training rows into device memory (pointer, rows); 0 stops."""
+        self._ck(self.L.couplb_ibm_record(self.h, C.c_void_p(rows_ptr or None), int(capacity)))
+
+    def ibm_record_count(self):
+        v = C.c_longlong(0)
+        self._ck(self.L.couplb_ibm_record_count(self.h, C.byref(v)))
+        return v.value
+
     def ibm_total_force(self, reset=False):
         out = np.zeros(3)
         self._ck(self.L.couplb_ibm_total_force(self.h, abi.dptr(out), int(reset)))

@@ -46,6 +46,23 @@ SIGNATURES = {
                                             C.c_void_p, C.c_void_p, C.c_int]),
     "couplb_ibm_total_force": (C.c_int, [_H, _D, C.c_int]),
     "couplb_read_status": (C.c_int, [_H, _I, _I, C.c_int]),
+    "couplb_set_ibm_method": (C.c_int, [_H, C.POINTER(abi.IbmMethod)]),
+    "couplb_ibm_slip": (C.c_int, [_H, _D, C.c_int]),
+    "couplb_ibm_record": (C.c_int, [_H, C.c_void_p, C.c_longlong]),
+    "couplb_ibm_record_count": (C.c_int, [_H, C.POINTER(C.c_longlong)]),
+    "couplb_mlp_create": (C.c_int, [C.c_int, C.c_ulonglong, C.POINTER(_H)]),
+    "couplb_mlp_destroy": (C.c_int, [_H]),
+    "couplb_mlp_last_error": (C.c_char_p, [_H]),
+    "couplb_mlp_set_stream": (C.c_int, [_H, C.c_void_p]),
+    "couplb_mlp_set_weights": (C.c_int, [_H, C.c_void_p, C.c_double, C.c_double]),
+    "couplb_mlp_get_weights": (C.c_int, [_H, C.c_void_p, _D, _D]),
+    "couplb_mlp_fit_scales": (C.c_int, [_H, C.c_void_p, C.c_longlong]),
+    "couplb_mlp_forward": (C.c_int, [_H, C.c_void_p, C.c_longlong, C.c_void_p]),
+    "couplb_mlp_loss_grad": (C.c_int, [_H, C.c_void_p, C.c_longlong, _D, C.c_void_p]),
+    "couplb_mlp_train": (C.c_int, [_H, C.c_void_p, C.c_longlong, C.POINTER(abi.MlpTrainParams),
+                                   _D, _D]),
+    "couplb_mlp_save": (C.c_int, [_H, C.c_char_p]),
+    "couplb_mlp_load": (C.c_int, [_H, C.c_char_p]),
     "couplb_device_bytes": (C.c_size_t, [_H]),
     "couplb_set_option": (C.c_int, [_H, C.c_char_p, C.c_longlong]),
     "couplb_get_option": (C.c_int, [_H, C.c_char_p, C.POINTER(C.c_longlong)]),

@@ -118,7 +118,8 @@ int  couplb_destroy(couplb_handle* h);
 const char* couplb_last_error(const couplb_handle* h);  /* h may be NULL */
 int  couplb_version(void);
 /* sizeof of the ABI structs, for bindings to check their layouts:
- * 0 lattice_params, 1 ibm_params, 2 diag, 3 fix_config, 4 domain, 5 atoms.
+ * 0 lattice_params, 1 ibm_params, 2 diag, 3 fix_config, 4 domain, 5 atoms,
+ * 6 ibm_method, 7 mlp_train_params.
  * No counterpart in the reference (binding support only). */
 size_t couplb_struct_size(int which);
 
@@ -226,6 +227,86 @@ int  couplb_ibm_substep_device(couplb_handle* h, int n, const double* d_x,
  * momentum balance of docs/theory.md (sub-stepped coupling).  No counterpart
  * function in the reference, which conserves this sum implicitly. */
 int  couplb_ibm_total_force(couplb_handle* h, double out[3], int reset);
+
+/* ---- IBM forcing methods and the no-slip correction network ----------
+ * No counterpart in the reference, which applies one penalty pass per
+ * sub-step (fix_couplb.cpp:777-792); these entry points are additions.
+ *
+ * u_corr(x) = u0(x) + (G(x)/rho(x) + g_lb)/2 is the fluid velocity the next
+ * collision sees (u0, rho of the refresh, G the IBM force so far, g_lb the body
+ * force of the last LB step).  A correction pass interpolates u_corr at every
+ * marker, adds dF = m xi/dt (U vs - v) to the atom and spreads -dF/(N fs) with
+ * the reference's weights; the slip of a marker is |U vs - v| (MD velocity
+ * units).  Exact for md_per_lb = 1; with sub-steps G holds those so far. */
+#define COUPLB_IBM_SINGLE    0  /* the reference's single pass (default)          */
+#define COUPLB_IBM_ITERATIVE 1  /* passes-1 correction passes, then the slip      */
+#define COUPLB_IBM_LEARNED   2  /* single pass + network correction (D3Q19, Roma);
+                                   slip check, and the passes-1 corrections run
+                                   when the RMS slip exceeds slip_tol           */
+
+typedef struct couplb_mlp couplb_mlp;   /* 84-64-64-3 network, BF16 weights */
+
+typedef struct couplb_ibm_method {
+  int    method;          /* COUPLB_IBM_*                                     */
+  int    passes;          /* total passes of the iterative method, >= 1       */
+  double slip_tol;        /* LEARNED: RMS slip above which the fallback runs  */
+  const couplb_mlp* model;/* LEARNED: the network (same device)               */
+} couplb_ibm_method;
+
+int  couplb_set_ibm_method(couplb_handle* h, const couplb_ibm_method* m);
+/* Slip of the last sub-step that measured it (synchronises):
+ * out[0] RMS slip after the last pass, out[1] its max, out[2] RMS slip of the
+ * learned check (0 if none), out[3] its max, out[4] markers, out[5] 1 if the
+ * last sub-step fell back, out[6] slip checks and out[7] fallbacks since
+ * the last reset (reset != 0 clears both counters). */
+int  couplb_ibm_slip(couplb_handle* h, double out[8], int reset);
+/* Training-sample capture: every later ITERATIVE or LEARNED sub-step appends
+ * one row of COUPLB_MLP_ROW floats per marker to d_rows (device memory of
+ * capacity rows) -- the network input (u0 at the 27 Roma nodes round(l)-1..
+ * round(l)+1, node-major z,y,x; then v / vel_scale), the correction beyond the
+ * penalty pass over (m xi vel_scale / dt), lattice velocity units, and a 0.
+ * Needs all atoms coupled (no group mask).  d_rows NULL stops the capture.
+ * A sub-step that would overflow the capacity records nothing. */
+#define COUPLB_MLP_IN  84
+#define COUPLB_MLP_HID 64
+#define COUPLB_MLP_OUT 3
+#define COUPLB_MLP_ROW 88
+#define COUPLB_MLP_NPARAM 9795   /* W1[64][84] b1 W2[64][64] b2 W3[3][64] b3 */
+int  couplb_ibm_record(couplb_handle* h, float* d_rows, long long capacity);
+int  couplb_ibm_record_count(couplb_handle* h, long long* rows);
+
+/* Network y = (W3 relu(W2 relu(W1 s_in x + b1) + b2) + b3) / s_out, FP32
+ * arithmetic with weights rounded to BF16.  Parameters flat as in
+ * COUPLB_MLP_NPARAM (FP32 master copy).  Training minimises the mean of
+ * (y s_out - t s_out)^2 over the three outputs with Adam. */
+typedef struct couplb_mlp_train_params {
+  int    epochs;          /* passes over the training rows                    */
+  int    batch;           /* rows per Adam step (multiple of 64)              */
+  double lr, lr_final;    /* cosine schedule from lr to lr_final              */
+  double beta1, beta2, eps;
+  unsigned long long seed;/* minibatch sampling                               */
+  long long n_val;        /* the last n_val rows are held out for validation  */
+} couplb_mlp_train_params;
+
+int  couplb_mlp_create(int device, unsigned long long seed, couplb_mlp** out);
+int  couplb_mlp_destroy(couplb_mlp* m);
+const char* couplb_mlp_last_error(const couplb_mlp* m);
+int  couplb_mlp_set_stream(couplb_mlp* m, void* cuda_stream);
+int  couplb_mlp_set_weights(couplb_mlp* m, const float* w, double s_in, double s_out);
+int  couplb_mlp_get_weights(couplb_mlp* m, float* w, double* s_in, double* s_out);
+/* s_in = 1 / RMS of the inputs, s_out = 1 / RMS of the targets of n rows. */
+int  couplb_mlp_fit_scales(couplb_mlp* m, const float* d_rows, long long n);
+/* Outputs (n x 3 floats, device) of n rows (device, COUPLB_MLP_ROW floats). */
+int  couplb_mlp_forward(couplb_mlp* m, const float* d_rows, long long n, float* d_out);
+/* Loss and its gradient (host, COUPLB_MLP_NPARAM floats) over n rows. */
+int  couplb_mlp_loss_grad(couplb_mlp* m, const float* d_rows, long long n, double* loss,
+                          float* grad);
+int  couplb_mlp_train(couplb_mlp* m, const float* d_rows, long long n,
+                      const couplb_mlp_train_params* tp, double* train_loss,
+                      double* val_loss);
+/* File: "CLBMLP01", s_in, s_out (double), COUPLB_MLP_NPARAM floats. */
+int  couplb_mlp_save(couplb_mlp* m, const char* path);
+int  couplb_mlp_load(couplb_mlp* m, const char* path);
 
 /* Device status word: counts of density clamps / non-finite densities seen by
  * the stepping kernels since the last reset.  Reading synchronises. */

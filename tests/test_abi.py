@@ -38,7 +38,8 @@ def test_every_declared_symbol_is_exported(cuda_lib):
 
 
 @pytest.mark.parametrize("which,cls", [(0, abi.LatticeParams), (1, abi.IbmParams), (2, abi.Diag),
-                                       (3, abi.FixConfig), (4, abi.Domain), (5, abi.Atoms)])
+                                       (3, abi.FixConfig), (4, abi.Domain), (5, abi.Atoms),
+                                       (6, abi.IbmMethod), (7, abi.MlpTrainParams)])
 def test_struct_layouts(cuda_lib, which, cls):
     assert cuda_lib.couplb_struct_size(which) == C.sizeof(cls)
 
