@@ -149,9 +149,10 @@ void bump_epoch(couplb_handle* h) {
 // Per-marker buffers of the correction passes and their state block.
 int ensure_method_buffers(couplb_handle* h, int n) {
   if (!h->d_pass) {
-    int rc = dalloc(h, &h->d_pass, sizeof(PassState));
+    int rc = dalloc(h, &h->d_pass, 2 * sizeof(PassState));
     if (rc) return rc;
-    CK(cudaMemsetAsync(h->d_pass, 0, sizeof(PassState), h->stream));
+    CK(cudaMemsetAsync(h->d_pass, 0, 2 * sizeof(PassState), h->stream));
+    h->pass_cur = 0;
   }
   if (h->method_cap >= n) return COUPLB_OK;
   void* p = h->d_corr; dfree(p); h->d_corr = nullptr;
@@ -729,6 +730,11 @@ int couplb_set_option(couplb_handle* h, const char* name, long long value) {
     h->kernel = (int)value;
     return COUPLB_OK;
   }
+  if (!std::strcmp(name, "ibm_resident")) {
+    if (value != 0 && value != 1) return fail(h, COUPLB_ERR_ARG, "ibm_resident must be 0 or 1");
+    h->ibm_resident = (int)value;
+    return COUPLB_OK;
+  }
   return fail(h, COUPLB_ERR_ARG, "unknown or read-only option '%s'", name);
 }
 
@@ -736,6 +742,7 @@ int couplb_get_option(couplb_handle* h, const char* name, long long* value) {
   if (!h || !name || !value) return COUPLB_ERR_ARG;
   if (!std::strcmp(name, "kernel")) { *value = h->kernel; return COUPLB_OK; }
   if (!std::strcmp(name, "last_kernel")) { *value = h->last_kernel; return COUPLB_OK; }
+  if (!std::strcmp(name, "ibm_resident")) { *value = h->ibm_resident; return COUPLB_OK; }
   if (!std::strcmp(name, "timeouts")) {
     int rc = set_device(h);
     if (rc) return rc;
@@ -765,26 +772,57 @@ int couplb_set_ibm_params(couplb_handle* h, const couplb_ibm_params* ip) {
 namespace couplb {
 
 // Shared body of the host- and device-array IBM sub-step.
-// Cooperative launch of the correction passes (all blocks resident at once,
-// which their grid barrier needs).
-template <class L, class S>
-int launch_passes(couplb_handle* h, PassArgs<S>& P, int delta, int n) {
-  void (*kern)(const PassArgs<S>) =
-      delta == COUPLB_DELTA_ROMA ? k_ibm_passes<L, S, 0> : k_ibm_passes<L, S, 1>;
-  int& resident = h->coop_blocks[delta == COUPLB_DELTA_ROMA ? 0 : 1][h->p.precision];
+// Blocks of a cooperative kernel that fit on the device at once (cached).
+template <class K>
+int coop_resident(couplb_handle* h, K kern, size_t smem, int slot, int* out) {
+  int& resident = h->coop_blocks[slot];
   if (resident == 0) {
     int coop = 0, sms = 0, per_sm = 0;
     CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, h->p.device));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->p.device));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
     if (!coop || per_sm < 1)
-      return fail(h, COUPLB_ERR_UNSUPPORTED, "the device cannot run the cooperative pass kernel");
+      return fail(h, COUPLB_ERR_UNSUPPORTED, "the device cannot run the cooperative IBM kernel");
     resident = per_sm * sms;
   }
+  *out = resident;
+  return COUPLB_OK;
+}
+
+// Cooperative launch of one ITERATIVE / LEARNED sub-step (all blocks
+// resident at once, which its grid barriers need).  In 3D, when every marker
+// gets a warp of its own, the register-resident form runs.
+template <class L, class S>
+int launch_method(couplb_handle* h, PassArgs<S>& P, int delta, bool learned, int n) {
+  using K = void (*)(const PassArgs<S>);
+  const int di = learned ? 2 : (delta == COUPLB_DELTA_ROMA ? 0 : 1);
+  const size_t smem = learned ? kLearnedSmem : 0;
   const long long want = ((long long)n * 32 + 255) / 256;
-  const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(want, resident));
   void* args[] = {&P};
-  CK(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(256), args, 0, h->stream));
+  int rc, resident = 0;
+  if constexpr (L::D == 3) {
+    if (h->ibm_resident) {
+      K kr = learned ? k_ibm_method_resident<L, S, 0, true>
+                     : (delta == COUPLB_DELTA_ROMA ? k_ibm_method_resident<L, S, 0, false>
+                                                   : k_ibm_method_resident<L, S, 1, false>);
+      if ((rc = coop_resident(h, kr, smem, 3 + di, &resident))) return rc;
+      if (want <= resident) {
+        CK(cudaLaunchCooperativeKernel((const void*)kr, dim3((unsigned)want), dim3(256), args, smem,
+                                       h->stream));
+        return COUPLB_OK;
+      }
+    }
+  }
+  K kern = nullptr;
+  if (learned) {
+    if constexpr (L::D == 3) kern = k_ibm_method<L, S, 0, true>;
+  } else {
+    kern = delta == COUPLB_DELTA_ROMA ? k_ibm_method<L, S, 0, false> : k_ibm_method<L, S, 1, false>;
+  }
+  if (!kern) return fail(h, COUPLB_ERR_UNSUPPORTED, "the learned correction is defined for D3Q19");
+  if ((rc = coop_resident(h, kern, smem, di, &resident))) return rc;
+  const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(want, resident));
+  CK(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(256), args, smem, h->stream));
   return COUPLB_OK;
 }
 
@@ -850,30 +888,26 @@ int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, co
     a.dvr = dv / cell_vol;
     a.corr = method != COUPLB_IBM_SINGLE ? h->d_corr : nullptr;
     a.mlp = (method == COUPLB_IBM_LEARNED) ? h->mlp->pack : nullptr;
-    if (refresh && !a.all_valid) k_ibm_prefetch<L, S><<<nb, bs, 0, h->stream>>>(a);
-    if (method == COUPLB_IBM_LEARNED) {
-      if constexpr (L::D == 3) k_ibm_substep_learned<L, S><<<nb, bs, kLearnedSmem, h->stream>>>(a);
-    } else if (ip.delta == COUPLB_DELTA_ROMA) {
-      k_ibm_substep<L, S, 0><<<nb, bs, 0, h->stream>>>(a);
+    if (method == COUPLB_IBM_SINGLE) {
+      if (refresh && !a.all_valid) k_ibm_prefetch<L, S><<<nb, bs, 0, h->stream>>>(a);
+      if (ip.delta == COUPLB_DELTA_ROMA) k_ibm_substep<L, S, 0><<<nb, bs, 0, h->stream>>>(a);
+      else k_ibm_substep<L, S, 1><<<nb, bs, 0, h->stream>>>(a);
     } else {
-      k_ibm_substep<L, S, 1><<<nb, bs, 0, h->stream>>>(a);
-    }
-    if (method != COUPLB_IBM_SINGLE) {
-      if (cudaMemsetAsync(h->d_pass, 0, sizeof(PassState), h->stream) != cudaSuccess) {
-        lrc = fail(h, COUPLB_ERR_CUDA, "cudaMemsetAsync of the pass state failed");
-        return;
-      }
+      PassState* ps = (PassState*)h->d_pass;
+      h->pass_cur ^= 1;
       PassArgs<S> P;
       P.a = a;
       P.dF = h->d_dF;
-      P.ps = (PassState*)h->d_pass;
+      P.ps = ps + h->pass_cur;
+      P.ps_next = ps + (h->pass_cur ^ 1);
+      P.fill = refresh && !a.all_valid;
       P.status = h->d_status;
       P.ncorr = h->ibm_passes - 1;
       P.check_first = method == COUPLB_IBM_LEARNED;
       P.slip_tol = h->slip_tol;
       for (int d = 0; d < 3; d++) P.g_lb[d] = h->g_lb[d];
       P.rows = record ? h->rec_rows + h->rec_count * kMlpRow : nullptr;
-      lrc = launch_passes<L, S>(h, P, ip.delta, n);
+      lrc = launch_method<L, S>(h, P, ip.delta, method == COUPLB_IBM_LEARNED, n);
     }
   });
   if (lrc) return lrc;
@@ -955,7 +989,9 @@ int couplb_ibm_slip(couplb_handle* h, double out[8], int reset) {
   for (int i = 0; i < 8; i++) out[i] = 0.0;
   unsigned char* hs = (unsigned char*)h->h_small;
   static_assert(sizeof(PassState) + 8 * sizeof(int) <= 4096, "h_small holds the pass state");
-  if (h->d_pass) CK(cudaMemcpyAsync(hs, h->d_pass, sizeof(PassState), cudaMemcpyDeviceToHost, h->stream));
+  if (h->d_pass)
+    CK(cudaMemcpyAsync(hs, (PassState*)h->d_pass + h->pass_cur, sizeof(PassState), cudaMemcpyDeviceToHost,
+                       h->stream));
   else std::memset(hs, 0, sizeof(PassState));
   int* st = (int*)(hs + sizeof(PassState));
   CK(cudaMemcpyAsync(st, h->d_status, sizeof(int) * 8, cudaMemcpyDeviceToHost, h->stream));

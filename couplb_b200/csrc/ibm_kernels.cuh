@@ -246,12 +246,13 @@ __device__ __forceinline__ void node_state(const IbmArgs<S>& a, bool hit, const 
 // nodes round(l)-1..round(l)+1 of each axis, then v / vel_scale) into the
 // warp's shared scratch xs, the warp runs the correction network, and the
 // marker force F = F_penalty + m xi/dt vs y is returned and spread.
+//
+// FILL: the stencil velocities are computed from the populations and written
+// to the marker's record (the work of k_ibm_prefetch, fused).
 template <class L, class S, int DELTA, bool LEARNED>
-__device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, const MlpPacked* P,
-                                                 float* xs, float* hs) {
+__device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, int lane, bool fill,
+                                                 const MlpPacked* P, float* xs, float* hs) {
   using R = typename S::C;
-  const int mk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
   if (mk >= a.n) return;
   if (a.active && !a.active[mk]) {
     if (!a.accumulate && lane < 3) a.fout[3 * mk + lane] = 0.0;
@@ -283,7 +284,7 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, const MlpP
   int row0 = 0, row1 = 0;
   const StencilKey key = a.skey[mk];
   const bool hit = key.epoch == a.cur_epoch && key.i0 == i0 && key.j0 == j0 && key.k0 == k0;
-  const typename S::A* rec = stencil_record(a, mk);
+  typename S::A* rec = stencil_record(a, mk);
 #pragma unroll
   for (int rep = 0; rep < 2; rep++) {
     const int s = lane + 32 * rep;
@@ -306,7 +307,14 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, const MlpP
     if (t < 0) {
       const size_t src = (size_t)ii + (size_t)g.nx * ((size_t)jj + (size_t)g.ny * kk);
       double u0, u1, u2;
-      node_velocity<L, S>(a, hit, rec, s, ii, jj, kk, src, u0, u1, u2);
+      if (fill) {
+        typename S::A v0, v1, v2, vr;
+        compute_velocity<L, S>(a, ii, jj, kk, src, v0, v1, v2, vr);
+        rec[s] = v0; rec[64 + s] = v1; rec[128 + s] = v2; rec[192 + s] = vr;
+        u0 = double(v0); u1 = double(v1); u2 = double(v2);
+      } else {
+        node_velocity<L, S>(a, hit, rec, s, ii, jj, kk, src, u0, u1, u2);
+      }
       ui += u0 * dd;
       vi += u1 * dd;
       wi += u2 * dd;
@@ -327,6 +335,7 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, const MlpP
       }
     }
   }
+  if (fill && lane == 0) a.skey[mk] = StencilKey{i0, j0, k0, a.cur_epoch};
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     ui += __shfl_xor_sync(0xffffffffu, ui, o);
@@ -390,24 +399,12 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, const MlpP
 
 template <class L, class S, int DELTA>
 __global__ void __launch_bounds__(256) k_ibm_substep(const IbmArgs<S> a) {
-  ibm_substep_body<L, S, DELTA, false>(a, nullptr, nullptr, nullptr);
+  ibm_substep_body<L, S, DELTA, false>(a, (blockIdx.x * blockDim.x + threadIdx.x) >> 5,
+                                       threadIdx.x & 31, false, nullptr, nullptr, nullptr);
 }
 
 // Per-warp shared scratch of the learned sub-step: 84 inputs + 64 hidden.
 constexpr int kMlpWarpScratch = kMlpIn + kMlpHid;
 constexpr size_t kLearnedSmem = sizeof(MlpPacked) + 8 * kMlpWarpScratch * sizeof(float);
-
-// The reference pass with the fused network correction (D3Q19, Roma; blocks
-// of 256 threads, dynamic shared memory kLearnedSmem).
-template <class L, class S>
-__global__ void __launch_bounds__(256) k_ibm_substep_learned(const IbmArgs<S> a) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  MlpPacked* P = reinterpret_cast<MlpPacked*>(smem);
-  float* scratch = reinterpret_cast<float*>(smem + sizeof(MlpPacked));
-  mlp_stage(P, a.mlp);
-  __syncthreads();
-  float* xs = scratch + (threadIdx.x >> 5) * kMlpWarpScratch;
-  ibm_substep_body<L, S, 0, true>(a, P, xs, xs + kMlpIn);
-}
 
 }  // namespace couplb

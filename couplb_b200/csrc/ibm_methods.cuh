@@ -12,11 +12,13 @@
 //               a pass are formed before any is spread (Jacobi);
 //   slip_i    = |U_i vs - v_i| after the last pass.
 //
-// One cooperative launch runs every pass of a sub-step: warps loop over the
-// markers, and a grid-wide barrier (bounded wait, error flag on timeout)
-// separates "form all dF" from "spread all dF".  The learned method measures
-// the slip first and runs the corrections only when its RMS exceeds the
-// tolerance, so the fallback costs nothing when the network is good enough.
+// One cooperative launch runs the whole sub-step: warps loop over the markers;
+// the first phase fills each marker's stencil record at a refresh, forms the
+// penalty force (plus the network correction) and spreads it, and grid-wide
+// barriers (bounded waits, error flag on timeout) separate it and each
+// "form all dF" from the following "spread all dF".  The learned method
+// measures the slip first and runs the corrections only when its RMS exceeds
+// the tolerance, so the fallback costs nothing when the network is good enough.
 #pragma once
 #include "ibm_kernels.cuh"
 
@@ -27,7 +29,8 @@ constexpr int kSlipSlots = 32;
 enum : int { kStSlipChecks = 4, kStFallbacks = 5 };
 constexpr long long kBarrierSpin = 1LL << 21;   // x ~100 ns sleeps
 
-// Zeroed before every launch of k_ibm_passes.
+// State of one launch of k_ibm_method.  Two alternate: each launch zeroes the
+// other one for the next launch.
 struct PassState {
   unsigned bar_count, bar_gen;
   int fell_back;                    // the learned method ran the corrections
@@ -41,7 +44,9 @@ template <class S>
 struct PassArgs {
   IbmArgs<S> a;
   double* dF;           // n*3: the increment of the current pass
-  PassState* ps;
+  PassState* ps;        // zeroed state of this launch
+  PassState* ps_next;   // zeroed here for the next launch
+  int fill;             // first phase computes the stencil records (refresh)
   int* status;
   int ncorr;            // iterative corrections (passes - 1)
   int check_first;      // learned: slip check first, corrections only above tol
@@ -288,14 +293,32 @@ __device__ __forceinline__ void record_marker(const PassArgs<S>& P, int mk, int 
   }
 }
 
-// All passes after the first of one sub-step (cooperative launch, blocks of
-// 256 threads, at most as many blocks as fit on the device at once).
-template <class L, class S, int DELTA>
-__global__ void __launch_bounds__(256) k_ibm_passes(const PassArgs<S> P) {
+// One sub-step of the ITERATIVE or LEARNED method (cooperative launch, blocks
+// of 256 threads, at most as many blocks as fit on the device at once;
+// LEARNED: D3Q19, Roma, dynamic shared memory kLearnedSmem).
+template <class L, class S, int DELTA, bool LEARNED>
+__global__ void __launch_bounds__(256) k_ibm_method(const PassArgs<S> P) {
+  extern __shared__ __align__(16) unsigned char smem[];
   const IbmArgs<S>& a = P.a;
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
+  MlpPacked* net = reinterpret_cast<MlpPacked*>(smem);
+  float* xs = nullptr;
+  if (LEARNED) {
+    mlp_stage(net, a.mlp);
+    __syncthreads();
+    xs = reinterpret_cast<float*>(smem + sizeof(MlpPacked)) + (threadIdx.x >> 5) * kMlpWarpScratch;
+  }
+  if (blockIdx.x == 0) {
+    unsigned* z = reinterpret_cast<unsigned*>(P.ps_next);
+    for (int i = threadIdx.x; i < (int)(sizeof(PassState) / 4); i += blockDim.x) z[i] = 0u;
+  }
+  // first pass: the reference's penalty pass (+ the network correction)
+  for (int mk = gw; mk < a.n; mk += nw)
+    ibm_substep_body<L, S, DELTA, LEARNED>(a, mk, lane, P.fill != 0, net, xs,
+                                           LEARNED ? xs + kMlpIn : nullptr);
+  if (!grid_barrier(P.ps, P.status)) return;
   if (P.check_first) {
     for (int mk = gw; mk < a.n; mk += nw)
       if (!a.active || a.active[mk]) measure_marker<L, S, DELTA>(P, mk, lane, 0);
@@ -343,6 +366,239 @@ __global__ void __launch_bounds__(256) k_ibm_passes(const PassArgs<S> P) {
     if (a.active && !a.active[mk]) continue;
     measure_marker<L, S, DELTA>(P, mk, lane, 1);
     if (P.rows) record_marker<L, S>(P, mk, lane);
+  }
+}
+
+// The same sub-step when every marker has a warp of its own (n <= resident
+// warps): a lane's two window nodes -- index, weight, type, u0 and 1/rho --
+// are computed once and kept in registers across all passes, so a correction
+// pass is two force-field loads, three warp reductions and two atomics per
+// lane.  Same arithmetic and order as k_ibm_method.
+template <class L, class S, int DELTA, bool LEARNED>
+__global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P) {
+  static_assert(L::D == 3, "resident form: D3Q19");
+  using R = typename S::C;
+  using A = typename S::A;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const IbmArgs<S>& a = P.a;
+  const Geom& g = a.g;
+  const int lane = threadIdx.x & 31;
+  const int mk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  MlpPacked* net = reinterpret_cast<MlpPacked*>(smem);
+  float* xs = nullptr;
+  if (LEARNED) {
+    mlp_stage(net, a.mlp);
+    __syncthreads();
+    xs = reinterpret_cast<float*>(smem + sizeof(MlpPacked)) + (threadIdx.x >> 5) * kMlpWarpScratch;
+  }
+  if (blockIdx.x == 0) {
+    unsigned* z = reinterpret_cast<unsigned*>(P.ps_next);
+    for (int i = threadIdx.x; i < (int)(sizeof(PassState) / 4); i += blockDim.x) z[i] = 0u;
+  }
+  const bool have = mk < a.n && (!a.active || a.active[mk]);
+  if (mk < a.n && !have && !a.accumulate && lane < 3) a.fout[3 * mk + lane] = 0.0;
+
+  // ---- first pass: window, stencil state, penalty (+ network) force, spread
+  long long nd[2] = {-1, -1};      // interior index of a fluid node, else -1
+  double dw[2] = {0.0, 0.0};       // delta weight
+  double uu[2][3] = {{0, 0, 0}, {0, 0, 0}}, ir[2] = {0.0, 0.0};
+  int rw[2] = {0, 0};
+  double ws = 0.0, wss = 0.0, uwx = 0.0, uwy = 0.0, uwz = 0.0;   // wall velocity sums
+  double F0 = 0, F1 = 0, F2 = 0, c0 = 0, c1 = 0, c2 = 0, mxi = 0, vx = 0, vy = 0, vz = 0;
+  if (have) {
+    const MarkerWindow w = marker_window<L, S>(a, mk);
+    const int gx = g.nx + 2, gy = g.ny + 2, gz = g.nz + 2;
+    const StencilKey key = a.skey[mk];
+    const bool fill = P.fill != 0;
+    const bool hit = key.epoch == a.cur_epoch && key.i0 == w.i0 && key.j0 == w.j0 && key.k0 == w.k0;
+    A* rec = stencil_record(a, mk);
+    int ox = 0, oy = 0, oz = 0;
+    if (LEARNED) {
+      ox = (w.lx - w.i0) >= 0.5 ? 1 : 0;
+      oy = (w.ly - w.j0) >= 0.5 ? 1 : 0;
+      oz = (w.lz - w.k0) >= 0.5 ? 1 : 0;
+      for (int t = lane; t < kMlpIn; t += 32) xs[t] = 0.f;
+      __syncwarp();
+    }
+    double ui = 0, vi = 0, wi = 0;
+#pragma unroll
+    for (int rep = 0; rep < 2; rep++) {
+      const int s = lane + 32 * rep;
+      const int ig = w.i0 - 1 + (s & 3), jg = w.j0 - 1 + ((s >> 2) & 3), kg = w.k0 - 1 + (s >> 4);
+      if (ig < 0 || ig >= gx || jg < 0 || jg >= gy || kg < 0 || kg >= gz) continue;
+      const R d = delta1<DELTA, R>(R(w.lx - ig)) * delta1<DELTA, R>(R(w.ly - jg)) *
+                  delta1<DELTA, R>(R(w.lz - kg));
+      const double dd = double(d);
+      int ii = 0, jj = 0, kk = 0;
+      const int t = classify_node(g, 3, ig, jg, kg, ii, jj, kk);
+      int p = -1;
+      if (LEARNED) {
+        const int rx = (s & 3) - ox, ry = ((s >> 2) & 3) - oy, rz = (s >> 4) - oz;
+        if (rx >= 0 && rx < 3 && ry >= 0 && ry < 3 && rz >= 0 && rz < 3) p = rx + 3 * ry + 9 * rz;
+      }
+      if (t < 0) {
+        const size_t n = (size_t)ii + (size_t)g.nx * ((size_t)jj + (size_t)g.ny * kk);
+        double u0, u1, u2, rho;
+        if (fill) {
+          A v0, v1, v2, vr;
+          compute_velocity<L, S>(a, ii, jj, kk, n, v0, v1, v2, vr);
+          rec[s] = v0; rec[64 + s] = v1; rec[128 + s] = v2; rec[192 + s] = vr;
+          u0 = double(v0); u1 = double(v1); u2 = double(v2); rho = double(vr);
+        } else {
+          node_state<L, S>(a, hit, rec, s, ii, jj, kk, n, u0, u1, u2, rho);
+        }
+        nd[rep] = (long long)n; dw[rep] = dd; rw[rep] = jj + g.ny * kk;
+        uu[rep][0] = u0; uu[rep][1] = u1; uu[rep][2] = u2; ir[rep] = 1.0 / rho;
+        ui += u0 * dd; vi += u1 * dd; wi += u2 * dd; ws += dd; wss += dd;
+        if (LEARNED && p >= 0) { xs[3 * p] = float(u0); xs[3 * p + 1] = float(u1); xs[3 * p + 2] = float(u2); }
+      } else if (t == 1 || t == 3) {
+        ws += dd;
+      } else if (t == 2) {
+        uwx += g.uw[0] * dd; uwy += g.uw[1] * dd; uwz += g.uw[2] * dd; ws += dd;
+        if (LEARNED && p >= 0) {
+          xs[3 * p] = float(g.uw[0]); xs[3 * p + 1] = float(g.uw[1]); xs[3 * p + 2] = float(g.uw[2]);
+        }
+      }
+    }
+    if (fill && lane == 0) a.skey[mk] = StencilKey{w.i0, w.j0, w.k0, a.cur_epoch};
+    ui += uwx; vi += uwy; wi += uwz;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      ui += __shfl_xor_sync(0xffffffffu, ui, o);
+      vi += __shfl_xor_sync(0xffffffffu, vi, o);
+      wi += __shfl_xor_sync(0xffffffffu, wi, o);
+      ws += __shfl_xor_sync(0xffffffffu, ws, o);
+      wss += __shfl_xor_sync(0xffffffffu, wss, o);
+      uwx += __shfl_xor_sync(0xffffffffu, uwx, o);
+      uwy += __shfl_xor_sync(0xffffffffu, uwy, o);
+      uwz += __shfl_xor_sync(0xffffffffu, uwz, o);
+    }
+    double U0 = 0, U1 = 0, U2 = 0;
+    if (ws > DELTA_TOL) {
+      const double iw = 1.0 / ws;
+      U0 = ui * iw; U1 = vi * iw; U2 = wi * iw;
+    }
+    mxi = a.m[mk] * a.xi_over_dt;
+    vx = a.v[3 * mk]; vy = a.v[3 * mk + 1]; vz = a.v[3 * mk + 2];
+    F0 = mxi * (U0 * a.vs - vx);
+    F1 = mxi * (U1 * a.vs - vy);
+    F2 = mxi * (U2 * a.vs - vz);
+    if (LEARNED) {
+      if (lane < 3) xs[81 + lane] = float(a.v[3 * mk + lane] / a.vs);
+      __syncwarp();
+      float y[3];
+      mlp_warp_forward(*net, xs, xs + kMlpIn, lane, y);
+      const double sc = mxi * a.vs;
+      c0 = sc * double(y[0]); c1 = sc * double(y[1]); c2 = sc * double(y[2]);
+      F0 += c0; F1 += c1; F2 += c2;
+    }
+    if (lane == 0) {
+      a.corr[3 * mk] = c0; a.corr[3 * mk + 1] = c1; a.corr[3 * mk + 2] = c2;
+      if (a.accumulate) {
+        a.fout[3 * mk] += F0; a.fout[3 * mk + 1] += F1; a.fout[3 * mk + 2] += F2;
+      } else {
+        a.fout[3 * mk] = F0; a.fout[3 * mk + 1] = F1; a.fout[3 * mk + 2] = F2;
+      }
+    }
+  }
+  // spread -F/(N fs) with w = d dvr / wss (couplb_ibm.h:124-132)
+  const double ssc = (have && wss >= DELTA_TOL) ? a.dvr / wss : 0.0;
+  auto spread = [&](double f0, double f1, double f2) {
+    if (!have || wss < DELTA_TOL) return;
+    const double fl0 = -f0 * a.inv_N / a.fs, fl1 = -f1 * a.inv_N / a.fs, fl2 = -f2 * a.inv_N / a.fs;
+#pragma unroll
+    for (int rep = 0; rep < 2; rep++) {
+      if (nd[rep] < 0) continue;
+      const double wgt = dw[rep] * ssc;
+      spread_add(a.F + 4 * nd[rep], fl0 * wgt, fl1 * wgt, fl2 * wgt);
+      if (a.row_force) a.row_force[rw[rep]] = 1;
+    }
+    if (lane == 0 && a.ftot) {
+      double* t = a.ftot + 4 * (mk & (kFtotSlots - 1));
+      atomicAdd(t, fl0 * a.dvr);
+      atomicAdd(t + 1, fl1 * a.dvr);
+      atomicAdd(t + 2, fl2 * a.dvr);
+    }
+  };
+  // interpolated u_corr from the registers and the current force field
+  auto interp_corr_reg = [&](double U[3]) {
+    double ui = 0, vi = 0, wi = 0;
+#pragma unroll
+    for (int rep = 0; rep < 2; rep++) {
+      if (nd[rep] < 0) continue;
+      double G[3];
+      load_force(a.F, (size_t)nd[rep], G);
+      const double c0 = uu[rep][0] + 0.5 * (G[0] * ir[rep] + P.g_lb[0]);
+      const double c1 = uu[rep][1] + 0.5 * (G[1] * ir[rep] + P.g_lb[1]);
+      const double c2 = uu[rep][2] + 0.5 * (G[2] * ir[rep] + P.g_lb[2]);
+      ui += c0 * dw[rep]; vi += c1 * dw[rep]; wi += c2 * dw[rep];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      ui += __shfl_xor_sync(0xffffffffu, ui, o);
+      vi += __shfl_xor_sync(0xffffffffu, vi, o);
+      wi += __shfl_xor_sync(0xffffffffu, wi, o);
+    }
+    if (ws > DELTA_TOL) {
+      const double iw = 1.0 / ws;
+      U[0] = (ui + uwx) * iw; U[1] = (vi + uwy) * iw; U[2] = (wi + uwz) * iw;
+    } else {
+      U[0] = U[1] = U[2] = 0.0;
+    }
+  };
+  auto measure = [&](int r) {
+    if (!have) return;
+    double U[3];
+    interp_corr_reg(U);
+    if (lane == 0) {
+      const double e0 = U[0] * a.vs - vx, e1 = U[1] * a.vs - vy, e2 = U[2] * a.vs - vz;
+      const double q = e0 * e0 + e1 * e1 + e2 * e2;
+      atomicAdd(&P.ps->s2[r][mk & (kSlipSlots - 1)], q);
+      atomicMax(&P.ps->max_bits[r], (unsigned long long)__double_as_longlong(sqrt(q)));
+      atomicAdd(&P.ps->count[r], 1);
+    }
+  };
+  spread(F0, F1, F2);
+  if (!grid_barrier(P.ps, P.status)) return;
+  if (P.check_first) {
+    measure(0);
+    if (!grid_barrier(P.ps, P.status)) return;
+    const bool fall = slip_rms(P.ps, 0) > P.slip_tol;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      P.ps->checked = 1;
+      if (P.status) atomicAdd(P.status + kStSlipChecks, 1);
+      if (fall) {
+        P.ps->fell_back = 1;
+        if (P.status) atomicAdd(P.status + kStFallbacks, 1);
+      }
+    }
+    if (!fall) {
+      if (P.rows && have) record_marker<L, S>(P, mk, lane);
+      return;
+    }
+  }
+  for (int it = 0; it < P.ncorr; it++) {
+    double d0 = 0, d1 = 0, d2 = 0;
+    if (have) {
+      double U[3];
+      interp_corr_reg(U);
+      d0 = mxi * (U[0] * a.vs - vx);
+      d1 = mxi * (U[1] * a.vs - vy);
+      d2 = mxi * (U[2] * a.vs - vz);
+      c0 += d0; c1 += d1; c2 += d2;
+      if (lane == 0) {
+        a.fout[3 * mk] += d0; a.fout[3 * mk + 1] += d1; a.fout[3 * mk + 2] += d2;
+      }
+    }
+    if (!grid_barrier(P.ps, P.status)) return;
+    spread(d0, d1, d2);
+    if (!grid_barrier(P.ps, P.status)) return;
+  }
+  if (have && lane == 0) { a.corr[3 * mk] = c0; a.corr[3 * mk + 1] = c1; a.corr[3 * mk + 2] = c2; }
+  measure(1);
+  if (P.rows && have) {
+    __syncwarp();
+    record_marker<L, S>(P, mk, lane);
   }
 }
 

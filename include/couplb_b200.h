@@ -320,6 +320,10 @@ int  couplb_read_status(couplb_handle* h, int* clamps, int* nonfinite, int reset
  *                 per thread in paired FP32 arithmetic; shifted formats, even
  *                 nx).  A variant that does not apply falls back to plain.
  *   "last_kernel" read-only: the variant the last LB step ran.
+ *   "ibm_resident" 1 (default): ITERATIVE / LEARNED sub-steps of a 3D lattice
+ *                 whose markers each fit a warp of one cooperative launch keep
+ *                 each marker's stencil in registers across passes; 0 always
+ *                 uses the general form (same results).
  *   "timeouts"    read-only: bounded device waits that gave up (synchronises). */
 int  couplb_set_option(couplb_handle* h, const char* name, long long value);
 int  couplb_get_option(couplb_handle* h, const char* name, long long* value);

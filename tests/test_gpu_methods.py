@@ -78,10 +78,12 @@ def run_steps(L, O, ip, method, passes, steps, slip_tol=0.0, net=None, w=None, s
     return out
 
 
+@pytest.mark.parametrize("resident", [1, 0])
 @pytest.mark.parametrize("delta", ["roma", "peskin4"])
 @pytest.mark.parametrize("passes", [1, 3, 5])
-def test_iterative_matches_oracle_fp64(cuda_lib, delta, passes):
+def test_iterative_matches_oracle_fp64(cuda_lib, delta, passes, resident):
     L, O, ip = make_pair("fp64", delta)
+    L.set_option("ibm_resident", resident)
     L.set_ibm_method("iterative", passes=passes)
     for fg, fo, sl, st in run_steps(L, O, ip, 1, passes, 3):
         assert rel(fg, fo) <= 1e-10, rel(fg, fo)
@@ -115,9 +117,11 @@ def test_iterative_fp32_close_to_oracle(cuda_lib):
     L.close()
 
 
+@pytest.mark.parametrize("resident", [1, 0])
 @pytest.mark.parametrize("tol,fell", [(1e9, 0), (0.0, 1)])
-def test_learned_matches_oracle(cuda_lib, tol, fell):
+def test_learned_matches_oracle(cuda_lib, tol, fell, resident):
     L, O, ip = make_pair("fp64", "roma")
+    L.set_option("ibm_resident", resident)
     w = random_net(3)
     s = (250.0, 400.0)
     net = CorrectionNet(0, seed=1)
@@ -134,9 +138,11 @@ def test_learned_matches_oracle(cuda_lib, tol, fell):
     net.close()
 
 
-def test_record_rows_match_oracle(cuda_lib):
+@pytest.mark.parametrize("resident", [1, 0])
+def test_record_rows_match_oracle(cuda_lib, resident):
     import torch
     L, O, ip = make_pair("fp64", "roma", wall=(0,) * 6)
+    L.set_option("ibm_resident", resident)
     L.set_ibm_method("iterative", passes=3)
     x, v, m = markers()
     n = x.shape[0]
