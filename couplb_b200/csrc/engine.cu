@@ -999,22 +999,32 @@ int couplb_ibm_slip(couplb_handle* h, double out[8], int reset) {
   CK(cudaStreamSynchronize(h->stream));
   PassState ps;
   std::memcpy(&ps, hs, sizeof ps);
+  auto count = [&](int r) {
+    int c = 0;
+    for (int i = 0; i < kSlipSlots; i++) c += ps.count[r][i];
+    return c;
+  };
   auto rms = [&](int r) {
     double s = 0.0;
     for (int i = 0; i < kSlipSlots; i++) s += ps.s2[r][i];
-    return ps.count[r] > 0 ? std::sqrt(s / ps.count[r]) : 0.0;
+    const int c = count(r);
+    return c > 0 ? std::sqrt(s / c) : 0.0;
   };
   auto mx = [&](int r) {
-    double v;
-    std::memcpy(&v, &ps.max_bits[r], sizeof v);
-    return v;
+    double m = 0.0;
+    for (int i = 0; i < kSlipSlots; i++) {
+      double v;
+      std::memcpy(&v, &ps.max_bits[r][i], sizeof v);
+      m = std::max(m, v);
+    }
+    return m;
   };
   const int r = (ps.checked && !ps.fell_back) ? 0 : 1;
   out[0] = rms(r);
   out[1] = mx(r);
   out[2] = ps.checked ? rms(0) : 0.0;
   out[3] = ps.checked ? mx(0) : 0.0;
-  out[4] = ps.count[r];
+  out[4] = count(r);
   out[5] = ps.fell_back;
   out[6] = st[kStSlipChecks];
   out[7] = st[kStFallbacks];

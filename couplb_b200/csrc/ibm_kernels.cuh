@@ -186,6 +186,9 @@ __global__ void __launch_bounds__(256) k_ibm_prefetch(const IbmArgs<S> a) {
   const int gx = g.nx + 2, gy = g.ny + 2, gz = (L::D == 3) ? g.nz + 2 : 1;
   constexpr int NS = (L::D == 3) ? 64 : 16;
   typename S::A* rec = stencil_record(a, mk);
+  // both nodes are computed before either is stored, so that their loads can
+  // be in flight together
+  typename S::A v[2][4] = {{0, 0, 0, 1}, {0, 0, 0, 1}};
 #pragma unroll
   for (int rep = 0; rep < 2; rep++) {
     const int s = lane + 32 * rep;
@@ -193,14 +196,18 @@ __global__ void __launch_bounds__(256) k_ibm_prefetch(const IbmArgs<S> a) {
     const int ig = i0 - 1 + (s & 3);
     const int jg = j0 - 1 + ((s >> 2) & 3);
     const int kg = (L::D == 3) ? k0 - 1 + (s >> 4) : 0;
-    typename S::A v0 = 0, v1 = 0, v2 = 0, vr = 1;
     int ii = 0, jj = 0, kk = 0;
     if (ig >= 0 && ig < gx && jg >= 0 && jg < gy && kg >= 0 && kg < gz &&
         classify_node(g, L::D, ig, jg, kg, ii, jj, kk) < 0) {
       const size_t n = (size_t)ii + (size_t)g.nx * ((size_t)jj + (size_t)g.ny * kk);
-      compute_velocity<L, S>(a, ii, jj, kk, n, v0, v1, v2, vr);
+      compute_velocity<L, S>(a, ii, jj, kk, n, v[rep][0], v[rep][1], v[rep][2], v[rep][3]);
     }
-    rec[s] = v0; rec[64 + s] = v1; rec[128 + s] = v2; rec[192 + s] = vr;
+  }
+#pragma unroll
+  for (int rep = 0; rep < 2; rep++) {
+    const int s = lane + 32 * rep;
+    if (s >= NS) break;
+    rec[s] = v[rep][0]; rec[64 + s] = v[rep][1]; rec[128 + s] = v[rep][2]; rec[192 + s] = v[rep][3];
   }
   if (lane == 0) a.skey[mk] = StencilKey{i0, j0, k0, a.cur_epoch};
 }

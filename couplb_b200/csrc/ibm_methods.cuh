@@ -31,13 +31,16 @@ constexpr long long kBarrierSpin = 1LL << 21;   // x ~100 ns sleeps
 
 // State of one launch of k_ibm_method.  Two alternate: each launch zeroes the
 // other one for the next launch.
+// Slip accumulators are striped over kSlipSlots by marker index: a single
+// word hit by every marker serialises in L2.  [0]: the learned check,
+// [1]: after the last pass.
 struct PassState {
   unsigned bar_count, bar_gen;
-  int fell_back;                    // the learned method ran the corrections
-  int checked;                      // a slip check ran
-  unsigned long long max_bits[2];   // max slip (non-negative double bits): [0] check, [1] final
-  int count[2];
-  double s2[2][kSlipSlots];         // slip^2 sums, striped by marker index
+  int fell_back;                               // the learned method ran the corrections
+  int checked;                                 // a slip check ran
+  double s2[2][kSlipSlots];                    // slip^2 sums
+  unsigned long long max_bits[2][kSlipSlots];  // max slip (non-negative double bits)
+  int count[2][kSlipSlots];                    // markers
 };
 
 template <class S>
@@ -239,17 +242,31 @@ __device__ __forceinline__ void measure_marker(const PassArgs<S>& P, int mk, int
       const double e = U[c] * a.vs - a.v[3 * mk + c];
       e2 += e * e;
     }
-    atomicAdd(&P.ps->s2[r][mk & (kSlipSlots - 1)], e2);
-    atomicMax(&P.ps->max_bits[r], (unsigned long long)__double_as_longlong(sqrt(e2)));
-    atomicAdd(&P.ps->count[r], 1);
+    const int sl = mk & (kSlipSlots - 1);
+    atomicAdd(&P.ps->s2[r][sl], e2);
+    atomicMax(&P.ps->max_bits[r][sl], (unsigned long long)__double_as_longlong(sqrt(e2)));
+    atomicAdd(&P.ps->count[r][sl], 1);
   }
 }
 
+// RMS slip of residual r after the barrier that closed it: warp 0 of the
+// block reads the slots (lane = slot) and shares the result; every block
+// reduces in the same order, so all take the same decision.
 __device__ __forceinline__ double slip_rms(const PassState* ps, int r) {
-  double s = 0.0;
-  for (int i = 0; i < kSlipSlots; i++) s += __ldcg(&ps->s2[r][i]);
-  const int c = __ldcg(&ps->count[r]);
-  return c > 0 ? sqrt(s / c) : 0.0;
+  static_assert(kSlipSlots == 32, "one slot per lane");
+  __shared__ double rms;
+  if (threadIdx.x < 32) {
+    double s = __ldcg(&ps->s2[r][threadIdx.x]);
+    int c = __ldcg(&ps->count[r][threadIdx.x]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s += __shfl_xor_sync(0xffffffffu, s, o);
+      c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    if (threadIdx.x == 0) rms = c > 0 ? sqrt(s / c) : 0.0;
+  }
+  __syncthreads();
+  return rms;
 }
 
 // Training row of marker mk: network input, then the correction beyond the
@@ -440,9 +457,10 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
         const size_t n = (size_t)ii + (size_t)g.nx * ((size_t)jj + (size_t)g.ny * kk);
         double u0, u1, u2, rho;
         if (fill) {
+          // the record is written after the loop, so that the loads of both
+          // nodes can be in flight together
           A v0, v1, v2, vr;
           compute_velocity<L, S>(a, ii, jj, kk, n, v0, v1, v2, vr);
-          rec[s] = v0; rec[64 + s] = v1; rec[128 + s] = v2; rec[192 + s] = vr;
           u0 = double(v0); u1 = double(v1); u2 = double(v2); rho = double(vr);
         } else {
           node_state<L, S>(a, hit, rec, s, ii, jj, kk, n, u0, u1, u2, rho);
@@ -460,7 +478,16 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
         }
       }
     }
-    if (fill && lane == 0) a.skey[mk] = StencilKey{w.i0, w.j0, w.k0, a.cur_epoch};
+    if (fill) {
+#pragma unroll
+      for (int rep = 0; rep < 2; rep++) {
+        if (nd[rep] < 0) continue;
+        const int s = lane + 32 * rep;
+        rec[s] = A(uu[rep][0]); rec[64 + s] = A(uu[rep][1]); rec[128 + s] = A(uu[rep][2]);
+        rec[192 + s] = A(1.0 / ir[rep]);
+      }
+      if (lane == 0) a.skey[mk] = StencilKey{w.i0, w.j0, w.k0, a.cur_epoch};
+    }
     ui += uwx; vi += uwy; wi += uwz;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -553,9 +580,10 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
     if (lane == 0) {
       const double e0 = U[0] * a.vs - vx, e1 = U[1] * a.vs - vy, e2 = U[2] * a.vs - vz;
       const double q = e0 * e0 + e1 * e1 + e2 * e2;
-      atomicAdd(&P.ps->s2[r][mk & (kSlipSlots - 1)], q);
-      atomicMax(&P.ps->max_bits[r], (unsigned long long)__double_as_longlong(sqrt(q)));
-      atomicAdd(&P.ps->count[r], 1);
+      const int sl = mk & (kSlipSlots - 1);
+      atomicAdd(&P.ps->s2[r][sl], q);
+      atomicMax(&P.ps->max_bits[r][sl], (unsigned long long)__double_as_longlong(sqrt(q)));
+      atomicAdd(&P.ps->count[r][sl], 1);
     }
   };
   spread(F0, F1, F2);
