@@ -47,6 +47,8 @@ def parse():
                     help="target CPU work of the timed CPU baseline sample")
     ap.add_argument("--ibm-cycles", type=int, default=50,
                     help="LB cycles of the 256^3 IBM point-marker workload (0 = skip)")
+    ap.add_argument("--sphere-steps", type=int, default=2000,
+                    help="LB steps of the 192^3 sphere-drag runs of the IBM methods (0 = skip)")
     ap.add_argument("--kernel", type=int, default=-1,
                     help="fused-kernel variant: -1 auto, 0 plain, 1 staged, 2 packed")
     ap.add_argument("--only", choices=["fp64", "fp32", "fp16"], default=None,
@@ -286,6 +288,66 @@ def ibm_bench(torch, device, prec, cycles, warmup, n=256, natoms=20000, md_per_l
             "momentum_rel_err_per_lb_interval": err, "nonfinite": nonfinite}
 
 
+def sphere_bench(torch, device, steps, window=500, sample_rows=2_000_000):
+    """Sphere drag with the IBM forcing methods (D3Q19 192^3 periodic, nu 0.1,
+    gx 2e-6, sphere R 12 of 1810 Fibonacci markers held fixed, Roma,
+    md_per_lb 1): training rows from 5-pass iterative runs (4 spheres at random
+    sub-cell offsets, gx 1e-6..3e-6, rows every 8th step), the network trained
+    on them on the GPU, then single pass / 5-pass iterative / learned runs of
+    `steps` LB steps from rest on an unseen offset.  slip = mean over the last
+    `window` steps of the RMS marker slip; drag = x force on the markers at
+    the last step, FP32-shifted and FP64 lattices; ms = device time of the IBM
+    call per LB step."""
+    from couplb_b200 import sphere_drag as SD
+    t0 = time.perf_counter()
+    every = 8
+    runs = max(1, int(round(sample_rows / (1810 * (steps // every + 1)))))
+    rows = SD.generate_rows(runs, steps + 200, every)
+    t1 = time.perf_counter()
+    net, tl, vl = SD.train_net(rows, epochs=30)
+    t2 = time.perf_counter()
+    off = (0.37, 0.61, 0.23)
+    cfgs = {"single": dict(method="iterative", passes=1),
+            "iterative5": dict(method="iterative", passes=5),
+            "learned": dict(method="learned", passes=5, slip_tol=1e30, net=net)}
+    out = {"workload": "d3q19_periodic_192^3_sphere_R12_1810_markers_roma_gx2e-6",
+           "steps": steps, "window": window,
+           "training": {"rows": int(rows.shape[0]), "runs": runs, "generate_s": t1 - t0,
+                        "train_s": t2 - t1, "epochs": 30, "train_loss": tl, "val_loss": vl}}
+    del rows
+    for name, kw in cfgs.items():
+        res = {}
+        for prec in ("fp32", "fp64"):
+            c = SD.SphereCase(offset=off, precision=prec, device=device)
+            c.set_method(**kw)
+            sl, drag = c.run(steps, slip_from=steps - window)
+            if prec == "fp32":
+                ibm, tot = c.time_forcing(200)
+                res.update(slip=float(np.mean(sl)), drag=drag, ms_ibm=ibm, ms_step=tot)
+            else:
+                res.update(slip_fp64=float(np.mean(sl)), drag_fp64=drag,
+                           drag_err_fp32_vs_fp64=abs(res["drag"] - drag) / abs(drag))
+            c.close()
+        out[name] = res
+    # the learned method judged by the iterative one: fallback above 1.1x its slip
+    c = SD.SphereCase(offset=off, device=device)
+    tol = 1.1 * out["iterative5"]["slip"]
+    c.set_method("learned", passes=5, slip_tol=tol, net=net)
+    c.L.ibm_slip(reset=True)
+    sl, drag = c.run(steps, slip_from=steps - window)
+    d = c.L.ibm_slip()
+    ibm, _ = c.time_forcing(200)
+    out["learned_with_fallback"] = {"slip_tol": tol, "slip": float(np.mean(sl)), "drag": drag,
+                                    "ms_ibm": ibm, "checks": int(d["checks"]),
+                                    "fallbacks": int(d["fallbacks"])}
+    c.close()
+    net.close()
+    out["slip_learned_over_iterative5"] = out["learned"]["slip"] / out["iterative5"]["slip"]
+    out["slip_single_over_iterative5"] = out["single"]["slip"] / out["iterative5"]["slip"]
+    out["speedup_learned_vs_iterative5"] = out["iterative5"]["ms_ibm"] / out["learned"]["ms_ibm"]
+    return out
+
+
 def cpu_baseline(nx, ny, nz, seconds):
     """The reference's CPU path (its own headers, OpenMP, all host threads)
     on a bounded number of LB steps of the same workload."""
@@ -405,6 +467,7 @@ def main():
     ibm = None
     if args.ibm_cycles > 0:
         ibm = {p: ibm_bench(torch, local, p, args.ibm_cycles, 3) for p in ("fp32", "fp64")}
+    methods = sphere_bench(torch, local, args.sphere_steps) if args.sphere_steps > 0 else None
 
     peaks = {}
     try:
@@ -441,6 +504,7 @@ def main():
                 "d2h_bytes_per_step": 8},
         "gpu_launches": args.steps,
         "ibm": ibm,
+        "ibm_methods": methods,
         "clocks": clk,
     }
     if rank == 0:

@@ -259,3 +259,34 @@ def test_method_errors(cuda_lib):
     L.close()
     L2.close()
     net.close()
+
+
+def test_trained_network_gains_over_single_pass(cuda_lib):
+    """Rows from 5-pass iterative runs of a small sphere train the network on
+    the GPU; on an unseen sub-cell offset the learned correction removes most
+    of the slip the single penalty pass leaves, and the check passes without
+    falling back at 1.5x the iterative slip."""
+    from couplb_b200 import sphere_drag as SD
+    kw = dict(n=48, radius=6.0, g=4e-6)
+    rows = SD.generate_rows(4, 400, 2, **{k: kw[k] for k in ("n", "radius")})
+    assert rows.shape[0] == 4 * 200 * 452
+    net, tl, vl = SD.train_net(rows, epochs=25, batch=2048)
+    assert vl < 0.2, (tl, vl)
+    slip = {}
+    for name, m in [("single", dict(method="iterative", passes=1)),
+                    ("iter5", dict(method="iterative", passes=5)),
+                    ("learned", dict(method="learned", passes=5, slip_tol=1e30, net=net))]:
+        c = SD.SphereCase(offset=(0.37, 0.61, 0.23), **kw)
+        c.set_method(**m)
+        sl, _ = c.run(400, slip_from=300)
+        slip[name] = float(np.mean(sl))
+        c.close()
+    assert slip["learned"] < 0.3 * slip["single"], slip
+    assert slip["learned"] < 1.5 * slip["iter5"], slip
+    c = SD.SphereCase(offset=(0.37, 0.61, 0.23), **kw)
+    c.set_method("learned", passes=5, slip_tol=1.5 * slip["iter5"], net=net)
+    c.run(400)
+    d = c.L.ibm_slip()
+    assert d["checks"] == 400 and d["fallbacks"] <= 40, d
+    c.close()
+    net.close()
