@@ -126,6 +126,10 @@ class FixConfig(C.Structure):
         ("restart_prefix", C.c_char * PATH_MAX),
         ("precision", C.c_int),
         ("dimension", C.c_int),
+        ("ibm_method", C.c_int),
+        ("ibm_passes", C.c_int),
+        ("slip_tol", C.c_double),
+        ("mlp_model", C.c_char * PATH_MAX),
     ]
 
 

@@ -28,10 +28,11 @@ constexpr int32_t kCkptVersion = 1;
 const char* const kKeywords[] = {"md_per_lb", "xi_ibm",      "gravity", "wall_x",     "wall_y",
                                  "wall_z",    "wall_vel",    "output",  "check_every", "kernel",
                                  "vtk",       "vtk_region",  "vtk_solid", "checkpoint", "restart",
-                                 "precision", nullptr};
+                                 "precision", "ibm_method", "ibm_passes", "slip_tol", "mlp_model",
+                                 nullptr};
 
-// is_couplb_keyword (fix_couplb.cpp:22-36), plus the `precision` keyword of
-// this implementation.
+// is_couplb_keyword (fix_couplb.cpp:22-36), plus the keywords of this
+// implementation (precision, IBM forcing method).
 bool is_keyword(const char* s) {
   for (int i = 0; kKeywords[i]; i++)
     if (std::strcmp(s, kKeywords[i]) == 0) return true;
@@ -79,6 +80,7 @@ void copy_str(char* dst, const char* src) {
 struct couplb_fix {
   couplb_fix_config cfg{};
   couplb_handle* h = nullptr;
+  couplb_mlp* mlp = nullptr;          // network of ibm_method learned
   int device = 0;
   int rank = 0;
   bool inited = false;
@@ -297,6 +299,9 @@ int couplb_fix_parse(int narg, const char* const* arg, int dimension, couplb_fix
     copy_str(c.checkpoint_prefix, "couplb_ckpt");
     c.delta = COUPLB_DELTA_ROMA;
     c.precision = COUPLB_FP64;
+    c.ibm_method = COUPLB_IBM_SINGLE;
+    c.ibm_passes = 5;
+    c.slip_tol = 0.0;
     int iarg = 8;
     while (iarg < narg) {
       const char* kw = arg[iarg];
@@ -399,6 +404,27 @@ int couplb_fix_parse(int narg, const char* const* arg, int dimension, couplb_fix
         else if (!std::strcmp(arg[iarg + 1], "fp16")) c.precision = COUPLB_FP16_SHIFTED;
         else perr("fix couplb precision: use fp64, fp32 or fp16");
         iarg += 2;
+      } else if (!std::strcmp(kw, "ibm_method")) {
+        if (iarg + 2 > narg) perr("fix couplb ibm_method: need 1 value");
+        if (!std::strcmp(arg[iarg + 1], "single")) c.ibm_method = COUPLB_IBM_SINGLE;
+        else if (!std::strcmp(arg[iarg + 1], "iterative")) c.ibm_method = COUPLB_IBM_ITERATIVE;
+        else if (!std::strcmp(arg[iarg + 1], "learned")) c.ibm_method = COUPLB_IBM_LEARNED;
+        else perr("fix couplb ibm_method: use single, iterative or learned");
+        iarg += 2;
+      } else if (!std::strcmp(kw, "ibm_passes")) {
+        if (iarg + 2 > narg) perr("fix couplb ibm_passes: need 1 value");
+        c.ibm_passes = to_int(arg[iarg + 1]);
+        if (c.ibm_passes < 1 || c.ibm_passes > 64) perr("fix couplb: ibm_passes must be 1..64");
+        iarg += 2;
+      } else if (!std::strcmp(kw, "slip_tol")) {
+        if (iarg + 2 > narg) perr("fix couplb slip_tol: need 1 value");
+        c.slip_tol = to_double(arg[iarg + 1]);
+        if (c.slip_tol < 0.0 || !std::isfinite(c.slip_tol)) perr("fix couplb: slip_tol must be >= 0");
+        iarg += 2;
+      } else if (!std::strcmp(kw, "mlp_model")) {
+        if (iarg + 2 > narg) perr("fix couplb mlp_model: need 1 value");
+        copy_str(c.mlp_model, arg[iarg + 1]);
+        iarg += 2;
       }
     }
     c.dimension = dimension;
@@ -425,6 +451,7 @@ int couplb_fix_create(const couplb_fix_config* cfg, couplb_fix** out) {
 int couplb_fix_destroy(couplb_fix* F) {
   if (!F) return COUPLB_OK;
   if (F->h) couplb_destroy(F->h);
+  if (F->mlp) couplb_mlp_destroy(F->mlp);
   delete F;
   return COUPLB_OK;
 }
@@ -580,6 +607,23 @@ int couplb_fix_init(couplb_fix* F, const couplb_domain* dom) {
   ip.force_scale = F->force_scale;
   for (int d = 0; d < 3; d++) { ip.domain_lo[d] = F->domain_lo[d]; ip.offset[d] = F->off[d]; }
   if ((rc = couplb_set_ibm_params(F->h, &ip))) return F->engine_fail(rc);
+  if (c.ibm_method != COUPLB_IBM_SINGLE) {
+    couplb_ibm_method m;
+    std::memset(&m, 0, sizeof(m));
+    m.method = c.ibm_method;
+    m.passes = c.ibm_passes;
+    m.slip_tol = c.slip_tol > 0.0 ? c.slip_tol : 1e300;
+    if (c.ibm_method == COUPLB_IBM_LEARNED) {
+      if (!c.mlp_model[0]) return F->fail(COUPLB_ERR_ARG, "fix couplb: ibm_method learned requires mlp_model");
+      if (F->mlp) { couplb_mlp_destroy(F->mlp); F->mlp = nullptr; }
+      if ((rc = couplb_mlp_create(F->device, 0, &F->mlp)))
+        return F->fail(rc, "fix couplb: cannot create the correction network");
+      if ((rc = couplb_mlp_load(F->mlp, c.mlp_model)))
+        return F->fail(rc, "fix couplb: %s", couplb_mlp_last_error(F->mlp));
+      m.model = F->mlp;
+    }
+    if ((rc = couplb_set_ibm_method(F->h, &m))) return F->engine_fail(rc);
+  }
 
   if (c.do_restart) {
     long long ck = 0;
@@ -626,6 +670,9 @@ int couplb_fix_init(couplb_fix* F, const couplb_domain* dom) {
   F->log("CoupLB: dx=%.4e dt_LBM=%.4e vel_scale=%.4e force_scale=%.4e\n", F->dx, F->dt_LBM, F->vel_scale,
          F->force_scale);
   F->log("CoupLB: kernel=%s xi_ibm=%.4f\n", c.delta == COUPLB_DELTA_ROMA ? "roma" : "peskin4", c.xi_ibm);
+  if (c.ibm_method != COUPLB_IBM_SINGLE)
+    F->log("CoupLB: ibm_method=%s passes=%d\n", c.ibm_method == COUPLB_IBM_LEARNED ? "learned" : "iterative",
+           c.ibm_passes);
   F->log("CoupLB: precision=%s device memory %.1f MB\n",
          c.precision == COUPLB_FP64 ? "fp64" : (c.precision == COUPLB_FP32_SHIFTED ? "fp32" : "fp16"),
          couplb_device_bytes(F->h) / 1048576.0);

@@ -364,6 +364,15 @@ typedef struct couplb_fix_config {
   char   restart_prefix[COUPLB_PATH_MAX];
   int    precision;                 /* `precision fp64|fp32|fp16`, default fp64 */
   int    dimension;                 /* domain->dimension                   */
+  /* IBM forcing method (keywords of this implementation, no reference
+   * counterpart): `ibm_method single|iterative|learned`, `ibm_passes N`
+   * (default 5), `slip_tol V` (MD velocity units; learned method: RMS slip
+   * above which the iterative passes run; 0 = never), `mlp_model FILE`
+   * (network file of couplb_mlp_save; required by `learned`). */
+  int    ibm_method;                /* COUPLB_IBM_*                        */
+  int    ibm_passes;
+  double slip_tol;
+  char   mlp_model[COUPLB_PATH_MAX];
 } couplb_fix_config;
 
 /* The MD side of one subdomain (LAMMPS: domain, update). */

@@ -616,6 +616,15 @@ int ORC_FN(grid_ibm_substep)(void* gp, const couplb_ibm_params* ip, int n,
 /* Streaming::exchange_forces as an entry point for the fix layer. */
 void ORC_FN(grid_fold_forces)(void* gp) { exchange_forces((orc_grid*)gp); }
 
+/* the port also restates the IBM forcing methods at the fix level */
+#define ORC_METHODS 1
+#define MLP_NPARAM_FIX 9795
+int ORC_FN(grid_ibm_substep_method)(void* gp, const couplb_ibm_params* ip, int n,
+                                    const double* x, const double* v, const double* mass,
+                                    const int* active, double* f_add, int refresh, int fold,
+                                    int method, int passes, double slip_tol,
+                                    const double* mlp_w, double s_in, double s_out,
+                                    const double g_lb[3], double* stats, double* rows);
 #include "oracle_fix.inc"
 
 /* ---- IBM forcing methods and the correction network ------------------

@@ -49,7 +49,7 @@ IBM_CASES = {
 
 def make_cfg(Nx, Ny, Nz, nu, rho, dimension=3, md_per_lb=1, xi_ibm=1.0, gravity=None, wall=(0,) * 6,
              wall_vel=(0.0,) * 3, delta=0, check_every=0, output_every=0, output_file="",
-             precision=0):
+             precision=0, ibm_method=0, ibm_passes=5, slip_tol=0.0, mlp_model=""):
     c = abi.FixConfig()
     c.Nx, c.Ny, c.Nz, c.nu, c.rho = Nx, Ny, Nz, nu, rho
     c.md_per_lb, c.xi_ibm = md_per_lb, xi_ibm
@@ -67,6 +67,8 @@ def make_cfg(Nx, Ny, Nz, nu, rho, dimension=3, md_per_lb=1, xi_ibm=1.0, gravity=
     c.output_file = output_file.encode()
     c.precision = precision
     c.dimension = dimension
+    c.ibm_method, c.ibm_passes, c.slip_tol = ibm_method, ibm_passes, slip_tol
+    c.mlp_model = mlp_model.encode()
     return c
 
 
@@ -86,6 +88,23 @@ FIX_CASES = {
                                    gravity=(2e-4, 0, 0), wall=(0, 0, 1, 1, 0, 0), check_every=8),
                           dimension=2, box=((0, 0, -0.5), (7.5, 6.25, 0.5)), dt=0.08333 / 4,
                           nsteps=24, seed=33, natoms=3, fext=None, mass=0.161),
+}
+
+# IBM forcing methods at the fix level (no reference counterpart: checked
+# against the port oracle only)
+METHOD_FIX_CASES = {
+    "cluster_iterative": dict(cmd=dict(Nx=16, Ny=14, Nz=12, nu=0.1, rho=1.0, md_per_lb=2, delta=0,
+                                       gravity=(3e-5, 0, 0), ibm_method=1, ibm_passes=3,
+                                       check_every=5),
+                              dimension=3, box=((0, 0, 0), (16, 14, 12)), dt=0.5, nsteps=20,
+                              seed=41, natoms=24, fext=None),
+    # xi 0.3, mass 2: with xi 1 and mass 1 the Peskin4 overlap of this cluster
+    # makes the correction gain exceed 2 and the passes diverge
+    "cluster_iterative_peskin_walls": dict(cmd=dict(Nx=16, Ny=14, Nz=12, nu=0.1, rho=1.0, md_per_lb=1,
+                                                    delta=1, gravity=(3e-5, 0, 0), ibm_method=1,
+                                                    ibm_passes=4, wall=(0, 0, 1, 1, 0, 0), xi_ibm=0.3),
+                                           dimension=3, box=((0, 0, 0), (16, 14, 12)), dt=1.0,
+                                           nsteps=12, seed=42, natoms=24, fext=None, mass=2.0),
 }
 
 

@@ -290,3 +290,33 @@ def test_trained_network_gains_over_single_pass(cuda_lib):
     assert d["checks"] == 400 and d["fallbacks"] <= 40, d
     c.close()
     net.close()
+
+
+@pytest.mark.parametrize("name", sorted(cases.METHOD_FIX_CASES))
+def test_fix_method_matches_port(cuda_lib, name):
+    """`fix couplb ... ibm_method iterative ibm_passes N` through the fix hooks
+    against the port oracle's fix sequencing (atoms move, sub-steps fold)."""
+    case = cases.METHOD_FIX_CASES[name]
+    ref = cases.run_fix_case(case, "port")
+    out = cases.run_fix_case(case, "gpu")
+    assert rel(out["f_atoms"], ref["f_atoms"]) <= 1e-10, rel(out["f_atoms"], ref["f_atoms"])
+    assert rel(out["x"], ref["x"]) <= 1e-12
+    assert np.abs(out["f"] - ref["f"]).max() <= 1e-12
+
+
+@pytest.mark.parametrize("slip_tol", [0.0, 1e-12])
+def test_fix_learned_matches_port(cuda_lib, tmp_path, slip_tol):
+    """`ibm_method learned mlp_model FILE`: never falling back (slip_tol 0)
+    and always falling back (slip_tol 1e-12)."""
+    net = CorrectionNet(0, seed=8)
+    net.set_weights(random_net(12, 0.2).astype(np.float32), 150.0, 300.0)
+    path = tmp_path / "net.clbmlp"
+    net.save(path)
+    net.close()
+    case = dict(cases.METHOD_FIX_CASES["cluster_iterative"])
+    case["cmd"] = dict(case["cmd"], ibm_method=2, ibm_passes=3, slip_tol=slip_tol, mlp_model=str(path))
+    ref = cases.run_fix_case(case, "port")
+    out = cases.run_fix_case(case, "gpu")
+    # FP32 network inside 20 coupled MD steps: differences grow with the dynamics
+    assert rel(out["f_atoms"], ref["f_atoms"]) <= 1e-4, rel(out["f_atoms"], ref["f_atoms"])
+    assert rel(out["x"], ref["x"]) <= 1e-6

@@ -77,3 +77,24 @@ def test_swimmer_deck_is_rejected_like_the_reference(cuda_lib):
     parser rejects (fix_couplb.cpp:119-120)."""
     with pytest.raises(CoupLBError):
         P("lb all couplb 64 64 1 0.1 1.0 xi_ibm 5.0", 2)
+
+
+def test_ibm_method_keywords(cuda_lib):
+    c = P("f all couplb 8 8 8 0.1 1.0")
+    assert c.ibm_method == abi.IBM_SINGLE and c.ibm_passes == 5 and c.slip_tol == 0.0
+    c = P("f all couplb 8 8 8 0.1 1.0 ibm_method learned ibm_passes 4 slip_tol 2e-4 mlp_model net.bin")
+    assert c.ibm_method == abi.IBM_LEARNED and c.ibm_passes == 4 and c.slip_tol == 2e-4
+    assert c.mlp_model == b"net.bin"
+    assert P("f all couplb 8 8 8 0.1 1.0 ibm_method iterative").ibm_method == abi.IBM_ITERATIVE
+
+
+@pytest.mark.parametrize("tail,msg", [
+    ("ibm_method fancy", "ibm_method: use single, iterative or learned"),
+    ("ibm_passes 0", "ibm_passes must be 1..64"),
+    ("slip_tol -1", "slip_tol must be >= 0"),
+    ("ibm_method", "ibm_method: need 1 value"),
+])
+def test_ibm_method_errors(cuda_lib, tail, msg):
+    with pytest.raises(CoupLBError) as e:
+        P("f all couplb 8 8 8 0.1 1.0 " + tail)
+    assert msg in e.value.msg
