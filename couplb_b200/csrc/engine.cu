@@ -85,6 +85,9 @@ void row_launch(const couplb_handle* h, dim3* grid, dim3* block) {
 
 unsigned flat_blocks(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
+// Force flags: one byte per 8 consecutive interior nodes (n >> 3).
+size_t seg_bytes(const couplb_handle* h) { return (h->N + 7) / 8; }
+
 int dalloc(couplb_handle* h, void** p, size_t bytes) {
   cudaError_t e = cudaMalloc(p, bytes);
   if (e != cudaSuccess)
@@ -343,7 +346,7 @@ int couplb_create(const couplb_lattice_params* p, couplb_handle** out) {
   h->idx32 = ((unsigned long long)Q * h->qs < (1ULL << 32));
   if (!rc) rc = dalloc(h, (void**)&h->d_status, sizeof(int) * 8);
   if (!rc) rc = dalloc(h, (void**)&h->d_ftot, sizeof(double) * 4 * kFtotSlots);
-  if (!rc) rc = dalloc(h, (void**)&h->row_force, (size_t)p->ny * p->nz);
+  if (!rc) rc = dalloc(h, (void**)&h->seg_force, seg_bytes(h));
   static_assert(sizeof(double) * 4 * kFtotSlots <= 4096, "h_small holds the force accumulators");
   if (!rc && cudaMallocHost(&h->h_small, 4096) != cudaSuccess)
     rc = fail(h, COUPLB_ERR_CUDA, "cudaMallocHost failed");
@@ -375,7 +378,7 @@ int couplb_destroy(couplb_handle* h) {
   for (int c = 0; c < 4; c++) dfree(h->macro[c]);
   dfree(h->rho_field);
   void* p = h->d_status; dfree(p);
-  p = h->row_force; dfree(p);
+  p = h->seg_force; dfree(p);
   p = h->skey; dfree(p);
   dfree(h->sbuf);
   p = h->d_ftot; dfree(p);
@@ -434,7 +437,7 @@ int couplb_init_equilibrium(couplb_handle* h, double rho, double ux, double uy, 
   h->poststream = 1;
   const size_t ab = elem_bytes_aux(h->p.precision);
   CK(cudaMemsetAsync(h->F, 0, 4 * ab * h->qs, h->stream));
-  CK(cudaMemsetAsync(h->row_force, 0, (size_t)h->p.ny * h->p.nz, h->stream));
+  CK(cudaMemsetAsync(h->seg_force, 0, seg_bytes(h), h->stream));
   h->force_dirty = 0;
   h->force_rows_all = 0;
   h->rho_state = h->p.body_force ? kRhoField : kRhoNone;
@@ -513,7 +516,7 @@ int couplb_lbm_step(couplb_handle* h, const double* g_lb) {
     a.fin = (const T*)h->f[h->cur];
     a.fout = (T*)h->f[1 - h->cur];
     a.F = h->force_dirty ? (A*)h->F : nullptr;
-    a.row_force = h->force_rows_all ? nullptr : h->row_force;
+    a.seg_force = h->force_rows_all ? nullptr : h->seg_force;
     a.rho_field = (A*)h->rho_field;
     a.rho_mode = rho_mode;
     a.write_rho = h->p.body_force ? 2 : (h->moving_walls ? 1 : 0);
@@ -556,8 +559,8 @@ int couplb_lbm_step(couplb_handle* h, const double* g_lb) {
   h->poststream = 0;
   h->lbm_steps++;
   if (h->force_dirty) {
-    // the kernel zeroed every force it read (clear_forces); reset the row flags
-    CK(cudaMemsetAsync(h->row_force, 0, (size_t)h->p.ny * h->p.nz, h->stream));
+    // the kernel zeroed every force it read (clear_forces); reset the flags
+    CK(cudaMemsetAsync(h->seg_force, 0, seg_bytes(h), h->stream));
     h->force_dirty = 0;
     h->force_rows_all = 0;
   }
@@ -643,7 +646,7 @@ int couplb_set_force_field(couplb_handle* h, const double* fx, const double* fy,
   });
   CK_LAUNCH();
   h->force_dirty = 1;
-  h->force_rows_all = 1;   // the row flags know nothing of these forces
+  h->force_rows_all = 1;   // the segment flags know nothing of these forces
   CK(cudaStreamSynchronize(h->stream));
   return COUPLB_OK;
 }
@@ -872,7 +875,7 @@ int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, co
     a.skey = h->skey;
     a.cur_epoch = h->cur_epoch;
     a.F = (A*)h->F;
-    a.row_force = h->row_force;
+    a.seg_force = h->seg_force;
     a.n = n;
     a.x = d_x; a.v = d_v; a.m = d_m; a.active = d_active;
     a.fout = d_fout;

@@ -24,8 +24,8 @@ struct couplb_handle {
   int poststream = 1;                // 1: f[cur] is post-stream S, 0: post-collision P
   void* F = nullptr;                 // Eulerian force field {fx, fy, fz, 0} per node
   int force_dirty = 0;               // F holds nonzero values
-  int force_rows_all = 0;            // F was set from outside: the row flags do not cover it
-  unsigned char* row_force = nullptr;   // per (j,k) row: IBM force spread there
+  int force_rows_all = 0;            // F was set from outside: the segment flags do not cover it
+  unsigned char* seg_force = nullptr;   // per 8 consecutive nodes: IBM force spread there
   unsigned cur_epoch = 0;            // epoch of the current population state
   void* sbuf = nullptr;              // IBM stencil velocity records (64 x 3 per marker slot)
   couplb::StencilKey* skey = nullptr;   // their keys

@@ -85,7 +85,7 @@ struct IbmArgs {
   StencilKey* skey;
   unsigned cur_epoch;
   typename S::A* F;                       // Eulerian force field {fx,fy,fz,0} per node
-  unsigned char* row_force;               // per (j,k) row: a force was spread there
+  unsigned char* seg_force;               // per 8 nodes (n >> 3): a force was spread there
   int n;
   const double* __restrict__ x;           // n*3, MD units
   const double* __restrict__ v;           // n*3
@@ -288,10 +288,23 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
   double ui = 0, vi = 0, wi = 0, ws = 0, wss = 0;
   long long sn0 = -1, sn1 = -1;   // fluid nodes of this lane (interior index)
   double sd0 = 0, sd1 = 0;
-  int row0 = 0, row1 = 0;
   const StencilKey key = a.skey[mk];
-  const bool hit = key.epoch == a.cur_epoch && key.i0 == i0 && key.j0 == j0 && key.k0 == k0;
   typename S::A* rec = stencil_record(a, mk);
+  // The record entries, the marker's velocity and mass are loaded before the
+  // key is compared (their addresses do not depend on it), so that their
+  // latencies overlap; a miss discards the record values.
+  const bool spec = !fill && !a.all_valid;
+  typename S::A pre[2][3] = {{0, 0, 0}, {0, 0, 0}};
+  if (spec) {
+#pragma unroll
+    for (int rep = 0; rep < 2; rep++) {
+      const int s = lane + 32 * rep;
+      if (s < NS) { pre[rep][0] = rec[s]; pre[rep][1] = rec[64 + s]; pre[rep][2] = rec[128 + s]; }
+    }
+  }
+  const double mass = a.m[mk];
+  const double vmk0 = a.v[3 * mk], vmk1 = a.v[3 * mk + 1], vmk2 = a.v[3 * mk + 2];
+  const bool hit = key.epoch == a.cur_epoch && key.i0 == i0 && key.j0 == j0 && key.k0 == k0;
 #pragma unroll
   for (int rep = 0; rep < 2; rep++) {
     const int s = lane + 32 * rep;
@@ -319,6 +332,8 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
         compute_velocity<L, S>(a, ii, jj, kk, src, v0, v1, v2, vr);
         rec[s] = v0; rec[64 + s] = v1; rec[128 + s] = v2; rec[192 + s] = vr;
         u0 = double(v0); u1 = double(v1); u2 = double(v2);
+      } else if (spec && hit) {
+        u0 = double(pre[rep][0]); u1 = double(pre[rep][1]); u2 = double(pre[rep][2]);
       } else {
         node_velocity<L, S>(a, hit, rec, s, ii, jj, kk, src, u0, u1, u2);
       }
@@ -327,8 +342,8 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
       wi += u2 * dd;
       ws += dd;
       wss += dd;
-      if (rep == 0) { sn0 = (long long)src; sd0 = dd; row0 = jj + g.ny * kk; }
-      else { sn1 = (long long)src; sd1 = dd; row1 = jj + g.ny * kk; }
+      if (rep == 0) { sn0 = (long long)src; sd0 = dd; }
+      else { sn1 = (long long)src; sd1 = dd; }
       if (LEARNED && p >= 0) { xs[3 * p] = float(u0); xs[3 * p + 1] = float(u1); xs[3 * p + 2] = float(u2); }
     } else if (t == 1 || t == 3) {
       ws += dd;
@@ -357,12 +372,11 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
     u0 = ui * iw; u1 = vi * iw; u2 = wi * iw;
   }
   // penalty force (fix_couplb.cpp:777-781)
-  const double mass = a.m[mk];
-  double F0 = mass * a.xi_over_dt * (u0 * a.vs - a.v[3 * mk]);
-  double F1 = mass * a.xi_over_dt * (u1 * a.vs - a.v[3 * mk + 1]);
-  double F2 = mass * a.xi_over_dt * (u2 * a.vs - a.v[3 * mk + 2]);
+  double F0 = mass * a.xi_over_dt * (u0 * a.vs - vmk0);
+  double F1 = mass * a.xi_over_dt * (u1 * a.vs - vmk1);
+  double F2 = mass * a.xi_over_dt * (u2 * a.vs - vmk2);
   if (LEARNED) {
-    if (lane < 3) xs[81 + lane] = float(a.v[3 * mk + lane] / a.vs);
+    if (lane < 3) xs[81 + lane] = float((lane == 0 ? vmk0 : (lane == 1 ? vmk1 : vmk2)) / a.vs);
     __syncwarp();
     float y[3];
     mlp_warp_forward(*P, xs, hs, lane, y);
@@ -387,12 +401,12 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
   if (sn0 >= 0) {
     const double w = sd0 * sc;   // couplb_ibm.h:128
     spread_add(a.F + 4 * sn0, fl0 * w, fl1 * w, fl2 * w);
-    if (a.row_force) a.row_force[row0] = 1;
+    if (a.seg_force) a.seg_force[sn0 >> 3] = 1;
   }
   if (sn1 >= 0) {
     const double w = sd1 * sc;
     spread_add(a.F + 4 * sn1, fl0 * w, fl1 * w, fl2 * w);
-    if (a.row_force) a.row_force[row1] = 1;
+    if (a.seg_force) a.seg_force[sn1 >> 3] = 1;
   }
   if (lane == 0 && a.ftot) {
     // one of kFtotSlots accumulators (32 B apart) by marker index: the

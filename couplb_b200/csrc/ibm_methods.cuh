@@ -186,7 +186,6 @@ __device__ __forceinline__ void spread_marker(const IbmArgs<S>& a, int mk, int l
   constexpr int NS = (L::D == 3) ? 64 : 16;
   long long sn0 = -1, sn1 = -1;
   double sd0 = 0.0, sd1 = 0.0;
-  int row0 = 0, row1 = 0;
   double wss = 0.0;
 #pragma unroll
   for (int rep = 0; rep < 2; rep++) {
@@ -203,8 +202,8 @@ __device__ __forceinline__ void spread_marker(const IbmArgs<S>& a, int mk, int l
     const double dd = double(d);
     wss += dd;
     const long long nn = (long long)((size_t)ii + (size_t)g.nx * ((size_t)jj + (size_t)g.ny * kk));
-    if (rep == 0) { sn0 = nn; sd0 = dd; row0 = jj + g.ny * kk; }
-    else { sn1 = nn; sd1 = dd; row1 = jj + g.ny * kk; }
+    if (rep == 0) { sn0 = nn; sd0 = dd; }
+    else { sn1 = nn; sd1 = dd; }
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) wss += __shfl_xor_sync(0xffffffffu, wss, o);
@@ -215,12 +214,12 @@ __device__ __forceinline__ void spread_marker(const IbmArgs<S>& a, int mk, int l
   if (sn0 >= 0) {
     const double wgt = sd0 * sc;
     spread_add(a.F + 4 * sn0, fl0 * wgt, fl1 * wgt, fl2 * wgt);
-    if (a.row_force) a.row_force[row0] = 1;
+    if (a.seg_force) a.seg_force[sn0 >> 3] = 1;
   }
   if (sn1 >= 0) {
     const double wgt = sd1 * sc;
     spread_add(a.F + 4 * sn1, fl0 * wgt, fl1 * wgt, fl2 * wgt);
-    if (a.row_force) a.row_force[row1] = 1;
+    if (a.seg_force) a.seg_force[sn1 >> 3] = 1;
   }
   if (lane == 0 && a.ftot) {
     double* t = a.ftot + 4 * (mk & (kFtotSlots - 1));
@@ -419,7 +418,6 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
   long long nd[2] = {-1, -1};      // interior index of a fluid node, else -1
   double dw[2] = {0.0, 0.0};       // delta weight
   double uu[2][3] = {{0, 0, 0}, {0, 0, 0}}, ir[2] = {0.0, 0.0};
-  int rw[2] = {0, 0};
   double ws = 0.0, wss = 0.0, uwx = 0.0, uwy = 0.0, uwz = 0.0;   // wall velocity sums
   double F0 = 0, F1 = 0, F2 = 0, c0 = 0, c1 = 0, c2 = 0, mxi = 0, vx = 0, vy = 0, vz = 0;
   if (have) {
@@ -465,7 +463,7 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
         } else {
           node_state<L, S>(a, hit, rec, s, ii, jj, kk, n, u0, u1, u2, rho);
         }
-        nd[rep] = (long long)n; dw[rep] = dd; rw[rep] = jj + g.ny * kk;
+        nd[rep] = (long long)n; dw[rep] = dd;
         uu[rep][0] = u0; uu[rep][1] = u1; uu[rep][2] = u2; ir[rep] = 1.0 / rho;
         ui += u0 * dd; vi += u1 * dd; wi += u2 * dd; ws += dd; wss += dd;
         if (LEARNED && p >= 0) { xs[3 * p] = float(u0); xs[3 * p + 1] = float(u1); xs[3 * p + 2] = float(u2); }
@@ -538,7 +536,7 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
       if (nd[rep] < 0) continue;
       const double wgt = dw[rep] * ssc;
       spread_add(a.F + 4 * nd[rep], fl0 * wgt, fl1 * wgt, fl2 * wgt);
-      if (a.row_force) a.row_force[rw[rep]] = 1;
+      if (a.seg_force) a.seg_force[nd[rep] >> 3] = 1;
     }
     if (lane == 0 && a.ftot) {
       double* t = a.ftot + 4 * (mk & (kFtotSlots - 1));

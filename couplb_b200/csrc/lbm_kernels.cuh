@@ -48,7 +48,7 @@ struct LBArgs {
   // reads it and leaves it zero (clear_forces, couplb_lattice.h:243-247) by
   // zeroing the nonzero entries
   typename S::A* __restrict__ F;
-  const unsigned char* __restrict__ row_force;  // per (j,k) row: force present, or null = all
+  const unsigned char* __restrict__ seg_force;  // per 8 nodes (n >> 3): force present, or null = all
   typename S::A* __restrict__ rho_field;  // stale density (see RhoMode)
   int rho_mode;
   int write_rho;
@@ -315,10 +315,22 @@ __device__ __forceinline__ void collide_store_conserved(const float (&f)[L::Q], 
 // populations in f.
 template <class L, class S, class I>
 __device__ __forceinline__ void node_update(const LBArgs<S>& a, typename S::C (&f)[L::Q], int i,
-                                            int j, int k, I n) {
+                                            int j, int k, I n, bool has_force) {
   using C = typename S::C;
   const Geom& g = a.g;
   const I qs = (I)g.qs;
+  // The force of a flagged node is loaded before any other memory operation
+  // of the update, so that its latency overlaps the population loads.
+  // apply_external_force (fix_couplb.cpp:693-707): F += g * rho[n], rho[n]
+  // being the density the last moment pass stored.
+  C Fx = C(0), Fy = C(0), Fz = C(0);
+  if (has_force) {
+    using A = typename S::A;
+    A* p = a.F + 4 * (size_t)n;
+    const A fx = p[0], fy = p[1], fz = p[2];
+    Fx = C(fx); Fy = C(fy); Fz = C(fz);
+    if (fx != A(0) || fy != A(0) || fz != A(0)) { p[0] = A(0); p[1] = A(0); p[2] = A(0); }
+  }
   C r, jx, jy, jz;
   moments<L, C>(f, r, jx, jy, jz);
   // r is rho (plain) or the density deviation (shifted)
@@ -326,16 +338,6 @@ __device__ __forceinline__ void node_update(const LBArgs<S>& a, typename S::C (&
   const C rho_c = clamp_rho(rho, a.status, kStClamps);
   if (rho_c != rho) { rho = rho_c; r = S::kShift ? rho - C(g.rho0) : rho; }
 
-  // apply_external_force (fix_couplb.cpp:693-707): F += g * rho[n], rho[n]
-  // being the density the last moment pass stored.
-  C Fx = C(0), Fy = C(0), Fz = C(0);
-  if (a.F && (!a.row_force || a.row_force[j + g.ny * k])) {
-    using A = typename S::A;
-    A* p = a.F + 4 * (size_t)n;
-    const A fx = p[0], fy = p[1], fz = p[2];
-    Fx = C(fx); Fy = C(fy); Fz = C(fz);
-    if (fx != A(0) || fy != A(0) || fz != A(0)) { p[0] = A(0); p[1] = A(0); p[2] = A(0); }
-  }
   if (a.rho_mode != kRhoNone) {
     C rp;
     if (a.rho_mode == kRhoField) rp = S::kShift ? C(g.rho0) + C(a.rho_field[n]) : C(a.rho_field[n]);
@@ -371,9 +373,10 @@ __global__ void __launch_bounds__(256) k_stream_collide(const LBArgs<S> a) {
   const int j = blockIdx.y, k = blockIdx.z;
   if (i >= g.nx) return;
   const I n = (I)i + (I)g.nx * ((I)j + (I)g.ny * (I)k);
+  const bool hf = a.F && (!a.seg_force || a.seg_force[n >> 3]);
   C f[L::Q];
   load_node<L, S, I, kPull>(g, a.fin, a.rho_field, i, j, k, n, f);
-  node_update<L, S, I>(a, f, i, j, k, n);
+  node_update<L, S, I>(a, f, i, j, k, n, hf);
 }
 
 // ---------------------------------------------------------------------------
@@ -506,6 +509,7 @@ __global__ void __launch_bounds__(256, sizeof(typename S::T) == 8 ? 2 : 3)
     const T* buf = stage0 + s * stage_elems;
     for (int i = threadIdx.x; i < g.nx; i += blockDim.x) {
       const I n = (I)i + (I)g.nx * ((I)j + (I)g.ny * (I)k);
+      const bool hf = a.F && (!a.seg_force || a.seg_force[n >> 3]);
       C f[L::Q];
       if (interior) {
         const int im = (i == 0) ? g.nx - 1 : i - 1;
@@ -518,7 +522,7 @@ __global__ void __launch_bounds__(256, sizeof(typename S::T) == 8 ? 2 : 3)
       } else {
         pull_general<L, S, I>(g, a.fin, a.rho_field, i, j, k, n, f);
       }
-      node_update<L, S, I>(a, f, i, j, k, n);
+      node_update<L, S, I>(a, f, i, j, k, n, hf);
     }
     __syncthreads();   // stage s fully consumed
     if (threadIdx.x == 0) {

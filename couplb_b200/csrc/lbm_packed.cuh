@@ -61,6 +61,9 @@ __global__ void __launch_bounds__(128, MINB) k_stream_collide_x2(const LBArgs<S>
   const I qs = (I)g.qs;
   const I sx = (I)g.nx, sxy = (I)g.nx * (I)g.ny;
   const I n0 = (I)i0 + (I)j * sx + (I)k * sxy;
+  // n0 even: both nodes in one force segment; the flag is read first and the
+  // force right after the populations, so the latencies overlap
+  const bool hf = a.F && (!a.seg_force || a.seg_force[n0 >> 3]);
 
   float2 f[L::Q];
   if (row_is_interior<L>(g, j, k)) {
@@ -88,6 +91,19 @@ __global__ void __launch_bounds__(128, MINB) k_stream_collide_x2(const LBArgs<S>
     for (int q = 0; q < L::Q; q++) f[q] = make_float2(fa[q], fb[q]);
   }
 
+  // apply_external_force (fix_couplb.cpp:693-707)
+  float2 Fx = f2(0.f), Fy = f2(0.f), Fz = f2(0.f);
+  if (hf) {
+    float4* p = reinterpret_cast<float4*>(a.F + 4 * (size_t)n0);
+    const float4 fa = p[0], fb = p[1];
+    Fx = make_float2(fa.x, fb.x);
+    Fy = make_float2(fa.y, fb.y);
+    Fz = make_float2(fa.z, fb.z);
+    // clear_forces: leave the field zero where it was read nonzero
+    if (fa.x != 0.f || fa.y != 0.f || fa.z != 0.f) p[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (fb.x != 0.f || fb.y != 0.f || fb.z != 0.f) p[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+
   // moments (density deviation and momentum), q order
   float2 r = f2(0.f), jx = f2(0.f), jy = f2(0.f), jz = f2(0.f);
 #pragma unroll
@@ -106,18 +122,6 @@ __global__ void __launch_bounds__(128, MINB) k_stream_collide_x2(const LBArgs<S>
     if (cy != rho.y) { rho.y = cy; r.y = cy - rho0; }
   }
 
-  // apply_external_force (fix_couplb.cpp:693-707)
-  float2 Fx = f2(0.f), Fy = f2(0.f), Fz = f2(0.f);
-  if (a.F && (!a.row_force || a.row_force[j + g.ny * k])) {
-    float4* p = reinterpret_cast<float4*>(a.F + 4 * (size_t)n0);
-    const float4 fa = p[0], fb = p[1];
-    Fx = make_float2(fa.x, fb.x);
-    Fy = make_float2(fa.y, fb.y);
-    Fz = make_float2(fa.z, fb.z);
-    // clear_forces: leave the field zero where it was read nonzero
-    if (fa.x != 0.f || fa.y != 0.f || fa.z != 0.f) p[0] = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (fb.x != 0.f || fb.y != 0.f || fb.z != 0.f) p[1] = make_float4(0.f, 0.f, 0.f, 0.f);
-  }
   if (a.rho_mode != kRhoNone) {
     float2 rp = rho;
     if (a.rho_mode == kRhoField) rp = add2(f2(rho0), *reinterpret_cast<const float2*>(a.rho_field + n0));
