@@ -47,6 +47,10 @@ def parse():
                     help="target CPU work of the timed CPU baseline sample")
     ap.add_argument("--ibm-cycles", type=int, default=50,
                     help="LB cycles of the 256^3 IBM point-marker workload (0 = skip)")
+    ap.add_argument("--rods-cycles", type=int, default=20,
+                    help="timed LB cycles of the 512x256x256 many-rod workload (0 = skip)")
+    ap.add_argument("--rods-accuracy-cycles", type=int, default=200,
+                    help="LB cycles of the rod FP32-vs-FP64 accuracy runs (0 = skip)")
     ap.add_argument("--sphere-steps", type=int, default=2000,
                     help="LB steps of the 192^3 sphere-drag runs of the IBM methods (0 = skip)")
     ap.add_argument("--kernel", type=int, default=-1,
@@ -213,31 +217,35 @@ def e2e_fix(steps, warmup, nx, ny, nz, device, torch):
     return dt
 
 
-def ibm_bench(torch, device, prec, cycles, warmup, n=256, natoms=20000, md_per_lb=4, seed=3):
-    """LBM + IBM on the D3Q19 256^3 periodic box with point markers (nu 0.1,
-    uniform random positions, v ~ N(0, 0.01^2), m 1, xi 1, Peskin4,
-    md_per_lb 4).  Markers stay on the device; a velocity-Verlet stand-in for
-    the MD side runs on the same stream.  Timed: the library's own calls (one
-    LB step + md_per_lb IBM sub-steps per LB cycle), CUDA events around them.
-    Also checks momentum conservation per LB interval in FP64."""
+def marker_bench(torch, device, prec, cycles, warmup, box, wall, tau, x0, v0, md_per_lb, workload,
+                 peak, momentum_check, fluid_out=False):
+    """LBM + IBM with point markers (m 1, xi 1, Peskin4).  Markers stay on the
+    device; a velocity-Verlet stand-in for the MD side (markers free, no
+    bonds) runs on the same stream.  Timed: the library's own calls (one LB
+    step + md_per_lb IBM sub-steps per LB cycle), CUDA events around them.
+    momentum_check: in a periodic box the fluid gains per LB interval what the
+    markers lose (FP64 sums on the device)."""
     from couplb_b200.lattice import Lattice
-    L = Lattice(3, n, n, n, tau=3 * 0.1 + 0.5, precision=prec, device=device)
+    nx, ny, nz = box
+    L = Lattice(3, nx, ny, nz, tau=tau, wall=wall, precision=prec, device=device)
     stream = torch.cuda.current_stream()
     L.set_stream(stream.cuda_stream)
     L.init_equilibrium(1.0)
     dt = 1.0 / md_per_lb
     L.set_ibm_params(delta="peskin4", md_per_lb=md_per_lb, xi_ibm=1.0, dt_lbm=1.0, dx=1.0)
-    g = torch.Generator(device="cpu").manual_seed(seed)
-    x = (torch.rand((natoms, 3), generator=g, dtype=torch.float64) * n).cuda()
-    v = (0.01 * torch.randn((natoms, 3), generator=g, dtype=torch.float64)).cuda()
+    natoms = x0.shape[0]
+    x = torch.from_numpy(np.ascontiguousarray(x0)).cuda()
+    v = torch.from_numpy(np.ascontiguousarray(v0)).cuda()
     m = torch.ones(natoms, dtype=torch.float64, device="cuda")
     f = torch.zeros((natoms, 3), dtype=torch.float64, device="cuda")
+    period = torch.tensor([float(nx), float(ny), float(nz)], dtype=torch.float64, device="cuda")
     evs = []
 
     def cycle(timed):
         for s in range(md_per_lb):
             v.add_(f, alpha=0.5 * dt)
-            x.add_(v, alpha=dt).remainder_(n)
+            x.add_(v, alpha=dt)
+            x.copy_(torch.remainder(x, period))
             f.zero_()
             if timed:
                 e0 = torch.cuda.Event(enable_timing=True)
@@ -259,33 +267,83 @@ def ibm_bench(torch, device, prec, cycles, warmup, n=256, natoms=20000, md_per_l
         cycle(True)
     torch.cuda.synchronize()
     ms = sum(a.elapsed_time(b) for a, b in evs) / cycles
-    # momentum balance of one LB interval: the fluid gains what the markers lose
-    L.lbm_step()   # consume the forces still pending from the timed cycles
-    L.macroscopic()
-    p0 = np.array(L.diagnostics().mom)
-    L.ibm_total_force(reset=True)
-    fsum = torch.zeros(3, dtype=torch.float64, device="cuda")
-    for s in range(md_per_lb):
-        f.zero_()
-        L.ibm_substep_device(natoms, x.data_ptr(), v.data_ptr(), m.data_ptr(), f.data_ptr(), 0,
-                             refresh=(s == 0))
-        fsum += f.sum(0)
-    L.lbm_step()
-    L.macroscopic()
-    dp = np.array(L.diagnostics().mom) - p0
-    expect = -(fsum.cpu().numpy()) / md_per_lb
-    err = float(np.abs(dp - expect).max() / max(np.abs(expect).max(), 1e-300))
+    out = {"workload": workload, "precision": prec, "cycles": cycles, "ms_per_lb_cycle": ms}
+    if momentum_check:
+        # momentum balance of one LB interval: the fluid gains what the markers lose
+        L.lbm_step()   # consume the forces still pending from the timed cycles
+        L.macroscopic()
+        p0 = np.array(L.diagnostics().mom)
+        L.ibm_total_force(reset=True)
+        fsum = torch.zeros(3, dtype=torch.float64, device="cuda")
+        for s in range(md_per_lb):
+            f.zero_()
+            L.ibm_substep_device(natoms, x.data_ptr(), v.data_ptr(), m.data_ptr(), f.data_ptr(), 0,
+                                 refresh=(s == 0))
+            fsum += f.sum(0)
+        L.lbm_step()
+        L.macroscopic()
+        dp = np.array(L.diagnostics().mom) - p0
+        expect = -(fsum.cpu().numpy()) / md_per_lb
+        out["momentum_rel_err_per_lb_interval"] = float(
+            np.abs(dp - expect).max() / max(np.abs(expect).max(), 1e-300))
+    if fluid_out:
+        out["_u"] = velocity(L)
+        out["_f"] = f.cpu().numpy()
     clamps, nonfinite = L.read_status()
     L.close()
-    nodes = n ** 3
-    mu = natoms * md_per_lb / (ms * 1e-3)
+    nodes = nx * ny * nz
     b_lu = BYTES_PER_LU[prec] + 3 * (8 if prec == "fp64" else 4)
     b_mk = 64 * (3 * (8 if prec == "fp64" else 4) * 3) + 72
-    return {"workload": f"d3q19_periodic_{n}^3_{natoms}_markers_peskin4_md_per_lb{md_per_lb}",
-            "precision": prec, "ms_per_lb_cycle": ms, "mlups": nodes / (ms * 1e-3) / 1e6,
-            "marker_updates_per_s": mu,
-            "roofline_frac": (nodes * b_lu + natoms * md_per_lb * b_mk) / (ms * 1e-3) / 1e9 / 6460.5,
-            "momentum_rel_err_per_lb_interval": err, "nonfinite": nonfinite}
+    out.update({"mlups": nodes / (ms * 1e-3) / 1e6,
+                "marker_updates_per_s": natoms * md_per_lb / (ms * 1e-3),
+                "bytes_per_lu": b_lu, "bytes_per_marker_update": b_mk,
+                "roofline_frac": (nodes * b_lu + natoms * md_per_lb * b_mk) / (ms * 1e-3) / 1e9 / peak,
+                "nonfinite": nonfinite})
+    return out
+
+
+def ibm_bench(torch, device, prec, cycles, warmup, peak, n=256, natoms=20000, md_per_lb=4, seed=3):
+    """D3Q19 256^3 periodic box, nu 0.1, 20000 point markers at uniform random
+    positions with v ~ N(0, 0.01^2), Peskin4, md_per_lb 4."""
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    x0 = (torch.rand((natoms, 3), generator=g, dtype=torch.float64) * n).numpy()
+    v0 = (0.01 * torch.randn((natoms, 3), generator=g, dtype=torch.float64)).numpy()
+    return marker_bench(torch, device, prec, cycles, warmup, (n, n, n), (0,) * 6, 3 * 0.1 + 0.5, x0, v0,
+                        md_per_lb, f"d3q19_periodic_{n}^3_{natoms}_markers_peskin4_md_per_lb{md_per_lb}",
+                        peak, momentum_check=True)
+
+
+def rods_bench(torch, device, cycles, warmup, acc_cycles, peak, seed=5):
+    """D3Q19 512x256x256, no-slip walls on y, nu 0.08, 2e5 markers as 1000 rods
+    of 200 at unit spacing (seeded centre and orientation, rods within 3 nodes
+    of the y walls redrawn), each rod given one random velocity N(0, 0.01^2),
+    Peskin4, md_per_lb 2.  The markers are free (the MD side has no bonds
+    here).  FP32-shifted and FP64 timed; accuracy: after acc_cycles LB cycles
+    from the same state, the relative L2 error of the FP32 fluid velocity and
+    of the marker forces against FP64."""
+    from couplb_b200.markers import random_rods
+    box = (512, 256, 256)
+    x0 = random_rods(1000, 200, box, seed, wall_margin=3.0)
+    rng = np.random.default_rng(seed + 1)
+    v0 = np.repeat(0.01 * rng.standard_normal((1000, 3)), 200, axis=0)
+    wl = (0, 0, 1, 1, 0, 0)
+    tau = 3 * 0.08 + 0.5
+    name = "d3q19_512x256x256_walls_y_1000_rods_x200_markers_peskin4_md_per_lb2"
+    out = {}
+    for prec in ("fp32", "fp64"):
+        out[prec] = marker_bench(torch, device, prec, cycles, warmup, box, wl, tau, x0, v0, 2, name, peak,
+                                 momentum_check=False)
+    if acc_cycles > 0:
+        r = {p: marker_bench(torch, device, p, acc_cycles, 0, box, wl, tau, x0, v0, 2, name, peak,
+                             momentum_check=False, fluid_out=True) for p in ("fp32", "fp64")}
+        u32, u64 = r["fp32"]["_u"], r["fp64"]["_u"]
+        f32, f64 = r["fp32"]["_f"], r["fp64"]["_f"]
+        out["accuracy"] = {
+            "lb_cycles": acc_cycles,
+            "l2_velocity_err_fp32_vs_fp64": float(np.sqrt(((u32 - u64) ** 2).sum() / (u64 ** 2).sum())),
+            "l2_marker_force_err_fp32_vs_fp64": float(np.sqrt(((f32 - f64) ** 2).sum() / (f64 ** 2).sum())),
+            "umax_fp64": float(np.abs(u64).max())}
+    return out
 
 
 def sphere_bench(torch, device, steps, window=500, sample_rows=2_000_000):
@@ -464,11 +522,6 @@ def main():
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_s = float(t.item())
     acc = accuracy_runs(f0, args.accuracy_steps, nx, ny, nz, local) if args.accuracy_steps else {}
-    ibm = None
-    if args.ibm_cycles > 0:
-        ibm = {p: ibm_bench(torch, local, p, args.ibm_cycles, 3) for p in ("fp32", "fp64")}
-    methods = sphere_bench(torch, local, args.sphere_steps) if args.sphere_steps > 0 else None
-
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -476,6 +529,13 @@ def main():
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+
+    ibm = None
+    if args.ibm_cycles > 0:
+        ibm = {p: ibm_bench(torch, local, p, args.ibm_cycles, 3, peak) for p in ("fp32", "fp64")}
+    rods = (rods_bench(torch, local, args.rods_cycles, 3, args.rods_accuracy_cycles, peak)
+            if args.rods_cycles > 0 else None)
+    methods = sphere_bench(torch, local, args.sphere_steps) if args.sphere_steps > 0 else None
 
     ms32 = results["fp32"]
     mlups = world * N / (ms32 * 1e-3) / 1e6
@@ -504,6 +564,7 @@ def main():
                 "d2h_bytes_per_step": 8},
         "gpu_launches": args.steps,
         "ibm": ibm,
+        "ibm_rods": rods,
         "ibm_methods": methods,
         "clocks": clk,
     }
