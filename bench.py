@@ -55,8 +55,11 @@ def parse():
                     help="LB steps of the 192^3 sphere-drag runs of the IBM methods (0 = skip)")
     ap.add_argument("--kernel", type=int, default=-1,
                     help="fused-kernel variant: -1 auto, 0 plain, 1 staged, 2 packed")
-    ap.add_argument("--only", choices=["fp64", "fp32", "fp16"], default=None,
-                    help="time the fused kernel of one precision only (profiling runs)")
+    ap.add_argument("--only", choices=["fp64", "fp32", "fp16", "ibm"], default=None,
+                    help="time the fused kernel of one precision only, or (ibm) the FP32 LBM + "
+                         "IBM point-marker cycles only (profiling runs)")
+    ap.add_argument("--ibm-n", type=int, default=256,
+                    help="edge of the periodic box of the point-marker workload")
     ap.add_argument("--nx", type=int, default=NX)
     ap.add_argument("--ny", type=int, default=NY)
     ap.add_argument("--nz", type=int, default=NZ)
@@ -83,51 +86,66 @@ def initial_populations(nx, ny, nz, seed=SEED):
 
 # --------------------------------------------------------------------------
 class Clocks:
-    """nvidia-smi sampling of SM clocks / throttle reasons during timing."""
+    """SM clock and clock-event (throttle) reasons sampled through NVML every
+    millisecond in a background thread while the timed region runs (the
+    timed region can be tens of milliseconds, shorter than nvidia-smi's
+    start-up).  start() returns once the first sample is taken."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+             "sw_power_cap": 0x4}
 
     def __init__(self, device):
         self.device = device
-        self.p = None
+        self.thread = None
+
+    def _handle(self, nv):
+        import torch
+        try:
+            pr = torch.cuda.get_device_properties(self.device)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return nv.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.device)
 
     def start(self):
+        import threading
         try:
-            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "100"],
-                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._handle(nv)
+            reasons_fn = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
         except Exception:
-            self.p = None
+            self.thread = None
+            return
+        self.samples, self.mask = [], 0
+        self.stop_ev, first = threading.Event(), threading.Event()
+
+        def run():
+            while not self.stop_ev.is_set():
+                try:
+                    self.samples.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                    self.mask |= int(reasons_fn(h))
+                except Exception:
+                    pass
+                first.set()
+                time.sleep(0.001)
+
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
+        first.wait(5.0)
 
     def stop(self):
-        if self.p is None:
+        if self.thread is None:
             return None
-        self.p.terminate()
-        try:
-            out, _ = self.p.communicate(timeout=5)
-        except Exception:
-            self.p.kill()
+        self.stop_ev.set()
+        self.thread.join(5.0)
+        if not self.samples:
             return None
-        mhz, mx, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in out.strip().splitlines():
-            parts = [s.strip() for s in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                mhz.append(float(parts[1]))
-                mx = max(mx, float(parts[2]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        if not mhz:
-            return None
-        return {"sm_mhz": float(np.median(mhz)), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(mhz)}
+        return {"sm_mhz": float(np.median(self.samples)), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(n for n, b in self.NAMES.items() if self.mask & b),
+                "samples": len(self.samples), "source": "nvml, 1 ms"}
 
 
 # --------------------------------------------------------------------------
@@ -462,6 +480,15 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def load_peak():
+    """HBM copy bandwidth (GB/s) measured on this pool, else the fallback."""
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
 def main():
     global KERNEL
     args = parse()
@@ -483,6 +510,10 @@ def main():
     f0 = initial_populations(nx, ny, nz)
     stream = torch.cuda.Stream()
 
+    if args.only == "ibm":
+        r = ibm_bench(torch, local, "fp32", args.ibm_cycles, args.warmup, load_peak()[0], n=args.ibm_n)
+        print(json.dumps(r), flush=True)
+        return
     if args.only:
         L = make_lattice(args.only, nx, ny, nz, local)
         L.set_stream(stream.cuda_stream)
@@ -522,13 +553,7 @@ def main():
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_s = float(t.item())
     acc = accuracy_runs(f0, args.accuracy_steps, nx, ny, nz, local) if args.accuracy_steps else {}
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except Exception:
-        pass
-    peak = float(peaks.get("hbm_gbs", 6650.0))
-    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    peak, peak_src = load_peak()
 
     ibm = None
     if args.ibm_cycles > 0:
