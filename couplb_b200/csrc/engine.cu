@@ -539,8 +539,13 @@ int couplb_lbm_step(couplb_handle* h, const double* g_lb) {
     }
     if (used == kKernelPlain && want == kKernelStaged && pull) {
       bool ok;
-      if constexpr (sizeof(typename S::T) == 8) ok = launch_staged<L, S, 2>(h, a);
-      else ok = launch_staged<L, S, 3>(h, a);
+      // the staged kernel copies plane rows: plane-major storage only
+      if constexpr (S::kTile == 0) {
+        if constexpr (sizeof(typename S::T) == 8) ok = launch_staged<L, S, 2>(h, a);
+        else ok = launch_staged<L, S, 3>(h, a);
+      } else {
+        ok = false;
+      }
       if (ok) used = kKernelStaged;
     }
     if (used == kKernelPlain) {

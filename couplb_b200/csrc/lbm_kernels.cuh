@@ -2,8 +2,8 @@
 //
 // Device layout (interior nodes only, no ghost layer):
 //   node n = i + nx*(j + ny*k), 0 <= i < nx, 0 <= j < ny, 0 <= k < nz
-//   population q of node n at f[q*qs + n], qs = N rounded up to 64 elements
-//   (every q plane starts 256-byte aligned).
+//   population q of node n at f[pidx(q, n)] = f[q*qs + n], qs = N rounded up
+//   to 64 elements (every q plane starts 256-byte aligned; storage.cuh).
 // Ghost planes of the reference (couplb_lattice.h:82-129) are not stored:
 // a neighbour index that leaves the box selects the wall rule of that face,
 // or wraps around on a periodic face -- the self-exchange of a one-rank
@@ -38,6 +38,16 @@ struct Geom {
   double uw[3];      // type-2 wall velocity
   double rho0;       // shift / reference density
 };
+
+// Element index of population q of interior node n (storage.cuh, kTile).
+template <class L, class S, class I>
+__device__ __forceinline__ I pidx(int q, I n, I qs) {
+  if constexpr (S::kTile == 0) {
+    return (I)q * qs + n;
+  } else {
+    return ((n / (I)S::kTile) * (I)L::Q + (I)q) * (I)S::kTile + n % (I)S::kTile;
+  }
+}
 
 template <class S>
 struct LBArgs {
@@ -117,7 +127,7 @@ __device__ __forceinline__ void pull_general(const Geom& g, const typename S::T*
     const bool oy = sj < 0 || sj >= g.ny;
     const bool oz = (L::D == 3) && (sk < 0 || sk >= g.nz);
     if (!(ox || oy || oz)) {
-      f[q] = S::ld(fin + (q * qs + (I)(si + (I)sj * sx + (I)sk * sxy)));
+      f[q] = S::ld(fin + pidx<L, S, I>(q, (I)(si + (I)sj * sx + (I)sk * sxy), qs));
       continue;
     }
     int t = 0, wd = 0;
@@ -128,17 +138,17 @@ __device__ __forceinline__ void pull_general(const Geom& g, const typename S::T*
       si = si < 0 ? si + g.nx : (si >= g.nx ? si - g.nx : si);
       sj = sj < 0 ? sj + g.ny : (sj >= g.ny ? sj - g.ny : sj);
       if (L::D == 3) sk = sk < 0 ? sk + g.nz : (sk >= g.nz ? sk - g.nz : sk);
-      f[q] = S::ld(fin + (q * qs + (I)si + (I)sj * sx + (I)sk * sxy));
+      f[q] = S::ld(fin + pidx<L, S, I>(q, (I)si + (I)sj * sx + (I)sk * sxy, qs));
     } else if (t == 1) {
-      f[q] = S::ld(fin + (L::opp(q) * qs + n));
+      f[q] = S::ld(fin + pidx<L, S, I>(L::opp(q), n, qs));
     } else if (t == 2) {
       const C eu = C(ex * g.uw[0] + ey * g.uw[1] + ez * g.uw[2]);
-      f[q] = S::ld(fin + (L::opp(q) * qs + n)) + C(2.0 * L::w(L::opp(q)) * 3.0) * rw * eu;
+      f[q] = S::ld(fin + pidx<L, S, I>(L::opp(q), n, qs)) + C(2.0 * L::w(L::opp(q)) * 3.0) * rw * eu;
     } else if (t == 3) {
       const int qr = wd == 0 ? L::refl(0, q) : (wd == 1 ? L::refl(1, q) : L::refl(2, q));
-      f[q] = S::ld(fin + (qr * qs + n));
+      f[q] = S::ld(fin + pidx<L, S, I>(qr, n, qs));
     } else {
-      f[q] = S::ld(fin + (q * qs + n));
+      f[q] = S::ld(fin + pidx<L, S, I>(q, n, qs));
     }
   }
 }
@@ -158,7 +168,7 @@ __device__ __forceinline__ void pull_interior(const Geom& g, const typename S::T
     const int ex = L::ex(q), ey = L::ey(q), ez = L::ez(q);
     const I xs = ex == 1 ? im : (ex == -1 ? ip : (I)i);
     const I ro = row - (I)(ey * g.nx) - (I)ez * sxy;   // unsigned wrap-around is exact
-    f[q] = S::ld(fin + (q * qs + ro + xs));
+    f[q] = S::ld(fin + pidx<L, S, I>(q, ro + xs, qs));
   }
 }
 
@@ -178,7 +188,7 @@ __device__ __forceinline__ void load_node(const Geom& g, const typename S::T* __
   if (!kPull) {
     const I qs = (I)g.qs;
 #pragma unroll
-    for (int q = 0; q < L::Q; q++) f[q] = S::ld(fin + (q * qs + n));
+    for (int q = 0; q < L::Q; q++) f[q] = S::ld(fin + pidx<L, S, I>(q, n, qs));
   } else if (row_is_interior<L>(g, j, k)) {
     pull_interior<L, S, I>(g, fin, i, j, k, f);
   } else {
@@ -292,18 +302,18 @@ __device__ __forceinline__ void collide_store_conserved(const float (&f)[L::Q], 
       da[q - 1] = dp;
       da[q] = dm;
     } else {
-      S::st(fout + (q * qs + n), f[q] + dp);
-      S::st(fout + ((q + 1) * qs + n), f[q + 1] + dm);
+      S::st(fout + pidx<L, S, I>(q, n, qs), f[q] + dp);
+      S::st(fout + pidx<L, S, I>(q + 1, n, qs), f[q + 1] + dm);
     }
   }
   // remove the residuals: mass from the rest population, momentum from the
   // axis pairs (q = 1,2 along x; 3,4 along y; 5,6 along z)
-  S::st(fout + n, f[0] + (d0 - m));
+  S::st(fout + pidx<L, S, I>(0, n, qs), f[0] + (d0 - m));
   const float pr[3] = {0.5f * px, 0.5f * py, 0.5f * pz};
 #pragma unroll
   for (int a = 0; a < L::D; a++) {
-    S::st(fout + ((2 * a + 1) * qs + n), f[2 * a + 1] + (da[2 * a] - pr[a]));
-    S::st(fout + ((2 * a + 2) * qs + n), f[2 * a + 2] + (da[2 * a + 1] + pr[a]));
+    S::st(fout + pidx<L, S, I>(2 * a + 1, n, qs), f[2 * a + 1] + (da[2 * a] - pr[a]));
+    S::st(fout + pidx<L, S, I>(2 * a + 2, n, qs), f[2 * a + 2] + (da[2 * a + 1] + pr[a]));
   }
 }
 
@@ -361,7 +371,7 @@ __device__ __forceinline__ void node_update(const LBArgs<S>& a, typename S::C (&
     C d[L::Q];
     collision_increment<L, C>(f, r, rho, ux, uy, uz, Fx, Fy, Fz, C(a.omega), false, d);
 #pragma unroll
-    for (int q = 0; q < L::Q; q++) S::st(a.fout + (q * qs + n), f[q] + d[q]);
+    for (int q = 0; q < L::Q; q++) S::st(a.fout + pidx<L, S, I>(q, n, qs), f[q] + d[q]);
   }
 }
 
@@ -457,6 +467,7 @@ __device__ __forceinline__ void stage_row(const LBArgs<S>& a, long long r, typen
     mbar_arrive(bar);   // nothing to copy: complete the phase
     return;
   }
+  static_assert(S::kTile == 0, "the staged kernel copies plane-major rows");
   const uint32_t rb = (uint32_t)(g.nx * sizeof(T));
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   mbar_arrive_expect_tx(bar, rb * L::Q);
@@ -595,7 +606,7 @@ __global__ void __launch_bounds__(256) k_materialize(Geom g, const typename S::T
   C f[L::Q];
   load_node<L, S, I, true>(g, fin, rho_field, i, j, k, n, f);
 #pragma unroll
-  for (int q = 0; q < L::Q; q++) S::st(fout + (q * (I)g.qs + n), f[q]);
+  for (int q = 0; q < L::Q; q++) S::st(fout + pidx<L, S, I>(q, n, (I)g.qs), f[q]);
 }
 
 // Equilibrium initial state (Grid::init_equilibrium, couplb_lattice.h:137-154).
@@ -611,7 +622,7 @@ __global__ void k_init_eq(Geom g, typename S::T* __restrict__ f, double rho, dou
   for (int q = 0; q < L::Q; q++) {
     const double eu = L::ex(q) * ux + L::ey(q) * uy + L::ez(q) * uz;
     const double fe = L::w(q) * rho * (1.0 + eu / cs2 + 0.5 * eu * eu / cs4 - 0.5 * uu / cs2);
-    S::st(f + q * g.qs + n, typename S::C(S::kShift ? fe - L::w(q) * g.rho0 : fe));
+    S::st(f + pidx<L, S, long long>(q, n, g.qs), typename S::C(S::kShift ? fe - L::w(q) * g.rho0 : fe));
   }
   if (rho_field) rho_field[n] = typename S::A(S::kShift ? rho - g.rho0 : rho);
 }
@@ -632,7 +643,7 @@ __global__ void k_import_f(Geom g, const double* __restrict__ src, long long G,
 #pragma unroll
   for (int q = 0; q < L::Q; q++) {
     const double v = src[q * G + gn];
-    S::st(f + q * g.qs + n, typename S::C(S::kShift ? v - L::w(q) * g.rho0 : v));
+    S::st(f + pidx<L, S, long long>(q, n, g.qs), typename S::C(S::kShift ? v - L::w(q) * g.rho0 : v));
   }
 }
 
@@ -673,7 +684,7 @@ __global__ void k_export_f(Geom g, const typename S::T* __restrict__ f, long lon
     double v;
     if (t > 0) v = L::w(q) * g.rho0;
     else {
-      v = double(S::ld(f + q * g.qs + src));
+      v = double(S::ld(f + pidx<L, S, long long>(q, src, g.qs)));
       if (S::kShift) v += L::w(q) * g.rho0;
     }
     dst[q * G + gn] = v;

@@ -73,14 +73,15 @@ __global__ void __launch_bounds__(128, MINB) k_stream_collide_x2(const LBArgs<S>
 #pragma unroll
     for (int q = 0; q < L::Q; q++) {
       const int ex = L::ex(q), ey = L::ey(q), ez = L::ez(q);
-      const T* base = a.fin + (q * qs + row - (I)(ey * g.nx) - (I)ez * sxy);
-      const float2 pr = Pair<S>::ld(base + i0);
+      const I ro = row - (I)(ey * g.nx) - (I)ez * sxy;   // source row (unsigned wrap is exact)
+      // ro + i0 is even (nx even): the pair sits in one tile, 2-element aligned
+      const float2 pr = Pair<S>::ld(a.fin + pidx<L, S, I>(q, ro + (I)i0, qs));
       if (ex == 0) {
         f[q] = pr;
       } else if (ex == 1) {
-        f[q] = make_float2(Pair<S>::ld1(base + im), pr.x);
+        f[q] = make_float2(Pair<S>::ld1(a.fin + pidx<L, S, I>(q, ro + im, qs)), pr.x);
       } else {
-        f[q] = make_float2(pr.y, Pair<S>::ld1(base + ip));
+        f[q] = make_float2(pr.y, Pair<S>::ld1(a.fin + pidx<L, S, I>(q, ro + ip, qs)));
       }
     }
   } else {
@@ -185,16 +186,16 @@ __global__ void __launch_bounds__(128, MINB) k_stream_collide_x2(const LBArgs<S>
       da[q - 1] = dp;
       da[q] = dm;
     } else {
-      Pair<S>::st(a.fout + (q * qs + n0), add2(f[q], dp));
-      Pair<S>::st(a.fout + ((q + 1) * qs + n0), add2(f[q + 1], dm));
+      Pair<S>::st(a.fout + pidx<L, S, I>(q, n0, qs), add2(f[q], dp));
+      Pair<S>::st(a.fout + pidx<L, S, I>(q + 1, n0, qs), add2(f[q + 1], dm));
     }
   }
-  Pair<S>::st(a.fout + n0, add2(f[0], sub2(d0, m)));
+  Pair<S>::st(a.fout + pidx<L, S, I>(0, n0, qs), add2(f[0], sub2(d0, m)));
   const float2 pr[3] = {mul2(half, px), mul2(half, py), mul2(half, pz)};
 #pragma unroll
   for (int c = 0; c < L::D; c++) {
-    Pair<S>::st(a.fout + ((2 * c + 1) * qs + n0), add2(f[2 * c + 1], sub2(da[2 * c], pr[c])));
-    Pair<S>::st(a.fout + ((2 * c + 2) * qs + n0), add2(f[2 * c + 2], add2(da[2 * c + 1], pr[c])));
+    Pair<S>::st(a.fout + pidx<L, S, I>(2 * c + 1, n0, qs), add2(f[2 * c + 1], sub2(da[2 * c], pr[c])));
+    Pair<S>::st(a.fout + pidx<L, S, I>(2 * c + 2, n0, qs), add2(f[2 * c + 2], add2(da[2 * c + 1], pr[c])));
   }
 }
 
