@@ -6,6 +6,7 @@ checks the sizes against the compiled library.
 import ctypes as C
 
 PATH_MAX = 256
+VTK_MAX_ATTR = 32
 
 OK = 0
 ERR_ARG = -1
@@ -130,6 +131,7 @@ class FixConfig(C.Structure):
         ("ibm_passes", C.c_int),
         ("slip_tol", C.c_double),
         ("mlp_model", C.c_char * PATH_MAX),
+        ("vtk_solid_attr", (C.c_char * 16) * VTK_MAX_ATTR),
     ]
 
 
@@ -155,6 +157,12 @@ class Atoms(C.Structure):
         ("rmass", C.POINTER(C.c_double)),
         ("mass", C.POINTER(C.c_double)),
         ("type", C.POINTER(C.c_int)),
+        ("tag", C.POINTER(C.c_longlong)),
+        ("molecule", C.POINTER(C.c_longlong)),
+        ("radius", C.POINTER(C.c_double)),
+        ("mu", C.POINTER(C.c_double)),
+        ("omega", C.POINTER(C.c_double)),
+        ("torque", C.POINTER(C.c_double)),
     ]
 
 

@@ -17,6 +17,12 @@
 #include <vector>
 
 #include "../../include/couplb_b200.h"
+#include "vtk_io.h"
+
+using couplb::VtkArray;
+using couplb::write_pvd;
+using couplb::write_vti;
+using couplb::write_vtp;
 
 namespace {
 
@@ -103,6 +109,9 @@ struct couplb_fix {
   std::vector<double> mass_buf;
   std::vector<int> active_buf;
   int vtk_region[6] = {0, 0, 0, 0, 0, 0};
+  double vtk_rlo[3] = {0, 0, 0}, vtk_rhi[3] = {0, 0, 0};   // clamped region, MD units
+  std::vector<long long> vtk_steps;   // steps with field output (the .pvd series)
+  long long vtk_last = -1;            // step of the last field output
 
   int fail(int code, const char* fmt, ...) {
     char buf[512];
@@ -159,6 +168,165 @@ int write_profile(couplb_fix* F, long long step) {
   }
   std::fprintf(fp, "\n");
   std::fclose(fp);
+  return COUPLB_OK;
+}
+
+// IO::write_vtk (couplb_io.h:42-281) + IO::write_pvd (:284-295): the cells of
+// the region (default: the whole grid) with rho * rho_phys, velocity *
+// vel_scale, the node type (0: interior) and the force field * force_scale,
+// as <prefix>_<step>.vti; the series is rewritten as <prefix>.pvd.
+int write_field_vtk(couplb_fix* F, long long step) {
+  const couplb_fix_config& c = F->cfg;
+  const int Nz = F->is3d ? c.Nz : 1;
+  const int r0[6] = {0, c.Nx, 0, c.Ny, 0, Nz};
+  const int* r = c.has_vtk_region ? F->vtk_region : r0;
+  const int ext[3] = {r[1] - r[0], r[3] - r[2], r[5] - r[4]};
+  const size_t ncell = (size_t)ext[0] * ext[1] * ext[2];
+  const size_t G = couplb_ghost_nodes(F->h);
+  std::vector<double> rho(G), ux(G), uy(G), uz(G), fx(G), fy(G), fz(G);
+  int rc = couplb_get_macroscopic(F->h, rho.data(), ux.data(), uy.data(), uz.data());
+  if (!rc) rc = couplb_get_force_field(F->h, fx.data(), fy.data(), fz.data());
+  if (rc) return F->engine_fail(rc);
+  const size_t gx = (size_t)F->nl[0] + 2, gy = (size_t)F->nl[1] + 2;
+  std::vector<VtkArray> a(4);
+  a[0].name = "rho";
+  a[1].name = "velocity_phys"; a[1].ncomp = 3;
+  a[2].name = "type"; a[2].is_int = true;
+  a[3].name = "force_phys"; a[3].ncomp = 3;
+  a[0].f.resize(ncell); a[1].f.resize(3 * ncell); a[2].i.assign(ncell, 0); a[3].f.resize(3 * ncell);
+  size_t c_ = 0;
+  for (int k = r[4]; k < r[5]; k++)
+    for (int j = r[2]; j < r[3]; j++)
+      for (int i = r[0]; i < r[1]; i++, c_++) {
+        const size_t n = (size_t)(i + 1) + gx * ((size_t)(j + 1) + gy * (size_t)(F->is3d ? k + 1 : 0));
+        a[0].f[c_] = rho[n] * c.rho;
+        a[1].f[3 * c_] = ux[n] * F->vel_scale;
+        a[1].f[3 * c_ + 1] = uy[n] * F->vel_scale;
+        a[1].f[3 * c_ + 2] = uz[n] * F->vel_scale;
+        a[3].f[3 * c_] = fx[n] * F->force_scale;
+        a[3].f[3 * c_ + 1] = fy[n] * F->force_scale;
+        a[3].f[3 * c_ + 2] = fz[n] * F->force_scale;
+      }
+  if (F->rank != 0) return COUPLB_OK;
+  char fname[COUPLB_PATH_MAX + 32];
+  std::snprintf(fname, sizeof fname, "%s_%06lld.vti", c.vtk_prefix, step);
+  const double origin[3] = {F->domain_lo[0] + r[0] * F->dx, F->domain_lo[1] + r[2] * F->dx,
+                            F->domain_lo[2] + r[4] * F->dx};
+  if (!write_vti(fname, ext, origin, F->dx, a)) {
+    F->log("CoupLB IO: cannot open %s\n", fname);
+    return COUPLB_OK;
+  }
+  F->log("CoupLB: VTK written at step %lld -> %s (%dx%dx%d region)\n", step, fname, ext[0], ext[1], ext[2]);
+  F->vtk_steps.push_back(step);
+  F->vtk_last = step;
+  write_pvd(std::string(c.vtk_prefix) + ".pvd", c.vtk_prefix, F->vtk_steps, F->dt, "vti");
+  return COUPLB_OK;
+}
+
+// Attributes of vtk_solid (couplb_io.h:366-411): scalars, and the vector
+// groups that are written as one 3-component array when all three
+// components are asked for.
+struct SolidAttr {
+  const char* name;
+  const char* group;   // vector group or nullptr
+  int comp;
+};
+const SolidAttr kSolidAttrs[] = {
+    {"id", nullptr, 0},         {"type", nullptr, 0},       {"mol", nullptr, 0},
+    {"mass", nullptr, 0},       {"diameter", nullptr, 0},   {"x", "position", 0},
+    {"y", "position", 1},       {"z", "position", 2},       {"vx", "velocity", 0},
+    {"vy", "velocity", 1},      {"vz", "velocity", 2},      {"fx", "force", 0},
+    {"fy", "force", 1},         {"fz", "force", 2},         {"mux", "dipole", 0},
+    {"muy", "dipole", 1},       {"muz", "dipole", 2},       {"omegax", "omega", 0},
+    {"omegay", "omega", 1},     {"omegaz", "omega", 2},     {"tqx", "torque", 0},
+    {"tqy", "torque", 1},       {"tqz", "torque", 2}};
+
+const SolidAttr* find_attr(const char* a) {
+  for (const SolidAttr& s : kSolidAttrs)
+    if (!std::strcmp(s.name, a)) return &s;
+  return nullptr;
+}
+
+bool solid_attr_known(const char* a) { return find_attr(a) != nullptr; }
+
+// Per-atom value of an attribute; false if the array is not available.
+bool attr_value(const couplb_atoms* at, const char* name, int i, double* v) {
+  const std::string a(name);
+  if (a == "id") { if (!at->tag) return false; *v = (double)at->tag[i]; }
+  else if (a == "type") { if (!at->type) return false; *v = at->type[i]; }
+  else if (a == "mol") { if (!at->molecule) return false; *v = (double)at->molecule[i]; }
+  else if (a == "mass") {
+    if (at->rmass) *v = at->rmass[i];
+    else if (at->mass && at->type) *v = at->mass[at->type[i]];
+    else return false;
+  } else if (a == "diameter") { if (!at->radius) return false; *v = 2.0 * at->radius[i]; }
+  else if (a == "x" || a == "y" || a == "z") *v = at->x[3 * i + (a[0] - 'x')];
+  else if (a == "vx" || a == "vy" || a == "vz") *v = at->v[3 * i + (a[1] - 'x')];
+  else if (a == "fx" || a == "fy" || a == "fz") *v = at->f[3 * i + (a[1] - 'x')];
+  else if (a.rfind("mu", 0) == 0) { if (!at->mu) return false; *v = at->mu[4 * i + (a[2] - 'x')]; }
+  else if (a.rfind("omega", 0) == 0) { if (!at->omega) return false; *v = at->omega[3 * i + (a[5] - 'x')]; }
+  else if (a.rfind("tq", 0) == 0) { if (!at->torque) return false; *v = at->torque[3 * i + (a[2] - 'x')]; }
+  else return false;
+  return true;
+}
+
+// IO::write_solid_vtk (couplb_io.h:309-614) + IO::write_pvd_vtp: the group's
+// atoms inside the clamped VTK region as PolyData vertices.
+int write_solid_vtk(couplb_fix* F, const couplb_atoms* at, long long step) {
+  const couplb_fix_config& c = F->cfg;
+  const int na = c.vtk_solid_nattr;
+  // output fields: a vector group once when all three components are asked
+  struct Out { std::string name; const char* comp[3]; int ncomp; };
+  std::vector<Out> outs;
+  std::vector<std::string> done;
+  for (int k = 0; k < na; k++) {
+    const SolidAttr* s = find_attr(c.vtk_solid_attr[k]);
+    if (!s) return F->fail(COUPLB_ERR_ARG, "fix couplb vtk_solid: unknown attribute '%s'", c.vtk_solid_attr[k]);
+    if (s->group) {
+      bool seen = false;
+      for (const std::string& d : done) seen |= (d == s->group);
+      if (seen) continue;
+      const char* comp[3] = {nullptr, nullptr, nullptr};
+      for (int m = 0; m < na; m++) {
+        const SolidAttr* q = find_attr(c.vtk_solid_attr[m]);
+        if (q && q->group && !std::strcmp(q->group, s->group)) comp[q->comp] = q->name;
+      }
+      if (comp[0] && comp[1] && comp[2]) {
+        outs.push_back({s->group, {comp[0], comp[1], comp[2]}, 3});
+        done.push_back(s->group);
+        continue;
+      }
+    }
+    outs.push_back({s->name, {s->name, nullptr, nullptr}, 1});
+  }
+  std::vector<double> pts;
+  std::vector<VtkArray> fields(outs.size());
+  for (size_t o = 0; o < outs.size(); o++) { fields[o].name = outs[o].name; fields[o].ncomp = outs[o].ncomp; }
+  for (int i = 0; i < at->nlocal; i++) {
+    if (at->mask && !(at->mask[i] & at->groupbit)) continue;
+    if (c.has_vtk_region) {
+      bool in = true;
+      for (int d = 0; d < 3; d++) in &= at->x[3 * i + d] >= F->vtk_rlo[d] && at->x[3 * i + d] < F->vtk_rhi[d];
+      if (!in) continue;
+    }
+    for (int d = 0; d < 3; d++) pts.push_back(at->x[3 * i + d]);
+    for (size_t o = 0; o < outs.size(); o++)
+      for (int d = 0; d < outs[o].ncomp; d++) {
+        double v = 0.0;
+        if (!attr_value(at, outs[o].comp[d], i, &v))
+          return F->fail(COUPLB_ERR_ARG, "fix couplb vtk_solid: attribute '%s' is not available for these atoms",
+                         outs[o].comp[d]);
+        fields[o].f.push_back(v);
+      }
+  }
+  if (F->rank != 0) return COUPLB_OK;
+  char fname[COUPLB_PATH_MAX + 40];
+  std::snprintf(fname, sizeof fname, "%s_solid_%06lld.vtp", c.vtk_prefix, step);
+  if (!write_vtp(fname, pts, fields)) return F->fail(COUPLB_ERR_IO, "CoupLB IO: cannot open %s", fname);
+  F->log("CoupLB: solid VTK written at step %lld -> %s (%d atoms, %d fields)\n", step, fname,
+         (int)(pts.size() / 3), (int)fields.size());
+  write_pvd(std::string(c.vtk_prefix) + "_solid.pvd", std::string(c.vtk_prefix) + "_solid", F->vtk_steps,
+            F->dt, "vtp");
   return COUPLB_OK;
 }
 
@@ -383,7 +551,12 @@ int couplb_fix_parse(int narg, const char* const* arg, int dimension, couplb_fix
         if (c.vtk_solid_nattr) perr("fix couplb vtk_solid: keyword specified more than once");
         iarg++;
         int na = 0;
-        while (iarg < narg && !is_keyword(arg[iarg])) { na++; iarg++; }
+        while (iarg < narg && !is_keyword(arg[iarg])) {
+          if (na >= COUPLB_VTK_MAX_ATTR) perr("fix couplb vtk_solid: too many attributes");
+          std::snprintf(c.vtk_solid_attr[na], sizeof(c.vtk_solid_attr[na]), "%s", arg[iarg]);
+          na++;
+          iarg++;
+        }
         if (na == 0) perr("fix couplb vtk_solid: need at least one attribute");
         c.vtk_solid_nattr = na;
       } else if (!std::strcmp(kw, "checkpoint")) {
@@ -646,6 +819,7 @@ int couplb_fix_init(couplb_fix* F, const couplb_domain* dom) {
       rlo[d] = std::max(c.vtk_rlo[d], F->domain_lo[d]);
       rhi[d] = std::min(c.vtk_rhi[d], F->domain_hi[d]);
     }
+    for (int d = 0; d < 3; d++) { F->vtk_rlo[d] = rlo[d]; F->vtk_rhi[d] = rhi[d]; }
     int* r = F->vtk_region;
     r[0] = (int)std::floor((rlo[0] - F->domain_lo[0]) / F->dx);
     r[1] = (int)std::ceil((rhi[0] - F->domain_lo[0]) / F->dx);
@@ -663,8 +837,11 @@ int couplb_fix_init(couplb_fix* F, const couplb_domain* dom) {
                      "fix couplb vtk_region: empty or inverted region ([%d,%d]x[%d,%d]x[%d,%d]). Check that xlo<xhi, ylo<yhi%s",
                      r[0], r[1], r[2], r[3], r[4], r[5], F->is3d ? ", zlo<zhi" : "");
   }
-  if (c.vtk_every > 0)
-    F->log("CoupLB WARNING: vtk output is not written by the GPU build (keyword accepted, ignored)\n");
+  for (int a = 0; a < c.vtk_solid_nattr; a++)
+    if (!solid_attr_known(c.vtk_solid_attr[a]))
+      return F->fail(COUPLB_ERR_ARG, "fix couplb vtk_solid: unknown attribute '%s'", c.vtk_solid_attr[a]);
+  F->vtk_steps.clear();
+  F->vtk_last = -1;
   F->log("CoupLB: %dD grid %dx%dx%d tau=%.6f nu=%.6f rho=%.4f\n", dim, c.Nx, c.Ny, c.Nz, F->tau, c.nu, c.rho);
   F->log("CoupLB: nu=%.4e -> nu_lb=%.6f\n", c.nu, F->nu_lb);
   F->log("CoupLB: dx=%.4e dt_LBM=%.4e vel_scale=%.4e force_scale=%.4e\n", F->dx, F->dt_LBM, F->vel_scale,
@@ -775,8 +952,15 @@ int couplb_fix_end_of_step(couplb_fix* F, long long step) {
     if (d.clamps > 0) F->log("CoupLB WARNING: %d nodes had density clamped at step %lld\n", d.clamps, step);
   }
   if (out && (rc = write_profile(F, step))) return rc;
+  if (vtk && (rc = write_field_vtk(F, step))) return rc;
   if (ckpt && (rc = write_checkpoint(F, step))) return rc;
   return COUPLB_OK;
+}
+
+int couplb_fix_write_solid(couplb_fix* F, const couplb_atoms* at, long long step) {
+  if (!F || !at) return COUPLB_ERR_ARG;
+  if (F->cfg.vtk_solid_nattr <= 0 || F->vtk_last != step) return COUPLB_OK;
+  return write_solid_vtk(F, at, step);
 }
 
 }  // extern "C"

@@ -120,6 +120,11 @@ class FixCoupLB:
     def end_of_step(self, ntimestep):
         self._ck(self.L.couplb_fix_end_of_step(self.h, ntimestep))
 
+    def write_solid(self, atoms, ntimestep):
+        """vtk_solid output of the step end_of_step just handled (no-op on
+        other steps)."""
+        self._ck(self.L.couplb_fix_write_solid(self.h, C.byref(atoms), ntimestep))
+
     # -- accessors ----------------------------------------------------------
     def scales(self):
         out = np.empty(6)

@@ -80,6 +80,7 @@ SIGNATURES = {
     "couplb_fix_setup": (C.c_int, [_H, C.POINTER(abi.Atoms), C.c_longlong]),
     "couplb_fix_post_force": (C.c_int, [_H, C.POINTER(abi.Atoms), C.c_longlong]),
     "couplb_fix_end_of_step": (C.c_int, [_H, C.c_longlong]),
+    "couplb_fix_write_solid": (C.c_int, [_H, C.POINTER(abi.Atoms), C.c_longlong]),
     "couplb_fix_handle": (_H, [_H]),
     "couplb_fix_scales": (C.c_int, [_H, _D]),
     "couplb_fix_last_diag": (C.c_int, [_H, C.POINTER(abi.Diag)]),

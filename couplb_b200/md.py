@@ -8,6 +8,8 @@ half-kicks again and calls end_of_step().  Any object with setup /
 post_force / end_of_step taking an Atoms struct works (the GPU FixCoupLB or
 the CPU oracle).
 """
+import ctypes as C
+
 import numpy as np
 
 from . import abi
@@ -16,7 +18,8 @@ from . import abi
 class Atoms:
     """Per-atom arrays in LAMMPS layout ((n,3) x, v, f; masses; group mask)."""
 
-    def __init__(self, x, v=None, mass=None, mask=None, groupbit=1, integrate=True):
+    def __init__(self, x, v=None, mass=None, mask=None, groupbit=1, integrate=True, tag=None,
+                 type_=None):
         self.x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 3)
         n = self.x.shape[0]
         self.v = np.zeros((n, 3)) if v is None else np.ascontiguousarray(v, dtype=np.float64).reshape(-1, 3)
@@ -26,6 +29,8 @@ class Atoms:
         self.groupbit = groupbit
         self.integrate = integrate
         self.fext = None   # constant external force (fix addforce), (n,3) or None
+        self.tag = None if tag is None else np.ascontiguousarray(tag, dtype=np.int64)
+        self.type = None if type_ is None else np.ascontiguousarray(type_, dtype=np.int32)
 
     @property
     def n(self):
@@ -34,8 +39,11 @@ class Atoms:
     def struct(self):
         if self.n == 0:
             return abi.make_atoms(None, None, None)
-        return abi.make_atoms(self.x, self.v, self.f, mask=self.mask, groupbit=self.groupbit,
-                              rmass=self.rmass)
+        at = abi.make_atoms(self.x, self.v, self.f, mask=self.mask, groupbit=self.groupbit,
+                            rmass=self.rmass, type_=self.type)
+        if self.tag is not None:
+            at.tag = self.tag.ctypes.data_as(C.POINTER(C.c_longlong))
+        return at
 
 
 def empty_atoms():
@@ -63,6 +71,8 @@ def run(fix, atoms, nsteps, dt, start_step=0, setup=True, box=None, on_step=None
         if atoms.n and atoms.integrate:
             atoms.v += 0.5 * dt * atoms.f * minv
         fix.end_of_step(step)
+        if hasattr(fix, "write_solid"):
+            fix.write_solid(at, step)
         if on_step is not None:
             on_step(step)
     return step

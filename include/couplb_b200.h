@@ -337,6 +337,8 @@ size_t couplb_device_bytes(const couplb_handle* h);
 
 #define COUPLB_PATH_MAX 256
 
+#define COUPLB_VTK_MAX_ATTR 32
+
 /* Parsed arguments of `fix couplb` (fix_couplb.cpp:71-238). */
 typedef struct couplb_fix_config {
   int    Nx, Ny, Nz;
@@ -373,6 +375,7 @@ typedef struct couplb_fix_config {
   int    ibm_passes;
   double slip_tol;
   char   mlp_model[COUPLB_PATH_MAX];
+  char   vtk_solid_attr[COUPLB_VTK_MAX_ATTR][16];  /* vtk_solid attribute names */
 } couplb_fix_config;
 
 /* The MD side of one subdomain (LAMMPS: domain, update). */
@@ -396,6 +399,13 @@ typedef struct couplb_atoms {
   const double* rmass;       /* nlocal per-atom masses, or NULL              */
   const double* mass;        /* per-type masses indexed by type, if !rmass   */
   const int*    type;        /* nlocal, used with mass                       */
+  /* optional arrays, read only by the vtk_solid output (NULL when absent) */
+  const long long* tag;      /* nlocal atom IDs                              */
+  const long long* molecule; /* nlocal molecule IDs                          */
+  const double* radius;      /* nlocal                                       */
+  const double* mu;          /* nlocal*4 dipole x, y, z, |mu|                */
+  const double* omega;       /* nlocal*3                                     */
+  const double* torque;      /* nlocal*3                                     */
 } couplb_atoms;
 
 typedef struct couplb_fix couplb_fix;
@@ -433,6 +443,15 @@ int  couplb_fix_setup(couplb_fix* fx, const couplb_atoms* at,
 int  couplb_fix_post_force(couplb_fix* fx, const couplb_atoms* at,
                            long long ntimestep);                      /* :640-651 */
 int  couplb_fix_end_of_step(couplb_fix* fx, long long ntimestep);     /* :846-901 */
+/* The solid part of end_of_step's VTK output (IO::write_solid_vtk,
+ * couplb_io.h:309-614, and the solid .pvd): the atoms are not an argument of
+ * end_of_step, so a driver calls this right after it with the same step.  It
+ * writes <prefix>_solid_<step>.vtp and <prefix>_solid.pvd when that
+ * end_of_step wrote field output and vtk_solid is set; otherwise it returns
+ * COUPLB_OK doing nothing.  Files are VTK XML with binary appended data (the
+ * reference writes ASCII) and the same names and layout. */
+int  couplb_fix_write_solid(couplb_fix* fx, const couplb_atoms* at,
+                            long long ntimestep);
 
 /* Accessors for drivers and tests. */
 couplb_handle* couplb_fix_handle(couplb_fix* fx);

@@ -98,3 +98,12 @@ def test_ibm_method_errors(cuda_lib, tail, msg):
     with pytest.raises(CoupLBError) as e:
         P("f all couplb 8 8 8 0.1 1.0 " + tail)
     assert msg in e.value.msg
+
+
+def test_vtk_solid_attribute_names(cuda_lib):
+    c = P("f all couplb 8 8 8 0.1 1.0 vtk 10 out vtk_solid x y z vx id md_per_lb 2")
+    assert c.vtk_solid_nattr == 5 and c.md_per_lb == 2
+    assert [c.vtk_solid_attr[i].value for i in range(5)] == [b"x", b"y", b"z", b"vx", b"id"]
+    with pytest.raises(CoupLBError) as e:
+        P("f all couplb 8 8 8 0.1 1.0 vtk_solid " + " ".join(["x"] * 40))
+    assert "too many attributes" in e.value.msg
