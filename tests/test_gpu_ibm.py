@@ -1,6 +1,6 @@
 """GPU immersed-boundary sub-step against the oracle and golden vectors.
 
-Tolerances (north star): per-atom IBM forces within 1e-11 relative, Eulerian
+Tolerances: per-atom IBM forces within 1e-11 relative, Eulerian
 force field within 1e-12 relative, FP64.  The FP32 path is bounded loosely.
 """
 import os

@@ -1,6 +1,6 @@
 """GPU lattice kernels against the CPU oracle and the reference's golden vectors.
 
-Tolerances (north star): the FP64 GPU path matches the oracle's fields within
+Tolerances: the FP64 GPU path matches the oracle's fields within
 1e-12 relative (max |a-b| / max |b| over the field); the FP32-shifted path is
 checked by its relative L2 velocity error against FP64; FP16 storage is
 reported with a loose bound.
