@@ -55,9 +55,10 @@ def parse():
                     help="LB steps of the 192^3 sphere-drag runs of the IBM methods (0 = skip)")
     ap.add_argument("--kernel", type=int, default=-1,
                     help="fused-kernel variant: -1 auto, 0 plain, 1 staged, 2 packed")
-    ap.add_argument("--only", choices=["fp64", "fp32", "fp16", "ibm"], default=None,
-                    help="time the fused kernel of one precision only, or (ibm) the FP32 LBM + "
-                         "IBM point-marker cycles only (profiling runs)")
+    ap.add_argument("--only", choices=["fp64", "fp32", "fp16", "ibm", "methods"], default=None,
+                    help="time the fused kernel of one precision only, (ibm) the FP32 LBM + "
+                         "IBM point-marker cycles only, or (methods) the IBM call of the "
+                         "sphere-drag methods with an untrained network (profiling runs)")
     ap.add_argument("--ibm-n", type=int, default=256,
                     help="edge of the periodic box of the point-marker workload")
     ap.add_argument("--nx", type=int, default=NX)
@@ -510,6 +511,22 @@ def main():
     f0 = initial_populations(nx, ny, nz)
     stream = torch.cuda.Stream()
 
+    if args.only == "methods":
+        from couplb_b200 import sphere_drag as SD
+        from couplb_b200.mlp import CorrectionNet
+        net = CorrectionNet(local, seed=1)
+        out = {}
+        for name, kw in (("single", dict(method="iterative", passes=1)),
+                         ("iterative5", dict(method="iterative", passes=5)),
+                         ("learned", dict(method="learned", passes=5, slip_tol=1e30, net=net))):
+            c = SD.SphereCase(device=local)
+            c.set_method(**kw)
+            c.run(args.warmup)
+            out[name] = c.time_forcing(args.steps)[0]
+            c.close()
+        net.close()
+        print(json.dumps({"only": "methods", "ms_ibm": out}), flush=True)
+        return
     if args.only == "ibm":
         r = ibm_bench(torch, local, "fp32", args.ibm_cycles, args.warmup, load_peak()[0], n=args.ibm_n)
         print(json.dumps(r), flush=True)
