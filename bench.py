@@ -208,7 +208,9 @@ def e2e_fix(steps, warmup, nx, ny, nz, device, torch):
     """Same metric through the fix hooks of the C ABI: per step one
     couplb_fix_post_force (host atom arrays; none in this workload) and one
     couplb_fix_end_of_step, then the device status word (clamp / non-finite
-    counts, 8 bytes) read back as the fix's per-step failure check."""
+    counts, 8 bytes) read back as the per-step failure check, pipelined: each
+    step posts its copy and checks the previous step's (couplb_status_post /
+    couplb_status_last), so the host never drains the device queue."""
     from couplb_b200 import md
     from couplb_b200.fix import FixCoupLB
     f0 = initial_populations(nx, ny, nz)
@@ -227,10 +229,13 @@ def e2e_fix(steps, warmup, nx, ny, nz, device, torch):
     for s in range(warmup + 1, warmup + steps + 1):
         fix.post_force(at, s)
         fix.end_of_step(s)
-        clamps, nonfinite = fix.lattice.read_status()
+        fix.lattice.status_post()
+        clamps, nonfinite = fix.lattice.status_last()
         if nonfinite:
             raise RuntimeError("non-finite density")
     torch.cuda.synchronize()
+    if fix.lattice.read_status()[1]:
+        raise RuntimeError("non-finite density")
     dt = (time.perf_counter() - t0) / steps
     fix.close()
     return dt

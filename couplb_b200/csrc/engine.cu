@@ -350,6 +350,11 @@ int couplb_create(const couplb_lattice_params* p, couplb_handle** out) {
   static_assert(sizeof(double) * 4 * kFtotSlots <= 4096, "h_small holds the force accumulators");
   if (!rc && cudaMallocHost(&h->h_small, 4096) != cudaSuccess)
     rc = fail(h, COUPLB_ERR_CUDA, "cudaMallocHost failed");
+  if (!rc && cudaMallocHost((void**)&h->h_status_ring, sizeof(int) * 16) != cudaSuccess)
+    rc = fail(h, COUPLB_ERR_CUDA, "cudaMallocHost failed");
+  for (int e = 0; e < 2 && !rc; e++)
+    if (cudaEventCreateWithFlags(&h->status_ev[e], cudaEventDisableTiming) != cudaSuccess)
+      rc = fail(h, COUPLB_ERR_CUDA, "cudaEventCreate failed");
   if (rc) {
     g_create_error = h->err;
     couplb_destroy(h);
@@ -390,6 +395,9 @@ int couplb_destroy(couplb_handle* h) {
   dfree(h->d_x); dfree(h->d_v); dfree(h->d_m); dfree(h->d_fout); dfree(h->d_active);
   if (h->h_fout) cudaFreeHost(h->h_fout);
   if (h->h_small) cudaFreeHost(h->h_small);
+  if (h->h_status_ring) cudaFreeHost(h->h_status_ring);
+  for (int e = 0; e < 2; e++)
+    if (h->status_ev[e]) cudaEventDestroy(h->status_ev[e]);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return COUPLB_OK;
@@ -727,6 +735,33 @@ int couplb_read_status(couplb_handle* h, int* clamps, int* nonfinite, int reset)
   CK(cudaStreamSynchronize(h->stream));
   if (clamps) *clamps = hi[kStClamps];
   if (nonfinite) *nonfinite = hi[kStNonfinite];
+  return COUPLB_OK;
+}
+
+int couplb_status_post(couplb_handle* h) {
+  if (!h) return COUPLB_ERR_ARG;
+  int rc = set_device(h);
+  if (rc) return rc;
+  const int slot = (int)(h->status_posts & 1);
+  CK(cudaMemcpyAsync(h->h_status_ring + 8 * slot, h->d_status, sizeof(int) * 2, cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaEventRecord(h->status_ev[slot], h->stream));
+  h->status_posts++;
+  return COUPLB_OK;
+}
+
+int couplb_status_last(couplb_handle* h, int* clamps, int* nonfinite) {
+  if (!h) return COUPLB_ERR_ARG;
+  int c = 0, nf = 0;
+  if (h->status_posts > 0) {
+    const long long want = h->status_posts >= 2 ? h->status_posts - 2 : 0;
+    const int slot = (int)(want & 1);
+    CK(cudaEventSynchronize(h->status_ev[slot]));
+    c = h->h_status_ring[8 * slot + kStClamps];
+    nf = h->h_status_ring[8 * slot + kStNonfinite];
+  }
+  if (clamps) *clamps = c;
+  if (nonfinite) *nonfinite = nf;
   return COUPLB_OK;
 }
 

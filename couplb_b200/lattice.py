@@ -112,6 +112,16 @@ class Lattice:
         self._ck(self.L.couplb_read_status(self.h, C.byref(a), C.byref(b), int(reset)))
         return a.value, b.value
 
+    def status_post(self):
+        """Enqueue a copy of the status word (pipelined per-step check)."""
+        self._ck(self.L.couplb_status_post(self.h))
+
+    def status_last(self):
+        """(clamps, nonfinite) of the post before the latest one."""
+        c, nf = C.c_int(0), C.c_int(0)
+        self._ck(self.L.couplb_status_last(self.h, C.byref(c), C.byref(nf)))
+        return c.value, nf.value
+
     def synchronize(self):
         self._ck(self.L.couplb_synchronize(self.h))
 

@@ -46,6 +46,8 @@ SIGNATURES = {
                                             C.c_void_p, C.c_void_p, C.c_int]),
     "couplb_ibm_total_force": (C.c_int, [_H, _D, C.c_int]),
     "couplb_read_status": (C.c_int, [_H, _I, _I, C.c_int]),
+    "couplb_status_post": (C.c_int, [_H]),
+    "couplb_status_last": (C.c_int, [_H, _I, _I]),
     "couplb_set_ibm_method": (C.c_int, [_H, C.POINTER(abi.IbmMethod)]),
     "couplb_ibm_slip": (C.c_int, [_H, _D, C.c_int]),
     "couplb_ibm_record": (C.c_int, [_H, C.c_void_p, C.c_longlong]),

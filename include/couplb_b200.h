@@ -311,6 +311,13 @@ int  couplb_mlp_load(couplb_mlp* m, const char* path);
 /* Device status word: counts of density clamps / non-finite densities seen by
  * the stepping kernels since the last reset.  Reading synchronises. */
 int  couplb_read_status(couplb_handle* h, int* clamps, int* nonfinite, int reset);
+/* Pipelined form of the same read (no counterpart in the reference): post
+ * enqueues a copy of the status word on the handle's stream; last returns the
+ * counts of the post before the latest one, waiting only for that copy, so a
+ * per-step failure check keeps the next step queued on the device.  With a
+ * single post, last waits for it.  Both return zeros before any post. */
+int  couplb_status_post(couplb_handle* h);
+int  couplb_status_last(couplb_handle* h, int* clamps, int* nonfinite);
 
 /* Runtime options of a handle (no counterpart in the reference):
  *   "kernel"      variant of the fused LB kernel: -1 auto (default: packed for

@@ -163,3 +163,25 @@ def test_nonfinite_density_is_reported_not_trapped(cuda_lib):
     L.set_populations(cases.initial_populations(3, (8, 6, 5), 3))
     L.lbm_step()
     assert L.read_status() == (0, 0)
+
+
+def test_pipelined_status_read(cuda_lib):
+    """couplb_status_post / couplb_status_last: the counts of the post before
+    the latest one, without draining the stream."""
+    n = (16, 12, 10)
+    L = Lattice(3, *n, tau=0.8)
+    assert L.status_last() == (0, 0)          # nothing posted yet
+    L.set_populations(cases.initial_populations(3, n, 5))
+    L.lbm_step()
+    L.status_post()
+    assert L.status_last() == (0, 0)          # one post: waits for it
+    f0 = cases.initial_populations(3, n, 5)
+    f0[4, 3, 3, 3] = np.nan
+    L.set_populations(f0)
+    L.lbm_step()
+    L.status_post()                           # sees the non-finite density
+    L.lbm_step()
+    L.status_post()
+    clamps, nonfinite = L.status_last()       # the previous post
+    assert nonfinite >= 1 and clamps >= 1
+    L.close()
