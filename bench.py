@@ -354,19 +354,19 @@ def rods_bench(torch, device, cycles, warmup, acc_cycles, peak, seed=5):
     tau = 3 * 0.08 + 0.5
     name = "d3q19_512x256x256_walls_y_1000_rods_x200_markers_peskin4_md_per_lb2"
     out = {}
-    for prec in ("fp32", "fp64"):
+    for prec in ("fp32", "fp16", "fp64"):
         out[prec] = marker_bench(torch, device, prec, cycles, warmup, box, wl, tau, x0, v0, 2, name, peak,
                                  momentum_check=False)
     if acc_cycles > 0:
         r = {p: marker_bench(torch, device, p, acc_cycles, 0, box, wl, tau, x0, v0, 2, name, peak,
-                             momentum_check=False, fluid_out=True) for p in ("fp32", "fp64")}
-        u32, u64 = r["fp32"]["_u"], r["fp64"]["_u"]
-        f32, f64 = r["fp32"]["_f"], r["fp64"]["_f"]
-        out["accuracy"] = {
-            "lb_cycles": acc_cycles,
-            "l2_velocity_err_fp32_vs_fp64": float(np.sqrt(((u32 - u64) ** 2).sum() / (u64 ** 2).sum())),
-            "l2_marker_force_err_fp32_vs_fp64": float(np.sqrt(((f32 - f64) ** 2).sum() / (f64 ** 2).sum())),
-            "umax_fp64": float(np.abs(u64).max())}
+                             momentum_check=False, fluid_out=True) for p in ("fp32", "fp16", "fp64")}
+        u64, f64 = r["fp64"]["_u"], r["fp64"]["_f"]
+        acc = {"lb_cycles": acc_cycles, "umax_fp64": float(np.abs(u64).max())}
+        for p in ("fp32", "fp16"):
+            u, f = r[p]["_u"], r[p]["_f"]
+            acc[f"l2_velocity_err_{p}_vs_fp64"] = float(np.sqrt(((u - u64) ** 2).sum() / (u64 ** 2).sum()))
+            acc[f"l2_marker_force_err_{p}_vs_fp64"] = float(np.sqrt(((f - f64) ** 2).sum() / (f64 ** 2).sum()))
+        out["accuracy"] = acc
     return out
 
 
@@ -399,16 +399,19 @@ def sphere_bench(torch, device, steps, window=500, sample_rows=2_000_000):
     del rows
     for name, kw in cfgs.items():
         res = {}
-        for prec in ("fp32", "fp64"):
+        for prec in ("fp32", "fp16", "fp64"):
             c = SD.SphereCase(offset=off, precision=prec, device=device)
             c.set_method(**kw)
             sl, drag = c.run(steps, slip_from=steps - window)
             if prec == "fp32":
                 ibm, tot = c.time_forcing(200)
                 res.update(slip=float(np.mean(sl)), drag=drag, ms_ibm=ibm, ms_step=tot)
+            elif prec == "fp16":
+                res.update(slip_fp16=float(np.mean(sl)), drag_fp16=drag)
             else:
                 res.update(slip_fp64=float(np.mean(sl)), drag_fp64=drag,
-                           drag_err_fp32_vs_fp64=abs(res["drag"] - drag) / abs(drag))
+                           drag_err_fp32_vs_fp64=abs(res["drag"] - drag) / abs(drag),
+                           drag_err_fp16_vs_fp64=abs(res["drag_fp16"] - drag) / abs(drag))
             c.close()
         out[name] = res
     # the learned method judged by the iterative one: fallback above 1.1x its slip
@@ -579,7 +582,7 @@ def main():
 
     ibm = None
     if args.ibm_cycles > 0:
-        ibm = {p: ibm_bench(torch, local, p, args.ibm_cycles, 3, peak) for p in ("fp32", "fp64")}
+        ibm = {p: ibm_bench(torch, local, p, args.ibm_cycles, 3, peak) for p in ("fp32", "fp16", "fp64")}
     rods = (rods_bench(torch, local, args.rods_cycles, 3, args.rods_accuracy_cycles, peak)
             if args.rods_cycles > 0 else None)
     methods = sphere_bench(torch, local, args.sphere_steps) if args.sphere_steps > 0 else None
