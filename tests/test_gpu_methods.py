@@ -320,3 +320,36 @@ def test_fix_learned_matches_port(cuda_lib, tmp_path, slip_tol):
     # FP32 network inside 20 coupled MD steps: differences grow with the dynamics
     assert rel(out["f_atoms"], ref["f_atoms"]) <= 1e-4, rel(out["f_atoms"], ref["f_atoms"])
     assert rel(out["x"], ref["x"]) <= 1e-6
+
+
+@pytest.mark.parametrize("delta", ["roma", "peskin4"])
+def test_iterative_2d_matches_oracle(cuda_lib, delta):
+    """D2Q9 (general form of the cooperative kernel): a ring of markers in a
+    channel with no-slip walls on y, 3 passes, against the port oracle."""
+    n2 = (24, 18, 1)
+    f0 = cases.initial_populations(2, n2, 13)
+    wall = (0, 0, 1, 1, 0, 0)
+    L = Lattice(2, 24, 18, tau=0.8, wall=wall, body_force=True)
+    L.set_populations(f0)
+    O = B.OracleGrid(2, 24, 18, 1, 0.8, wall=wall)
+    O.set_f(f0)
+    ip = L.set_ibm_params(delta=delta, md_per_lb=1, xi_ibm=0.8)
+    L.set_ibm_method("iterative", passes=3)
+    th = np.linspace(0, 2 * np.pi, 20, endpoint=False)
+    x = np.stack([12.2 + 4 * np.cos(th), 9.1 + 4 * np.sin(th), np.zeros_like(th)], 1)
+    v = np.zeros_like(x)
+    m = np.ones(len(x))
+    g2 = (2e-5, 0.0, 0.0)
+    L.lbm_step(g2)
+    O.lbm_step(g2)
+    for step in range(3):
+        fg = np.zeros_like(x)
+        L.ibm_substep(x, v, m, fg, refresh=True)
+        sl = L.ibm_slip()
+        fo = np.zeros_like(x)
+        _, st, _ = O.ibm_substep_method(ip, x, v, m, fo, 1, 3, g_lb=g2)
+        assert rel(fg, fo) <= 1e-10, rel(fg, fo)
+        assert abs(sl["rms"] - st[2]) <= 1e-9 * st[2]
+        L.lbm_step(g2)
+        O.lbm_step(g2)
+    L.close()
