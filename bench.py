@@ -55,10 +55,14 @@ def parse():
                     help="LB steps of the 192^3 sphere-drag runs of the IBM methods (0 = skip)")
     ap.add_argument("--kernel", type=int, default=-1,
                     help="fused-kernel variant: -1 auto, 0 plain, 1 staged, 2 packed")
-    ap.add_argument("--only", choices=["fp64", "fp32", "fp16", "ibm", "methods"], default=None,
+    ap.add_argument("--only", choices=["fp64", "fp32", "fp16", "ibm", "rods", "methods"], default=None,
                     help="time the fused kernel of one precision only, (ibm) the FP32 LBM + "
-                         "IBM point-marker cycles only, or (methods) the IBM call of the "
+                         "IBM point-marker cycles only, (rods) the FP32 rod cycles only, or "
+                         "(methods) the IBM call of the "
                          "sphere-drag methods with an untrained network (profiling runs)")
+    ap.add_argument("--rods-box", type=int, nargs=3, default=[512, 256, 256],
+                    help="box of --only rods (profiling of smaller cases)")
+    ap.add_argument("--rods-count", type=int, default=1000, help="rods of --only rods")
     ap.add_argument("--ibm-n", type=int, default=256,
                     help="edge of the periodic box of the point-marker workload")
     ap.add_argument("--nx", type=int, default=NX)
@@ -337,7 +341,8 @@ def ibm_bench(torch, device, prec, cycles, warmup, peak, n=256, natoms=20000, md
                         peak, momentum_check=True)
 
 
-def rods_bench(torch, device, cycles, warmup, acc_cycles, peak, seed=5):
+def rods_bench(torch, device, cycles, warmup, acc_cycles, peak, seed=5, precs=("fp32", "fp16", "fp64"),
+               box=(512, 256, 256), n_rods=1000):
     """D3Q19 512x256x256, no-slip walls on y, nu 0.08, 2e5 markers as 1000 rods
     of 200 at unit spacing (seeded centre and orientation, rods within 3 nodes
     of the y walls redrawn), each rod given one random velocity N(0, 0.01^2),
@@ -346,15 +351,14 @@ def rods_bench(torch, device, cycles, warmup, acc_cycles, peak, seed=5):
     from the same state, the relative L2 error of the FP32 fluid velocity and
     of the marker forces against FP64."""
     from couplb_b200.markers import random_rods
-    box = (512, 256, 256)
-    x0 = random_rods(1000, 200, box, seed, wall_margin=3.0)
+    x0 = random_rods(n_rods, 200, box, seed, wall_margin=3.0)
     rng = np.random.default_rng(seed + 1)
-    v0 = np.repeat(0.01 * rng.standard_normal((1000, 3)), 200, axis=0)
+    v0 = np.repeat(0.01 * rng.standard_normal((n_rods, 3)), 200, axis=0)
     wl = (0, 0, 1, 1, 0, 0)
     tau = 3 * 0.08 + 0.5
-    name = "d3q19_512x256x256_walls_y_1000_rods_x200_markers_peskin4_md_per_lb2"
+    name = f"d3q19_{box[0]}x{box[1]}x{box[2]}_walls_y_{n_rods}_rods_x200_markers_peskin4_md_per_lb2"
     out = {}
-    for prec in ("fp32", "fp16", "fp64"):
+    for prec in precs:
         out[prec] = marker_bench(torch, device, prec, cycles, warmup, box, wl, tau, x0, v0, 2, name, peak,
                                  momentum_check=False)
     if acc_cycles > 0:
@@ -537,6 +541,11 @@ def main():
         return
     if args.only == "ibm":
         r = ibm_bench(torch, local, "fp32", args.ibm_cycles, args.warmup, load_peak()[0], n=args.ibm_n)
+        print(json.dumps(r), flush=True)
+        return
+    if args.only == "rods":
+        r = rods_bench(torch, local, args.rods_cycles, args.warmup, 0, load_peak()[0], precs=("fp32",),
+                       box=tuple(args.rods_box), n_rods=args.rods_count)
         print(json.dumps(r), flush=True)
         return
     if args.only:

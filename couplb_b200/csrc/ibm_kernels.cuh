@@ -23,34 +23,29 @@
 
 namespace couplb {
 
-// delta_roma (couplb_ibm.h:11-22)
+// delta_roma (couplb_ibm.h:11-22).  Both branches of the reference are
+// formed and one is selected (no divergence between the lanes of a warp); the
+// arithmetic of each branch is the reference's.
 template <class R>
 __device__ __forceinline__ R delta_roma(R r) {
   const R ar = fabs(r);
-  if (ar <= R(0.5)) {
-    const R a = R(1) - R(3) * r * r;
-    return (R(1) + sqrt(a > R(0) ? a : R(0))) / R(3);
-  }
-  if (ar <= R(1.5)) {
-    const R a = R(-2) + R(6) * ar - R(3) * r * r;
-    return (R(5) - R(3) * ar - sqrt(a > R(0) ? a : R(0))) / R(6);
-  }
-  return R(0);
+  const bool inner = ar <= R(0.5);
+  const R a = inner ? R(1) - R(3) * r * r : R(-2) + R(6) * ar - R(3) * r * r;
+  const R sq = sqrt(a > R(0) ? a : R(0));
+  const R num = inner ? R(1) + sq : R(5) - R(3) * ar - sq;
+  const R v = num / (inner ? R(3) : R(6));
+  return ar <= R(1.5) ? v : R(0);
 }
 
-// delta_peskin4 (couplb_ibm.h:24-35)
+// delta_peskin4 (couplb_ibm.h:24-35), branch-free like delta_roma
 template <class R>
 __device__ __forceinline__ R delta_peskin4(R r) {
   const R ar = fabs(r);
-  if (ar <= R(1)) {
-    const R a = R(1) + R(4) * ar - R(4) * ar * ar;
-    return (R(3) - R(2) * ar + sqrt(a > R(0) ? a : R(0))) / R(8);
-  }
-  if (ar <= R(2)) {
-    const R a = R(-7) + R(12) * ar - R(4) * ar * ar;
-    return (R(5) - R(2) * ar - sqrt(a > R(0) ? a : R(0))) / R(8);
-  }
-  return R(0);
+  const bool inner = ar <= R(1);
+  const R a = inner ? R(1) + R(4) * ar - R(4) * ar * ar : R(-7) + R(12) * ar - R(4) * ar * ar;
+  const R sq = sqrt(a > R(0) ? a : R(0));
+  const R v = (inner ? R(3) - R(2) * ar + sq : R(5) - R(2) * ar - sq) / R(8);
+  return ar <= R(2) ? v : R(0);
 }
 
 template <int DELTA, class R>
@@ -131,6 +126,86 @@ __device__ __forceinline__ int classify_node(const Geom& g, int D, int ig, int j
   j = j < 0 ? g.ny - 1 : (j >= g.ny ? 0 : j);
   if (D == 3) k = k < 0 ? g.nz - 1 : (k >= g.nz ? 0 : k);
   return -1;
+}
+
+// The window nodes of one lane: s = lane and s = lane + 32 of the 4^D window
+// (3D; s = lane < 16 in 2D).  Both share the x offset lane & 3 and the y
+// offset (lane >> 2) & 3 and differ only in z, so the x/y part of the
+// classification is done once.  The 1D weights of the window's 4 offsets per
+// axis are evaluated once per warp (lane t < 4 D: offset t & 3 of axis t >> 2)
+// and fetched with shuffles; a node's weight is (wx * wy) * wz as in
+// IBM::interpolate / spread (couplb_ibm.h:68-86, 110-123).  All 32 lanes of
+// the warp must call it.
+template <class R>
+struct LaneNodes {
+  int t[2];          // -2 outside the ghost-inclusive box, -1 fluid, else wall type
+  long long n[2];    // interior index of a fluid node (or of its periodic image)
+  R d[2];            // weight
+  int i, j, k[2];    // interior coordinates of a fluid node
+};
+
+template <class L, int DELTA, class R>
+__device__ __forceinline__ LaneNodes<R> lane_nodes(const Geom& g, double lx, double ly, double lz,
+                                                   int i0, int j0, int k0, int lane) {
+  R w1 = R(0);
+  {
+    const int ax = lane >> 2, o = lane & 3;
+    if (ax < L::D) {
+      const double l = ax == 0 ? lx : (ax == 1 ? ly : lz);
+      const int b = ax == 0 ? i0 : (ax == 1 ? j0 : k0);
+      w1 = delta1<DELTA, R>(R(l - (b - 1 + o)));
+    }
+  }
+  const int sx = lane & 3, sy = (lane >> 2) & 3;
+  const R wx = __shfl_sync(0xffffffffu, w1, sx);
+  const R wy = __shfl_sync(0xffffffffu, w1, 4 + sy);
+  const R wxy = wx * wy;
+  const int gx = g.nx + 2, gy = g.ny + 2;
+  const int ig = i0 - 1 + sx, jg = j0 - 1 + sy;
+  const bool inxy = ig >= 0 && ig < gx && jg >= 0 && jg < gy;
+  // classify_node, x then y (a later axis overrides)
+  int txy = 0;
+  if (ig == 0 || ig == gx - 1) { const int ft = ig == 0 ? g.face[0] : g.face[1]; if (ft) txy = ft; }
+  if (jg == 0 || jg == gy - 1) { const int ft = jg == 0 ? g.face[2] : g.face[3]; if (ft) txy = ft; }
+  int ii = ig - 1, jj = jg - 1;
+  ii = ii < 0 ? g.nx - 1 : (ii >= g.nx ? 0 : ii);
+  jj = jj < 0 ? g.ny - 1 : (jj >= g.ny ? 0 : jj);
+  const long long nxy = (long long)ii + (long long)g.nx * jj;
+  LaneNodes<R> out;
+  out.i = ii;
+  out.j = jj;
+#pragma unroll
+  for (int rep = 0; rep < 2; rep++) {
+    out.t[rep] = -2;
+    out.n[rep] = -1;
+    out.d[rep] = R(0);
+    out.k[rep] = 0;
+  }
+  if (L::D == 2) {
+    if (lane < 16 && inxy) {
+      out.t[0] = txy ? txy : -1;
+      out.n[0] = nxy;
+      out.d[0] = wxy;
+    }
+    return out;
+  }
+  const int gz = g.nz + 2;
+#pragma unroll
+  for (int rep = 0; rep < 2; rep++) {
+    const int oz = (lane >> 4) + 2 * rep;
+    const R wz = __shfl_sync(0xffffffffu, w1, 8 + oz);
+    const int kg = k0 - 1 + oz;
+    if (!inxy || kg < 0 || kg >= gz) continue;
+    int t = txy;
+    if (kg == 0 || kg == gz - 1) { const int ft = kg == 0 ? g.face[4] : g.face[5]; if (ft) t = ft; }
+    int kk = kg - 1;
+    kk = kk < 0 ? g.nz - 1 : (kk >= g.nz ? 0 : kk);
+    out.t[rep] = t ? t : -1;
+    out.n[rep] = nxy + (long long)g.nx * g.ny * kk;
+    out.d[rep] = wxy * wz;
+    out.k[rep] = kk;
+  }
+  return out;
 }
 
 // Velocity of interior node (i,j,k) = n of the post-stream state, with the
@@ -273,7 +348,6 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
   const double lz = (L::D == 3) ? ((zp - a.lo[2]) * a.inv_dx - a.off[2] + 1.0) : 0.0;
   const int i0 = (int)floor(lx), j0 = (int)floor(ly);
   const int k0 = (L::D == 3) ? (int)floor(lz) : 0;
-  const int gx = g.nx + 2, gy = g.ny + 2, gz = (L::D == 3) ? g.nz + 2 : 1;
   constexpr int NS = (L::D == 3) ? 64 : 16;
   // first node of the 27-node network window, in window coordinates
   int ox = 0, oy = 0, oz = 0;
@@ -305,19 +379,15 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
   const double mass = a.m[mk];
   const double vmk0 = a.v[3 * mk], vmk1 = a.v[3 * mk + 1], vmk2 = a.v[3 * mk + 2];
   const bool hit = key.epoch == a.cur_epoch && key.i0 == i0 && key.j0 == j0 && key.k0 == k0;
+  const LaneNodes<R> ln = lane_nodes<L, DELTA, R>(g, lx, ly, lz, i0, j0, k0, lane);
+  bool wall_seen = false;   // a wall node adds to ws but not to wss
 #pragma unroll
   for (int rep = 0; rep < 2; rep++) {
     const int s = lane + 32 * rep;
     if (s >= NS) break;
-    const int ig = i0 - 1 + (s & 3);
-    const int jg = j0 - 1 + ((s >> 2) & 3);
-    const int kg = (L::D == 3) ? k0 - 1 + (s >> 4) : 0;
-    if (ig < 0 || ig >= gx || jg < 0 || jg >= gy || kg < 0 || kg >= gz) continue;
-    R d = delta1<DELTA, R>(R(lx - ig)) * delta1<DELTA, R>(R(ly - jg));
-    if (L::D == 3) d *= delta1<DELTA, R>(R(lz - kg));
-    int ii = 0, jj = 0, kk = 0;
-    const int t = classify_node(g, L::D, ig, jg, kg, ii, jj, kk);
-    const double dd = double(d);
+    const int t = ln.t[rep];
+    if (t == -2) continue;
+    const double dd = double(ln.d[rep]);
     // slot of this node in the network input, or -1
     int p = -1;
     if (LEARNED) {
@@ -325,7 +395,8 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
       if (rx >= 0 && rx < 3 && ry >= 0 && ry < 3 && rz >= 0 && rz < 3) p = rx + 3 * ry + 9 * rz;
     }
     if (t < 0) {
-      const size_t src = (size_t)ii + (size_t)g.nx * ((size_t)jj + (size_t)g.ny * kk);
+      const size_t src = (size_t)ln.n[rep];
+      const int ii = ln.i, jj = ln.j, kk = ln.k[rep];
       double u0, u1, u2;
       if (fill) {
         typename S::A v0, v1, v2, vr;
@@ -347,24 +418,33 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
       if (LEARNED && p >= 0) { xs[3 * p] = float(u0); xs[3 * p + 1] = float(u1); xs[3 * p + 2] = float(u2); }
     } else if (t == 1 || t == 3) {
       ws += dd;
+      wall_seen = true;
     } else if (t == 2) {
       ui += g.uw[0] * dd;
       vi += g.uw[1] * dd;
       wi += (L::D == 3 ? g.uw[2] : 0.0) * dd;
       ws += dd;
+      wall_seen = true;
       if (LEARNED && p >= 0) {
         xs[3 * p] = float(g.uw[0]); xs[3 * p + 1] = float(g.uw[1]); xs[3 * p + 2] = float(g.uw[2]);
       }
     }
   }
   if (fill && lane == 0) a.skey[mk] = StencilKey{i0, j0, k0, a.cur_epoch};
+  // without wall nodes in the window ws and wss are the same sums
+  const bool walls = __any_sync(0xffffffffu, wall_seen);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     ui += __shfl_xor_sync(0xffffffffu, ui, o);
     vi += __shfl_xor_sync(0xffffffffu, vi, o);
     wi += __shfl_xor_sync(0xffffffffu, wi, o);
     ws += __shfl_xor_sync(0xffffffffu, ws, o);
-    wss += __shfl_xor_sync(0xffffffffu, wss, o);
+  }
+  if (walls) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) wss += __shfl_xor_sync(0xffffffffu, wss, o);
+  } else {
+    wss = ws;
   }
   double u0 = 0, u1 = 0, u2 = 0;
   if (ws > DELTA_TOL) {

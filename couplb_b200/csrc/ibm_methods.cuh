@@ -123,29 +123,23 @@ __device__ __forceinline__ void interp_corr(const PassArgs<S>& P, int mk, int la
   const IbmArgs<S>& a = P.a;
   const Geom& g = a.g;
   const MarkerWindow w = marker_window<L, S>(a, mk);
-  const int gx = g.nx + 2, gy = g.ny + 2, gz = (L::D == 3) ? g.nz + 2 : 1;
   constexpr int NS = (L::D == 3) ? 64 : 16;
   const StencilKey key = a.skey[mk];
   const bool hit = key.epoch == a.cur_epoch && key.i0 == w.i0 && key.j0 == w.j0 && key.k0 == w.k0;
   const typename S::A* rec = stencil_record(a, mk);
+  const LaneNodes<R> ln = lane_nodes<L, DELTA, R>(g, w.lx, w.ly, w.lz, w.i0, w.j0, w.k0, lane);
   double ui = 0, vi = 0, wi = 0, ws = 0;
 #pragma unroll
   for (int rep = 0; rep < 2; rep++) {
     const int s = lane + 32 * rep;
     if (s >= NS) break;
-    const int ig = w.i0 - 1 + (s & 3);
-    const int jg = w.j0 - 1 + ((s >> 2) & 3);
-    const int kg = (L::D == 3) ? w.k0 - 1 + (s >> 4) : 0;
-    if (ig < 0 || ig >= gx || jg < 0 || jg >= gy || kg < 0 || kg >= gz) continue;
-    R d = delta1<DELTA, R>(R(w.lx - ig)) * delta1<DELTA, R>(R(w.ly - jg));
-    if (L::D == 3) d *= delta1<DELTA, R>(R(w.lz - kg));
-    const double dd = double(d);
-    int ii = 0, jj = 0, kk = 0;
-    const int t = classify_node(g, L::D, ig, jg, kg, ii, jj, kk);
+    const int t = ln.t[rep];
+    if (t == -2) continue;
+    const double dd = double(ln.d[rep]);
     if (t < 0) {
-      const size_t n = (size_t)ii + (size_t)g.nx * ((size_t)jj + (size_t)g.ny * kk);
+      const size_t n = (size_t)ln.n[rep];
       double u0, u1, u2, rho;
-      node_state<L, S>(a, hit, rec, s, ii, jj, kk, n, u0, u1, u2, rho);
+      node_state<L, S>(a, hit, rec, s, ln.i, ln.j, ln.k[rep], n, u0, u1, u2, rho);
       double G[3];
       load_force(a.F, n, G);
       const double ir = 1.0 / rho;
@@ -182,28 +176,20 @@ __device__ __forceinline__ void spread_marker(const IbmArgs<S>& a, int mk, int l
   using R = typename S::C;
   const Geom& g = a.g;
   const MarkerWindow w = marker_window<L, S>(a, mk);
-  const int gx = g.nx + 2, gy = g.ny + 2, gz = (L::D == 3) ? g.nz + 2 : 1;
   constexpr int NS = (L::D == 3) ? 64 : 16;
   long long sn0 = -1, sn1 = -1;
   double sd0 = 0.0, sd1 = 0.0;
   double wss = 0.0;
+  const LaneNodes<R> ln = lane_nodes<L, DELTA, R>(g, w.lx, w.ly, w.lz, w.i0, w.j0, w.k0, lane);
 #pragma unroll
   for (int rep = 0; rep < 2; rep++) {
     const int s = lane + 32 * rep;
     if (s >= NS) break;
-    const int ig = w.i0 - 1 + (s & 3);
-    const int jg = w.j0 - 1 + ((s >> 2) & 3);
-    const int kg = (L::D == 3) ? w.k0 - 1 + (s >> 4) : 0;
-    if (ig < 0 || ig >= gx || jg < 0 || jg >= gy || kg < 0 || kg >= gz) continue;
-    int ii = 0, jj = 0, kk = 0;
-    if (classify_node(g, L::D, ig, jg, kg, ii, jj, kk) >= 0) continue;
-    R d = delta1<DELTA, R>(R(w.lx - ig)) * delta1<DELTA, R>(R(w.ly - jg));
-    if (L::D == 3) d *= delta1<DELTA, R>(R(w.lz - kg));
-    const double dd = double(d);
+    if (ln.t[rep] != -1) continue;
+    const double dd = double(ln.d[rep]);
     wss += dd;
-    const long long nn = (long long)((size_t)ii + (size_t)g.nx * ((size_t)jj + (size_t)g.ny * kk));
-    if (rep == 0) { sn0 = nn; sd0 = dd; }
-    else { sn1 = nn; sd1 = dd; }
+    if (rep == 0) { sn0 = ln.n[0]; sd0 = dd; }
+    else { sn1 = ln.n[1]; sd1 = dd; }
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) wss += __shfl_xor_sync(0xffffffffu, wss, o);
@@ -422,7 +408,6 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
   double F0 = 0, F1 = 0, F2 = 0, c0 = 0, c1 = 0, c2 = 0, mxi = 0, vx = 0, vy = 0, vz = 0;
   if (have) {
     const MarkerWindow w = marker_window<L, S>(a, mk);
-    const int gx = g.nx + 2, gy = g.ny + 2, gz = g.nz + 2;
     const StencilKey key = a.skey[mk];
     const bool fill = P.fill != 0;
     const bool hit = key.epoch == a.cur_epoch && key.i0 == w.i0 && key.j0 == w.j0 && key.k0 == w.k0;
@@ -436,23 +421,21 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
       __syncwarp();
     }
     double ui = 0, vi = 0, wi = 0;
+    const LaneNodes<R> ln = lane_nodes<L, DELTA, R>(g, w.lx, w.ly, w.lz, w.i0, w.j0, w.k0, lane);
 #pragma unroll
     for (int rep = 0; rep < 2; rep++) {
       const int s = lane + 32 * rep;
-      const int ig = w.i0 - 1 + (s & 3), jg = w.j0 - 1 + ((s >> 2) & 3), kg = w.k0 - 1 + (s >> 4);
-      if (ig < 0 || ig >= gx || jg < 0 || jg >= gy || kg < 0 || kg >= gz) continue;
-      const R d = delta1<DELTA, R>(R(w.lx - ig)) * delta1<DELTA, R>(R(w.ly - jg)) *
-                  delta1<DELTA, R>(R(w.lz - kg));
-      const double dd = double(d);
-      int ii = 0, jj = 0, kk = 0;
-      const int t = classify_node(g, 3, ig, jg, kg, ii, jj, kk);
+      const int t = ln.t[rep];
+      if (t == -2) continue;
+      const double dd = double(ln.d[rep]);
+      const int ii = ln.i, jj = ln.j, kk = ln.k[rep];
       int p = -1;
       if (LEARNED) {
         const int rx = (s & 3) - ox, ry = ((s >> 2) & 3) - oy, rz = (s >> 4) - oz;
         if (rx >= 0 && rx < 3 && ry >= 0 && ry < 3 && rz >= 0 && rz < 3) p = rx + 3 * ry + 9 * rz;
       }
       if (t < 0) {
-        const size_t n = (size_t)ii + (size_t)g.nx * ((size_t)jj + (size_t)g.ny * kk);
+        const size_t n = (size_t)ln.n[rep];
         double u0, u1, u2, rho;
         if (fill) {
           // the record is written after the loop, so that the loads of both
