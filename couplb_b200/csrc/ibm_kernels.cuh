@@ -333,7 +333,8 @@ __device__ __forceinline__ void node_state(const IbmArgs<S>& a, bool hit, const 
 // to the marker's record (the work of k_ibm_prefetch, fused).
 template <class L, class S, int DELTA, bool LEARNED>
 __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, int lane, bool fill,
-                                                 const MlpPacked* P, float* xs, float* hs) {
+                                                 const MlpPacked* P, float* xs, float* hs,
+                                                 double* tot3 = nullptr) {
   using R = typename S::C;
   if (mk >= a.n) return;
   if (a.active && !a.active[mk]) {
@@ -488,7 +489,12 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
     spread_add(a.F + 4 * sn1, fl0 * w, fl1 * w, fl2 * w);
     if (a.seg_force) a.seg_force[sn1 >> 3] = 1;
   }
-  if (lane == 0 && a.ftot) {
+  if (lane == 0 && tot3) {
+    // the caller sums the markers of its block before one atomic each
+    tot3[0] = fl0 * a.dvr;
+    tot3[1] = fl1 * a.dvr;
+    tot3[2] = fl2 * a.dvr;
+  } else if (lane == 0 && a.ftot) {
     // one of kFtotSlots accumulators (32 B apart) by marker index: the
     // same-address FP64 atomics of all markers would serialise in L2
     double* t = a.ftot + 4 * (mk & (kFtotSlots - 1));
@@ -498,10 +504,26 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
   }
 }
 
+// One sub-step, one warp per marker.  The total spread force of the block's
+// markers is summed in shared memory and added to accumulator slot
+// blockIdx % kFtotSlots with three FP64 atomics per block: with a few
+// thousand blocks per launch, per-marker atomics on the 64 slots queued in
+// L2 and took about as long as the rest of the sub-step (2e5 markers).
 template <class L, class S, int DELTA>
 __global__ void __launch_bounds__(256) k_ibm_substep(const IbmArgs<S> a) {
-  ibm_substep_body<L, S, DELTA, false>(a, (blockIdx.x * blockDim.x + threadIdx.x) >> 5,
-                                       threadIdx.x & 31, false, nullptr, nullptr, nullptr);
+  __shared__ double part[8][3];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double t3[3] = {0.0, 0.0, 0.0};
+  ibm_substep_body<L, S, DELTA, false>(a, (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane, false,
+                                       nullptr, nullptr, nullptr, t3);
+  if (!a.ftot) return;
+  if (lane == 0) { part[warp][0] = t3[0]; part[warp][1] = t3[1]; part[warp][2] = t3[2]; }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double sum = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) sum += part[w][threadIdx.x];
+    atomicAdd(a.ftot + 4 * (blockIdx.x & (kFtotSlots - 1)) + threadIdx.x, sum);
+  }
 }
 
 // Per-warp shared scratch of the learned sub-step: 84 inputs + 64 hidden.
