@@ -511,22 +511,34 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
   }
   // spread -F/(N fs) with w = d dvr / wss (couplb_ibm.h:124-132)
   const double ssc = (have && wss >= DELTA_TOL) ? a.dvr / wss : 0.0;
+  // Per-block sums before the FP64 slot atomics (total force, slip): one
+  // atomic per block and quantity instead of one per marker.  Every thread of
+  // the block calls spread and measure at the same points.
+  __shared__ double bsum[8][3];
+  const int warp = threadIdx.x >> 5;
+  const int nwarp = (int)(blockDim.x >> 5);
   auto spread = [&](double f0, double f1, double f2) {
-    if (!have || wss < DELTA_TOL) return;
-    const double fl0 = -f0 * a.inv_N / a.fs, fl1 = -f1 * a.inv_N / a.fs, fl2 = -f2 * a.inv_N / a.fs;
+    double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+    if (have && wss >= DELTA_TOL) {
+      const double fl0 = -f0 * a.inv_N / a.fs, fl1 = -f1 * a.inv_N / a.fs, fl2 = -f2 * a.inv_N / a.fs;
 #pragma unroll
-    for (int rep = 0; rep < 2; rep++) {
-      if (nd[rep] < 0) continue;
-      const double wgt = dw[rep] * ssc;
-      spread_add(a.F + 4 * nd[rep], fl0 * wgt, fl1 * wgt, fl2 * wgt);
-      if (a.seg_force) a.seg_force[nd[rep] >> 3] = 1;
+      for (int rep = 0; rep < 2; rep++) {
+        if (nd[rep] < 0) continue;
+        const double wgt = dw[rep] * ssc;
+        spread_add(a.F + 4 * nd[rep], fl0 * wgt, fl1 * wgt, fl2 * wgt);
+        if (a.seg_force) a.seg_force[nd[rep] >> 3] = 1;
+      }
+      t0 = fl0 * a.dvr; t1 = fl1 * a.dvr; t2 = fl2 * a.dvr;
     }
-    if (lane == 0 && a.ftot) {
-      double* t = a.ftot + 4 * (mk & (kFtotSlots - 1));
-      atomicAdd(t, fl0 * a.dvr);
-      atomicAdd(t + 1, fl1 * a.dvr);
-      atomicAdd(t + 2, fl2 * a.dvr);
+    if (!a.ftot) return;
+    if (lane == 0) { bsum[warp][0] = t0; bsum[warp][1] = t1; bsum[warp][2] = t2; }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+      double sum = 0.0;
+      for (int w = 0; w < nwarp; w++) sum += bsum[w][threadIdx.x];
+      atomicAdd(a.ftot + 4 * (blockIdx.x & (kFtotSlots - 1)) + threadIdx.x, sum);
     }
+    __syncthreads();
   };
   // interpolated u_corr from the registers and the current force field
   auto interp_corr_reg = [&](double U[3]) {
@@ -555,17 +567,32 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
     }
   };
   auto measure = [&](int r) {
-    if (!have) return;
-    double U[3];
-    interp_corr_reg(U);
-    if (lane == 0) {
+    double q = 0.0;
+    if (have) {
+      double U[3];
+      interp_corr_reg(U);
       const double e0 = U[0] * a.vs - vx, e1 = U[1] * a.vs - vy, e2 = U[2] * a.vs - vz;
-      const double q = e0 * e0 + e1 * e1 + e2 * e2;
-      const int sl = mk & (kSlipSlots - 1);
-      atomicAdd(&P.ps->s2[r][sl], q);
-      atomicMax(&P.ps->max_bits[r][sl], (unsigned long long)__double_as_longlong(sqrt(q)));
-      atomicAdd(&P.ps->count[r][sl], 1);
+      q = e0 * e0 + e1 * e1 + e2 * e2;
     }
+    if (lane == 0) { bsum[warp][0] = q; bsum[warp][1] = have ? 1.0 : 0.0; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double sum = 0.0, mx = 0.0;
+      int cnt = 0;
+      for (int w = 0; w < nwarp; w++) {
+        if (bsum[w][1] == 0.0) continue;
+        sum += bsum[w][0];
+        mx = fmax(mx, sqrt(bsum[w][0]));
+        cnt++;
+      }
+      if (cnt) {
+        const int sl = blockIdx.x & (kSlipSlots - 1);
+        atomicAdd(&P.ps->s2[r][sl], sum);
+        atomicMax(&P.ps->max_bits[r][sl], (unsigned long long)__double_as_longlong(mx));
+        atomicAdd(&P.ps->count[r][sl], cnt);
+      }
+    }
+    __syncthreads();
   };
   spread(F0, F1, F2);
   if (!grid_barrier(P.ps, P.status)) return;
