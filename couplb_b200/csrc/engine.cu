@@ -62,6 +62,12 @@ void with_types(int dim, int prec, Fn&& fn) {
   }
 }
 
+// Copy of the status word (clamp and non-finite counts) into a posted slot of
+// mapped pinned host memory; read by the host after the slot's event.
+__global__ void k_status_publish(const int* __restrict__ st, int* ring_slot) {
+  if (threadIdx.x < 2) ring_slot[threadIdx.x] = st[threadIdx.x];
+}
+
 size_t elem_bytes_pop(int prec) { return prec == COUPLB_FP64 ? 8 : (prec == COUPLB_FP32_SHIFTED ? 4 : 2); }
 size_t elem_bytes_aux(int prec) { return prec == COUPLB_FP64 ? 8 : 4; }
 
@@ -350,8 +356,13 @@ int couplb_create(const couplb_lattice_params* p, couplb_handle** out) {
   static_assert(sizeof(double) * 4 * kFtotSlots <= 4096, "h_small holds the force accumulators");
   if (!rc && cudaMallocHost(&h->h_small, 4096) != cudaSuccess)
     rc = fail(h, COUPLB_ERR_CUDA, "cudaMallocHost failed");
-  if (!rc && cudaMallocHost((void**)&h->h_status_ring, sizeof(int) * 16) != cudaSuccess)
-    rc = fail(h, COUPLB_ERR_CUDA, "cudaMallocHost failed");
+  // mapped, so that status_post publishes with a one-warp kernel instead of a
+  // copy-engine transfer (a small D2H copy on the stream left a gap of ~10 us
+  // before the next step's kernel)
+  if (!rc && cudaHostAlloc((void**)&h->h_status_ring, sizeof(int) * 16, cudaHostAllocMapped) != cudaSuccess)
+    rc = fail(h, COUPLB_ERR_CUDA, "cudaHostAlloc failed");
+  if (!rc && cudaHostGetDevicePointer((void**)&h->d_status_ring, h->h_status_ring, 0) != cudaSuccess)
+    rc = fail(h, COUPLB_ERR_CUDA, "cudaHostGetDevicePointer failed");
   for (int e = 0; e < 2 && !rc; e++)
     if (cudaEventCreateWithFlags(&h->status_ev[e], cudaEventDisableTiming) != cudaSuccess)
       rc = fail(h, COUPLB_ERR_CUDA, "cudaEventCreate failed");
@@ -743,8 +754,8 @@ int couplb_status_post(couplb_handle* h) {
   int rc = set_device(h);
   if (rc) return rc;
   const int slot = (int)(h->status_posts & 1);
-  CK(cudaMemcpyAsync(h->h_status_ring + 8 * slot, h->d_status, sizeof(int) * 2, cudaMemcpyDeviceToHost,
-                     h->stream));
+  k_status_publish<<<1, 32, 0, h->stream>>>(h->d_status, h->d_status_ring + 8 * slot);
+  CK_LAUNCH();
   CK(cudaEventRecord(h->status_ev[slot], h->stream));
   h->status_posts++;
   return COUPLB_OK;
@@ -757,8 +768,9 @@ int couplb_status_last(couplb_handle* h, int* clamps, int* nonfinite) {
     const long long want = h->status_posts >= 2 ? h->status_posts - 2 : 0;
     const int slot = (int)(want & 1);
     CK(cudaEventSynchronize(h->status_ev[slot]));
-    c = h->h_status_ring[8 * slot + kStClamps];
-    nf = h->h_status_ring[8 * slot + kStNonfinite];
+    const volatile int* ring = h->h_status_ring;
+    c = ring[8 * slot + kStClamps];
+    nf = ring[8 * slot + kStNonfinite];
   }
   if (clamps) *clamps = c;
   if (nonfinite) *nonfinite = nf;

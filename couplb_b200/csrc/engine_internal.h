@@ -43,7 +43,8 @@ struct couplb_handle {
   int* d_status = nullptr;           // clamp / non-finite counters
   double* d_ftot = nullptr;          // FP64 sum of the spread IBM force
   void* h_small = nullptr;           // pinned host scratch for small read-backs
-  int* h_status_ring = nullptr;      // pinned: two posted copies of the status word
+  int* h_status_ring = nullptr;      // pinned, mapped: two posted copies of the status word
+  int* d_status_ring = nullptr;      // the same memory as seen by kernels
   cudaEvent_t status_ev[2] = {nullptr, nullptr};
   long long status_posts = 0;
   void* d_staging = nullptr;         // import / export staging
