@@ -49,6 +49,8 @@ def parse():
                     help="LB cycles of the 256^3 IBM point-marker workload (0 = skip)")
     ap.add_argument("--rods-cycles", type=int, default=20,
                     help="timed LB cycles of the 512x256x256 many-rod workload (0 = skip)")
+    ap.add_argument("--rods-method-cycles", type=int, default=10,
+                    help="timed LB cycles of the rod workload per IBM forcing method (0 = skip)")
     ap.add_argument("--rods-accuracy-cycles", type=int, default=200,
                     help="LB cycles of the rod FP32-vs-FP64 accuracy runs (0 = skip)")
     ap.add_argument("--sphere-steps", type=int, default=2000,
@@ -246,13 +248,19 @@ def e2e_fix(steps, warmup, nx, ny, nz, device, torch):
 
 
 def marker_bench(torch, device, prec, cycles, warmup, box, wall, tau, x0, v0, md_per_lb, workload,
-                 peak, momentum_check, fluid_out=False):
+                 peak, momentum_check, fluid_out=False, method=None, record=None, slip_cycles=0,
+                 prescribed=False):
     """LBM + IBM with point markers (m 1, xi 1, Peskin4).  Markers stay on the
     device; a velocity-Verlet stand-in for the MD side (markers free, no
     bonds) runs on the same stream.  Timed: the library's own calls (one LB
     step + md_per_lb IBM sub-steps per LB cycle), CUDA events around them.
     momentum_check: in a periodic box the fluid gains per LB interval what the
-    markers lose (FP64 sums on the device)."""
+    markers lose (FP64 sums on the device).  method: IBM forcing method
+    (dict of Lattice.set_ibm_method arguments); record: a device tensor that
+    receives the training rows of the timed cycles; slip_cycles: untimed
+    cycles after the timed ones whose RMS slip (after the last pass) is
+    averaged; prescribed: the markers keep their initial velocities (the IBM
+    force does not act back on them)."""
     from couplb_b200.lattice import Lattice
     nx, ny, nz = box
     L = Lattice(3, nx, ny, nz, tau=tau, wall=wall, precision=prec, device=device)
@@ -261,6 +269,8 @@ def marker_bench(torch, device, prec, cycles, warmup, box, wall, tau, x0, v0, md
     L.init_equilibrium(1.0)
     dt = 1.0 / md_per_lb
     L.set_ibm_params(delta="peskin4", md_per_lb=md_per_lb, xi_ibm=1.0, dt_lbm=1.0, dx=1.0)
+    if method:
+        L.set_ibm_method(**method)
     natoms = x0.shape[0]
     x = torch.from_numpy(np.ascontiguousarray(x0)).cuda()
     v = torch.from_numpy(np.ascontiguousarray(v0)).cuda()
@@ -269,9 +279,10 @@ def marker_bench(torch, device, prec, cycles, warmup, box, wall, tau, x0, v0, md
     period = torch.tensor([float(nx), float(ny), float(nz)], dtype=torch.float64, device="cuda")
     evs = []
 
-    def cycle(timed):
+    def cycle(timed, slips=None):
         for s in range(md_per_lb):
-            v.add_(f, alpha=0.5 * dt)
+            if not prescribed:
+                v.add_(f, alpha=0.5 * dt)
             x.add_(v, alpha=dt)
             x.copy_(torch.remainder(x, period))
             f.zero_()
@@ -286,16 +297,33 @@ def marker_bench(torch, device, prec, cycles, warmup, box, wall, tau, x0, v0, md
                 e1 = torch.cuda.Event(enable_timing=True)
                 e1.record(stream)
                 evs.append((e0, e1))
-            v.add_(f, alpha=0.5 * dt)
+            if slips is not None:
+                slips.append(L.ibm_slip()["rms"])
+            if not prescribed:
+                v.add_(f, alpha=0.5 * dt)
 
     for _ in range(warmup):
         cycle(False)
     torch.cuda.synchronize()
+    if record is not None:
+        L.ibm_record(record.data_ptr(), record.shape[0])
     for _ in range(cycles):
         cycle(True)
     torch.cuda.synchronize()
     ms = sum(a.elapsed_time(b) for a, b in evs) / cycles
     out = {"workload": workload, "precision": prec, "cycles": cycles, "ms_per_lb_cycle": ms}
+    if record is not None:
+        out["rows"] = L.ibm_record_count()
+        L.ibm_record(0, 0)
+    if method:
+        out["method"] = {k: v for k, v in method.items() if k != "model"}
+        sl = L.ibm_slip(reset=True)
+        out["slip_checks"], out["fallbacks"] = sl["checks"], sl["fallbacks"]
+    if slip_cycles:
+        rms = []
+        for _ in range(slip_cycles):
+            cycle(False, rms)
+        out["slip_rms"] = float(np.mean(rms))
     if momentum_check:
         # momentum balance of one LB interval: the fluid gains what the markers lose
         L.lbm_step()   # consume the forces still pending from the timed cycles
@@ -342,14 +370,23 @@ def ibm_bench(torch, device, prec, cycles, warmup, peak, n=256, natoms=20000, md
 
 
 def rods_bench(torch, device, cycles, warmup, acc_cycles, peak, seed=5, precs=("fp32", "fp16", "fp64"),
-               box=(512, 256, 256), n_rods=1000):
+               box=(512, 256, 256), n_rods=1000, method_cycles=0, slip_cycles=5, train_rows=2_000_000):
     """D3Q19 512x256x256, no-slip walls on y, nu 0.08, 2e5 markers as 1000 rods
     of 200 at unit spacing (seeded centre and orientation, rods within 3 nodes
     of the y walls redrawn), each rod given one random velocity N(0, 0.01^2),
     Peskin4, md_per_lb 2.  The markers are free (the MD side has no bonds
     here).  FP32-shifted and FP64 timed; accuracy: after acc_cycles LB cycles
     from the same state, the relative L2 error of the FP32 fluid velocity and
-    of the marker forces against FP64."""
+    of the marker forces against FP64.
+
+    method_cycles: the same workload with the IBM forcing methods, FP32-shifted,
+    the rods moving at their prescribed velocities (with free markers and
+    xi = 1 the extra force of the correction passes makes the explicit marker
+    update overshoot, and the 5-pass run diverges): 5-pass iterative cycles
+    timed while their training rows are captured, the network trained on the
+    rows on the GPU, then learned (no fallback) and single-pass cycles timed;
+    the RMS slip after the last pass is averaged over slip_cycles further
+    cycles of each."""
     from couplb_b200.markers import random_rods
     x0 = random_rods(n_rods, 200, box, seed, wall_margin=3.0)
     rng = np.random.default_rng(seed + 1)
@@ -371,6 +408,33 @@ def rods_bench(torch, device, cycles, warmup, acc_cycles, peak, seed=5, precs=("
             acc[f"l2_velocity_err_{p}_vs_fp64"] = float(np.sqrt(((u - u64) ** 2).sum() / (u64 ** 2).sum()))
             acc[f"l2_marker_force_err_{p}_vs_fp64"] = float(np.sqrt(((f - f64) ** 2).sum() / (f64 ** 2).sum()))
         out["accuracy"] = acc
+    if method_cycles > 0:
+        from couplb_b200 import abi
+        from couplb_b200 import sphere_drag as SD
+        rows = torch.zeros((train_rows, abi.MLP_ROW), dtype=torch.float32, device=f"cuda:{device}")
+        meth = {}
+        meth["iterative5"] = marker_bench(torch, device, "fp32", method_cycles, warmup, box, wl, tau, x0, v0, 2,
+                                          name, peak, False, method=dict(method="iterative", passes=5),
+                                          record=rows, slip_cycles=slip_cycles, prescribed=True)
+        n_rows = meth["iterative5"].pop("rows")
+        t0 = time.perf_counter()
+        net, tl, vl = SD.train_net(rows[:n_rows], epochs=30, device=device)
+        meth["training"] = {"rows": n_rows, "epochs": 30, "train_s": time.perf_counter() - t0,
+                            "train_loss": tl, "val_loss": vl}
+        del rows
+        meth["learned"] = marker_bench(torch, device, "fp32", method_cycles, warmup, box, wl, tau, x0, v0, 2,
+                                       name, peak, False,
+                                       method=dict(method="learned", passes=5, slip_tol=1e30, model=net),
+                                       slip_cycles=slip_cycles, prescribed=True)
+        meth["single"] = marker_bench(torch, device, "fp32", method_cycles, warmup, box, wl, tau, x0, v0, 2,
+                                      name, peak, False, method=dict(method="iterative", passes=1),
+                                      slip_cycles=slip_cycles, prescribed=True)
+        net.close()
+        it, le = meth["iterative5"], meth["learned"]
+        meth["slip_learned_over_iterative5"] = le["slip_rms"] / it["slip_rms"]
+        meth["slip_single_over_iterative5"] = meth["single"]["slip_rms"] / it["slip_rms"]
+        meth["speedup_learned_vs_iterative5"] = it["ms_per_lb_cycle"] / le["ms_per_lb_cycle"]
+        out["methods"] = meth
     return out
 
 
@@ -545,7 +609,8 @@ def main():
         return
     if args.only == "rods":
         r = rods_bench(torch, local, args.rods_cycles, args.warmup, 0, load_peak()[0], precs=("fp32",),
-                       box=tuple(args.rods_box), n_rods=args.rods_count)
+                       box=tuple(args.rods_box), n_rods=args.rods_count,
+                       method_cycles=args.rods_method_cycles)
         print(json.dumps(r), flush=True)
         return
     if args.only:
@@ -592,7 +657,8 @@ def main():
     ibm = None
     if args.ibm_cycles > 0:
         ibm = {p: ibm_bench(torch, local, p, args.ibm_cycles, 3, peak) for p in ("fp32", "fp16", "fp64")}
-    rods = (rods_bench(torch, local, args.rods_cycles, 3, args.rods_accuracy_cycles, peak)
+    rods = (rods_bench(torch, local, args.rods_cycles, 3, args.rods_accuracy_cycles, peak,
+                       method_cycles=args.rods_method_cycles)
             if args.rods_cycles > 0 else None)
     methods = sphere_bench(torch, local, args.sphere_steps) if args.sphere_steps > 0 else None
 

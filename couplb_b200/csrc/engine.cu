@@ -850,17 +850,17 @@ int coop_resident(couplb_handle* h, K kern, size_t smem, int slot, int* out) {
 template <class L, class S>
 int launch_method(couplb_handle* h, PassArgs<S>& P, int delta, bool learned, int n) {
   using K = void (*)(const PassArgs<S>);
-  const int di = learned ? 2 : (delta == COUPLB_DELTA_ROMA ? 0 : 1);
+  const bool roma = delta == COUPLB_DELTA_ROMA;
+  const int di = (learned ? 2 : 0) + (roma ? 0 : 1);
   const size_t smem = learned ? kLearnedSmem : 0;
   const long long want = ((long long)n * 32 + 255) / 256;
   void* args[] = {&P};
   int rc, resident = 0;
   if constexpr (L::D == 3) {
     if (h->ibm_resident) {
-      K kr = learned ? k_ibm_method_resident<L, S, 0, true>
-                     : (delta == COUPLB_DELTA_ROMA ? k_ibm_method_resident<L, S, 0, false>
-                                                   : k_ibm_method_resident<L, S, 1, false>);
-      if ((rc = coop_resident(h, kr, smem, 3 + di, &resident))) return rc;
+      K kr = learned ? (roma ? k_ibm_method_resident<L, S, 0, true> : k_ibm_method_resident<L, S, 1, true>)
+                     : (roma ? k_ibm_method_resident<L, S, 0, false> : k_ibm_method_resident<L, S, 1, false>);
+      if ((rc = coop_resident(h, kr, smem, 4 + di, &resident))) return rc;
       if (want <= resident) {
         CK(cudaLaunchCooperativeKernel((const void*)kr, dim3((unsigned)want), dim3(256), args, smem,
                                        h->stream));
@@ -870,9 +870,9 @@ int launch_method(couplb_handle* h, PassArgs<S>& P, int delta, bool learned, int
   }
   K kern = nullptr;
   if (learned) {
-    if constexpr (L::D == 3) kern = k_ibm_method<L, S, 0, true>;
+    if constexpr (L::D == 3) kern = roma ? k_ibm_method<L, S, 0, true> : k_ibm_method<L, S, 1, true>;
   } else {
-    kern = delta == COUPLB_DELTA_ROMA ? k_ibm_method<L, S, 0, false> : k_ibm_method<L, S, 1, false>;
+    kern = roma ? k_ibm_method<L, S, 0, false> : k_ibm_method<L, S, 1, false>;
   }
   if (!kern) return fail(h, COUPLB_ERR_UNSUPPORTED, "the learned correction is defined for D3Q19");
   if ((rc = coop_resident(h, kern, smem, di, &resident))) return rc;
@@ -888,8 +888,8 @@ int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, co
   if (n <= 0) return COUPLB_OK;
   const couplb_ibm_params& ip = h->ip;
   const int method = h->ibm_method;
-  if (method == COUPLB_IBM_LEARNED && (ip.delta != COUPLB_DELTA_ROMA || h->p.dim != 3 || !h->mlp))
-    return fail(h, COUPLB_ERR_UNSUPPORTED, "the learned correction needs D3Q19, the Roma kernel and a network");
+  if (method == COUPLB_IBM_LEARNED && (h->p.dim != 3 || !h->mlp))
+    return fail(h, COUPLB_ERR_UNSUPPORTED, "the learned correction needs D3Q19 and a network");
   // The refresh of compute_macroscopic(false) (fix_couplb.cpp:757-760): the
   // velocities are computed on demand by the kernel; the density it would
   // store is what the next LB step's body force reads.

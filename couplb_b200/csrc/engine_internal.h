@@ -73,8 +73,9 @@ struct couplb_handle {
   void* d_pass = nullptr;            // two couplb::PassState, alternating per sub-step
   int pass_cur = 0;                  // the one of the last sub-step
   int ibm_resident = 1;              // option: register-resident form when markers fit
-  int coop_blocks[6] = {0, 0, 0, 0, 0, 0};   // resident blocks of k_ibm_method (Roma, Peskin4,
-                                             // learned), then of its register-resident form
+  int coop_blocks[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // resident blocks of k_ibm_method (Roma,
+                                                   // Peskin4, learned Roma, learned Peskin4),
+                                                   // then of its register-resident form
   double g_lb[3] = {0.0, 0.0, 0.0};  // body force of the last LB step
   float* rec_rows = nullptr;         // training-sample capture
   long long rec_cap = 0, rec_count = 0;

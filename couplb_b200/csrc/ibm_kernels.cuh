@@ -324,7 +324,7 @@ __device__ __forceinline__ void node_state(const IbmArgs<S>& a, bool hit, const 
 // Weight arithmetic in the storage's compute type: FP64 for the parity form,
 // FP32 for the shifted forms.  Sums are carried in FP64 either way.
 //
-// LEARNED (D3Q19, Roma): the lanes also gather the network input (u0 at the 27
+// LEARNED (D3Q19): the lanes also gather the network input (u0 at the 27
 // nodes round(l)-1..round(l)+1 of each axis, then v / vel_scale) into the
 // warp's shared scratch xs, the warp runs the correction network, and the
 // marker force F = F_penalty + m xi/dt vs y is returned and spread.

@@ -297,7 +297,7 @@ __device__ __forceinline__ void record_marker(const PassArgs<S>& P, int mk, int 
 
 // One sub-step of the ITERATIVE or LEARNED method (cooperative launch, blocks
 // of 256 threads, at most as many blocks as fit on the device at once;
-// LEARNED: D3Q19, Roma, dynamic shared memory kLearnedSmem).
+// LEARNED: D3Q19, dynamic shared memory kLearnedSmem).
 template <class L, class S, int DELTA, bool LEARNED>
 __global__ void __launch_bounds__(256) k_ibm_method(const PassArgs<S> P) {
   extern __shared__ __align__(16) unsigned char smem[];

@@ -6,7 +6,8 @@
 // W3[3][64], b3[3].  The network computes in FP32 with weights rounded to
 // BF16 (round to nearest even) and FP32 biases:
 //   h1 = relu(W1 (s_in x) + b1), h2 = relu(W2 h1 + b2), y = (W3 h2 + b3) / s_out.
-// x = (u0 at the 27 Roma nodes, node-major dz,dy,dx; then v / vel_scale), all
+// x = (u0 at the 27 nodes round(l)-1..round(l)+1 of the marker, node-major
+// dz,dy,dx; then v / vel_scale), all
 // lattice velocities; y is the force correction over m xi vel_scale / dt.
 #pragma once
 #include <cuda_bf16.h>

@@ -2,7 +2,7 @@
 GPU training, through the couplb_mlp_* C ABI.
 
 Rows are COUPLB_MLP_ROW = 88 floats in device memory: 84 inputs (u0 at the 27
-Roma nodes of a marker, then v / vel_scale), 3 targets (the correction beyond
+nodes round(l)-1..round(l)+1 of a marker, then v / vel_scale), 3 targets (the correction beyond
 the penalty pass over m xi vel_scale / dt), 1 unused.
 """
 import ctypes as C

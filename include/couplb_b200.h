@@ -240,7 +240,7 @@ int  couplb_ibm_total_force(couplb_handle* h, double out[3], int reset);
  * units).  Exact for md_per_lb = 1; with sub-steps G holds those so far. */
 #define COUPLB_IBM_SINGLE    0  /* the reference's single pass (default)          */
 #define COUPLB_IBM_ITERATIVE 1  /* passes-1 correction passes, then the slip      */
-#define COUPLB_IBM_LEARNED   2  /* single pass + network correction (D3Q19, Roma);
+#define COUPLB_IBM_LEARNED   2  /* single pass + network correction (D3Q19);
                                    slip check, and the passes-1 corrections run
                                    when the RMS slip exceeds slip_tol           */
 
@@ -262,7 +262,7 @@ int  couplb_set_ibm_method(couplb_handle* h, const couplb_ibm_method* m);
 int  couplb_ibm_slip(couplb_handle* h, double out[8], int reset);
 /* Training-sample capture: every later ITERATIVE or LEARNED sub-step appends
  * one row of COUPLB_MLP_ROW floats per marker to d_rows (device memory of
- * capacity rows) -- the network input (u0 at the 27 Roma nodes round(l)-1..
+ * capacity rows) -- the network input (u0 at the 27 nodes round(l)-1..
  * round(l)+1, node-major z,y,x; then v / vel_scale), the correction beyond the
  * penalty pass over (m xi vel_scale / dt), lattice velocity units, and a 0.
  * Needs all atoms coupled (no group mask).  d_rows NULL stops the capture.

@@ -117,10 +117,11 @@ def test_iterative_fp32_close_to_oracle(cuda_lib):
     L.close()
 
 
+@pytest.mark.parametrize("delta", ["roma", "peskin4"])
 @pytest.mark.parametrize("resident", [1, 0])
 @pytest.mark.parametrize("tol,fell", [(1e9, 0), (0.0, 1)])
-def test_learned_matches_oracle(cuda_lib, tol, fell, resident):
-    L, O, ip = make_pair("fp64", "roma")
+def test_learned_matches_oracle(cuda_lib, tol, fell, resident, delta):
+    L, O, ip = make_pair("fp64", delta)
     L.set_option("ibm_resident", resident)
     w = random_net(3)
     s = (250.0, 400.0)
@@ -249,10 +250,6 @@ def test_method_errors(cuda_lib):
         L.set_ibm_method("iterative", passes=0)
     net = CorrectionNet(0)
     L.set_ibm_method("learned", passes=5, slip_tol=1e-3, model=net)
-    x = np.array([[4.2, 4.1, 3.9]])
-    with pytest.raises(CoupLBError) as e:                 # Peskin4: unsupported
-        L.ibm_substep(x, np.zeros_like(x), np.ones(1), np.zeros_like(x))
-    assert e.value.code == abi.ERR_UNSUPPORTED
     L2 = Lattice(2, 8, 8, tau=0.8)
     with pytest.raises(CoupLBError):
         L2.set_ibm_method("learned", passes=5, model=net)
