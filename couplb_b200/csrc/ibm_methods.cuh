@@ -172,7 +172,7 @@ __device__ __forceinline__ void interp_corr(const PassArgs<S>& P, int mk, int la
 // (couplb_ibm.h:92-133).
 template <class L, class S, int DELTA>
 __device__ __forceinline__ void spread_marker(const IbmArgs<S>& a, int mk, int lane,
-                                              const double dF[3]) {
+                                              const double dF[3], double* tot3 = nullptr) {
   using R = typename S::C;
   const Geom& g = a.g;
   const MarkerWindow w = marker_window<L, S>(a, mk);
@@ -207,7 +207,11 @@ __device__ __forceinline__ void spread_marker(const IbmArgs<S>& a, int mk, int l
     spread_add(a.F + 4 * sn1, fl0 * wgt, fl1 * wgt, fl2 * wgt);
     if (a.seg_force) a.seg_force[sn1 >> 3] = 1;
   }
-  if (lane == 0 && a.ftot) {
+  if (lane == 0 && tot3) {
+    tot3[0] += fl0 * a.dvr;
+    tot3[1] += fl1 * a.dvr;
+    tot3[2] += fl2 * a.dvr;
+  } else if (lane == 0 && a.ftot) {
     double* t = a.ftot + 4 * (mk & (kFtotSlots - 1));
     atomicAdd(t, fl0 * a.dvr);
     atomicAdd(t + 1, fl1 * a.dvr);
@@ -215,9 +219,17 @@ __device__ __forceinline__ void spread_marker(const IbmArgs<S>& a, int mk, int l
   }
 }
 
-// Slip of marker mk into residual r of the pass state.
+// A warp's running slip sums (lane 0) until its block adds them.
+struct SlipAcc {
+  double s2 = 0.0, mx = 0.0;
+  int cnt = 0;
+};
+
+// Slip of marker mk into residual r of the pass state, or (acc) into the
+// warp's running sums.
 template <class L, class S, int DELTA>
-__device__ __forceinline__ void measure_marker(const PassArgs<S>& P, int mk, int lane, int r) {
+__device__ __forceinline__ void measure_marker(const PassArgs<S>& P, int mk, int lane, int r,
+                                               SlipAcc* acc = nullptr) {
   double U[3];
   interp_corr<L, S, DELTA>(P, mk, lane, U);
   if (lane == 0) {
@@ -227,11 +239,60 @@ __device__ __forceinline__ void measure_marker(const PassArgs<S>& P, int mk, int
       const double e = U[c] * a.vs - a.v[3 * mk + c];
       e2 += e * e;
     }
+    if (acc) {
+      acc->s2 += e2;
+      acc->mx = fmax(acc->mx, sqrt(e2));
+      acc->cnt++;
+      return;
+    }
     const int sl = mk & (kSlipSlots - 1);
     atomicAdd(&P.ps->s2[r][sl], e2);
     atomicMax(&P.ps->max_bits[r][sl], (unsigned long long)__double_as_longlong(sqrt(e2)));
     atomicAdd(&P.ps->count[r][sl], 1);
   }
+}
+
+// Per-block sums of the warps' running accumulators, then one set of FP64
+// atomics per block: with 2e5 markers, per-marker atomics on the 64 force
+// and 32 slip slots queued in L2 for a large part of each pass.  Every thread
+// of the block calls these at the same point.
+__device__ __forceinline__ void block_add_ftot(double* ftot, double t[3]) {
+  __shared__ double part[8][3];
+  const int warp = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) { part[warp][0] = t[0]; part[warp][1] = t[1]; part[warp][2] = t[2]; }
+  __syncthreads();
+  if (ftot && threadIdx.x < 3) {
+    double sum = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) sum += part[w][threadIdx.x];
+    atomicAdd(ftot + 4 * (blockIdx.x & (kFtotSlots - 1)) + threadIdx.x, sum);
+  }
+  __syncthreads();
+  t[0] = t[1] = t[2] = 0.0;
+}
+
+__device__ __forceinline__ void block_add_slip(PassState* ps, int r, SlipAcc& acc) {
+  __shared__ double ps2[8], pmx[8];
+  __shared__ int pcnt[8];
+  const int warp = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) { ps2[warp] = acc.s2; pmx[warp] = acc.mx; pcnt[warp] = acc.cnt; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sum = 0.0, mx = 0.0;
+    int cnt = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+      sum += ps2[w];
+      mx = fmax(mx, pmx[w]);
+      cnt += pcnt[w];
+    }
+    if (cnt) {
+      const int sl = blockIdx.x & (kSlipSlots - 1);
+      atomicAdd(&ps->s2[r][sl], sum);
+      atomicMax(&ps->max_bits[r][sl], (unsigned long long)__double_as_longlong(mx));
+      atomicAdd(&ps->count[r][sl], cnt);
+    }
+  }
+  __syncthreads();
+  acc = SlipAcc();
 }
 
 // RMS slip of residual r after the barrier that closed it: warp 0 of the
@@ -316,14 +377,21 @@ __global__ void __launch_bounds__(256) k_ibm_method(const PassArgs<S> P) {
     unsigned* z = reinterpret_cast<unsigned*>(P.ps_next);
     for (int i = threadIdx.x; i < (int)(sizeof(PassState) / 4); i += blockDim.x) z[i] = 0u;
   }
+  double ft[3] = {0.0, 0.0, 0.0};
+  SlipAcc acc;
   // first pass: the reference's penalty pass (+ the network correction)
-  for (int mk = gw; mk < a.n; mk += nw)
+  for (int mk = gw; mk < a.n; mk += nw) {
+    double t3[3] = {0.0, 0.0, 0.0};
     ibm_substep_body<L, S, DELTA, LEARNED>(a, mk, lane, P.fill != 0, net, xs,
-                                           LEARNED ? xs + kMlpIn : nullptr);
+                                           LEARNED ? xs + kMlpIn : nullptr, t3);
+    ft[0] += t3[0]; ft[1] += t3[1]; ft[2] += t3[2];
+  }
+  block_add_ftot(a.ftot, ft);
   if (!grid_barrier(P.ps, P.status)) return;
   if (P.check_first) {
     for (int mk = gw; mk < a.n; mk += nw)
-      if (!a.active || a.active[mk]) measure_marker<L, S, DELTA>(P, mk, lane, 0);
+      if (!a.active || a.active[mk]) measure_marker<L, S, DELTA>(P, mk, lane, 0, &acc);
+    block_add_slip(P.ps, 0, acc);
     if (!grid_barrier(P.ps, P.status)) return;
     const bool fall = slip_rms(P.ps, 0) > P.slip_tol;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -360,15 +428,17 @@ __global__ void __launch_bounds__(256) k_ibm_method(const PassArgs<S> P) {
       if (a.active && !a.active[mk]) continue;
       const double dF[3] = {__ldcg(P.dF + 3 * mk), __ldcg(P.dF + 3 * mk + 1),
                             __ldcg(P.dF + 3 * mk + 2)};
-      spread_marker<L, S, DELTA>(a, mk, lane, dF);
+      spread_marker<L, S, DELTA>(a, mk, lane, dF, ft);
     }
+    block_add_ftot(a.ftot, ft);
     if (!grid_barrier(P.ps, P.status)) return;
   }
   for (int mk = gw; mk < a.n; mk += nw) {
     if (a.active && !a.active[mk]) continue;
-    measure_marker<L, S, DELTA>(P, mk, lane, 1);
+    measure_marker<L, S, DELTA>(P, mk, lane, 1, &acc);
     if (P.rows) record_marker<L, S>(P, mk, lane);
   }
+  block_add_slip(P.ps, 1, acc);
 }
 
 // The same sub-step when every marker has a warp of its own (n <= resident
