@@ -563,6 +563,19 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(torch, x):
+    """Max of a per-rank number over the process group (the slowest rank's
+    time); x itself without a group.  NCCL reduces a device tensor, other
+    backends (gloo) a host one."""
+    dist = torch.distributed
+    if not (dist.is_available() and dist.is_initialized()):
+        return float(x)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def load_peak():
     """HBM copy bandwidth (GB/s) measured on this pool, else the fallback."""
     try:
@@ -646,17 +659,9 @@ def main():
         if nonfinite:
             raise RuntimeError(f"{prec}: non-finite densities")
         L.close()
-        if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
-        results[prec] = ms
+        results[prec] = max_over_ranks(torch, ms)
 
-    e2e_s = e2e_fix(args.steps, args.warmup, nx, ny, nz, local, torch)
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(torch, e2e_fix(args.steps, args.warmup, nx, ny, nz, local, torch))
     acc = accuracy_runs(f0, args.accuracy_steps, nx, ny, nz, local) if args.accuracy_steps else {}
     peak, peak_src = load_peak()
 
