@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--sphere-steps", type=int, default=2000,
                     help="LB steps of the 192^3 sphere-drag runs of the IBM methods (0 = skip)")
     ap.add_argument("--kernel", type=int, default=-1,
-                    help="fused-kernel variant: -1 auto, 0 plain, 1 staged, 2 packed")
+                    help="fused-kernel variant: -1 auto, 0 plain, 2 packed")
     ap.add_argument("--only", choices=["fp64", "fp32", "fp16", "ibm", "rods", "methods"], default=None,
                     help="time the fused kernel of one precision only, (ibm) the FP32 LBM + "
                          "IBM point-marker cycles only, (rods) the FP32 rod cycles only, or "
@@ -65,6 +65,12 @@ def parse():
     ap.add_argument("--rods-box", type=int, nargs=3, default=[512, 256, 256],
                     help="box of --only rods (profiling of smaller cases)")
     ap.add_argument("--rods-count", type=int, default=1000, help="rods of --only rods")
+    ap.add_argument("--refresh-lag", type=int, default=None,
+                    help="z planes between an LB block and the markers whose refresh it fills")
+    ap.add_argument("--fused-refresh", type=int, default=1,
+                    help="1: the LB launch fills the refresh's stencil records, 0: separate kernel")
+    ap.add_argument("--ibm-e2e", type=int, default=1,
+                    help="with --only ibm: also time the workload through the fix hooks (1) or not (0)")
     ap.add_argument("--ibm-n", type=int, default=256,
                     help="edge of the periodic box of the point-marker workload")
     ap.add_argument("--nx", type=int, default=NX)
@@ -157,6 +163,7 @@ class Clocks:
 
 # --------------------------------------------------------------------------
 KERNEL = -1
+LATTICE_OPTIONS = {}   # handle options of the marker workloads (--refresh-lag, --fused-refresh)
 
 
 def make_lattice(prec, nx, ny, nz, device):
@@ -249,7 +256,7 @@ def e2e_fix(steps, warmup, nx, ny, nz, device, torch):
 
 def marker_bench(torch, device, prec, cycles, warmup, box, wall, tau, x0, v0, md_per_lb, workload,
                  peak, momentum_check, fluid_out=False, method=None, record=None, slip_cycles=0,
-                 prescribed=False):
+                 prescribed=False, combined=None):
     """LBM + IBM with point markers (m 1, xi 1, Peskin4).  Markers stay on the
     device; a velocity-Verlet stand-in for the MD side (markers free, no
     bonds) runs on the same stream.  Timed: the library's own calls (one LB
@@ -260,10 +267,17 @@ def marker_bench(torch, device, prec, cycles, warmup, box, wall, tau, x0, v0, md
     receives the training rows of the timed cycles; slip_cycles: untimed
     cycles after the timed ones whose RMS slip (after the last pass) is
     averaged; prescribed: the markers keep their initial velocities (the IBM
-    force does not act back on them)."""
+    force does not act back on them); combined: the first sub-step of a
+    cycle shares one call with the LB step (couplb_lbm_step_ibm_device;
+    default: runs without a forcing method), else lbm_step +
+    ibm_substep_device."""
     from couplb_b200.lattice import Lattice
+    if combined is None:
+        combined = method is None
     nx, ny, nz = box
     L = Lattice(3, nx, ny, nz, tau=tau, wall=wall, precision=prec, device=device)
+    for k, val in LATTICE_OPTIONS.items():
+        L.set_option(k, val)
     stream = torch.cuda.current_stream()
     L.set_stream(stream.cuda_stream)
     L.init_equilibrium(1.0)
@@ -289,18 +303,24 @@ def marker_bench(torch, device, prec, cycles, warmup, box, wall, tau, x0, v0, md
             if timed:
                 e0 = torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
-            if s == 0:
-                L.lbm_step()
-            if timed:
-                ei = torch.cuda.Event(enable_timing=True)
-                ei.record(stream)
-            L.ibm_substep_device(natoms, x.data_ptr(), v.data_ptr(), m.data_ptr(), f.data_ptr(),
-                                 0, refresh=(s == 0))
+            if s == 0 and combined:
+                # LB step + refresh sub-step in one call (the LB launch fills
+                # the refresh's stencil records)
+                L.lbm_step_ibm_device(natoms, x.data_ptr(), v.data_ptr(), m.data_ptr(), f.data_ptr(), 0)
+            else:
+                if s == 0:
+                    L.lbm_step()
+                if timed:
+                    ei = torch.cuda.Event(enable_timing=True)
+                    ei.record(stream)
+                L.ibm_substep_device(natoms, x.data_ptr(), v.data_ptr(), m.data_ptr(), f.data_ptr(),
+                                     0, refresh=(s == 0))
             if timed:
                 e1 = torch.cuda.Event(enable_timing=True)
                 e1.record(stream)
                 evs.append((e0, e1))
-                ievs.append((ei, e1))
+                if not (s == 0 and combined):
+                    ievs.append((ei, e1))
             if slips is not None:
                 slips.append(L.ibm_slip()["rms"])
             if not prescribed:
@@ -315,8 +335,14 @@ def marker_bench(torch, device, prec, cycles, warmup, box, wall, tau, x0, v0, md
         cycle(True)
     torch.cuda.synchronize()
     ms = sum(a.elapsed_time(b) for a, b in evs) / cycles
-    out = {"workload": workload, "precision": prec, "cycles": cycles, "ms_per_lb_cycle": ms,
-           "ms_ibm_per_lb_cycle": sum(a.elapsed_time(b) for a, b in ievs) / cycles}
+    out = {"workload": workload, "precision": prec, "cycles": cycles, "ms_per_lb_cycle": ms}
+    if combined:
+        # the refresh sub-step shares its call with the LB step
+        out["ms_later_substeps_per_lb_cycle"] = sum(a.elapsed_time(b) for a, b in ievs) / cycles
+        out["refresh"] = "lbm_step_ibm (LB launch fills the stencil records)"
+        out["refresh_filled"] = L.get_option("refresh_filled")
+    else:
+        out["ms_ibm_per_lb_cycle"] = sum(a.elapsed_time(b) for a, b in ievs) / cycles
     if record is not None:
         out["rows"] = L.ibm_record_count()
         L.ibm_record(0, 0)
@@ -363,12 +389,84 @@ def marker_bench(torch, device, prec, cycles, warmup, box, wall, tau, x0, v0, md
     return out
 
 
-def ibm_bench(torch, device, prec, cycles, warmup, peak, n=256, natoms=20000, md_per_lb=4, seed=3):
-    """D3Q19 256^3 periodic box, nu 0.1, 20000 point markers at uniform random
-    positions with v ~ N(0, 0.01^2), Peskin4, md_per_lb 4."""
+def ibm_markers(torch, n, natoms, seed):
+    """20000 point markers of the 256^3 workload: positions uniform in the
+    box, velocities N(0, 0.01^2) per component (torch's CPU generator)."""
     g = torch.Generator(device="cpu").manual_seed(seed)
     x0 = (torch.rand((natoms, 3), generator=g, dtype=torch.float64) * n).numpy()
     v0 = (0.01 * torch.randn((natoms, 3), generator=g, dtype=torch.float64)).numpy()
+    return x0, v0
+
+
+def e2e_ibm_fix(torch, device, cycles, warmup, peak, n=256, natoms=20000, md_per_lb=4, seed=3):
+    """The 256^3 point-marker workload end to end through the fix hooks of the
+    C ABI, as an MD code drives it: atom arrays x, v, f in pinned host memory
+    (LAMMPS layout), per MD step couplb_fix_post_force (an LB step on the
+    first sub-step of each cycle, then the IBM sub-step: x, v, mass and the
+    group mask copied to the device, the IBM force copied back and added to f)
+    and couplb_fix_end_of_step.  The MD side (velocity Verlet, markers free)
+    runs on the host between the calls and is not timed; the timed region is
+    the wall time of the two hook calls, which return with the forces on the
+    host."""
+    from couplb_b200 import md
+    from couplb_b200.fix import FixCoupLB
+    x0, v0 = ibm_markers(torch, n, natoms, seed)
+    dt = 1.0 / md_per_lb
+
+    def pinned(a):
+        t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        return t, t.numpy()
+
+    xt, x = pinned(x0)
+    vt, v = pinned(v0)
+    ft, f = pinned(np.zeros((natoms, 3)))
+    at = md.Atoms(x, v, np.ones(natoms))
+    at.f = f
+    assert at.x.ctypes.data == xt.data_ptr() and at.v.ctypes.data == vt.data_ptr()
+    fix = FixCoupLB(f"flow all couplb {n} {n} {n} 0.1 1.0 md_per_lb {md_per_lb} xi_ibm 1.0 "
+                    f"kernel peskin4 precision fp32".split(), dimension=3, device=device)
+    fix.init(boxlo=(0, 0, 0), boxhi=(n, n, n), dt=dt)
+    st = at.struct()
+    f[:] = 0.0
+    fix.setup(st, 0)
+    box = float(n)
+    timed = 0.0
+    step = 0
+    for c in range(warmup + cycles):
+        for _ in range(md_per_lb):
+            step += 1
+            v += 0.5 * dt * f
+            x += dt * v
+            np.mod(x, box, out=x)
+            f[:] = 0.0
+            if c == warmup and step == warmup * md_per_lb + 1:
+                torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fix.post_force(st, step)
+            fix.end_of_step(step)
+            if c >= warmup:
+                timed += time.perf_counter() - t0
+            v += 0.5 * dt * f
+    clamps, nonfinite = fix.lattice.read_status()
+    fix.close()
+    ms = timed / cycles * 1e3
+    nodes = n ** 3
+    b_lu = BYTES_PER_LU["fp32"] + 12
+    b_mk = 64 * (3 * 4 * 3) + 72
+    return {"workload": f"d3q19_periodic_{n}^3_{natoms}_markers_peskin4_md_per_lb{md_per_lb}",
+            "precision": "fp32", "cycles": cycles, "ms_per_lb_cycle": ms,
+            "mlups": nodes / (ms * 1e-3) / 1e6, "marker_updates_per_s": natoms * md_per_lb / (ms * 1e-3),
+            "roofline_frac": (nodes * b_lu + natoms * md_per_lb * b_mk) / (ms * 1e-3) / 1e9 / peak,
+            "h2d_bytes_per_lb_cycle": md_per_lb * natoms * (3 * 8 + 3 * 8 + 8 + 4),
+            "d2h_bytes_per_lb_cycle": md_per_lb * natoms * 3 * 8,
+            "path": "couplb_fix_post_force + couplb_fix_end_of_step, pinned host atom arrays",
+            "nonfinite": nonfinite}
+
+
+def ibm_bench(torch, device, prec, cycles, warmup, peak, n=256, natoms=20000, md_per_lb=4, seed=3):
+    """D3Q19 256^3 periodic box, nu 0.1, 20000 point markers at uniform random
+    positions with v ~ N(0, 0.01^2), Peskin4, md_per_lb 4."""
+    x0, v0 = ibm_markers(torch, n, natoms, seed)
     return marker_bench(torch, device, prec, cycles, warmup, (n, n, n), (0,) * 6, 3 * 0.1 + 0.5, x0, v0,
                         md_per_lb, f"d3q19_periodic_{n}^3_{natoms}_markers_peskin4_md_per_lb{md_per_lb}",
                         peak, momentum_check=True)
@@ -535,16 +633,31 @@ def cpu_baseline(nx, ny, nz, seconds):
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     kind_name = "reference" if kind.startswith("ref") else "port"
     return {"value": nx * ny * nz / dt / 1e6, "unit": "MLUPS", "cores": cores, "kind": kind_name,
+            "cpu_model": cpu_model(),
             "sample": f"{steps} LB steps of the {nx}x{ny}x{nz} D3Q19 channel, FP64, "
                       f"fix post_force + end_of_step ({kind} build)"}
 
 
-# DRAM bytes (read + write) per launch of the fused FP32 kernel on this
-# workload, from the ncu launch list summarised in
-# profiles/k_stream_collide_x2_d3q19_channel_256x128x128.md: read 335.6 MB
-# (318.8 MB populations + 16.8 MB density field), write 283.3 MB (the write
-# total of a single launch excludes lines still dirty in L2 when it ends).
-NCU_TRAFFIC_FP32 = 335.6e6 + 283.3e6
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo), or the platform string."""
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or platform.machine()
+
+
+# DRAM bytes (read + write) of one launch of the fused FP32 kernel on the
+# 256x128x128 channel, taken from an ncu capture of a steady-state launch
+# (dram__bytes_read.sum + dram__bytes_write.sum, the launch after 20 warm-up
+# launches, so that the writes of earlier launches still dirty in L2 are
+# counted as they are evicted).  A constant of that capture, not measured by
+# this run: the line labels it so.
+NCU_TRAFFIC_FP32 = None
 
 
 def run_reference(args):
@@ -589,6 +702,9 @@ def main():
     global KERNEL
     args = parse()
     KERNEL = args.kernel
+    LATTICE_OPTIONS["fused_refresh"] = args.fused_refresh
+    if args.refresh_lag is not None:
+        LATTICE_OPTIONS["refresh_lag"] = args.refresh_lag
     if args.impl == "reference":
         return run_reference(args)
     import torch
@@ -624,6 +740,8 @@ def main():
         return
     if args.only == "ibm":
         r = ibm_bench(torch, local, "fp32", args.ibm_cycles, args.warmup, load_peak()[0], n=args.ibm_n)
+        if args.ibm_e2e:
+            r["e2e"] = e2e_ibm_fix(torch, local, args.ibm_cycles, args.warmup, load_peak()[0], n=args.ibm_n)
         print(json.dumps(r), flush=True)
         return
     if args.only == "rods":
@@ -668,6 +786,7 @@ def main():
     ibm = None
     if args.ibm_cycles > 0:
         ibm = {p: ibm_bench(torch, local, p, args.ibm_cycles, 3, peak) for p in ("fp32", "fp16", "fp64")}
+        ibm["fp32"]["e2e"] = e2e_ibm_fix(torch, local, args.ibm_cycles, 3, peak)
     rods = (rods_bench(torch, local, args.rods_cycles, 3, args.rods_accuracy_cycles, peak,
                        method_cycles=args.rods_method_cycles)
             if args.rods_cycles > 0 else None)
@@ -677,6 +796,9 @@ def main():
     mlups = world * N / (ms32 * 1e-3) / 1e6
     achieved = BYTES_PER_LU["fp32"] * N / (ms32 * 1e-3) / 1e9
     traffic = NCU_TRAFFIC_FP32 if (nx, ny, nz) == (NX, NY, NZ) else None
+    traffic_src = ("ncu capture of a steady-state launch of this kernel and workload "
+                   "(dram__bytes_read.sum + dram__bytes_write.sum); a constant, not measured by this run"
+                   if traffic else None)
     line = {
         "metric": "D3Q19 MLUPS: FP32-shifted vs plain FP64 on B200 at <=1e-6 L2 velocity error",
         "value": mlups, "unit": "MLUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -692,7 +814,8 @@ def main():
                       "l2_velocity_err_fp16_vs_fp64": acc["fp16"], "umax": acc["umax_fp64"]}
                      if acc else None),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                     "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_src,
+                     "peak_source": peak_src,
                      "bytes_per_lu": BYTES_PER_LU["fp32"],
                      "fp64_frac": BYTES_PER_LU["fp64"] * N / (results["fp64"] * 1e-3) / 1e9 / peak,
                      "fp16_frac": BYTES_PER_LU["fp16"] * N / (results["fp16"] * 1e-3) / 1e9 / peak},

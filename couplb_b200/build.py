@@ -11,7 +11,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 LIB = os.path.join(HERE, "libcouplb_b200.so")
-SOURCES = ["engine.cu", "fix_core.cpp", "noalloc.cu", "mlp.cu", "vtk_io.cpp"]
+SOURCES = ["engine.cu", "engine_ibm.cu", "engine_methods_f64.cu", "engine_methods_f32.cu",
+           "engine_methods_f16.cu", "fix_core.cpp", "noalloc.cu", "mlp.cu", "vtk_io.cpp"]
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo",
     "-gencode", "arch=compute_100a,code=sm_100a",

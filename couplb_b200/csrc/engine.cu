@@ -1,231 +1,20 @@
 // engine.cu -- layer 1 of the C ABI (include/couplb_b200.h): one handle per
 // LBM subdomain, all state resident in device memory, kernels on one stream.
-#include <cuda_runtime.h>
-
-#include <algorithm>
-#include <cmath>
-#include <cstdarg>
-#include <cstdio>
-#include <cstring>
-#include <string>
-#include <vector>
-
-#include "../../include/couplb_b200.h"
-#include "engine_internal.h"
-#include "ibm_kernels.cuh"
-#include "ibm_methods.cuh"
-#include "lbm_kernels.cuh"
+// This file: the lattice (create, LB step, moments, populations, force
+// field, diagnostics, options); engine_ibm.cu: the immersed-boundary part.
+#include "engine_common.cuh"
 #include "lbm_packed.cuh"
 #include "mlp_internal.h"
 
 using namespace couplb;
+using namespace couplb::eng;
 
 namespace {
-
-thread_local std::string g_create_error;
-
-int fail(couplb_handle* h, int code, const char* fmt, ...) {
-  char buf[512];
-  va_list ap;
-  va_start(ap, fmt);
-  vsnprintf(buf, sizeof(buf), fmt, ap);
-  va_end(ap);
-  if (h) h->err = buf;
-  else g_create_error = buf;
-  return code;
-}
-
-#define CK(call)                                                                   \
-  do {                                                                             \
-    cudaError_t e_ = (call);                                                       \
-    if (e_ != cudaSuccess)                                                         \
-      return fail(h, COUPLB_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
-  } while (0)
-
-#define CK_LAUNCH()                                                                \
-  do {                                                                             \
-    cudaError_t e_ = cudaGetLastError();                                           \
-    if (e_ != cudaSuccess)                                                         \
-      return fail(h, COUPLB_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e_)); \
-  } while (0)
-
-template <class Fn>
-void with_types(int dim, int prec, Fn&& fn) {
-  if (dim == 3) {
-    if (prec == COUPLB_FP64) fn(D3Q19{}, StoreF64{});
-    else if (prec == COUPLB_FP32_SHIFTED) fn(D3Q19{}, StoreF32S{});
-    else fn(D3Q19{}, StoreF16S{});
-  } else {
-    if (prec == COUPLB_FP64) fn(D2Q9{}, StoreF64{});
-    else if (prec == COUPLB_FP32_SHIFTED) fn(D2Q9{}, StoreF32S{});
-    else fn(D2Q9{}, StoreF16S{});
-  }
-}
 
 // Copy of the status word (clamp and non-finite counts) into a posted slot of
 // mapped pinned host memory; read by the host after the slot's event.
 __global__ void k_status_publish(const int* __restrict__ st, int* ring_slot) {
   if (threadIdx.x < 2) ring_slot[threadIdx.x] = st[threadIdx.x];
-}
-
-size_t elem_bytes_pop(int prec) { return prec == COUPLB_FP64 ? 8 : (prec == COUPLB_FP32_SHIFTED ? 4 : 2); }
-size_t elem_bytes_aux(int prec) { return prec == COUPLB_FP64 ? 8 : 4; }
-
-Geom make_geom(const couplb_handle* h) {
-  Geom g;
-  g.nx = h->p.nx; g.ny = h->p.ny; g.nz = h->p.nz;
-  g.qs = (long long)h->qs;
-  for (int f = 0; f < 6; f++) g.face[f] = h->p.wall[f];
-  if (h->p.dim == 2) g.face[4] = g.face[5] = 0;
-  for (int d = 0; d < 3; d++) g.uw[d] = h->p.wall_vel[d];
-  if (h->p.dim == 2) g.uw[2] = 0.0;
-  g.rho0 = h->p.rho0;
-  return g;
-}
-
-void row_launch(const couplb_handle* h, dim3* grid, dim3* block) {
-  const int bx = std::min(256, ((h->p.nx + 31) / 32) * 32);
-  *block = dim3(bx, 1, 1);
-  *grid = dim3((h->p.nx + bx - 1) / bx, h->p.ny, h->p.nz);
-}
-
-unsigned flat_blocks(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
-
-// Force flags: one byte per 8 consecutive interior nodes (n >> 3).
-size_t seg_bytes(const couplb_handle* h) { return (h->N + 7) / 8; }
-
-int dalloc(couplb_handle* h, void** p, size_t bytes) {
-  cudaError_t e = cudaMalloc(p, bytes);
-  if (e != cudaSuccess)
-    return fail(h, COUPLB_ERR_CUDA, "cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
-  h->device_bytes += bytes;
-  return COUPLB_OK;
-}
-
-void dfree(void*& p) {
-  if (p) cudaFree(p);
-  p = nullptr;
-}
-
-int ensure_macro(couplb_handle* h) {
-  if (h->macro[0]) return COUPLB_OK;
-  const size_t b = h->qs * elem_bytes_aux(h->p.precision);
-  for (int c = 0; c < 4; c++) {
-    int rc = dalloc(h, &h->macro[c], b);
-    if (rc) return rc;
-    CK(cudaMemsetAsync(h->macro[c], 0, b, h->stream));
-  }
-  return COUPLB_OK;
-}
-
-int ensure_staging(couplb_handle* h, size_t bytes) {
-  if (h->staging_bytes >= bytes) return COUPLB_OK;
-  dfree(h->d_staging);
-  h->staging_bytes = 0;
-  int rc = dalloc(h, &h->d_staging, bytes);
-  if (rc) return rc;
-  h->staging_bytes = bytes;
-  return COUPLB_OK;
-}
-
-// Stencil velocity records of the IBM sub-step, one per marker slot
-// (StencilKey + 64 x {ux, uy, uz, rho}).  Keys start with epoch 0xffffffff, which
-// cur_epoch never takes, so a fresh record never hits.
-int ensure_stencil_cache(couplb_handle* h, int n) {
-  if (h->stencil_cap >= n) return COUPLB_OK;
-  dfree(h->sbuf);
-  void* k = h->skey;
-  dfree(k);
-  h->skey = nullptr;
-  h->stencil_cap = 0;
-  const int cap = std::max(n, 1024);
-  int rc;
-  if ((rc = dalloc(h, &h->sbuf, elem_bytes_aux(h->p.precision) * kRecStride * (size_t)cap))) return rc;
-  if ((rc = dalloc(h, (void**)&h->skey, sizeof(couplb::StencilKey) * (size_t)cap))) return rc;
-  CK(cudaMemsetAsync(h->skey, 0xff, sizeof(couplb::StencilKey) * (size_t)cap, h->stream));
-  h->stencil_cap = cap;
-  return COUPLB_OK;
-}
-
-// The population state changed: every cached stencil velocity is stale.
-void bump_epoch(couplb_handle* h) {
-  if (++h->cur_epoch == 0xffffffffu) {
-    h->cur_epoch = 0;
-    if (h->skey) cudaMemsetAsync(h->skey, 0xff, sizeof(couplb::StencilKey) * (size_t)h->stencil_cap, h->stream);
-  }
-}
-
-// Per-marker buffers of the correction passes and their state block.
-int ensure_method_buffers(couplb_handle* h, int n) {
-  if (!h->d_pass) {
-    int rc = dalloc(h, &h->d_pass, 2 * sizeof(PassState));
-    if (rc) return rc;
-    CK(cudaMemsetAsync(h->d_pass, 0, 2 * sizeof(PassState), h->stream));
-    h->pass_cur = 0;
-  }
-  if (h->method_cap >= n) return COUPLB_OK;
-  void* p = h->d_corr; dfree(p); h->d_corr = nullptr;
-  p = h->d_dF; dfree(p); h->d_dF = nullptr;
-  h->method_cap = 0;
-  const int cap = std::max(n, 1024);
-  int rc;
-  if ((rc = dalloc(h, (void**)&h->d_corr, sizeof(double) * 3 * cap))) return rc;
-  if ((rc = dalloc(h, (void**)&h->d_dF, sizeof(double) * 3 * cap))) return rc;
-  h->method_cap = cap;
-  return COUPLB_OK;
-}
-
-int ensure_atoms(couplb_handle* h, int n) {
-  if (h->atom_cap >= n) return COUPLB_OK;
-  dfree(h->d_x); dfree(h->d_v); dfree(h->d_m); dfree(h->d_fout); dfree(h->d_active);
-  if (h->h_fout) { cudaFreeHost(h->h_fout); h->h_fout = nullptr; }
-  const int cap = std::max(n, 1024);
-  int rc;
-  if ((rc = dalloc(h, &h->d_x, sizeof(double) * 3 * cap))) return rc;
-  if ((rc = dalloc(h, &h->d_v, sizeof(double) * 3 * cap))) return rc;
-  if ((rc = dalloc(h, &h->d_m, sizeof(double) * cap))) return rc;
-  if ((rc = dalloc(h, &h->d_fout, sizeof(double) * 3 * cap))) return rc;
-  if ((rc = dalloc(h, &h->d_active, sizeof(int) * cap))) return rc;
-  CK(cudaMallocHost(&h->h_fout, sizeof(double) * 3 * cap));
-  h->atom_cap = cap;
-  return COUPLB_OK;
-}
-
-int set_device(couplb_handle* h) {
-  CK(cudaSetDevice(h->p.device));
-  return COUPLB_OK;
-}
-
-// Launch of the bulk-copy staged fused kernel: returns false (nothing
-// launched) when the row layout does not meet the copy alignment rules or the
-// stages do not fit in shared memory, so the caller uses the plain kernel.
-template <class L, class S, int STAGES>
-bool launch_staged(couplb_handle* h, const LBArgs<S>& a) {
-  using T = typename S::T;
-  const size_t row_bytes = (size_t)h->p.nx * sizeof(T);
-  if (row_bytes % 16 != 0 || (h->qs * sizeof(T)) % 16 != 0) return false;
-  if (h->p.wall[0] != 0 || h->p.wall[1] != 0) return false;   // no interior rows
-  const size_t smem = (size_t)STAGES * L::Q * row_bytes;
-  if (smem > 200 * 1024) return false;
-  static bool configured = false;   // per template instance
-  auto kern = k_stream_collide_tma<L, S, STAGES>;
-  if (!configured) {
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-      return false;
-    configured = true;
-  } else {
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  }
-  const int threads = std::min(256, ((h->p.nx + 31) / 32) * 32);
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1)
-    return false;
-  int sms = 0;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->p.device);
-  const long long rows = (long long)h->p.ny * h->p.nz;
-  const int grid = (int)std::min<long long>(rows, (long long)sms * per_sm);
-  kern<<<grid, threads, smem, h->stream>>>(a);
-  return true;
 }
 
 // Populations as post-stream state in buffer `cur` (materialise if needed).
@@ -253,6 +42,15 @@ int materialize(couplb_handle* h) {
 // ===========================================================================
 // internal entry points shared with the fix core and the profile writer
 namespace couplb {
+
+int engine_atom_host_buffers(couplb_handle* h, int n, double** mass, int** active) {
+  int rc = set_device(h);
+  if (rc) return rc;
+  if ((rc = ensure_atoms(h, n))) return rc;
+  *mass = h->h_mass;
+  *active = h->h_active;
+  return COUPLB_OK;
+}
 
 int engine_macro(couplb_handle* h) {
   int rc = ensure_macro(h);
@@ -403,8 +201,12 @@ int couplb_destroy(couplb_handle* h) {
   dfree(h->d_pass);
   dfree(h->d_staging);
   dfree(h->d_scratch);
+  p = h->d_refresh; dfree(p);
+  p = h->d_bidx; dfree(p);
   dfree(h->d_x); dfree(h->d_v); dfree(h->d_m); dfree(h->d_fout); dfree(h->d_active);
   if (h->h_fout) cudaFreeHost(h->h_fout);
+  if (h->h_mass) cudaFreeHost(h->h_mass);
+  if (h->h_active) cudaFreeHost(h->h_active);
   if (h->h_small) cudaFreeHost(h->h_small);
   if (h->h_status_ring) cudaFreeHost(h->h_status_ring);
   for (int e = 0; e < 2; e++)
@@ -514,10 +316,50 @@ int couplb_get_populations(couplb_handle* h, double* f_host) {
 
 int couplb_lbm_step(couplb_handle* h, const double* g_lb) {
   if (!h) return COUPLB_ERR_ARG;
+  return engine_lbm_step(h, g_lb, nullptr);
+}
+
+}  // extern "C"
+
+namespace {
+
+// Bucket buffers of the fused refresh for n markers.
+int ensure_refresh(couplb_handle* h, int n) {
+  const int nz = h->p.nz;
+  const int bcap = std::max(64, 2 * ((n + nz - 1) / nz) + 64);
+  if (h->d_refresh && h->refresh_nz == nz && h->refresh_bcap >= bcap) return COUPLB_OK;
+  void* p = h->d_refresh; dfree(p); h->d_refresh = nullptr;
+  p = h->d_bidx; dfree(p); h->d_bidx = nullptr;
+  int rc;
+  if ((rc = dalloc(h, (void**)&h->d_refresh, sizeof(int) * (2 * (size_t)nz + 1)))) return rc;
+  if ((rc = dalloc(h, (void**)&h->d_bidx, sizeof(int) * (size_t)nz * bcap))) return rc;
+  h->refresh_nz = nz;
+  h->refresh_bcap = bcap;
+  return COUPLB_OK;
+}
+
+}  // namespace
+
+namespace couplb {
+
+int engine_lbm_step(couplb_handle* h, const double* g_lb, const RefreshReq* rq) {
   if (g_lb && !h->p.body_force)
     return fail(h, COUPLB_ERR_STATE, "gravity given to a lattice created with body_force = 0");
   int rc = set_device(h);
   if (rc) return rc;
+  // the fused refresh: D3Q19, shifted storage on the packed kernel, IBM
+  // constants set, and an epoch that does not wrap at this step
+  const bool fuse = rq && rq->n > 0 && h->fused_refresh && h->p.dim == 3 && h->ip_set &&
+                    h->p.precision != COUPLB_FP64 && !h->poststream && h->idx32 && h->p.nx % 2 == 0 &&
+                    (h->kernel == kKernelAuto || h->kernel == kKernelPacked) &&
+                    h->cur_epoch + 1 != 0xffffffffu;
+  h->refresh_prefilled = 0;
+  h->refresh_last_fused = 0;
+  if (fuse) {
+    if ((rc = ensure_stencil_cache(h, rq->n))) return rc;
+    if ((rc = ensure_refresh(h, rq->n))) return rc;
+    CK(cudaMemsetAsync(h->d_refresh, 0, sizeof(int) * (2 * (size_t)h->p.nz + 1), h->stream));
+  }
   const bool g_active = g_lb && !(std::fabs(g_lb[0]) < ZERO_TOL && std::fabs(g_lb[1]) < ZERO_TOL &&
                                   std::fabs(g_lb[2]) < ZERO_TOL);
   dim3 grid, block;
@@ -544,7 +386,7 @@ int couplb_lbm_step(couplb_handle* h, const double* g_lb) {
     a.omega = 1.0 / h->p.tau;
     a.status = h->d_status;
     // kernel choice: packed (shifted formats, pull, even nx, 32-bit indices),
-    // else staged (when asked for), else plain
+    // else plain
     int used = kKernelPlain;
     int want = h->kernel;
     if (want == kKernelAuto) want = S::kShift ? kKernelPacked : kKernelPlain;
@@ -552,20 +394,42 @@ int couplb_lbm_step(couplb_handle* h, const double* g_lb) {
       if (want == kKernelPacked && pull && h->idx32 && h->p.nx % 2 == 0) {
         const int pairs = h->p.nx / 2;
         const dim3 pg((pairs + 127) / 128, h->p.ny, h->p.nz);
-        k_stream_collide_x2<L, S><<<pg, 128, 0, h->stream>>>(a);
+        LBRefresh<S> r{};
+        if constexpr (L::D == 3) {
+          if (fuse) {
+            IbmArgs<S>& ia = r.ia;
+            ia.g = g;
+            ia.fin = a.fout;
+            ia.rho_field = a.rho_field;
+            ia.pull = 1;
+            ia.sbuf = (A*)h->sbuf;
+            ia.skey = h->skey;
+            ia.n = rq->n;
+            ia.x = rq->d_x;
+            ia.active = rq->d_active;
+            for (int d = 0; d < 3; d++) { ia.lo[d] = h->ip.domain_lo[d]; ia.off[d] = h->ip.offset[d]; }
+            ia.inv_dx = 1.0 / h->ip.dx;
+            r.plane_done = h->d_refresh;
+            r.bcount = h->d_refresh + h->p.nz;
+            r.bidx = h->d_bidx;
+            r.bcap = h->refresh_bcap;
+            r.lag = h->refresh_lag;
+            r.blocks_per_plane = (int)pg.x * h->p.ny;
+            r.filled = h->d_refresh + 2 * h->p.nz;
+            r.epoch = h->cur_epoch + 1;
+            k_ibm_bucket<L, S><<<flat_blocks(rq->n, 256), 256, 0, h->stream>>>(
+                ia, h->d_refresh + h->p.nz, h->d_bidx, h->refresh_bcap);
+            k_stream_collide_x2<L, S, 5, true><<<pg, 128, 0, h->stream>>>(a, r);
+            h->refresh_prefilled = 1;
+            h->refresh_last_fused = 1;
+          } else {
+            k_stream_collide_x2<L, S><<<pg, 128, 0, h->stream>>>(a, r);
+          }
+        } else {
+          k_stream_collide_x2<L, S><<<pg, 128, 0, h->stream>>>(a, r);
+        }
         used = kKernelPacked;
       }
-    }
-    if (used == kKernelPlain && want == kKernelStaged && pull) {
-      bool ok;
-      // the staged kernel copies plane rows: plane-major storage only
-      if constexpr (S::kTile == 0) {
-        if constexpr (sizeof(typename S::T) == 8) ok = launch_staged<L, S, 2>(h, a);
-        else ok = launch_staged<L, S, 3>(h, a);
-      } else {
-        ok = false;
-      }
-      if (ok) used = kKernelStaged;
     }
     if (used == kKernelPlain) {
       if (h->idx32) {
@@ -593,6 +457,10 @@ int couplb_lbm_step(couplb_handle* h, const double* g_lb) {
   bump_epoch(h);
   return COUPLB_OK;
 }
+
+}  // namespace couplb
+
+extern "C" {
 
 int couplb_macroscopic(couplb_handle* h) {
   if (!h) return COUPLB_ERR_ARG;
@@ -780,14 +648,29 @@ int couplb_status_last(couplb_handle* h, int* clamps, int* nonfinite) {
 int couplb_set_option(couplb_handle* h, const char* name, long long value) {
   if (!h || !name) return COUPLB_ERR_ARG;
   if (!std::strcmp(name, "kernel")) {
-    if (value < kKernelAuto || value > kKernelPacked)
-      return fail(h, COUPLB_ERR_ARG, "kernel must be -1 (auto), 0 (plain), 1 (staged) or 2 (packed)");
+    if (value != kKernelAuto && value != kKernelPlain && value != kKernelPacked)
+      return fail(h, COUPLB_ERR_ARG, "kernel must be -1 (auto), 0 (plain) or 2 (packed)");
     h->kernel = (int)value;
     return COUPLB_OK;
   }
   if (!std::strcmp(name, "ibm_resident")) {
     if (value != 0 && value != 1) return fail(h, COUPLB_ERR_ARG, "ibm_resident must be 0 or 1");
     h->ibm_resident = (int)value;
+    return COUPLB_OK;
+  }
+  if (!std::strcmp(name, "barrier_spin")) {
+    if (value < 0 || value > (1LL << 40)) return fail(h, COUPLB_ERR_ARG, "barrier_spin must be 0..2^40");
+    h->barrier_spin = value;
+    return COUPLB_OK;
+  }
+  if (!std::strcmp(name, "fused_refresh")) {
+    if (value != 0 && value != 1) return fail(h, COUPLB_ERR_ARG, "fused_refresh must be 0 or 1");
+    h->fused_refresh = (int)value;
+    return COUPLB_OK;
+  }
+  if (!std::strcmp(name, "refresh_lag")) {
+    if (value < 0 || value > 1 << 20) return fail(h, COUPLB_ERR_ARG, "refresh_lag must be 0..2^20");
+    h->refresh_lag = (int)value;
     return COUPLB_OK;
   }
   return fail(h, COUPLB_ERR_ARG, "unknown or read-only option '%s'", name);
@@ -798,6 +681,20 @@ int couplb_get_option(couplb_handle* h, const char* name, long long* value) {
   if (!std::strcmp(name, "kernel")) { *value = h->kernel; return COUPLB_OK; }
   if (!std::strcmp(name, "last_kernel")) { *value = h->last_kernel; return COUPLB_OK; }
   if (!std::strcmp(name, "ibm_resident")) { *value = h->ibm_resident; return COUPLB_OK; }
+  if (!std::strcmp(name, "barrier_spin")) { *value = h->barrier_spin; return COUPLB_OK; }
+  if (!std::strcmp(name, "fused_refresh")) { *value = h->fused_refresh; return COUPLB_OK; }
+  if (!std::strcmp(name, "refresh_lag")) { *value = h->refresh_lag; return COUPLB_OK; }
+  if (!std::strcmp(name, "refresh_filled")) {
+    // records the last fused launch filled (-1: the last LB step did not fuse)
+    if (!h->refresh_last_fused || !h->d_refresh) { *value = -1; return COUPLB_OK; }
+    int rc = set_device(h);
+    if (rc) return rc;
+    int* hi = (int*)h->h_small;
+    CK(cudaMemcpyAsync(hi, h->d_refresh + 2 * h->p.nz, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    *value = hi[0];
+    return COUPLB_OK;
+  }
   if (!std::strcmp(name, "timeouts")) {
     int rc = set_device(h);
     if (rc) return rc;
@@ -808,311 +705,6 @@ int couplb_get_option(couplb_handle* h, const char* name, long long* value) {
     return COUPLB_OK;
   }
   return fail(h, COUPLB_ERR_ARG, "unknown option '%s'", name);
-}
-
-int couplb_set_ibm_params(couplb_handle* h, const couplb_ibm_params* ip) {
-  if (!h || !ip) return fail(h, COUPLB_ERR_ARG, "null argument");
-  if (ip->md_per_lb < 1) return fail(h, COUPLB_ERR_ARG, "md_per_lb must be >= 1");
-  if (ip->delta != COUPLB_DELTA_ROMA && ip->delta != COUPLB_DELTA_PESKIN4)
-    return fail(h, COUPLB_ERR_ARG, "unknown delta kernel %d", ip->delta);
-  if (!(ip->dx > 0) || !(ip->dt_lbm > 0) || !(ip->force_scale > 0))
-    return fail(h, COUPLB_ERR_ARG, "dx, dt_lbm and force_scale must be positive");
-  h->ip = *ip;
-  h->ip_set = 1;
-  return COUPLB_OK;
-}
-
-}  // extern "C"
-
-namespace couplb {
-
-// Shared body of the host- and device-array IBM sub-step.
-// Blocks of a cooperative kernel that fit on the device at once (cached).
-template <class K>
-int coop_resident(couplb_handle* h, K kern, size_t smem, int slot, int* out) {
-  int& resident = h->coop_blocks[slot];
-  if (resident == 0) {
-    int coop = 0, sms = 0, per_sm = 0;
-    CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, h->p.device));
-    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->p.device));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
-    if (!coop || per_sm < 1)
-      return fail(h, COUPLB_ERR_UNSUPPORTED, "the device cannot run the cooperative IBM kernel");
-    resident = per_sm * sms;
-  }
-  *out = resident;
-  return COUPLB_OK;
-}
-
-// Cooperative launch of one ITERATIVE / LEARNED sub-step (all blocks
-// resident at once, which its grid barriers need).  In 3D, when every marker
-// gets a warp of its own, the register-resident form runs.
-template <class L, class S>
-int launch_method(couplb_handle* h, PassArgs<S>& P, int delta, bool learned, int n) {
-  using K = void (*)(const PassArgs<S>);
-  const bool roma = delta == COUPLB_DELTA_ROMA;
-  const int di = (learned ? 2 : 0) + (roma ? 0 : 1);
-  const size_t smem = learned ? kLearnedSmem : 0;
-  const long long want = ((long long)n * 32 + 255) / 256;
-  void* args[] = {&P};
-  int rc, resident = 0;
-  if constexpr (L::D == 3) {
-    if (h->ibm_resident) {
-      K kr = learned ? (roma ? k_ibm_method_resident<L, S, 0, true> : k_ibm_method_resident<L, S, 1, true>)
-                     : (roma ? k_ibm_method_resident<L, S, 0, false> : k_ibm_method_resident<L, S, 1, false>);
-      if ((rc = coop_resident(h, kr, smem, 4 + di, &resident))) return rc;
-      if (want <= resident) {
-        CK(cudaLaunchCooperativeKernel((const void*)kr, dim3((unsigned)want), dim3(256), args, smem,
-                                       h->stream));
-        return COUPLB_OK;
-      }
-    }
-  }
-  K kern = nullptr;
-  if (learned) {
-    if constexpr (L::D == 3) kern = roma ? k_ibm_method<L, S, 0, true> : k_ibm_method<L, S, 1, true>;
-  } else {
-    kern = roma ? k_ibm_method<L, S, 0, false> : k_ibm_method<L, S, 1, false>;
-  }
-  if (!kern) return fail(h, COUPLB_ERR_UNSUPPORTED, "the learned correction is defined for D3Q19");
-  if ((rc = coop_resident(h, kern, smem, di, &resident))) return rc;
-  const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(want, resident));
-  CK(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(256), args, smem, h->stream));
-  return COUPLB_OK;
-}
-
-int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, const double* d_m,
-               const int* d_active, double* d_fout, int accumulate, int refresh) {
-  // no coupled atoms: the reference returns before refreshing the moments
-  // (fix_couplb.cpp:750-753)
-  if (n <= 0) return COUPLB_OK;
-  const couplb_ibm_params& ip = h->ip;
-  const int method = h->ibm_method;
-  if (method == COUPLB_IBM_LEARNED && (h->p.dim != 3 || !h->mlp))
-    return fail(h, COUPLB_ERR_UNSUPPORTED, "the learned correction needs D3Q19 and a network");
-  // The refresh of compute_macroscopic(false) (fix_couplb.cpp:757-760): the
-  // velocities are computed on demand by the kernel; the density it would
-  // store is what the next LB step's body force reads.
-  if (refresh && h->p.body_force) h->rho_state = kRhoCurrent;
-  int rc = ensure_stencil_cache(h, n);
-  if (rc) return rc;
-  bool record = false;
-  if (method != COUPLB_IBM_SINGLE) {
-    if ((rc = ensure_method_buffers(h, n))) return rc;
-    if (h->rec_rows) {
-      if (d_active) return fail(h, COUPLB_ERR_STATE, "sample capture needs every atom coupled");
-      record = h->rec_count + n <= h->rec_cap;
-    }
-  }
-  const double dxp = ip.dx;
-  const double dv = (h->p.dim == 3) ? dxp * dxp * dxp : dxp * dxp;
-  const double cell_vol = dxp * dxp * ((h->p.dim == 3) ? dxp : 1.0);
-  const Geom g = make_geom(h);
-  const int bs = 256;
-  const unsigned nb = (unsigned)(((long long)n * 32 + bs - 1) / bs);
-  int lrc = COUPLB_OK;
-  with_types(h->p.dim, h->p.precision, [&](auto l, auto s) {
-    using L = decltype(l);
-    using S = decltype(s);
-    using A = typename S::A;
-    IbmArgs<S> a;
-    a.g = g;
-    a.fin = (const typename S::T*)h->f[h->cur];
-    a.rho_field = (const A*)h->rho_field;
-    a.pull = h->poststream ? 0 : 1;
-    a.cux = (const A*)h->macro[1]; a.cuy = (const A*)h->macro[2]; a.cuz = (const A*)h->macro[3];
-    a.all_valid = h->macro_valid;
-    a.crho = (const A*)h->macro[0];
-    a.sbuf = (A*)h->sbuf;
-    a.skey = h->skey;
-    a.cur_epoch = h->cur_epoch;
-    a.F = (A*)h->F;
-    a.seg_force = h->seg_force;
-    a.n = n;
-    a.x = d_x; a.v = d_v; a.m = d_m; a.active = d_active;
-    a.fout = d_fout;
-    a.accumulate = accumulate;
-    a.ftot = h->d_ftot;
-    for (int d = 0; d < 3; d++) { a.lo[d] = ip.domain_lo[d]; a.off[d] = ip.offset[d]; }
-    if (h->p.dim == 2) a.off[2] = 0;
-    a.inv_dx = 1.0 / dxp;
-    a.xi_over_dt = ip.xi_ibm / ip.dt_lbm;
-    a.inv_N = 1.0 / (double)ip.md_per_lb;
-    a.vs = ip.vel_scale;
-    a.fs = ip.force_scale;
-    a.dvr = dv / cell_vol;
-    a.corr = method != COUPLB_IBM_SINGLE ? h->d_corr : nullptr;
-    a.mlp = (method == COUPLB_IBM_LEARNED) ? h->mlp->pack : nullptr;
-    if (method == COUPLB_IBM_SINGLE) {
-      if (refresh && !a.all_valid) k_ibm_prefetch<L, S><<<nb, bs, 0, h->stream>>>(a);
-      if (ip.delta == COUPLB_DELTA_ROMA) k_ibm_substep<L, S, 0><<<nb, bs, 0, h->stream>>>(a);
-      else k_ibm_substep<L, S, 1><<<nb, bs, 0, h->stream>>>(a);
-    } else {
-      PassState* ps = (PassState*)h->d_pass;
-      h->pass_cur ^= 1;
-      PassArgs<S> P;
-      P.a = a;
-      P.dF = h->d_dF;
-      P.ps = ps + h->pass_cur;
-      P.ps_next = ps + (h->pass_cur ^ 1);
-      P.fill = refresh && !a.all_valid;
-      P.status = h->d_status;
-      P.ncorr = h->ibm_passes - 1;
-      P.check_first = method == COUPLB_IBM_LEARNED;
-      P.slip_tol = h->slip_tol;
-      for (int d = 0; d < 3; d++) P.g_lb[d] = h->g_lb[d];
-      P.rows = record ? h->rec_rows + h->rec_count * kMlpRow : nullptr;
-      lrc = launch_method<L, S>(h, P, ip.delta, method == COUPLB_IBM_LEARNED, n);
-    }
-  });
-  if (lrc) return lrc;
-  CK_LAUNCH();
-  if (record) h->rec_count += n;
-  h->force_dirty = 1;
-  return COUPLB_OK;
-}
-
-}  // namespace couplb
-
-extern "C" {
-
-int couplb_ibm_substep(couplb_handle* h, int n, const double* x, const double* v,
-                       const double* mass, const int* active, double* f_add, int refresh,
-                       int* ncoupled) {
-  if (!h) return COUPLB_ERR_ARG;
-  if (!h->ip_set) return fail(h, COUPLB_ERR_STATE, "couplb_set_ibm_params not called");
-  if (n < 0 || (n > 0 && (!x || !v || !mass || !f_add))) return fail(h, COUPLB_ERR_ARG, "bad atom arrays");
-  int rc = set_device(h);
-  if (rc) return rc;
-  int nc = 0;
-  for (int a = 0; a < n; a++) nc += active ? (active[a] != 0) : 1;
-  if (ncoupled) *ncoupled = nc;
-  if ((rc = ensure_atoms(h, n))) return rc;
-  if (n > 0) {
-    CK(cudaMemcpyAsync(h->d_x, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->d_v, v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->d_m, mass, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
-    if (active) CK(cudaMemcpyAsync(h->d_active, active, sizeof(int) * n, cudaMemcpyHostToDevice, h->stream));
-  }
-  rc = engine_ibm(h, nc > 0 ? n : 0, (const double*)h->d_x, (const double*)h->d_v,
-                  (const double*)h->d_m, active ? (const int*)h->d_active : nullptr,
-                  (double*)h->d_fout, 0, refresh);
-  if (rc) return rc;
-  if (nc > 0) {
-    CK(cudaMemcpyAsync(h->h_fout, h->d_fout, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    for (int a = 0; a < 3 * n; a++) f_add[a] += h->h_fout[a];
-  }
-  return COUPLB_OK;
-}
-
-int couplb_ibm_substep_device(couplb_handle* h, int n, const double* d_x, const double* d_v,
-                              const double* d_mass, const int* d_active, double* d_f_add,
-                              int refresh) {
-  if (!h) return COUPLB_ERR_ARG;
-  if (!h->ip_set) return fail(h, COUPLB_ERR_STATE, "couplb_set_ibm_params not called");
-  if (n < 0 || (n > 0 && (!d_x || !d_v || !d_mass || !d_f_add))) return fail(h, COUPLB_ERR_ARG, "bad atom arrays");
-  int rc = set_device(h);
-  if (rc) return rc;
-  return engine_ibm(h, n, d_x, d_v, d_mass, d_active, d_f_add, 1, refresh);
-}
-
-int couplb_set_ibm_method(couplb_handle* h, const couplb_ibm_method* m) {
-  if (!h || !m) return COUPLB_ERR_ARG;
-  if (m->method < COUPLB_IBM_SINGLE || m->method > COUPLB_IBM_LEARNED)
-    return fail(h, COUPLB_ERR_ARG, "unknown IBM method %d", m->method);
-  if (m->passes < 1 || m->passes > 64) return fail(h, COUPLB_ERR_ARG, "passes must be 1..64");
-  if (m->method == COUPLB_IBM_LEARNED) {
-    if (!m->model) return fail(h, COUPLB_ERR_ARG, "the learned method needs a network");
-    if (h->p.dim != 3) return fail(h, COUPLB_ERR_UNSUPPORTED, "the learned correction is defined for D3Q19");
-    if (m->model->device != h->p.device)
-      return fail(h, COUPLB_ERR_ARG, "the network lives on device %d, the lattice on %d", m->model->device,
-                  h->p.device);
-    if (!(m->slip_tol >= 0.0)) return fail(h, COUPLB_ERR_ARG, "slip_tol must be >= 0");
-  }
-  h->ibm_method = m->method;
-  h->ibm_passes = m->passes;
-  h->slip_tol = m->slip_tol;
-  h->mlp = m->method == COUPLB_IBM_LEARNED ? m->model : nullptr;
-  return COUPLB_OK;
-}
-
-int couplb_ibm_slip(couplb_handle* h, double out[8], int reset) {
-  if (!h || !out) return COUPLB_ERR_ARG;
-  int rc = set_device(h);
-  if (rc) return rc;
-  for (int i = 0; i < 8; i++) out[i] = 0.0;
-  unsigned char* hs = (unsigned char*)h->h_small;
-  static_assert(sizeof(PassState) + 8 * sizeof(int) <= 4096, "h_small holds the pass state");
-  if (h->d_pass)
-    CK(cudaMemcpyAsync(hs, (PassState*)h->d_pass + h->pass_cur, sizeof(PassState), cudaMemcpyDeviceToHost,
-                       h->stream));
-  else std::memset(hs, 0, sizeof(PassState));
-  int* st = (int*)(hs + sizeof(PassState));
-  CK(cudaMemcpyAsync(st, h->d_status, sizeof(int) * 8, cudaMemcpyDeviceToHost, h->stream));
-  if (reset) CK(cudaMemsetAsync(h->d_status + kStSlipChecks, 0, sizeof(int) * 2, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
-  PassState ps;
-  std::memcpy(&ps, hs, sizeof ps);
-  auto count = [&](int r) {
-    int c = 0;
-    for (int i = 0; i < kSlipSlots; i++) c += ps.count[r][i];
-    return c;
-  };
-  auto rms = [&](int r) {
-    double s = 0.0;
-    for (int i = 0; i < kSlipSlots; i++) s += ps.s2[r][i];
-    const int c = count(r);
-    return c > 0 ? std::sqrt(s / c) : 0.0;
-  };
-  auto mx = [&](int r) {
-    double m = 0.0;
-    for (int i = 0; i < kSlipSlots; i++) {
-      double v;
-      std::memcpy(&v, &ps.max_bits[r][i], sizeof v);
-      m = std::max(m, v);
-    }
-    return m;
-  };
-  const int r = (ps.checked && !ps.fell_back) ? 0 : 1;
-  out[0] = rms(r);
-  out[1] = mx(r);
-  out[2] = ps.checked ? rms(0) : 0.0;
-  out[3] = ps.checked ? mx(0) : 0.0;
-  out[4] = count(r);
-  out[5] = ps.fell_back;
-  out[6] = st[kStSlipChecks];
-  out[7] = st[kStFallbacks];
-  return COUPLB_OK;
-}
-
-int couplb_ibm_record(couplb_handle* h, float* d_rows, long long capacity) {
-  if (!h) return COUPLB_ERR_ARG;
-  if (d_rows && capacity < 0) return fail(h, COUPLB_ERR_ARG, "negative capacity");
-  h->rec_rows = d_rows;
-  h->rec_cap = d_rows ? capacity : 0;
-  h->rec_count = 0;
-  return COUPLB_OK;
-}
-
-int couplb_ibm_record_count(couplb_handle* h, long long* rows) {
-  if (!h || !rows) return COUPLB_ERR_ARG;
-  *rows = h->rec_count;
-  return COUPLB_OK;
-}
-
-int couplb_ibm_total_force(couplb_handle* h, double out[3], int reset) {
-  if (!h || !out) return COUPLB_ERR_ARG;
-  int rc = set_device(h);
-  if (rc) return rc;
-  double* hs = (double*)h->h_small;
-  CK(cudaMemcpyAsync(hs, h->d_ftot, sizeof(double) * 4 * kFtotSlots, cudaMemcpyDeviceToHost, h->stream));
-  if (reset) CK(cudaMemsetAsync(h->d_ftot, 0, sizeof(double) * 4 * kFtotSlots, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
-  out[0] = out[1] = out[2] = 0.0;
-  for (int s = 0; s < kFtotSlots; s++)
-    for (int c = 0; c < 3; c++) out[c] += hs[4 * s + c];
-  return COUPLB_OK;
 }
 
 }  // extern "C"

@@ -1,0 +1,327 @@
+// engine_ibm.cu -- layer 1 of the C ABI, immersed-boundary part: the IBM
+// constants, the sub-steps (single pass, iterative and learned methods),
+// slip, training-sample capture and the total-force accumulator.
+#include "engine_common.cuh"
+#include "engine_methods.cuh"
+#include "mlp_internal.h"
+
+using namespace couplb;
+using namespace couplb::eng;
+
+extern "C" {
+
+int couplb_set_ibm_params(couplb_handle* h, const couplb_ibm_params* ip) {
+  if (!h || !ip) return fail(h, COUPLB_ERR_ARG, "null argument");
+  if (ip->md_per_lb < 1) return fail(h, COUPLB_ERR_ARG, "md_per_lb must be >= 1");
+  if (ip->delta != COUPLB_DELTA_ROMA && ip->delta != COUPLB_DELTA_PESKIN4)
+    return fail(h, COUPLB_ERR_ARG, "unknown delta kernel %d", ip->delta);
+  if (!(ip->dx > 0) || !(ip->dt_lbm > 0) || !(ip->force_scale > 0))
+    return fail(h, COUPLB_ERR_ARG, "dx, dt_lbm and force_scale must be positive");
+  h->ip = *ip;
+  h->ip_set = 1;
+  return COUPLB_OK;
+}
+
+
+}  // extern "C"
+
+namespace couplb {
+
+// Shared body of the host- and device-array IBM sub-step.  The launches of
+// the method kernels (launch_method) are compiled in engine_methods_*.cu.
+int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, const double* d_m,
+               const int* d_active, double* d_fout, int accumulate, int refresh) {
+  // no coupled atoms: the reference returns before refreshing the moments
+  // (fix_couplb.cpp:750-753)
+  if (n <= 0) return COUPLB_OK;
+  const couplb_ibm_params& ip = h->ip;
+  const int method = h->ibm_method;
+  if (method == COUPLB_IBM_LEARNED && (h->p.dim != 3 || !h->mlp))
+    return fail(h, COUPLB_ERR_UNSUPPORTED, "the learned correction needs D3Q19 and a network");
+  // The refresh of compute_macroscopic(false) (fix_couplb.cpp:757-760): the
+  // velocities are computed on demand by the kernel; the density it would
+  // store is what the next LB step's body force reads.
+  if (refresh && h->p.body_force) h->rho_state = kRhoCurrent;
+  int rc = ensure_stencil_cache(h, n);
+  if (rc) return rc;
+  bool record = false;
+  if (method != COUPLB_IBM_SINGLE) {
+    if ((rc = ensure_method_buffers(h, n))) return rc;
+    if (h->rec_rows) {
+      if (d_active) return fail(h, COUPLB_ERR_STATE, "sample capture needs every atom coupled");
+      record = h->rec_count + n <= h->rec_cap;
+    }
+  }
+  const double dxp = ip.dx;
+  const double dv = (h->p.dim == 3) ? dxp * dxp * dxp : dxp * dxp;
+  const double cell_vol = dxp * dxp * ((h->p.dim == 3) ? dxp : 1.0);
+  const Geom g = make_geom(h);
+  const int bs = 256;
+  const unsigned nb = (unsigned)(((long long)n * 32 + bs - 1) / bs);
+  int lrc = COUPLB_OK;
+  with_types(h->p.dim, h->p.precision, [&](auto l, auto s) {
+    using L = decltype(l);
+    using S = decltype(s);
+    using A = typename S::A;
+    IbmArgs<S> a;
+    a.g = g;
+    a.fin = (const typename S::T*)h->f[h->cur];
+    a.rho_field = (const A*)h->rho_field;
+    a.pull = h->poststream ? 0 : 1;
+    a.cux = (const A*)h->macro[1]; a.cuy = (const A*)h->macro[2]; a.cuz = (const A*)h->macro[3];
+    a.all_valid = h->macro_valid;
+    a.crho = (const A*)h->macro[0];
+    a.sbuf = (A*)h->sbuf;
+    a.skey = h->skey;
+    a.cur_epoch = h->cur_epoch;
+    a.F = (A*)h->F;
+    a.seg_force = h->seg_force;
+    a.n = n;
+    a.x = d_x; a.v = d_v; a.m = d_m; a.active = d_active;
+    a.fout = d_fout;
+    a.accumulate = accumulate;
+    a.ftot = h->d_ftot;
+    for (int d = 0; d < 3; d++) { a.lo[d] = ip.domain_lo[d]; a.off[d] = ip.offset[d]; }
+    if (h->p.dim == 2) a.off[2] = 0;
+    a.inv_dx = 1.0 / dxp;
+    a.xi_over_dt = ip.xi_ibm / ip.dt_lbm;
+    a.inv_N = 1.0 / (double)ip.md_per_lb;
+    a.vs = ip.vel_scale;
+    a.fs = ip.force_scale;
+    a.dvr = dv / cell_vol;
+    a.corr = method != COUPLB_IBM_SINGLE ? h->d_corr : nullptr;
+    a.mlp = (method == COUPLB_IBM_LEARNED) ? h->mlp->pack : nullptr;
+    // records filled by the LB launch (couplb_lbm_step_ibm*): the refresh
+    // sub-step only fills the records of markers the launch left out
+    const bool prefilled = refresh && !a.all_valid && h->refresh_prefilled;
+    a.fill_miss = prefilled ? 1 : 0;
+    if (method == COUPLB_IBM_SINGLE) {
+      if (refresh && !a.all_valid && !prefilled) k_ibm_prefetch<L, S><<<nb, bs, 0, h->stream>>>(a);
+      if (ip.delta == COUPLB_DELTA_ROMA) k_ibm_substep<L, S, 0><<<nb, bs, 0, h->stream>>>(a);
+      else k_ibm_substep<L, S, 1><<<nb, bs, 0, h->stream>>>(a);
+    } else {
+      PassState* ps = (PassState*)h->d_pass;
+      h->pass_cur ^= 1;
+      PassArgs<S> P;
+      P.a = a;
+      P.dF = h->d_dF;
+      P.ps = ps + h->pass_cur;
+      P.ps_next = ps + (h->pass_cur ^ 1);
+      P.fill = refresh && !a.all_valid && !prefilled;
+      P.status = h->d_status;
+      P.ncorr = h->ibm_passes - 1;
+      P.check_first = method == COUPLB_IBM_LEARNED;
+      P.slip_tol = h->slip_tol;
+      for (int d = 0; d < 3; d++) P.g_lb[d] = h->g_lb[d];
+      P.rows = record ? h->rec_rows + h->rec_count * kMlpRow : nullptr;
+      P.spin = h->barrier_spin;
+      lrc = launch_method<L, S>(h, P, ip.delta, method == COUPLB_IBM_LEARNED, n);
+    }
+  });
+  if (lrc) return lrc;
+  CK_LAUNCH();
+  if (record) h->rec_count += n;
+  h->force_dirty = 1;
+  if (refresh) h->refresh_prefilled = 0;
+  return COUPLB_OK;
+}
+
+}  // namespace couplb
+
+extern "C" {
+
+}  // extern "C"
+
+namespace {
+
+// Host atom arrays of one sub-step copied to the handle's device buffers
+// (queued on the stream); *nc = atoms in the group.
+int stage_host_atoms(couplb_handle* h, int n, const double* x, const double* v, const double* mass,
+                     const int* active, int* nc) {
+  if (n < 0 || (n > 0 && (!x || !v || !mass))) return fail(h, COUPLB_ERR_ARG, "bad atom arrays");
+  int rc = ensure_atoms(h, n);
+  if (rc) return rc;
+  int c = 0;
+  for (int a = 0; a < n; a++) c += active ? (active[a] != 0) : 1;
+  *nc = c;
+  if (n > 0) {
+    CK(cudaMemcpyAsync(h->d_x, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_v, v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_m, mass, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+    if (active) CK(cudaMemcpyAsync(h->d_active, active, sizeof(int) * n, cudaMemcpyHostToDevice, h->stream));
+  }
+  return COUPLB_OK;
+}
+
+// The sub-step of staged host atoms, then the forces back to the host.
+int substep_staged(couplb_handle* h, int n, const int* active, int nc, double* f_add, int refresh) {
+  int rc = engine_ibm(h, nc > 0 ? n : 0, (const double*)h->d_x, (const double*)h->d_v,
+                      (const double*)h->d_m, active ? (const int*)h->d_active : nullptr,
+                      (double*)h->d_fout, 0, refresh);
+  if (rc) return rc;
+  if (nc > 0) {
+    CK(cudaMemcpyAsync(h->h_fout, h->d_fout, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int a = 0; a < 3 * n; a++) f_add[a] += h->h_fout[a];
+  }
+  return COUPLB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int couplb_ibm_substep(couplb_handle* h, int n, const double* x, const double* v,
+                       const double* mass, const int* active, double* f_add, int refresh,
+                       int* ncoupled) {
+  if (!h) return COUPLB_ERR_ARG;
+  if (!h->ip_set) return fail(h, COUPLB_ERR_STATE, "couplb_set_ibm_params not called");
+  if (n > 0 && !f_add) return fail(h, COUPLB_ERR_ARG, "bad atom arrays");
+  int rc = set_device(h);
+  if (rc) return rc;
+  int nc = 0;
+  if ((rc = stage_host_atoms(h, n, x, v, mass, active, &nc))) return rc;
+  if (ncoupled) *ncoupled = nc;
+  return substep_staged(h, n, active, nc, f_add, refresh);
+}
+
+int couplb_lbm_step_ibm(couplb_handle* h, const double* g_lb, int n, const double* x, const double* v,
+                        const double* mass, const int* active, double* f_add, int* ncoupled) {
+  if (!h) return COUPLB_ERR_ARG;
+  if (!h->ip_set) return fail(h, COUPLB_ERR_STATE, "couplb_set_ibm_params not called");
+  if (n > 0 && !f_add) return fail(h, COUPLB_ERR_ARG, "bad atom arrays");
+  int rc = set_device(h);
+  if (rc) return rc;
+  int nc = 0;
+  // the atoms go to the device first, so that the LB launch can fill their
+  // stencil records
+  if ((rc = stage_host_atoms(h, n, x, v, mass, active, &nc))) return rc;
+  if (ncoupled) *ncoupled = nc;
+  const RefreshReq rq{nc > 0 ? n : 0, (const double*)h->d_x, active ? (const int*)h->d_active : nullptr};
+  if ((rc = engine_lbm_step(h, g_lb, &rq))) return rc;
+  return substep_staged(h, n, active, nc, f_add, 1);
+}
+
+int couplb_lbm_step_ibm_device(couplb_handle* h, const double* g_lb, int n, const double* d_x,
+                               const double* d_v, const double* d_mass, const int* d_active,
+                               double* d_f_add) {
+  if (!h) return COUPLB_ERR_ARG;
+  if (!h->ip_set) return fail(h, COUPLB_ERR_STATE, "couplb_set_ibm_params not called");
+  if (n < 0 || (n > 0 && (!d_x || !d_v || !d_mass || !d_f_add))) return fail(h, COUPLB_ERR_ARG, "bad atom arrays");
+  int rc = set_device(h);
+  if (rc) return rc;
+  const RefreshReq rq{n, d_x, d_active};
+  if ((rc = engine_lbm_step(h, g_lb, &rq))) return rc;
+  return engine_ibm(h, n, d_x, d_v, d_mass, d_active, d_f_add, 1, 1);
+}
+
+int couplb_ibm_substep_device(couplb_handle* h, int n, const double* d_x, const double* d_v,
+                              const double* d_mass, const int* d_active, double* d_f_add,
+                              int refresh) {
+  if (!h) return COUPLB_ERR_ARG;
+  if (!h->ip_set) return fail(h, COUPLB_ERR_STATE, "couplb_set_ibm_params not called");
+  if (n < 0 || (n > 0 && (!d_x || !d_v || !d_mass || !d_f_add))) return fail(h, COUPLB_ERR_ARG, "bad atom arrays");
+  int rc = set_device(h);
+  if (rc) return rc;
+  return engine_ibm(h, n, d_x, d_v, d_mass, d_active, d_f_add, 1, refresh);
+}
+
+int couplb_set_ibm_method(couplb_handle* h, const couplb_ibm_method* m) {
+  if (!h || !m) return COUPLB_ERR_ARG;
+  if (m->method < COUPLB_IBM_SINGLE || m->method > COUPLB_IBM_LEARNED)
+    return fail(h, COUPLB_ERR_ARG, "unknown IBM method %d", m->method);
+  if (m->passes < 1 || m->passes > 64) return fail(h, COUPLB_ERR_ARG, "passes must be 1..64");
+  if (m->method == COUPLB_IBM_LEARNED) {
+    if (!m->model) return fail(h, COUPLB_ERR_ARG, "the learned method needs a network");
+    if (h->p.dim != 3) return fail(h, COUPLB_ERR_UNSUPPORTED, "the learned correction is defined for D3Q19");
+    if (m->model->device != h->p.device)
+      return fail(h, COUPLB_ERR_ARG, "the network lives on device %d, the lattice on %d", m->model->device,
+                  h->p.device);
+    if (!(m->slip_tol >= 0.0)) return fail(h, COUPLB_ERR_ARG, "slip_tol must be >= 0");
+  }
+  h->ibm_method = m->method;
+  h->ibm_passes = m->passes;
+  h->slip_tol = m->slip_tol;
+  h->mlp = m->method == COUPLB_IBM_LEARNED ? m->model : nullptr;
+  return COUPLB_OK;
+}
+
+int couplb_ibm_slip(couplb_handle* h, double out[8], int reset) {
+  if (!h || !out) return COUPLB_ERR_ARG;
+  int rc = set_device(h);
+  if (rc) return rc;
+  for (int i = 0; i < 8; i++) out[i] = 0.0;
+  unsigned char* hs = (unsigned char*)h->h_small;
+  static_assert(sizeof(PassState) + 8 * sizeof(int) <= 4096, "h_small holds the pass state");
+  if (h->d_pass)
+    CK(cudaMemcpyAsync(hs, (PassState*)h->d_pass + h->pass_cur, sizeof(PassState), cudaMemcpyDeviceToHost,
+                       h->stream));
+  else std::memset(hs, 0, sizeof(PassState));
+  int* st = (int*)(hs + sizeof(PassState));
+  CK(cudaMemcpyAsync(st, h->d_status, sizeof(int) * 8, cudaMemcpyDeviceToHost, h->stream));
+  if (reset) CK(cudaMemsetAsync(h->d_status + kStSlipChecks, 0, sizeof(int) * 2, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  PassState ps;
+  std::memcpy(&ps, hs, sizeof ps);
+  auto count = [&](int r) {
+    int c = 0;
+    for (int i = 0; i < kSlipSlots; i++) c += ps.count[r][i];
+    return c;
+  };
+  auto rms = [&](int r) {
+    double s = 0.0;
+    for (int i = 0; i < kSlipSlots; i++) s += ps.s2[r][i];
+    const int c = count(r);
+    return c > 0 ? std::sqrt(s / c) : 0.0;
+  };
+  auto mx = [&](int r) {
+    double m = 0.0;
+    for (int i = 0; i < kSlipSlots; i++) {
+      double v;
+      std::memcpy(&v, &ps.max_bits[r][i], sizeof v);
+      m = std::max(m, v);
+    }
+    return m;
+  };
+  const int r = (ps.checked && !ps.fell_back) ? 0 : 1;
+  out[0] = rms(r);
+  out[1] = mx(r);
+  out[2] = ps.checked ? rms(0) : 0.0;
+  out[3] = ps.checked ? mx(0) : 0.0;
+  out[4] = count(r);
+  out[5] = ps.fell_back;
+  out[6] = st[kStSlipChecks];
+  out[7] = st[kStFallbacks];
+  return COUPLB_OK;
+}
+
+int couplb_ibm_record(couplb_handle* h, float* d_rows, long long capacity) {
+  if (!h) return COUPLB_ERR_ARG;
+  if (d_rows && capacity < 0) return fail(h, COUPLB_ERR_ARG, "negative capacity");
+  h->rec_rows = d_rows;
+  h->rec_cap = d_rows ? capacity : 0;
+  h->rec_count = 0;
+  return COUPLB_OK;
+}
+
+int couplb_ibm_record_count(couplb_handle* h, long long* rows) {
+  if (!h || !rows) return COUPLB_ERR_ARG;
+  *rows = h->rec_count;
+  return COUPLB_OK;
+}
+
+int couplb_ibm_total_force(couplb_handle* h, double out[3], int reset) {
+  if (!h || !out) return COUPLB_ERR_ARG;
+  int rc = set_device(h);
+  if (rc) return rc;
+  double* hs = (double*)h->h_small;
+  CK(cudaMemcpyAsync(hs, h->d_ftot, sizeof(double) * 4 * kFtotSlots, cudaMemcpyDeviceToHost, h->stream));
+  if (reset) CK(cudaMemsetAsync(h->d_ftot, 0, sizeof(double) * 4 * kFtotSlots, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  out[0] = out[1] = out[2] = 0.0;
+  for (int s = 0; s < kFtotSlots; s++)
+    for (int c = 0; c < 3; c++) out[c] += hs[4 * s + c];
+  return COUPLB_OK;
+}
+
+}  // extern "C"

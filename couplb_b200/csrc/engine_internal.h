@@ -60,6 +60,8 @@ struct couplb_handle {
   void* d_fout = nullptr;
   void* d_active = nullptr;
   double* h_fout = nullptr;
+  double* h_mass = nullptr;          // pinned host staging of the per-atom masses
+  int* h_active = nullptr;           // pinned host staging of the group flags
   int atom_cap = 0;
 
   // IBM forcing method (couplb_set_ibm_method)
@@ -73,6 +75,15 @@ struct couplb_handle {
   void* d_pass = nullptr;            // two couplb::PassState, alternating per sub-step
   int pass_cur = 0;                  // the one of the last sub-step
   int ibm_resident = 1;              // option: register-resident form when markers fit
+  long long barrier_spin = 1LL << 21;   // option: grid-barrier poll limit of the method kernels
+  // IBM refresh fused into the LB launch (couplb_lbm_step_ibm*)
+  int fused_refresh = 1;             // option: allow it
+  int refresh_lag = 8;               // option: planes between a block and the bucket it fills
+  int* d_refresh = nullptr;          // per z plane: done counters, then bucket counts; filled count
+  int* d_bidx = nullptr;             // bucket lists
+  int refresh_nz = 0, refresh_bcap = 0;
+  int refresh_prefilled = 0;         // the records of the pending refresh are filled
+  int refresh_last_fused = 0;        // the last LB launch filled stencil records
   int coop_blocks[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // resident blocks of k_ibm_method (Roma,
                                                    // Peskin4, learned Roma, learned Peskin4),
                                                    // then of its register-resident form
@@ -86,6 +97,20 @@ struct couplb_handle {
 
 namespace couplb {
 int engine_macro(couplb_handle* h);
+// The markers whose refresh a fused LB launch fills (device arrays).
+struct RefreshReq {
+  int n;
+  const double* d_x;
+  const int* d_active;
+};
+// One LB step; with rq (and a D3Q19 shifted lattice on the packed kernel)
+// the launch also fills the stencil records of the refresh of those markers.
+int engine_lbm_step(couplb_handle* h, const double* g_lb, const RefreshReq* rq);
+// Pinned host buffers of n masses and n group flags owned by the handle (valid
+// until the next call with a larger n), for host drivers that assemble those
+// arrays before couplb_ibm_substep, so that every host->device copy of a
+// sub-step starts from pinned memory.
+int engine_atom_host_buffers(couplb_handle* h, int n, double** mass, int** active);
 int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, const double* d_m,
                const int* d_active, double* d_fout, int accumulate, int refresh);
 }  // namespace couplb

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/couplb_b200.h"
+#include "engine_internal.h"
 #include "vtk_io.h"
 
 using couplb::VtkArray;
@@ -106,8 +107,6 @@ struct couplb_fix {
   void* logctx = nullptr;
   couplb_diag last_diag{};
   std::string err;
-  std::vector<double> mass_buf;
-  std::vector<int> active_buf;
   int vtk_region[6] = {0, 0, 0, 0, 0, 0};
   double vtk_rlo[3] = {0, 0, 0}, vtk_rhi[3] = {0, 0, 0};   // clamped region, MD units
   std::vector<long long> vtk_steps;   // steps with field output (the .pvd series)
@@ -415,28 +414,40 @@ int read_checkpoint(couplb_fix* F, long long* step_out) {
   return COUPLB_OK;
 }
 
-// FixCoupLB::do_ibm_sub_coupling (fix_couplb.cpp:730-798).
-int ibm_sub_coupling(couplb_fix* F, const couplb_atoms* at) {
+// FixCoupLB::do_ibm_sub_coupling (fix_couplb.cpp:730-798).  With lbm, the
+// LB step of the cycle (do_lbm_step with body force g_lb, or none when
+// g_lb is null) runs first, in the same engine call when there are atoms
+// (couplb_lbm_step_ibm: the LB launch fills the refresh's stencil records).
+int ibm_sub_coupling(couplb_fix* F, const couplb_atoms* at, bool lbm = false,
+                     const double* g_lb = nullptr) {
   const bool first = (F->md_sub_count == 0);
   const int nl = at ? at->nlocal : 0;
-  F->active_buf.resize(nl > 0 ? nl : 1);
-  F->mass_buf.resize(nl > 0 ? nl : 1);
+  // masses and group flags go to pinned buffers of the lattice handle, so the
+  // engine's host->device copies of a sub-step start from pinned memory
+  double* mass_buf = nullptr;
+  int* active_buf = nullptr;
+  int rc0 = couplb::engine_atom_host_buffers(F->h, nl, &mass_buf, &active_buf);
+  if (rc0) return F->engine_fail(rc0);
   int ng = 0;
   for (int i = 0; i < nl; i++) {
     const int act = at->mask ? ((at->mask[i] & at->groupbit) != 0) : 1;
-    F->active_buf[i] = act;
+    active_buf[i] = act;
     ng += act;
-    F->mass_buf[i] = at->rmass ? at->rmass[i] : (at->mass ? at->mass[at->type[i]] : 1.0);
+    mass_buf[i] = at->rmass ? at->rmass[i] : (at->mass ? at->mass[at->type[i]] : 1.0);
   }
   if (ng == 0) {
     F->ibm_has_particles = false;
+    if (lbm) {
+      const int rc = couplb_lbm_step(F->h, g_lb);
+      if (rc) return F->engine_fail(rc);
+    }
     return COUPLB_OK;
   }
   const int refresh = (first || !F->ibm_has_particles) ? 1 : 0;
   F->ibm_has_particles = true;
   int nc = 0;
-  const int rc = couplb_ibm_substep(F->h, nl, at->x, at->v, F->mass_buf.data(), F->active_buf.data(),
-                                    at->f, refresh, &nc);
+  const int rc = lbm ? couplb_lbm_step_ibm(F->h, g_lb, nl, at->x, at->v, mass_buf, active_buf, at->f, &nc)
+                     : couplb_ibm_substep(F->h, nl, at->x, at->v, mass_buf, active_buf, at->f, refresh, &nc);
   if (rc) return F->engine_fail(rc);
   return COUPLB_OK;
 }
@@ -752,6 +763,21 @@ int couplb_fix_init(couplb_fix* F, const couplb_domain* dom) {
   if (!F->is3d) { F->nl[2] = 1; F->off[2] = 0; }
   if (F->nl[0] <= 0 || F->nl[1] <= 0 || (F->is3d && F->nl[2] <= 0))
     return F->fail(COUPLB_ERR_ARG, "fix couplb: local grid empty");
+  // One lattice per fix: the kernels wrap every non-wall face of the local
+  // grid onto itself (the self-exchange of a one-rank run), so a sub-box that
+  // is only part of the box would silently simulate a periodic slab of its
+  // own.  The reference splits the grid over ranks with ghost exchanges
+  // (fix_couplb.cpp:494-500, couplb_streaming.h:176-245); that is refused.
+  {
+    const int full[3] = {c.Nx, c.Ny, F->is3d ? c.Nz : 1};
+    for (int d = 0; d < (F->is3d ? 3 : 2); d++)
+      if (F->off[d] != 0 || F->nl[d] != full[d])
+        return F->fail(COUPLB_ERR_UNSUPPORTED,
+                       "fix couplb: the MD sub-box covers nodes %d..%d of %d along %c, but this build "
+                       "runs the whole lattice on one rank (sub-box must equal the box; no domain "
+                       "decomposition across ranks)",
+                       F->off[d], F->off[d] + F->nl[d] - 1, full[d], "xyz"[d]);
+  }
   if (F->h) { couplb_destroy(F->h); F->h = nullptr; }
   couplb_lattice_params lp;
   std::memset(&lp, 0, sizeof(lp));
@@ -893,11 +919,12 @@ int couplb_fix_post_force(couplb_fix* F, const couplb_atoms* at, long long ntime
   const couplb_fix_config& c = F->cfg;
   int rc;
   if (F->md_sub_count == 0) {
+    // do_lbm_step (with the gravity of update_gravity_variables), then the
+    // refresh sub-step, in one engine call
     const bool none = c.gstyle[0] == COUPLB_G_NONE && c.gstyle[1] == COUPLB_G_NONE &&
                       c.gstyle[2] == COUPLB_G_NONE;
-    if (none) {
-      rc = couplb_lbm_step(F->h, nullptr);
-    } else {
+    double gl[3] = {0.0, 0.0, 0.0};
+    if (!none) {
       double gv[3];
       for (int d = 0; d < 3; d++) {
         if (c.gstyle[d] == COUPLB_G_EQUAL) {
@@ -913,14 +940,15 @@ int couplb_fix_post_force(couplb_fix* F, const couplb_atoms* at, long long ntime
         }
       }
       const double ac = F->dt_LBM * F->dt_LBM / F->dx;
-      const double gl[3] = {gv[0] * ac, gv[1] * ac, gv[2] * ac};
-      rc = couplb_lbm_step(F->h, gl);
+      for (int d = 0; d < 3; d++) gl[d] = gv[d] * ac;
     }
-    if (rc) return F->engine_fail(rc);
+    rc = ibm_sub_coupling(F, at, true, none ? nullptr : gl);
+    if (rc) return rc;
     F->lbm_step_count++;
+  } else {
+    rc = ibm_sub_coupling(F, at);
+    if (rc) return rc;
   }
-  rc = ibm_sub_coupling(F, at);
-  if (rc) return rc;
   F->md_sub_count = (F->md_sub_count + 1) % c.md_per_lb;
   return COUPLB_OK;
 }

@@ -95,6 +95,7 @@ struct IbmArgs {
   // forcing methods beyond the single pass (null / unused otherwise)
   double* corr;                           // n*3: correction beyond the penalty pass
   const MlpPacked* mlp;                   // learned correction network
+  int fill_miss;                          // a marker whose record misses computes and stores it
 };
 
 // Add a spread force to one node of the interleaved force field: one vector
@@ -210,14 +211,15 @@ __device__ __forceinline__ LaneNodes<R> lane_nodes(const Geom& g, double lx, dou
 
 // Velocity of interior node (i,j,k) = n of the post-stream state, with the
 // arithmetic of k_macro (compute_macroscopic(false), couplb_lattice.h:155-202).
-template <class L, class S>
+// CG: the populations were written earlier in the same launch (read at L2).
+template <class L, class S, bool CG = false>
 __device__ __forceinline__ void compute_velocity(const IbmArgs<S>& a, int i, int j, int k, size_t n,
                                                  typename S::A& v0, typename S::A& v1,
                                                  typename S::A& v2, typename S::A& vr) {
   using C = typename S::C;
   C f[L::Q];
-  if (a.pull) load_node<L, S, size_t, true>(a.g, a.fin, a.rho_field, i, j, k, n, f);
-  else load_node<L, S, size_t, false>(a.g, a.fin, a.rho_field, i, j, k, n, f);
+  if (a.pull) load_node<L, S, size_t, true, CG>(a.g, a.fin, a.rho_field, i, j, k, n, f);
+  else load_node<L, S, size_t, false, CG>(a.g, a.fin, a.rho_field, i, j, k, n, f);
   C r, jx, jy, jz;
   moments<L, C>(f, r, jx, jy, jz);
   C rho = S::kShift ? C(a.g.rho0) + r : r;
@@ -245,13 +247,10 @@ __device__ __forceinline__ typename S::A* stencil_record(const IbmArgs<S>& a, in
   return a.sbuf + (size_t)mk * kRecStride;
 }
 
-// Refresh prefetch: one warp per active marker fills its slot's record.
-template <class L, class S>
-__global__ void __launch_bounds__(256) k_ibm_prefetch(const IbmArgs<S> a) {
-  const int mk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (mk >= a.n) return;
-  if (a.active && !a.active[mk]) return;
+// Refresh prefetch of marker mk by one warp: fills its slot's record and key
+// (epoch `epoch`).  CG: populations written earlier in the same launch.
+template <class L, class S, bool CG>
+__device__ __forceinline__ void prefetch_marker(const IbmArgs<S>& a, int mk, int lane, unsigned epoch) {
   const Geom& g = a.g;
   const double lx = (a.x[3 * mk] - a.lo[0]) * a.inv_dx - a.off[0] + 1.0;
   const double ly = (a.x[3 * mk + 1] - a.lo[1]) * a.inv_dx - a.off[1] + 1.0;
@@ -275,7 +274,7 @@ __global__ void __launch_bounds__(256) k_ibm_prefetch(const IbmArgs<S> a) {
     if (ig >= 0 && ig < gx && jg >= 0 && jg < gy && kg >= 0 && kg < gz &&
         classify_node(g, L::D, ig, jg, kg, ii, jj, kk) < 0) {
       const size_t n = (size_t)ii + (size_t)g.nx * ((size_t)jj + (size_t)g.ny * kk);
-      compute_velocity<L, S>(a, ii, jj, kk, n, v[rep][0], v[rep][1], v[rep][2], v[rep][3]);
+      compute_velocity<L, S, CG>(a, ii, jj, kk, n, v[rep][0], v[rep][1], v[rep][2], v[rep][3]);
     }
   }
 #pragma unroll
@@ -284,7 +283,126 @@ __global__ void __launch_bounds__(256) k_ibm_prefetch(const IbmArgs<S> a) {
     if (s >= NS) break;
     rec[s] = v[rep][0]; rec[64 + s] = v[rep][1]; rec[128 + s] = v[rep][2]; rec[192 + s] = v[rep][3];
   }
-  if (lane == 0) a.skey[mk] = StencilKey{i0, j0, k0, a.cur_epoch};
+  if (lane == 0) a.skey[mk] = StencilKey{i0, j0, k0, epoch};
+}
+
+// Refresh prefetch: one warp per active marker fills its slot's record.
+template <class L, class S>
+__global__ void __launch_bounds__(256) k_ibm_prefetch(const IbmArgs<S> a) {
+  const int mk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (mk >= a.n) return;
+  if (a.active && !a.active[mk]) return;
+  prefetch_marker<L, S, false>(a, mk, lane, a.cur_epoch);
+}
+
+// Interior z planes whose populations the refresh of a marker with base cell
+// k0 reads (with repeats, at most 12): the stencil planes kg = k0-1 .. k0+2 of
+// the ghost-inclusive box, a periodic ghost plane as its interior image, and
+// for each the planes its pull reads (kk-1, kk, kk+1, wrapped across a
+// periodic z face; a wall face is read at the node itself).  A superset of
+// what compute_velocity reads: x / y walls only remove nodes.
+template <class L>
+__device__ __forceinline__ int refresh_planes(const Geom& g, int k0, int (&pl)[12]) {
+  if (L::D != 3) {
+    pl[0] = 0;
+    return 1;
+  }
+  const int gz = g.nz + 2;
+  int np = 0;
+#pragma unroll
+  for (int o = 0; o < 4; o++) {
+    const int kg = k0 - 1 + o;
+    if (kg < 0 || kg >= gz) continue;
+    int kk;
+    if (kg == 0) {
+      if (g.face[4]) continue;
+      kk = g.nz - 1;
+    } else if (kg == gz - 1) {
+      if (g.face[5]) continue;
+      kk = 0;
+    } else {
+      kk = kg - 1;
+    }
+    pl[np++] = kk;
+    if (kk > 0) pl[np++] = kk - 1;
+    else if (!g.face[4]) pl[np++] = g.nz - 1;
+    if (kk < g.nz - 1) pl[np++] = kk + 1;
+    else if (!g.face[5]) pl[np++] = 0;
+  }
+  return np;
+}
+
+// Refresh bucketing ahead of a fused LB launch (k_stream_collide_x2 with
+// refresh): the markers whose refresh reads plane b last (b = the largest
+// plane of refresh_planes) are listed in bucket b, at most bcap of them; a
+// marker beyond the capacity, or reading no plane, is not listed (its first
+// sub-step computes its record).  bcount starts at zero.
+template <class L, class S>
+__global__ void __launch_bounds__(256) k_ibm_bucket(const IbmArgs<S> a, int* __restrict__ bcount,
+                                                   int* __restrict__ bidx, int bcap) {
+  const int mk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (mk >= a.n) return;
+  if (a.active && !a.active[mk]) return;
+  const double lz = (a.x[3 * mk + 2] - a.lo[2]) * a.inv_dx - a.off[2] + 1.0;
+  int pl[12];
+  const int np = refresh_planes<L>(a.g, (int)floor(lz), pl);
+  if (np == 0) return;
+  int key = pl[0];
+  for (int t = 1; t < np; t++) key = pl[t] > key ? pl[t] : key;
+  const int pos = atomicAdd(bcount + key, 1);
+  if (pos < bcap) bidx[(size_t)key * bcap + pos] = mk;
+}
+
+// Refresh work inside a fused LB launch: after its block has stored its
+// nodes, warp `warp` of the block takes slot (block of the plane) * 4 + warp
+// of bucket k - lag, where k is the block's z plane, and fills that marker's
+// record when every plane its refresh reads is complete (all blocks of the
+// plane counted in plane_done).  The populations are read at L2 (written in
+// this launch); a marker left out is filled by its first sub-step.
+template <class S>
+struct LBRefresh {
+  IbmArgs<S> ia;            // fin / rho_field = the launch's outputs, pull = 1
+  int* plane_done;          // per z plane: blocks that stored their nodes
+  const int* bcount;        // per bucket: markers listed
+  const int* bidx;          // bucket lists, bcap entries each
+  int bcap;
+  int lag;                  // planes between a block's plane and the bucket it serves
+  int blocks_per_plane;
+  unsigned epoch;           // population epoch after the launch
+  int* filled;              // records filled in the launch
+};
+
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+template <class L, class S>
+__device__ __forceinline__ void lb_refresh_tail(const LBRefresh<S>& r, int block_in_plane, int k) {
+  __syncthreads();   // every thread of the block has issued its stores
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(r.plane_done + k, 1);
+  }
+  const int b = k - r.lag;
+  if (b < 0) return;
+  const int cnt = min(r.bcount[b], r.bcap);
+  const int slot = block_in_plane * (int)(blockDim.x >> 5) + (int)(threadIdx.x >> 5);
+  if (slot >= cnt) return;
+  const int mk = r.bidx[(size_t)b * r.bcap + slot];
+  const IbmArgs<S>& a = r.ia;
+  const double lz = (a.x[3 * mk + 2] - a.lo[2]) * a.inv_dx - a.off[2] + 1.0;
+  int pl[12];
+  const int np = refresh_planes<L>(a.g, (int)floor(lz), pl);
+  bool ready = true;
+  for (int t = 0; t < np; t++) ready = ready && (ld_acquire_gpu(r.plane_done + pl[t]) == r.blocks_per_plane);
+  // the counters are read by every lane; a lane that saw a plane incomplete
+  // vetoes the warp (the counters only grow, so lanes may disagree)
+  if (!__all_sync(0xffffffffu, ready)) return;
+  prefetch_marker<L, S, true>(a, mk, threadIdx.x & 31, r.epoch);
+  if ((threadIdx.x & 31) == 0) atomicAdd(r.filled, 1);
 }
 
 // Velocity of stencil slot s of marker mk (node (i,j,k) = n).
@@ -380,6 +498,9 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
   const double mass = a.m[mk];
   const double vmk0 = a.v[3 * mk], vmk1 = a.v[3 * mk + 1], vmk2 = a.v[3 * mk + 2];
   const bool hit = key.epoch == a.cur_epoch && key.i0 == i0 && key.j0 == j0 && key.k0 == k0;
+  // a miss of the first sub-step after an LB step whose launch filled the
+  // records computes and stores its record (warp-uniform: one key per warp)
+  fill = fill || (a.fill_miss && !hit && !a.all_valid);
   const LaneNodes<R> ln = lane_nodes<L, DELTA, R>(g, lx, ly, lz, i0, j0, k0, lane);
   bool wall_seen = false;   // a wall node adds to ws but not to wss
 #pragma unroll

@@ -27,7 +27,10 @@ namespace couplb {
 constexpr int kSlipSlots = 32;
 // status words (cumulative until reset): slip checks made, fallbacks taken
 enum : int { kStSlipChecks = 4, kStFallbacks = 5 };
-constexpr long long kBarrierSpin = 1LL << 21;   // x ~100 ns sleeps
+// default poll limit of a grid barrier (each failed poll sleeps ~100 ns);
+// the handle option "barrier_spin" replaces it (tests drive a barrier to its
+// limit with 0)
+constexpr long long kBarrierSpin = 1LL << 21;
 
 // State of one launch of k_ibm_method.  Two alternate: each launch zeroes the
 // other one for the next launch.
@@ -56,11 +59,16 @@ struct PassArgs {
   double slip_tol;      // MD velocity units
   double g_lb[3];       // body force of the LB steps, lattice units
   float* rows;          // n x kMlpRow training rows, or null
+  long long spin;       // grid-barrier poll limit
 };
 
 // Grid-wide barrier of a cooperative launch.  Returns false (and counts a
-// timeout) if the other blocks did not arrive within the spin limit.
-__device__ __forceinline__ bool grid_barrier(PassState* ps, int* status) {
+// timeout) if the other blocks did not arrive within `spin` failed polls; the
+// caller then returns, so every block ends after at most one wait per
+// remaining barrier.  The arrival counter of a launch that gave up is left
+// behind in its PassState, which the next launch does not use (it zeroes it
+// for the launch after).
+__device__ __forceinline__ bool grid_barrier(PassState* ps, int* status, long long spin) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -75,7 +83,7 @@ __device__ __forceinline__ bool grid_barrier(PassState* ps, int* status) {
     } else {
       long long it = 0;
       while (*gen == g0) {
-        if (++it > kBarrierSpin) {
+        if (++it > spin) {
           good = 0;
           if (status) atomicAdd(status + kStTimeout, 1);
           break;
@@ -387,12 +395,12 @@ __global__ void __launch_bounds__(256) k_ibm_method(const PassArgs<S> P) {
     ft[0] += t3[0]; ft[1] += t3[1]; ft[2] += t3[2];
   }
   block_add_ftot(a.ftot, ft);
-  if (!grid_barrier(P.ps, P.status)) return;
+  if (!grid_barrier(P.ps, P.status, P.spin)) return;
   if (P.check_first) {
     for (int mk = gw; mk < a.n; mk += nw)
       if (!a.active || a.active[mk]) measure_marker<L, S, DELTA>(P, mk, lane, 0, &acc);
     block_add_slip(P.ps, 0, acc);
-    if (!grid_barrier(P.ps, P.status)) return;
+    if (!grid_barrier(P.ps, P.status, P.spin)) return;
     const bool fall = slip_rms(P.ps, 0) > P.slip_tol;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       P.ps->checked = 1;
@@ -423,7 +431,7 @@ __global__ void __launch_bounds__(256) k_ibm_method(const PassArgs<S> P) {
         }
       }
     }
-    if (!grid_barrier(P.ps, P.status)) return;
+    if (!grid_barrier(P.ps, P.status, P.spin)) return;
     for (int mk = gw; mk < a.n; mk += nw) {
       if (a.active && !a.active[mk]) continue;
       const double dF[3] = {__ldcg(P.dF + 3 * mk), __ldcg(P.dF + 3 * mk + 1),
@@ -431,7 +439,7 @@ __global__ void __launch_bounds__(256) k_ibm_method(const PassArgs<S> P) {
       spread_marker<L, S, DELTA>(a, mk, lane, dF, ft);
     }
     block_add_ftot(a.ftot, ft);
-    if (!grid_barrier(P.ps, P.status)) return;
+    if (!grid_barrier(P.ps, P.status, P.spin)) return;
   }
   for (int mk = gw; mk < a.n; mk += nw) {
     if (a.active && !a.active[mk]) continue;
@@ -479,8 +487,9 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
   if (have) {
     const MarkerWindow w = marker_window<L, S>(a, mk);
     const StencilKey key = a.skey[mk];
-    const bool fill = P.fill != 0;
     const bool hit = key.epoch == a.cur_epoch && key.i0 == w.i0 && key.j0 == w.j0 && key.k0 == w.k0;
+    // a refresh whose records the LB launch filled: only misses fill
+    const bool fill = P.fill != 0 || (a.fill_miss && !hit && !a.all_valid);
     A* rec = stencil_record(a, mk);
     int ox = 0, oy = 0, oz = 0;
     if (LEARNED) {
@@ -665,10 +674,10 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
     __syncthreads();
   };
   spread(F0, F1, F2);
-  if (!grid_barrier(P.ps, P.status)) return;
+  if (!grid_barrier(P.ps, P.status, P.spin)) return;
   if (P.check_first) {
     measure(0);
-    if (!grid_barrier(P.ps, P.status)) return;
+    if (!grid_barrier(P.ps, P.status, P.spin)) return;
     const bool fall = slip_rms(P.ps, 0) > P.slip_tol;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       P.ps->checked = 1;
@@ -696,9 +705,9 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
         a.fout[3 * mk] += d0; a.fout[3 * mk + 1] += d1; a.fout[3 * mk + 2] += d2;
       }
     }
-    if (!grid_barrier(P.ps, P.status)) return;
+    if (!grid_barrier(P.ps, P.status, P.spin)) return;
     spread(d0, d1, d2);
-    if (!grid_barrier(P.ps, P.status)) return;
+    if (!grid_barrier(P.ps, P.status, P.spin)) return;
   }
   if (have && lane == 0) { a.corr[3 * mk] = c0; a.corr[3 * mk + 1] = c1; a.corr[3 * mk + 2] = c2; }
   measure(1);

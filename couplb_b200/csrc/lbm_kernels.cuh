@@ -28,7 +28,8 @@ namespace couplb {
 enum RhoMode : int { kRhoNone = 0, kRhoField = 1, kRhoCurrent = 2 };
 enum StatusSlot : int { kStClamps = 0, kStNonfinite = 1, kStMacroClamps = 2 };
 // variants of the fused LB kernel (the "kernel" option of a handle)
-enum KernelKind : int { kKernelAuto = -1, kKernelPlain = 0, kKernelStaged = 1, kKernelPacked = 2 };
+// (value 1 was a shared-memory staged variant, since removed)
+enum KernelKind : int { kKernelAuto = -1, kKernelPlain = 0, kKernelPacked = 2 };
 
 // Geometry + boundary description shared by all lattice kernels.
 struct Geom {
@@ -88,11 +89,12 @@ __device__ __forceinline__ Cf clamp_rho(Cf r, int* status, int slot) {
 // (couplb_streaming.h:86,112-118): rho[n] of the last compute_macroscopic(true),
 // i.e. the clamped density the previous fused launch computed at n, which it
 // stored in the density field; floored at RHO_CLAMP_FRAC * rho0.
-template <class S>
+template <class S, bool CG = false>
 __device__ __forceinline__ typename S::C moving_wall_rho(const typename S::A* rho_field, size_t n,
                                                          double rho0) {
   using C = typename S::C;
-  const C r = S::kShift ? C(rho0) + C(rho_field[n]) : C(rho_field[n]);
+  const C rf = CG ? C(__ldcg(rho_field + n)) : C(rho_field[n]);
+  const C r = S::kShift ? C(rho0) + rf : rf;
   const C fl = C(RHO_CLAMP_FRAC * rho0 < RHO_MIN ? RHO_MIN : RHO_CLAMP_FRAC * rho0);
   return (r < fl) ? fl : r;
 }
@@ -105,12 +107,20 @@ __device__ __forceinline__ bool near_moving_wall(const Geom& g, int i, int j, in
   return m;
 }
 
+// Population load: read-only path, or at L2 (CG) for populations written
+// earlier in the same launch (storage.cuh).
+template <class S, bool CG>
+__device__ __forceinline__ typename S::C ld_pop(const typename S::T* p) {
+  if constexpr (CG) return S::ld_cg(p);
+  else return S::ld(p);
+}
+
 // Pull of all Q populations of node (i,j,k) with the reference's boundary
 // rules (couplb_streaming.h:99-129).  The source x - e_q of an interior node
 // is either interior, or on one or more ghost planes; on a ghost node the wall
 // set last (x, then y, then z: couplb_boundary.h, fix_couplb.cpp:529-531)
 // decides the rule, and a ghost node without wall is a periodic image.
-template <class L, class S, class I>
+template <class L, class S, class I, bool CG = false>
 __device__ __forceinline__ void pull_general(const Geom& g, const typename S::T* __restrict__ fin,
                                              const typename S::A* __restrict__ rho_field, int i,
                                              int j, int k, I n, typename S::C (&f)[L::Q]) {
@@ -118,7 +128,7 @@ __device__ __forceinline__ void pull_general(const Geom& g, const typename S::T*
   const I qs = (I)g.qs;
   const I sx = (I)g.nx, sxy = (I)g.nx * (I)g.ny;
   C rw = C(0);
-  if (near_moving_wall<L>(g, i, j, k)) rw = moving_wall_rho<S>(rho_field, n, g.rho0);
+  if (near_moving_wall<L>(g, i, j, k)) rw = moving_wall_rho<S, CG>(rho_field, n, g.rho0);
 #pragma unroll
   for (int q = 0; q < L::Q; q++) {
     const int ex = L::ex(q), ey = L::ey(q), ez = L::ez(q);
@@ -127,7 +137,7 @@ __device__ __forceinline__ void pull_general(const Geom& g, const typename S::T*
     const bool oy = sj < 0 || sj >= g.ny;
     const bool oz = (L::D == 3) && (sk < 0 || sk >= g.nz);
     if (!(ox || oy || oz)) {
-      f[q] = S::ld(fin + pidx<L, S, I>(q, (I)(si + (I)sj * sx + (I)sk * sxy), qs));
+      f[q] = ld_pop<S, CG>(fin + pidx<L, S, I>(q, (I)(si + (I)sj * sx + (I)sk * sxy), qs));
       continue;
     }
     int t = 0, wd = 0;
@@ -138,24 +148,24 @@ __device__ __forceinline__ void pull_general(const Geom& g, const typename S::T*
       si = si < 0 ? si + g.nx : (si >= g.nx ? si - g.nx : si);
       sj = sj < 0 ? sj + g.ny : (sj >= g.ny ? sj - g.ny : sj);
       if (L::D == 3) sk = sk < 0 ? sk + g.nz : (sk >= g.nz ? sk - g.nz : sk);
-      f[q] = S::ld(fin + pidx<L, S, I>(q, (I)si + (I)sj * sx + (I)sk * sxy, qs));
+      f[q] = ld_pop<S, CG>(fin + pidx<L, S, I>(q, (I)si + (I)sj * sx + (I)sk * sxy, qs));
     } else if (t == 1) {
-      f[q] = S::ld(fin + pidx<L, S, I>(L::opp(q), n, qs));
+      f[q] = ld_pop<S, CG>(fin + pidx<L, S, I>(L::opp(q), n, qs));
     } else if (t == 2) {
       const C eu = C(ex * g.uw[0] + ey * g.uw[1] + ez * g.uw[2]);
-      f[q] = S::ld(fin + pidx<L, S, I>(L::opp(q), n, qs)) + C(2.0 * L::w(L::opp(q)) * 3.0) * rw * eu;
+      f[q] = ld_pop<S, CG>(fin + pidx<L, S, I>(L::opp(q), n, qs)) + C(2.0 * L::w(L::opp(q)) * 3.0) * rw * eu;
     } else if (t == 3) {
       const int qr = wd == 0 ? L::refl(0, q) : (wd == 1 ? L::refl(1, q) : L::refl(2, q));
-      f[q] = S::ld(fin + pidx<L, S, I>(qr, n, qs));
+      f[q] = ld_pop<S, CG>(fin + pidx<L, S, I>(qr, n, qs));
     } else {
-      f[q] = S::ld(fin + pidx<L, S, I>(q, n, qs));
+      f[q] = ld_pop<S, CG>(fin + pidx<L, S, I>(q, n, qs));
     }
   }
 }
 
 // Pull for rows that touch no wall: only x can wrap, handled by selecting the
 // wrapped column; y/z offsets are constants of q.
-template <class L, class S, class I>
+template <class L, class S, class I, bool CG = false>
 __device__ __forceinline__ void pull_interior(const Geom& g, const typename S::T* __restrict__ fin,
                                               int i, int j, int k, typename S::C (&f)[L::Q]) {
   const I qs = (I)g.qs;
@@ -168,7 +178,7 @@ __device__ __forceinline__ void pull_interior(const Geom& g, const typename S::T
     const int ex = L::ex(q), ey = L::ey(q), ez = L::ez(q);
     const I xs = ex == 1 ? im : (ex == -1 ? ip : (I)i);
     const I ro = row - (I)(ey * g.nx) - (I)ez * sxy;   // unsigned wrap-around is exact
-    f[q] = S::ld(fin + pidx<L, S, I>(q, ro + xs, qs));
+    f[q] = ld_pop<S, CG>(fin + pidx<L, S, I>(q, ro + xs, qs));
   }
 }
 
@@ -181,18 +191,18 @@ __device__ __forceinline__ bool row_is_interior(const Geom& g, int j, int k) {
   return yin && zin && g.face[0] == 0 && g.face[1] == 0;
 }
 
-template <class L, class S, class I, bool kPull>
+template <class L, class S, class I, bool kPull, bool CG = false>
 __device__ __forceinline__ void load_node(const Geom& g, const typename S::T* __restrict__ fin,
                                           const typename S::A* __restrict__ rho_field, int i,
                                           int j, int k, I n, typename S::C (&f)[L::Q]) {
   if (!kPull) {
     const I qs = (I)g.qs;
 #pragma unroll
-    for (int q = 0; q < L::Q; q++) f[q] = S::ld(fin + pidx<L, S, I>(q, n, qs));
+    for (int q = 0; q < L::Q; q++) f[q] = ld_pop<S, CG>(fin + pidx<L, S, I>(q, n, qs));
   } else if (row_is_interior<L>(g, j, k)) {
-    pull_interior<L, S, I>(g, fin, i, j, k, f);
+    pull_interior<L, S, I, CG>(g, fin, i, j, k, f);
   } else {
-    pull_general<L, S, I>(g, fin, rho_field, i, j, k, n, f);
+    pull_general<L, S, I, CG>(g, fin, rho_field, i, j, k, n, f);
   }
 }
 
@@ -389,168 +399,9 @@ __global__ void __launch_bounds__(256) k_stream_collide(const LBArgs<S> a) {
   node_update<L, S, I>(a, f, i, j, k, n, hf);
 }
 
-// ---------------------------------------------------------------------------
-// K1 with bulk-copy staging (the pull form for rows that touch no wall).
-//
-// A persistent CTA walks x-rows r = blockIdx.x + t * gridDim.x.  For an
-// interior row (j, k) the Q source rows (j - ey_q, k - ez_q) of the pull are
-// whole, contiguous rows of the q planes; one thread copies them into a
-// shared-memory stage with cp.async.bulk, completing on an mbarrier, STAGES
-// rows ahead of the row being computed.  Threads then read f_q(i - ex_q) from
-// shared memory, which also makes the periodic x wrap an index wrap.  Rows next
-// to a wall take the general pull from global memory.  The copies keep
-// Q * nx * sizeof(T) * STAGES bytes per CTA in flight without registers.
-//
-// Every wait on an mbarrier is bounded: after kMaxSpin failed polls the CTA
-// counts a timeout in status[kStTimeout], waits (bounded again) for its own
-// copies still in flight and returns.
+// Status word slot of the bounded device waits (grid barriers of the
+// cooperative IBM kernels) that gave up.
 enum : int { kStTimeout = 3 };
-constexpr unsigned kMaxSpin = 1u << 22;
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_addr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-  for (unsigned it = 0; it < kMaxSpin; ++it)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
-}
-// 1D bulk copy global -> shared; both addresses 16-byte aligned, bytes % 16 == 0.
-__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes,
-                                              uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(bar))
-      : "memory");
-}
-
-template <class L>
-struct TmaRow {
-  // rows are numbered r = j + ny * k
-  __device__ __forceinline__ static void jk(const Geom& g, long long r, int& j, int& k) {
-    j = (int)(r % g.ny);
-    k = (int)(r / g.ny);
-  }
-};
-
-// Issue the Q row copies of row r into stage buffer `buf` (thread 0 only).
-template <class L, class S>
-__device__ __forceinline__ void stage_row(const LBArgs<S>& a, long long r, typename S::T* buf,
-                                          uint64_t* bar) {
-  using T = typename S::T;
-  const Geom& g = a.g;
-  int j, k;
-  TmaRow<L>::jk(g, r, j, k);
-  if (!row_is_interior<L>(g, j, k)) {
-    mbar_arrive(bar);   // nothing to copy: complete the phase
-    return;
-  }
-  static_assert(S::kTile == 0, "the staged kernel copies plane-major rows");
-  const uint32_t rb = (uint32_t)(g.nx * sizeof(T));
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  mbar_arrive_expect_tx(bar, rb * L::Q);
-  const size_t sxy = (size_t)g.nx * g.ny;
-#pragma unroll
-  for (int q = 0; q < L::Q; q++) {
-    const size_t src = (size_t)q * g.qs + (size_t)g.nx * (j - L::ey(q)) + sxy * (k - L::ez(q));
-    bulk_copy_g2s(buf + (size_t)q * g.nx, a.fin + src, rb, bar);
-  }
-}
-
-template <class L, class S, int STAGES>
-__global__ void __launch_bounds__(256, sizeof(typename S::T) == 8 ? 2 : 3)
-    k_stream_collide_tma(const LBArgs<S> a) {
-  using C = typename S::C;
-  using T = typename S::T;
-  using I = size_t;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t bars[STAGES];
-  const Geom& g = a.g;
-  const long long nrows = (long long)g.ny * g.nz;
-  T* stage0 = reinterpret_cast<T*>(smem_raw);
-  const size_t stage_elems = (size_t)L::Q * g.nx;
-
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; s++) mbar_init(&bars[s], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; s++) {
-      const long long r = blockIdx.x + (long long)s * gridDim.x;
-      if (r < nrows) stage_row<L, S>(a, r, stage0 + s * stage_elems, &bars[s]);
-    }
-  }
-  long long t_fail = -1;
-  for (long long t = 0;; ++t) {
-    const long long r = blockIdx.x + t * gridDim.x;
-    if (r >= nrows) break;
-    const int s = (int)(t % STAGES);
-    const uint32_t parity = (uint32_t)((t / STAGES) & 1);
-    const bool ok = mbar_wait_bounded(&bars[s], parity);
-    if (__syncthreads_or(!ok)) {   // CTA-uniform decision
-      t_fail = t;
-      break;
-    }
-    int j, k;
-    TmaRow<L>::jk(g, r, j, k);
-    const bool interior = row_is_interior<L>(g, j, k);
-    const T* buf = stage0 + s * stage_elems;
-    for (int i = threadIdx.x; i < g.nx; i += blockDim.x) {
-      const I n = (I)i + (I)g.nx * ((I)j + (I)g.ny * (I)k);
-      const bool hf = a.F && (!a.seg_force || a.seg_force[n >> 3]);
-      C f[L::Q];
-      if (interior) {
-        const int im = (i == 0) ? g.nx - 1 : i - 1;
-        const int ip = (i == g.nx - 1) ? 0 : i + 1;
-#pragma unroll
-        for (int q = 0; q < L::Q; q++) {
-          const int xs = L::ex(q) == 1 ? im : (L::ex(q) == -1 ? ip : i);
-          f[q] = S::ld_shared(buf + q * g.nx + xs);
-        }
-      } else {
-        pull_general<L, S, I>(g, a.fin, a.rho_field, i, j, k, n, f);
-      }
-      node_update<L, S, I>(a, f, i, j, k, n, hf);
-    }
-    __syncthreads();   // stage s fully consumed
-    if (threadIdx.x == 0) {
-      const long long rn = r + (long long)STAGES * gridDim.x;
-      if (rn < nrows) stage_row<L, S>(a, rn, stage0 + s * stage_elems, &bars[s]);
-    }
-  }
-  if (t_fail >= 0 && threadIdx.x == 0) {
-    atomicAdd(a.status + kStTimeout, 1);
-    // Rows t_fail .. t_fail + STAGES - 1 were issued and not consumed: let
-    // their copies land (bounded) before the CTA's shared memory is released.
-    for (long long t = t_fail; t < t_fail + STAGES; ++t) {
-      if (blockIdx.x + t * gridDim.x >= nrows) break;
-      (void)mbar_wait_bounded(&bars[t % STAGES], (uint32_t)((t / STAGES) & 1));
-    }
-  }
-}
 
 // ---------------------------------------------------------------------------
 // K2: moments of the post-stream state without the Guo term
@@ -804,7 +655,7 @@ __global__ void __launch_bounds__(256) k_diag_partial(long long N, double rho0,
   }
 }
 
-__global__ void k_reduce_final(int nblocks, const double* __restrict__ part,
+static __global__ void k_reduce_final(int nblocks, const double* __restrict__ part,
                                double* __restrict__ out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double o[5] = {0, 0, 0, 0, 0};

@@ -12,7 +12,15 @@
 //
 // The arithmetic is that of k_stream_collide for the shifted formats (BGK +
 // Guo with the exact mass / momentum correction); nx must be even.
+//
+// REFRESH (D3Q19): the same launch also fills the IBM stencil records of the
+// refresh that follows the LB step (compute_macroscopic(false) at the stencil
+// nodes, fix_couplb.cpp:757-760): blocks are dispatched plane by plane in z,
+// and after storing its nodes a block fills the records of markers whose
+// planes were completed a few planes earlier, while those populations are
+// still in L2 (ibm_kernels.cuh, lb_refresh_tail).
 #pragma once
+#include "ibm_kernels.cuh"
 #include "lbm_kernels.cuh"
 
 namespace couplb {
@@ -50,14 +58,11 @@ struct Pair<StoreF16S> {
   }
 };
 
-template <class L, class S, int MINB = 5>
-__global__ void __launch_bounds__(128, MINB) k_stream_collide_x2(const LBArgs<S> a) {
+template <class L, class S>
+__device__ __forceinline__ void x2_node_pair(const LBArgs<S>& a, int i0, int j, int k) {
   using T = typename S::T;
   using I = unsigned;
   const Geom& g = a.g;
-  const int i0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
-  const int j = blockIdx.y, k = blockIdx.z;
-  if (i0 >= g.nx) return;
   const I qs = (I)g.qs;
   const I sx = (I)g.nx, sxy = (I)g.nx * (I)g.ny;
   const I n0 = (I)i0 + (I)j * sx + (I)k * sxy;
@@ -197,6 +202,14 @@ __global__ void __launch_bounds__(128, MINB) k_stream_collide_x2(const LBArgs<S>
     Pair<S>::st(a.fout + pidx<L, S, I>(2 * c + 1, n0, qs), add2(f[2 * c + 1], sub2(da[2 * c], pr[c])));
     Pair<S>::st(a.fout + pidx<L, S, I>(2 * c + 2, n0, qs), add2(f[2 * c + 2], add2(da[2 * c + 1], pr[c])));
   }
+}
+
+template <class L, class S, int MINB = 5, bool REFRESH = false>
+__global__ void __launch_bounds__(128, MINB) k_stream_collide_x2(const LBArgs<S> a, const LBRefresh<S> r) {
+  const int i0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = blockIdx.y, k = blockIdx.z;
+  if (i0 < a.g.nx) x2_node_pair<L, S>(a, i0, j, k);
+  if constexpr (REFRESH) lb_refresh_tail<L, S>(r, blockIdx.x + gridDim.x * j, k);
 }
 
 }  // namespace couplb

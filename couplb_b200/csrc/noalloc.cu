@@ -19,6 +19,12 @@
 // start at zero; but all calls share the one array, so calls whose kernels
 // overlap on the GPU (different streams, or different host threads) race on
 // it and must be serialised by the caller.
+//
+// Unlike couplb_diagnostics, which follows the reference's max_velocity
+// (std::max drops a NaN speed, and non-finite densities are counted in the
+// status word instead), the maximum here propagates NaN: this entry point
+// returns no non-finite count, so a caller watching max |u| for stability
+// sees NaN as soon as one node's velocity is NaN.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -29,6 +35,12 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kMaxDevices = 64;
+
+// max that keeps a NaN of either argument (fmax and a plain comparison drop it)
+__device__ __forceinline__ double max_keep_nan(double a, double b) {
+  if (a != a) return a;
+  return (b != b || b > a) ? b : a;
+}
 
 static __device__ __align__(256) double g_diag_scratch[COUPLB_NOALLOC_MAX_PARTIALS * 5];
 
@@ -66,7 +78,7 @@ __global__ void __launch_bounds__(kThreads) k_diag_chunks(long long n, double rh
     if (kShift) r += rho0;
     const double a = double(ux[i]), b = double(uy[i]), c = double(uz[i]);
     const double u2 = a * a + b * b + c * c;
-    m2 = u2 > m2 ? u2 : m2;
+    m2 = max_keep_nan(m2, u2);
     sm += r;
     px += r * a; py += r * b; pz += r * c;
   }
@@ -74,7 +86,7 @@ __global__ void __launch_bounds__(kThreads) k_diag_chunks(long long n, double rh
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
-    m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+    m2 = max_keep_nan(m2, __shfl_xor_sync(0xffffffffu, m2, o));
     sm += __shfl_xor_sync(0xffffffffu, sm, o);
     px += __shfl_xor_sync(0xffffffffu, px, o);
     py += __shfl_xor_sync(0xffffffffu, py, o);
@@ -85,23 +97,37 @@ __global__ void __launch_bounds__(kThreads) k_diag_chunks(long long n, double rh
   if (threadIdx.x == 0) {
     double o[5] = {0, 0, 0, 0, 0};
     for (int w = 0; w < kThreads / 32; w++) {
-      o[0] = fmax(o[0], sh[0][w]);
+      o[0] = max_keep_nan(o[0], sh[0][w]);
       for (int c = 1; c < 5; c++) o[c] += sh[c][w];
     }
     for (int c = 0; c < 5; c++) part[blockIdx.x * 5 + c] = o[c];
   }
 }
 
-// Slots summed in slot order (deterministic), result to the caller's output.
-__global__ void k_diag_finish(int nparts, const double* __restrict__ part, double* __restrict__ out) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// One block sums the slots: thread t takes slots t, t + 256, ... in slot
+// order, then a fixed-shape shared-memory tree combines the 256 partials, so
+// the result does not depend on scheduling.
+__global__ void __launch_bounds__(kThreads) k_diag_finish(int nparts, const double* __restrict__ part,
+                                                          double* __restrict__ out) {
   double o[5] = {0, 0, 0, 0, 0};
-  for (int b = 0; b < nparts; b++) {
-    o[0] = fmax(o[0], part[b * 5]);
+  for (int b = threadIdx.x; b < nparts; b += kThreads) {
+    o[0] = max_keep_nan(o[0], part[b * 5]);
     for (int c = 1; c < 5; c++) o[c] += part[b * 5 + c];
   }
-  out[0] = sqrt(o[0]);
-  for (int c = 1; c < 5; c++) out[c] = o[c];
+  __shared__ double sh[5][kThreads];
+  for (int c = 0; c < 5; c++) sh[c][threadIdx.x] = o[c];
+  __syncthreads();
+  for (int h = kThreads / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) {
+      sh[0][threadIdx.x] = max_keep_nan(sh[0][threadIdx.x], sh[0][threadIdx.x + h]);
+      for (int c = 1; c < 5; c++) sh[c][threadIdx.x] += sh[c][threadIdx.x + h];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[0] = sqrt(sh[0][0]);
+    for (int c = 1; c < 5; c++) out[c] = sh[c][0];
+  }
 }
 
 }  // namespace
@@ -127,7 +153,7 @@ extern "C" int couplb_diagnostics_noalloc(const void* d_rho, const void* d_ux, c
     k_diag_chunks<float, true><<<(unsigned)nparts, kThreads, 0, s>>>(
         n, rho0, (const float*)d_rho, (const float*)d_ux, (const float*)d_uy, (const float*)d_uz, part);
   if (cudaGetLastError() != cudaSuccess) return COUPLB_ERR_CUDA;
-  k_diag_finish<<<1, 32, 0, s>>>((int)nparts, part, d_out);
+  k_diag_finish<<<1, kThreads, 0, s>>>((int)nparts, part, d_out);
   if (cudaGetLastError() != cudaSuccess) return COUPLB_ERR_CUDA;
   return COUPLB_OK;
 }

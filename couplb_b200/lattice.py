@@ -164,6 +164,30 @@ class Lattice:
                                            C.byref(nc)))
         return nc.value
 
+    @staticmethod
+    def _gptr(g_lb):
+        if g_lb is None:
+            return C.POINTER(C.c_double)()
+        return C.cast((C.c_double * 3)(*g_lb), C.POINTER(C.c_double))
+
+    def lbm_step_ibm(self, x, v, mass, f_add, g_lb=None, active=None):
+        """LB step + the refresh IBM sub-step of its cycle (host arrays);
+        f_add (n,3) is incremented in place.  Same results as lbm_step then
+        ibm_substep(refresh=True)."""
+        n = int(x.shape[0])
+        nc = C.c_int(0)
+        g = self._gptr(g_lb)
+        self._ck(self.L.couplb_lbm_step_ibm(self.h, g, n, abi.dptr(x), abi.dptr(v), abi.dptr(mass),
+                                            abi.iptr(active), abi.dptr(f_add), C.byref(nc)))
+        return nc.value
+
+    def lbm_step_ibm_device(self, n, x_ptr, v_ptr, m_ptr, f_ptr, active_ptr=0, g_lb=None):
+        """LB step + the refresh IBM sub-step of its cycle (device pointers)."""
+        g = self._gptr(g_lb)
+        self._ck(self.L.couplb_lbm_step_ibm_device(self.h, g, n, C.c_void_p(x_ptr), C.c_void_p(v_ptr),
+                                                   C.c_void_p(m_ptr), C.c_void_p(active_ptr or None),
+                                                   C.c_void_p(f_ptr)))
+
     def ibm_substep_device(self, n, x_ptr, v_ptr, m_ptr, f_ptr, active_ptr=0, refresh=True):
         """Device-array IBM sub-step (raw device pointers, e.g. tensor.data_ptr())."""
         self._ck(self.L.couplb_ibm_substep_device(self.h, n, C.c_void_p(x_ptr), C.c_void_p(v_ptr),

@@ -45,6 +45,9 @@ SIGNATURES = {
     "couplb_ibm_substep_device": (C.c_int, [_H, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                             C.c_void_p, C.c_void_p, C.c_int]),
     "couplb_ibm_total_force": (C.c_int, [_H, _D, C.c_int]),
+    "couplb_lbm_step_ibm": (C.c_int, [_H, _D, C.c_int, _D, _D, _D, _I, _D, _I]),
+    "couplb_lbm_step_ibm_device": (C.c_int, [_H, _D, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.c_void_p]),
     "couplb_read_status": (C.c_int, [_H, _I, _I, C.c_int]),
     "couplb_status_post": (C.c_int, [_H]),
     "couplb_status_last": (C.c_int, [_H, _I, _I]),

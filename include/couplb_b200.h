@@ -187,7 +187,9 @@ int  couplb_diagnostics(couplb_handle* h, couplb_diag* out);
  * device current), so make that first call before any stream capture.  All
  * calls share the array and it keeps the last call's contents; nothing in it
  * needs to start at zero, but calls whose kernels overlap on the GPU race on
- * it and must be serialised by the caller. */
+ * it and must be serialised by the caller.  max |u| is NaN when any node's
+ * velocity is NaN (couplb_diagnostics follows the reference, whose maximum
+ * skips NaN, and reports non-finite densities in its own count). */
 #define COUPLB_NOALLOC_CHUNK        2048        /* nodes reduced per block      */
 #define COUPLB_NOALLOC_MAX_PARTIALS 32768       /* scratch slots                */
 #define COUPLB_NOALLOC_MAX_NODES    (COUPLB_NOALLOC_CHUNK * (long long)COUPLB_NOALLOC_MAX_PARTIALS)
@@ -221,6 +223,25 @@ int  couplb_ibm_substep_device(couplb_handle* h, int n, const double* d_x,
                                const double* d_v, const double* d_mass,
                                const int* d_active, double* d_f_add,
                                int refresh);
+
+/* One LB step and the first IBM sub-step of its cycle in one call: the
+ * sequence FixCoupLB::post_force runs on the first MD sub-step of an LB cycle
+ * (fix_couplb.cpp:640-651: do_lbm_step, :659-669, then do_ibm_sub_coupling
+ * with the refresh, :730-798), i.e. couplb_lbm_step(h, g_lb) followed by
+ * couplb_ibm_substep(h, n, ..., refresh = 1, ncoupled), with the same
+ * results.  The atom positions reach the device before the LB launch, so on a
+ * D3Q19 lattice in a shifted format the launch itself computes the fluid
+ * velocities of the refresh at the markers' stencil nodes while those
+ * populations are still in L2 (option "fused_refresh"). */
+int  couplb_lbm_step_ibm(couplb_handle* h, const double* g_lb, int n, const double* x,
+                         const double* v, const double* mass, const int* active,
+                         double* f_add, int* ncoupled);
+/* Same with device-resident atom arrays: couplb_lbm_step followed by
+ * couplb_ibm_substep_device(..., refresh = 1). */
+int  couplb_lbm_step_ibm_device(couplb_handle* h, const double* g_lb, int n,
+                                const double* d_x, const double* d_v,
+                                const double* d_mass, const int* d_active,
+                                double* d_f_add);
 
 /* FP64 sum over all spread markers of the force given to the grid (lattice
  * units), accumulated on the device since the last reset: the fluid side of the
@@ -322,15 +343,27 @@ int  couplb_status_last(couplb_handle* h, int* clamps, int* nonfinite);
 /* Runtime options of a handle (no counterpart in the reference):
  *   "kernel"      variant of the fused LB kernel: -1 auto (default: packed for
  *                 the shifted formats, plain for FP64), 0 plain (one node per
- *                 thread), 1 staged (interior rows copied to shared memory with
- *                 bulk copies; same arithmetic as plain), 2 packed (two nodes
- *                 per thread in paired FP32 arithmetic; shifted formats, even
- *                 nx).  A variant that does not apply falls back to plain.
+ *                 thread), 2 packed (two nodes per thread in paired FP32
+ *                 arithmetic; shifted formats, even nx).  A variant that does
+ *                 not apply falls back to plain.
  *   "last_kernel" read-only: the variant the last LB step ran.
  *   "ibm_resident" 1 (default): ITERATIVE / LEARNED sub-steps of a 3D lattice
  *                 whose markers each fit a warp of one cooperative launch keep
  *                 each marker's stencil in registers across passes; 0 always
  *                 uses the general form (same results).
+ *   "barrier_spin" poll limit of each grid-wide barrier of the ITERATIVE /
+ *                 LEARNED sub-step kernels (default 2^21 polls of ~100 ns).
+ *                 A block whose barrier runs out counts a timeout and returns;
+ *                 the sub-step's results are then invalid, the next launch
+ *                 starts clean.  0 gives up at the first failed poll (tests).
+ *   "fused_refresh" 1 (default): couplb_lbm_step_ibm* fill the IBM stencil
+ *                 records inside the LB launch where the lattice allows it; 0
+ *                 runs the separate refresh kernel (same results).
+ *   "refresh_lag" z planes between an LB block and the markers whose records
+ *                 it fills (default 8): a marker is filled once every plane
+ *                 its refresh reads is complete, else by its first sub-step.
+ *   "refresh_filled" read-only: records the last LB launch filled, -1 when it
+ *                 did not fill any (synchronises).
  *   "timeouts"    read-only: bounded device waits that gave up (synchronises). */
 int  couplb_set_option(couplb_handle* h, const char* name, long long value);
 int  couplb_get_option(couplb_handle* h, const char* name, long long* value);

@@ -97,12 +97,11 @@ def test_larger_grid_matches_oracle(cuda_lib):
 @pytest.mark.parametrize("prec", ["fp64", "fp32", "fp16"])
 @pytest.mark.parametrize("wall", [(0, 0, 1, 1, 1, 1), (0, 0, 2, 3, 4, 1), (0,) * 6, (1, 2, 0, 0, 3, 3)])
 def test_kernel_variants_agree(cuda_lib, prec, wall):
-    """The fused-kernel variants: staged (shared-memory bulk copies) does the
-    plain kernel's arithmetic bit for bit; packed (paired FP32) agrees within
-    FP32 rounding; every wall layout."""
+    """The fused-kernel variants: packed (paired FP32) agrees with plain
+    within FP32 rounding; every wall layout."""
     n = (64, 20, 12)
     res = {}
-    for kern in (0, 1, 2):
+    for kern in (0, 2):
         L = Lattice(3, *n, tau=0.7, wall=wall, wall_vel=(0.02, 0.01, 0), body_force=True, precision=prec)
         L.set_option("kernel", kern)
         L.set_populations(cases.initial_populations(3, n, 21))
@@ -111,11 +110,8 @@ def test_kernel_variants_agree(cuda_lib, prec, wall):
         res[kern] = (L.get_populations(), L.get_option("last_kernel"))
         assert L.get_option("timeouts") == 0
         L.close()
-    x_periodic = wall[0] == 0 and wall[1] == 0
     assert res[0][1] == 0
-    assert res[1][1] == (1 if x_periodic else 0)
     assert res[2][1] == (0 if prec == "fp64" else 2)
-    np.testing.assert_array_equal(res[1][0], res[0][0])
     tol = {"fp64": 0.0, "fp32": 1e-6, "fp16": 2e-3}[prec]
     assert np.abs(res[2][0] - res[0][0]).max() <= tol * np.abs(res[0][0]).max()
 

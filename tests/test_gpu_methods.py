@@ -93,6 +93,36 @@ def test_iterative_matches_oracle_fp64(cuda_lib, delta, passes, resident):
     L.close()
 
 
+@pytest.mark.parametrize("resident", [1, 0])
+def test_grid_barrier_timeout_returns_and_next_call_works(cuda_lib, resident):
+    """The grid barriers of the cooperative sub-step kernel are bounded
+    waits.  With a poll limit of 0 every block that is not the last to
+    arrive gives up at once: the launch must end, count its timeouts and
+    leave the handle usable.  With the default limit restored (and the state
+    reset) the next sub-steps match the oracle again and count no timeout."""
+    L, O, ip = make_pair("fp64", "peskin4")
+    L.set_option("ibm_resident", resident)
+    L.set_ibm_method("iterative", passes=3)
+    default = L.get_option("barrier_spin")
+    assert default > 0 and L.get_option("timeouts") == 0
+    x, v, m = markers()
+    assert x.shape[0] > 8            # more than one block of eight marker warps
+    L.set_option("barrier_spin", 0)
+    L.lbm_step(G_LB)
+    L.ibm_substep(x, v, m, np.zeros_like(x), refresh=True)
+    t = L.get_option("timeouts")
+    assert t > 0
+    # restore the state (the timed-out sub-step left partial spreads behind)
+    L.set_option("barrier_spin", default)
+    z = np.zeros(L.G)
+    L.set_force_field(z, z, z)
+    L.set_populations(cases.initial_populations(3, N, 11))
+    for fg, fo, sl, st in run_steps(L, O, ip, 1, 3, 2):
+        assert rel(fg, fo) <= 1e-10, rel(fg, fo)
+    assert L.get_option("timeouts") == t
+    L.close()
+
+
 def test_iterative_reduces_slip(cuda_lib):
     """Fixed sphere in a uniform stream: each correction pass lowers the slip."""
     x, _, _ = markers()

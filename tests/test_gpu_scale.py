@@ -1,0 +1,143 @@
+"""FP64 GPU path against the reference build at the benchmark sizes.
+
+The golden and oracle tests elsewhere run on grids of a few thousand nodes;
+these run the FP64 GPU lattice and the reference's own headers (the `ref`
+build of oracle/Makefile: couplb_{lattice,collision,streaming,boundary,ibm}.h
+compiled unmodified, driven by the harness that restates fix_couplb.cpp's
+sequencing) on the full workloads the benchmark times, for a few steps each:
+
+- the D3Q19 channel 256x128x128 (walls y and z, gx 1e-6, seeded noise), 10 LB
+  steps: populations and moments within 1e-12;
+- the D3Q19 periodic 256^3 box with 20000 Peskin4 markers, md_per_lb 4, two
+  LB cycles: per-atom forces within 1e-11, force field within 1e-12;
+- a 512x256x64 slice of the many-rod geometry (walls on y, 50 rods of 200
+  markers, Peskin4, md_per_lb 2), one LB cycle: same tolerances;
+- the D2Q9 Poiseuille channel of the reference quick start (8x32, walls y,
+  gx 5e-6) for all of its 50000 steps: fields within 1e-12 of the reference
+  build, and the profile within 1 % of the analytic parabola
+  (tests/poiseuille2d/validate.py:99,111).
+
+Relative errors are max |a - b| / max |b| per field (velocity components
+against the largest velocity component).  Markers move with prescribed
+velocities between sub-steps, the same on both sides.
+"""
+import numpy as np
+import pytest
+
+import cases
+from couplb_b200.lattice import Lattice
+from couplb_b200.markers import random_rods
+from oracle import bindings as B
+
+pytestmark = pytest.mark.gpu
+KIND = "ref" if B.available("ref") else "port"
+
+
+def rel(a, b, scale=None):
+    s = np.abs(b).max() if scale is None else scale
+    return float(np.abs(a - b).max() / max(s, 1e-300))
+
+
+def ibm_params(L, delta, md_per_lb):
+    return L.set_ibm_params(delta=delta, md_per_lb=md_per_lb, xi_ibm=1.0, dt_lbm=1.0, dx=1.0)
+
+
+def run_marker_cycles(n, tau, wall, u0, x0, v0, delta, md_per_lb, cycles):
+    """LB cycles (one LB step + md_per_lb sub-steps, refresh on the first) on
+    the GPU (FP64) and on the reference build from the same uniform flow.
+    Returns the per-sub-step atom forces and the force fields after the last
+    sub-step, for both."""
+    box = np.array(n, dtype=np.float64)
+    L = Lattice(3, *n, tau=tau, wall=wall, precision="fp64")
+    L.init_equilibrium(1.0, *u0)
+    ip = ibm_params(L, delta, md_per_lb)
+    O = B.OracleGrid(3, *n, tau, wall=wall, kind=KIND)
+    O.init_equilibrium(1.0, *u0)
+    dt = 1.0 / md_per_lb
+    x = x0.copy()
+    fg_all, fo_all = [], []
+    for c in range(cycles):
+        L.lbm_step()
+        O.lbm_step()
+        for s in range(md_per_lb):
+            x = np.ascontiguousarray(np.mod(x + dt * v0, box))
+            m = np.ones(x.shape[0])
+            fg = np.zeros_like(x)
+            L.ibm_substep(x, v0, m, fg, refresh=(s == 0))
+            fo = np.zeros_like(x)
+            O.ibm_substep(ip, x, v0, m, fo, refresh=(s == 0), fold=(s == md_per_lb - 1))
+            fg_all.append(fg)
+            fo_all.append(fo)
+    gf = [cases.interior(a, 3) for a in L.get_force_field()]
+    of = [cases.interior(a, 3) for a in O.get_force()]
+    L.close()
+    O.close()
+    return np.stack(fg_all), np.stack(fo_all), gf, of
+
+
+def test_channel_256x128x128_ten_steps_match_reference():
+    import bench
+    n = (256, 128, 128)
+    f0 = bench.initial_populations(*n)
+    g = (1e-6, 0.0, 0.0)
+    L = Lattice(3, *n, tau=bench.TAU, wall=bench.WALL, body_force=True, precision="fp64")
+    L.set_populations(f0)
+    O = B.OracleGrid(3, *n, bench.TAU, wall=bench.WALL, kind=KIND)
+    O.set_f(f0)
+    del f0
+    for _ in range(10):
+        L.lbm_step(g)
+        O.lbm_step(g)
+    L.macroscopic()
+    O.macroscopic(False)
+    gm = [cases.interior(a, 3) for a in L.get_macroscopic()]
+    om = [cases.interior(a, 3) for a in O.get_macro()]
+    us = max(np.abs(a).max() for a in om[1:])
+    errs = {"rho": rel(gm[0], om[0])}
+    for k, a, b in zip(("ux", "uy", "uz"), gm[1:], om[1:]):
+        errs[k] = rel(a, b, us)
+    del gm, om
+    errs["f"] = rel(cases.interior(L.get_populations(), 3), cases.interior(O.get_f(), 3))
+    L.close()
+    O.close()
+    assert max(errs.values()) <= 1e-12, errs
+
+
+def test_periodic_256cubed_20000_markers_two_cycles_match_reference():
+    n = (256, 256, 256)
+    rng = np.random.default_rng(3)
+    x0 = rng.uniform(0.0, 256.0, (20000, 3))
+    v0 = 0.01 * rng.standard_normal((20000, 3))
+    fg, fo, gf, of = run_marker_cycles(n, 0.8, (0,) * 6, (0.01, -0.004, 0.002), x0, v0, "peskin4", 4, 2)
+    assert rel(fg, fo) <= 1e-11, rel(fg, fo)
+    for c in range(3):
+        assert rel(gf[c], of[c]) <= 1e-12, (c, rel(gf[c], of[c]))
+
+
+def test_rod_slice_512x256x64_one_cycle_matches_reference():
+    n = (512, 256, 64)
+    x0 = random_rods(50, 200, n, 5, wall_margin=3.0)
+    rng = np.random.default_rng(6)
+    v0 = np.repeat(0.01 * rng.standard_normal((50, 3)), 200, axis=0)
+    fg, fo, gf, of = run_marker_cycles(n, 3 * 0.08 + 0.5, (0, 0, 1, 1, 0, 0), (0.01, 0.0, 0.003), x0, v0,
+                                       "peskin4", 2, 1)
+    assert rel(fg, fo) <= 1e-11, rel(fg, fo)
+    for c in range(3):
+        assert rel(gf[c], of[c]) <= 1e-12, (c, rel(gf[c], of[c]))
+
+
+def test_d2q9_poiseuille_50000_steps_matches_reference_and_analytic():
+    case = dict(cases.LB_CASES["d2q9_poiseuille"], steps=50000)
+    out = cases.run_lb_case_gpu(case, "fp64")
+    ref = cases.run_lb_case_oracle(case, KIND)
+    us = max(np.abs(ref[k]).max() for k in ("ux", "uy", "uz"))
+    errs = {k: rel(out[k], ref[k], us if k in ("ux", "uy", "uz") else None) for k in ref}
+    assert max(errs.values()) <= 1e-12, errs
+    # analytic profile u(y) = g/(2 nu) (y + 1/2)(H - 1/2 - y) for bounce-back
+    # walls half a node outside the first and last rows (validate.py:99)
+    nu = (case["tau"] - 0.5) / 3.0
+    H = case["n"][1]
+    y = np.arange(H)
+    ua = case["gravity"][0] / (2 * nu) * (y + 0.5) * (H - 0.5 - y)
+    prof = out["ux"][0].mean(axis=1)
+    assert np.abs(prof - ua).max() <= 0.01 * ua.max()

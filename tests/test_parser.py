@@ -107,3 +107,23 @@ def test_vtk_solid_attribute_names(cuda_lib):
     with pytest.raises(CoupLBError) as e:
         P("f all couplb 8 8 8 0.1 1.0 vtk_solid " + " ".join(["x"] * 40))
     assert "too many attributes" in e.value.msg
+
+
+@pytest.mark.parametrize("axis,dim", [(0, 3), (1, 3), (2, 3), (0, 2)])
+def test_init_refuses_a_sub_box_smaller_than_the_box(cuda_lib, axis, dim):
+    """Under a domain decomposition each rank's sub-box is part of the box
+    (fix_couplb.cpp:494-500).  One lattice per fix cannot exchange ghost
+    layers with other ranks, so init refuses such a sub-box instead of
+    simulating a periodic slab; no device work happens before the check."""
+    import ctypes as C
+    from couplb_b200.fix import FixCoupLB
+    nz = 8 if dim == 3 else 1
+    fx = FixCoupLB(f"f all couplb 16 8 {nz} 0.1 1.0".split(), dimension=dim)
+    hi = (16.0, 8.0, float(nz))
+    d = abi.make_domain(dim, (0.0, 0.0, 0.0), hi, 0.1)
+    d.subhi[axis] = hi[axis] / 2
+    rc = fx.L.couplb_fix_init(fx.h, C.byref(d))
+    assert rc == abi.ERR_UNSUPPORTED
+    msg = fx.L.couplb_fix_last_error(fx.h).decode()
+    assert "sub-box must equal the box" in msg and "xyz"[axis] in msg
+    fx.close()

@@ -72,3 +72,26 @@ def test_noalloc_rejects_sizes_above_its_capacity(cuda_lib):
     rc = cuda_lib.couplb_diagnostics_noalloc(t.data_ptr(), t.data_ptr(), t.data_ptr(), t.data_ptr(),
                                              too_many, abi.FP64, 1.0, out.data_ptr(), None)
     assert rc == abi.ERR_TOO_LARGE
+
+
+def test_noalloc_max_speed_propagates_nan(cuda_lib):
+    """A NaN velocity at one node makes max |u| NaN (there is no separate
+    non-finite count in this entry point), on two calls in a row."""
+    import torch
+    n = 5000
+    g = torch.Generator().manual_seed(3)
+    fields = [torch.rand(n, generator=g, dtype=torch.float64).cuda() * 1e-2 for _ in range(4)]
+    fields[0] += 1.0
+    out = torch.zeros(5, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    for call, bad in enumerate((4321, 17)):
+        fields[2][bad] = float("nan")
+        torch.cuda.synchronize()
+        rc = cuda_lib.couplb_diagnostics_noalloc(*[t.data_ptr() for t in fields], n, abi.FP64, 1.0,
+                                                 out.data_ptr(), stream)
+        assert rc == abi.OK
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        assert np.isnan(got[0]), (call, got)
+        assert np.isfinite(got[1])
+        fields[2][bad] = 0.0
