@@ -65,10 +65,6 @@ def parse():
     ap.add_argument("--rods-box", type=int, nargs=3, default=[512, 256, 256],
                     help="box of --only rods (profiling of smaller cases)")
     ap.add_argument("--rods-count", type=int, default=1000, help="rods of --only rods")
-    ap.add_argument("--refresh-lag", type=int, default=None,
-                    help="z planes between an LB block and the markers whose refresh it fills")
-    ap.add_argument("--fused-refresh", type=int, default=1,
-                    help="1: the LB launch fills the refresh's stencil records, 0: separate kernel")
     ap.add_argument("--ibm-e2e", type=int, default=1,
                     help="with --only ibm: also time the workload through the fix hooks (1) or not (0)")
     ap.add_argument("--ibm-n", type=int, default=256,
@@ -163,7 +159,6 @@ class Clocks:
 
 # --------------------------------------------------------------------------
 KERNEL = -1
-LATTICE_OPTIONS = {}   # handle options of the marker workloads (--refresh-lag, --fused-refresh)
 
 
 def make_lattice(prec, nx, ny, nz, device):
@@ -276,8 +271,6 @@ def marker_bench(torch, device, prec, cycles, warmup, box, wall, tau, x0, v0, md
         combined = method is None
     nx, ny, nz = box
     L = Lattice(3, nx, ny, nz, tau=tau, wall=wall, precision=prec, device=device)
-    for k, val in LATTICE_OPTIONS.items():
-        L.set_option(k, val)
     stream = torch.cuda.current_stream()
     L.set_stream(stream.cuda_stream)
     L.init_equilibrium(1.0)
@@ -304,8 +297,7 @@ def marker_bench(torch, device, prec, cycles, warmup, box, wall, tau, x0, v0, md
                 e0 = torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
             if s == 0 and combined:
-                # LB step + refresh sub-step in one call (the LB launch fills
-                # the refresh's stencil records)
+                # LB step + refresh sub-step in one call
                 L.lbm_step_ibm_device(natoms, x.data_ptr(), v.data_ptr(), m.data_ptr(), f.data_ptr(), 0)
             else:
                 if s == 0:
@@ -339,8 +331,7 @@ def marker_bench(torch, device, prec, cycles, warmup, box, wall, tau, x0, v0, md
     if combined:
         # the refresh sub-step shares its call with the LB step
         out["ms_later_substeps_per_lb_cycle"] = sum(a.elapsed_time(b) for a, b in ievs) / cycles
-        out["refresh"] = "lbm_step_ibm (LB launch fills the stencil records)"
-        out["refresh_filled"] = L.get_option("refresh_filled")
+        out["first_substep"] = "couplb_lbm_step_ibm_device (LB step + refresh sub-step in one call)"
     else:
         out["ms_ibm_per_lb_cycle"] = sum(a.elapsed_time(b) for a, b in ievs) / cycles
     if record is not None:
@@ -702,9 +693,6 @@ def main():
     global KERNEL
     args = parse()
     KERNEL = args.kernel
-    LATTICE_OPTIONS["fused_refresh"] = args.fused_refresh
-    if args.refresh_lag is not None:
-        LATTICE_OPTIONS["refresh_lag"] = args.refresh_lag
     if args.impl == "reference":
         return run_reference(args)
     import torch

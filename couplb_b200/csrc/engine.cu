@@ -201,8 +201,9 @@ int couplb_destroy(couplb_handle* h) {
   dfree(h->d_pass);
   dfree(h->d_staging);
   dfree(h->d_scratch);
-  p = h->d_refresh; dfree(p);
-  p = h->d_bidx; dfree(p);
+  if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+  for (int e = 0; e < 2; e++)
+    if (h->copy_ev[e]) cudaEventDestroy(h->copy_ev[e]);
   dfree(h->d_x); dfree(h->d_v); dfree(h->d_m); dfree(h->d_fout); dfree(h->d_active);
   if (h->h_fout) cudaFreeHost(h->h_fout);
   if (h->h_mass) cudaFreeHost(h->h_mass);
@@ -316,50 +317,18 @@ int couplb_get_populations(couplb_handle* h, double* f_host) {
 
 int couplb_lbm_step(couplb_handle* h, const double* g_lb) {
   if (!h) return COUPLB_ERR_ARG;
-  return engine_lbm_step(h, g_lb, nullptr);
+  return engine_lbm_step(h, g_lb);
 }
 
 }  // extern "C"
 
-namespace {
-
-// Bucket buffers of the fused refresh for n markers.
-int ensure_refresh(couplb_handle* h, int n) {
-  const int nz = h->p.nz;
-  const int bcap = std::max(64, 2 * ((n + nz - 1) / nz) + 64);
-  if (h->d_refresh && h->refresh_nz == nz && h->refresh_bcap >= bcap) return COUPLB_OK;
-  void* p = h->d_refresh; dfree(p); h->d_refresh = nullptr;
-  p = h->d_bidx; dfree(p); h->d_bidx = nullptr;
-  int rc;
-  if ((rc = dalloc(h, (void**)&h->d_refresh, sizeof(int) * (2 * (size_t)nz + 1)))) return rc;
-  if ((rc = dalloc(h, (void**)&h->d_bidx, sizeof(int) * (size_t)nz * bcap))) return rc;
-  h->refresh_nz = nz;
-  h->refresh_bcap = bcap;
-  return COUPLB_OK;
-}
-
-}  // namespace
-
 namespace couplb {
 
-int engine_lbm_step(couplb_handle* h, const double* g_lb, const RefreshReq* rq) {
+int engine_lbm_step(couplb_handle* h, const double* g_lb) {
   if (g_lb && !h->p.body_force)
     return fail(h, COUPLB_ERR_STATE, "gravity given to a lattice created with body_force = 0");
   int rc = set_device(h);
   if (rc) return rc;
-  // the fused refresh: D3Q19, shifted storage on the packed kernel, IBM
-  // constants set, and an epoch that does not wrap at this step
-  const bool fuse = rq && rq->n > 0 && h->fused_refresh && h->p.dim == 3 && h->ip_set &&
-                    h->p.precision != COUPLB_FP64 && !h->poststream && h->idx32 && h->p.nx % 2 == 0 &&
-                    (h->kernel == kKernelAuto || h->kernel == kKernelPacked) &&
-                    h->cur_epoch + 1 != 0xffffffffu;
-  h->refresh_prefilled = 0;
-  h->refresh_last_fused = 0;
-  if (fuse) {
-    if ((rc = ensure_stencil_cache(h, rq->n))) return rc;
-    if ((rc = ensure_refresh(h, rq->n))) return rc;
-    CK(cudaMemsetAsync(h->d_refresh, 0, sizeof(int) * (2 * (size_t)h->p.nz + 1), h->stream));
-  }
   const bool g_active = g_lb && !(std::fabs(g_lb[0]) < ZERO_TOL && std::fabs(g_lb[1]) < ZERO_TOL &&
                                   std::fabs(g_lb[2]) < ZERO_TOL);
   dim3 grid, block;
@@ -394,40 +363,7 @@ int engine_lbm_step(couplb_handle* h, const double* g_lb, const RefreshReq* rq) 
       if (want == kKernelPacked && pull && h->idx32 && h->p.nx % 2 == 0) {
         const int pairs = h->p.nx / 2;
         const dim3 pg((pairs + 127) / 128, h->p.ny, h->p.nz);
-        LBRefresh<S> r{};
-        if constexpr (L::D == 3) {
-          if (fuse) {
-            IbmArgs<S>& ia = r.ia;
-            ia.g = g;
-            ia.fin = a.fout;
-            ia.rho_field = a.rho_field;
-            ia.pull = 1;
-            ia.sbuf = (A*)h->sbuf;
-            ia.skey = h->skey;
-            ia.n = rq->n;
-            ia.x = rq->d_x;
-            ia.active = rq->d_active;
-            for (int d = 0; d < 3; d++) { ia.lo[d] = h->ip.domain_lo[d]; ia.off[d] = h->ip.offset[d]; }
-            ia.inv_dx = 1.0 / h->ip.dx;
-            r.plane_done = h->d_refresh;
-            r.bcount = h->d_refresh + h->p.nz;
-            r.bidx = h->d_bidx;
-            r.bcap = h->refresh_bcap;
-            r.lag = h->refresh_lag;
-            r.blocks_per_plane = (int)pg.x * h->p.ny;
-            r.filled = h->d_refresh + 2 * h->p.nz;
-            r.epoch = h->cur_epoch + 1;
-            k_ibm_bucket<L, S><<<flat_blocks(rq->n, 256), 256, 0, h->stream>>>(
-                ia, h->d_refresh + h->p.nz, h->d_bidx, h->refresh_bcap);
-            k_stream_collide_x2<L, S, 5, true><<<pg, 128, 0, h->stream>>>(a, r);
-            h->refresh_prefilled = 1;
-            h->refresh_last_fused = 1;
-          } else {
-            k_stream_collide_x2<L, S><<<pg, 128, 0, h->stream>>>(a, r);
-          }
-        } else {
-          k_stream_collide_x2<L, S><<<pg, 128, 0, h->stream>>>(a, r);
-        }
+        k_stream_collide_x2<L, S><<<pg, 128, 0, h->stream>>>(a);
         used = kKernelPacked;
       }
     }
@@ -663,16 +599,6 @@ int couplb_set_option(couplb_handle* h, const char* name, long long value) {
     h->barrier_spin = value;
     return COUPLB_OK;
   }
-  if (!std::strcmp(name, "fused_refresh")) {
-    if (value != 0 && value != 1) return fail(h, COUPLB_ERR_ARG, "fused_refresh must be 0 or 1");
-    h->fused_refresh = (int)value;
-    return COUPLB_OK;
-  }
-  if (!std::strcmp(name, "refresh_lag")) {
-    if (value < 0 || value > 1 << 20) return fail(h, COUPLB_ERR_ARG, "refresh_lag must be 0..2^20");
-    h->refresh_lag = (int)value;
-    return COUPLB_OK;
-  }
   return fail(h, COUPLB_ERR_ARG, "unknown or read-only option '%s'", name);
 }
 
@@ -682,19 +608,6 @@ int couplb_get_option(couplb_handle* h, const char* name, long long* value) {
   if (!std::strcmp(name, "last_kernel")) { *value = h->last_kernel; return COUPLB_OK; }
   if (!std::strcmp(name, "ibm_resident")) { *value = h->ibm_resident; return COUPLB_OK; }
   if (!std::strcmp(name, "barrier_spin")) { *value = h->barrier_spin; return COUPLB_OK; }
-  if (!std::strcmp(name, "fused_refresh")) { *value = h->fused_refresh; return COUPLB_OK; }
-  if (!std::strcmp(name, "refresh_lag")) { *value = h->refresh_lag; return COUPLB_OK; }
-  if (!std::strcmp(name, "refresh_filled")) {
-    // records the last fused launch filled (-1: the last LB step did not fuse)
-    if (!h->refresh_last_fused || !h->d_refresh) { *value = -1; return COUPLB_OK; }
-    int rc = set_device(h);
-    if (rc) return rc;
-    int* hi = (int*)h->h_small;
-    CK(cudaMemcpyAsync(hi, h->d_refresh + 2 * h->p.nz, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    *value = hi[0];
-    return COUPLB_OK;
-  }
   if (!std::strcmp(name, "timeouts")) {
     int rc = set_device(h);
     if (rc) return rc;

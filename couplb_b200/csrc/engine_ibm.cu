@@ -88,15 +88,12 @@ int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, co
     a.inv_N = 1.0 / (double)ip.md_per_lb;
     a.vs = ip.vel_scale;
     a.fs = ip.force_scale;
+    a.spread_c = a.inv_N / a.fs;
     a.dvr = dv / cell_vol;
     a.corr = method != COUPLB_IBM_SINGLE ? h->d_corr : nullptr;
     a.mlp = (method == COUPLB_IBM_LEARNED) ? h->mlp->pack : nullptr;
-    // records filled by the LB launch (couplb_lbm_step_ibm*): the refresh
-    // sub-step only fills the records of markers the launch left out
-    const bool prefilled = refresh && !a.all_valid && h->refresh_prefilled;
-    a.fill_miss = prefilled ? 1 : 0;
     if (method == COUPLB_IBM_SINGLE) {
-      if (refresh && !a.all_valid && !prefilled) k_ibm_prefetch<L, S><<<nb, bs, 0, h->stream>>>(a);
+      if (refresh && !a.all_valid) k_ibm_prefetch<L, S><<<nb, bs, 0, h->stream>>>(a);
       if (ip.delta == COUPLB_DELTA_ROMA) k_ibm_substep<L, S, 0><<<nb, bs, 0, h->stream>>>(a);
       else k_ibm_substep<L, S, 1><<<nb, bs, 0, h->stream>>>(a);
     } else {
@@ -107,7 +104,7 @@ int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, co
       P.dF = h->d_dF;
       P.ps = ps + h->pass_cur;
       P.ps_next = ps + (h->pass_cur ^ 1);
-      P.fill = refresh && !a.all_valid && !prefilled;
+      P.fill = refresh && !a.all_valid;
       P.status = h->d_status;
       P.ncorr = h->ibm_passes - 1;
       P.check_first = method == COUPLB_IBM_LEARNED;
@@ -122,7 +119,6 @@ int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, co
   CK_LAUNCH();
   if (record) h->rec_count += n;
   h->force_dirty = 1;
-  if (refresh) h->refresh_prefilled = 0;
   return COUPLB_OK;
 }
 
@@ -134,10 +130,10 @@ extern "C" {
 
 namespace {
 
-// Host atom arrays of one sub-step copied to the handle's device buffers
-// (queued on the stream); *nc = atoms in the group.
-int stage_host_atoms(couplb_handle* h, int n, const double* x, const double* v, const double* mass,
-                     const int* active, int* nc) {
+// Host atom arrays of one sub-step copied to the handle's device buffers,
+// queued on stream s; *nc = atoms in the group.
+int stage_host_atoms(couplb_handle* h, cudaStream_t s, int n, const double* x, const double* v,
+                     const double* mass, const int* active, int* nc) {
   if (n < 0 || (n > 0 && (!x || !v || !mass))) return fail(h, COUPLB_ERR_ARG, "bad atom arrays");
   int rc = ensure_atoms(h, n);
   if (rc) return rc;
@@ -145,10 +141,10 @@ int stage_host_atoms(couplb_handle* h, int n, const double* x, const double* v, 
   for (int a = 0; a < n; a++) c += active ? (active[a] != 0) : 1;
   *nc = c;
   if (n > 0) {
-    CK(cudaMemcpyAsync(h->d_x, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->d_v, v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->d_m, mass, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
-    if (active) CK(cudaMemcpyAsync(h->d_active, active, sizeof(int) * n, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_x, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h->d_v, v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h->d_m, mass, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    if (active) CK(cudaMemcpyAsync(h->d_active, active, sizeof(int) * n, cudaMemcpyHostToDevice, s));
   }
   return COUPLB_OK;
 }
@@ -180,7 +176,7 @@ int couplb_ibm_substep(couplb_handle* h, int n, const double* x, const double* v
   int rc = set_device(h);
   if (rc) return rc;
   int nc = 0;
-  if ((rc = stage_host_atoms(h, n, x, v, mass, active, &nc))) return rc;
+  if ((rc = stage_host_atoms(h, h->stream, n, x, v, mass, active, &nc))) return rc;
   if (ncoupled) *ncoupled = nc;
   return substep_staged(h, n, active, nc, f_add, refresh);
 }
@@ -192,13 +188,22 @@ int couplb_lbm_step_ibm(couplb_handle* h, const double* g_lb, int n, const doubl
   if (n > 0 && !f_add) return fail(h, COUPLB_ERR_ARG, "bad atom arrays");
   int rc = set_device(h);
   if (rc) return rc;
+  // the atom copies run on a copy stream while the LB kernel runs (the
+  // previous sub-step, which read the same buffers, is complete: the host
+  // path synchronises at its end; the copy stream still waits for the main
+  // stream to reach this point)
+  if (!h->copy_stream) {
+    CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+    for (int e = 0; e < 2; e++) CK(cudaEventCreateWithFlags(&h->copy_ev[e], cudaEventDisableTiming));
+  }
+  CK(cudaEventRecord(h->copy_ev[0], h->stream));
+  CK(cudaStreamWaitEvent(h->copy_stream, h->copy_ev[0], 0));
   int nc = 0;
-  // the atoms go to the device first, so that the LB launch can fill their
-  // stencil records
-  if ((rc = stage_host_atoms(h, n, x, v, mass, active, &nc))) return rc;
+  if ((rc = stage_host_atoms(h, h->copy_stream, n, x, v, mass, active, &nc))) return rc;
+  CK(cudaEventRecord(h->copy_ev[1], h->copy_stream));
   if (ncoupled) *ncoupled = nc;
-  const RefreshReq rq{nc > 0 ? n : 0, (const double*)h->d_x, active ? (const int*)h->d_active : nullptr};
-  if ((rc = engine_lbm_step(h, g_lb, &rq))) return rc;
+  if ((rc = engine_lbm_step(h, g_lb))) return rc;
+  CK(cudaStreamWaitEvent(h->stream, h->copy_ev[1], 0));
   return substep_staged(h, n, active, nc, f_add, 1);
 }
 
@@ -210,8 +215,7 @@ int couplb_lbm_step_ibm_device(couplb_handle* h, const double* g_lb, int n, cons
   if (n < 0 || (n > 0 && (!d_x || !d_v || !d_mass || !d_f_add))) return fail(h, COUPLB_ERR_ARG, "bad atom arrays");
   int rc = set_device(h);
   if (rc) return rc;
-  const RefreshReq rq{n, d_x, d_active};
-  if ((rc = engine_lbm_step(h, g_lb, &rq))) return rc;
+  if ((rc = engine_lbm_step(h, g_lb))) return rc;
   return engine_ibm(h, n, d_x, d_v, d_mass, d_active, d_f_add, 1, 1);
 }
 

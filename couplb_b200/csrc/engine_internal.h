@@ -76,14 +76,8 @@ struct couplb_handle {
   int pass_cur = 0;                  // the one of the last sub-step
   int ibm_resident = 1;              // option: register-resident form when markers fit
   long long barrier_spin = 1LL << 21;   // option: grid-barrier poll limit of the method kernels
-  // IBM refresh fused into the LB launch (couplb_lbm_step_ibm*)
-  int fused_refresh = 1;             // option: allow it
-  int refresh_lag = 8;               // option: planes between a block and the bucket it fills
-  int* d_refresh = nullptr;          // per z plane: done counters, then bucket counts; filled count
-  int* d_bidx = nullptr;             // bucket lists
-  int refresh_nz = 0, refresh_bcap = 0;
-  int refresh_prefilled = 0;         // the records of the pending refresh are filled
-  int refresh_last_fused = 0;        // the last LB launch filled stencil records
+  cudaStream_t copy_stream = nullptr;   // host->device atom copies of couplb_lbm_step_ibm
+  cudaEvent_t copy_ev[2] = {nullptr, nullptr};   // main stream reached / copies done
   int coop_blocks[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // resident blocks of k_ibm_method (Roma,
                                                    // Peskin4, learned Roma, learned Peskin4),
                                                    // then of its register-resident form
@@ -97,15 +91,8 @@ struct couplb_handle {
 
 namespace couplb {
 int engine_macro(couplb_handle* h);
-// The markers whose refresh a fused LB launch fills (device arrays).
-struct RefreshReq {
-  int n;
-  const double* d_x;
-  const int* d_active;
-};
-// One LB step; with rq (and a D3Q19 shifted lattice on the packed kernel)
-// the launch also fills the stencil records of the refresh of those markers.
-int engine_lbm_step(couplb_handle* h, const double* g_lb, const RefreshReq* rq);
+// One LB step (couplb_lbm_step).
+int engine_lbm_step(couplb_handle* h, const double* g_lb);
 // Pinned host buffers of n masses and n group flags owned by the handle (valid
 // until the next call with a larger n), for host drivers that assemble those
 // arrays before couplb_ibm_substep, so that every host->device copy of a

@@ -92,14 +92,17 @@ struct IbmArgs {
   double lo[3];
   int off[3];
   double inv_dx, xi_over_dt, inv_N, vs, fs, dvr;
+  double spread_c;                        // inv_N / fs: marker force -> spread force
   // forcing methods beyond the single pass (null / unused otherwise)
   double* corr;                           // n*3: correction beyond the penalty pass
   const MlpPacked* mlp;                   // learned correction network
-  int fill_miss;                          // a marker whose record misses computes and stores it
 };
 
 // Add a spread force to one node of the interleaved force field: one vector
 // atomic (16 B, sm_90+) for FP32; three FP64 atomics otherwise.
+__device__ __forceinline__ void spread_add(float* p, float a, float b, float c) {
+  atomicAdd(reinterpret_cast<float4*>(p), make_float4(a, b, c, 0.f));
+}
 __device__ __forceinline__ void spread_add(float* p, double a, double b, double c) {
   atomicAdd(reinterpret_cast<float4*>(p), make_float4(float(a), float(b), float(c), 0.f));
 }
@@ -211,15 +214,14 @@ __device__ __forceinline__ LaneNodes<R> lane_nodes(const Geom& g, double lx, dou
 
 // Velocity of interior node (i,j,k) = n of the post-stream state, with the
 // arithmetic of k_macro (compute_macroscopic(false), couplb_lattice.h:155-202).
-// CG: the populations were written earlier in the same launch (read at L2).
-template <class L, class S, bool CG = false>
+template <class L, class S>
 __device__ __forceinline__ void compute_velocity(const IbmArgs<S>& a, int i, int j, int k, size_t n,
                                                  typename S::A& v0, typename S::A& v1,
                                                  typename S::A& v2, typename S::A& vr) {
   using C = typename S::C;
   C f[L::Q];
-  if (a.pull) load_node<L, S, size_t, true, CG>(a.g, a.fin, a.rho_field, i, j, k, n, f);
-  else load_node<L, S, size_t, false, CG>(a.g, a.fin, a.rho_field, i, j, k, n, f);
+  if (a.pull) load_node<L, S, size_t, true>(a.g, a.fin, a.rho_field, i, j, k, n, f);
+  else load_node<L, S, size_t, false>(a.g, a.fin, a.rho_field, i, j, k, n, f);
   C r, jx, jy, jz;
   moments<L, C>(f, r, jx, jy, jz);
   C rho = S::kShift ? C(a.g.rho0) + r : r;
@@ -247,9 +249,8 @@ __device__ __forceinline__ typename S::A* stencil_record(const IbmArgs<S>& a, in
   return a.sbuf + (size_t)mk * kRecStride;
 }
 
-// Refresh prefetch of marker mk by one warp: fills its slot's record and key
-// (epoch `epoch`).  CG: populations written earlier in the same launch.
-template <class L, class S, bool CG>
+// Refresh prefetch of marker mk by one warp: fills its slot's record and key.
+template <class L, class S>
 __device__ __forceinline__ void prefetch_marker(const IbmArgs<S>& a, int mk, int lane, unsigned epoch) {
   const Geom& g = a.g;
   const double lx = (a.x[3 * mk] - a.lo[0]) * a.inv_dx - a.off[0] + 1.0;
@@ -274,7 +275,7 @@ __device__ __forceinline__ void prefetch_marker(const IbmArgs<S>& a, int mk, int
     if (ig >= 0 && ig < gx && jg >= 0 && jg < gy && kg >= 0 && kg < gz &&
         classify_node(g, L::D, ig, jg, kg, ii, jj, kk) < 0) {
       const size_t n = (size_t)ii + (size_t)g.nx * ((size_t)jj + (size_t)g.ny * kk);
-      compute_velocity<L, S, CG>(a, ii, jj, kk, n, v[rep][0], v[rep][1], v[rep][2], v[rep][3]);
+      compute_velocity<L, S>(a, ii, jj, kk, n, v[rep][0], v[rep][1], v[rep][2], v[rep][3]);
     }
   }
 #pragma unroll
@@ -293,116 +294,7 @@ __global__ void __launch_bounds__(256) k_ibm_prefetch(const IbmArgs<S> a) {
   const int lane = threadIdx.x & 31;
   if (mk >= a.n) return;
   if (a.active && !a.active[mk]) return;
-  prefetch_marker<L, S, false>(a, mk, lane, a.cur_epoch);
-}
-
-// Interior z planes whose populations the refresh of a marker with base cell
-// k0 reads (with repeats, at most 12): the stencil planes kg = k0-1 .. k0+2 of
-// the ghost-inclusive box, a periodic ghost plane as its interior image, and
-// for each the planes its pull reads (kk-1, kk, kk+1, wrapped across a
-// periodic z face; a wall face is read at the node itself).  A superset of
-// what compute_velocity reads: x / y walls only remove nodes.
-template <class L>
-__device__ __forceinline__ int refresh_planes(const Geom& g, int k0, int (&pl)[12]) {
-  if (L::D != 3) {
-    pl[0] = 0;
-    return 1;
-  }
-  const int gz = g.nz + 2;
-  int np = 0;
-#pragma unroll
-  for (int o = 0; o < 4; o++) {
-    const int kg = k0 - 1 + o;
-    if (kg < 0 || kg >= gz) continue;
-    int kk;
-    if (kg == 0) {
-      if (g.face[4]) continue;
-      kk = g.nz - 1;
-    } else if (kg == gz - 1) {
-      if (g.face[5]) continue;
-      kk = 0;
-    } else {
-      kk = kg - 1;
-    }
-    pl[np++] = kk;
-    if (kk > 0) pl[np++] = kk - 1;
-    else if (!g.face[4]) pl[np++] = g.nz - 1;
-    if (kk < g.nz - 1) pl[np++] = kk + 1;
-    else if (!g.face[5]) pl[np++] = 0;
-  }
-  return np;
-}
-
-// Refresh bucketing ahead of a fused LB launch (k_stream_collide_x2 with
-// refresh): the markers whose refresh reads plane b last (b = the largest
-// plane of refresh_planes) are listed in bucket b, at most bcap of them; a
-// marker beyond the capacity, or reading no plane, is not listed (its first
-// sub-step computes its record).  bcount starts at zero.
-template <class L, class S>
-__global__ void __launch_bounds__(256) k_ibm_bucket(const IbmArgs<S> a, int* __restrict__ bcount,
-                                                   int* __restrict__ bidx, int bcap) {
-  const int mk = blockIdx.x * blockDim.x + threadIdx.x;
-  if (mk >= a.n) return;
-  if (a.active && !a.active[mk]) return;
-  const double lz = (a.x[3 * mk + 2] - a.lo[2]) * a.inv_dx - a.off[2] + 1.0;
-  int pl[12];
-  const int np = refresh_planes<L>(a.g, (int)floor(lz), pl);
-  if (np == 0) return;
-  int key = pl[0];
-  for (int t = 1; t < np; t++) key = pl[t] > key ? pl[t] : key;
-  const int pos = atomicAdd(bcount + key, 1);
-  if (pos < bcap) bidx[(size_t)key * bcap + pos] = mk;
-}
-
-// Refresh work inside a fused LB launch: after its block has stored its
-// nodes, warp `warp` of the block takes slot (block of the plane) * 4 + warp
-// of bucket k - lag, where k is the block's z plane, and fills that marker's
-// record when every plane its refresh reads is complete (all blocks of the
-// plane counted in plane_done).  The populations are read at L2 (written in
-// this launch); a marker left out is filled by its first sub-step.
-template <class S>
-struct LBRefresh {
-  IbmArgs<S> ia;            // fin / rho_field = the launch's outputs, pull = 1
-  int* plane_done;          // per z plane: blocks that stored their nodes
-  const int* bcount;        // per bucket: markers listed
-  const int* bidx;          // bucket lists, bcap entries each
-  int bcap;
-  int lag;                  // planes between a block's plane and the bucket it serves
-  int blocks_per_plane;
-  unsigned epoch;           // population epoch after the launch
-  int* filled;              // records filled in the launch
-};
-
-__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
-  int v;
-  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-template <class L, class S>
-__device__ __forceinline__ void lb_refresh_tail(const LBRefresh<S>& r, int block_in_plane, int k) {
-  __syncthreads();   // every thread of the block has issued its stores
-  if (threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(r.plane_done + k, 1);
-  }
-  const int b = k - r.lag;
-  if (b < 0) return;
-  const int cnt = min(r.bcount[b], r.bcap);
-  const int slot = block_in_plane * (int)(blockDim.x >> 5) + (int)(threadIdx.x >> 5);
-  if (slot >= cnt) return;
-  const int mk = r.bidx[(size_t)b * r.bcap + slot];
-  const IbmArgs<S>& a = r.ia;
-  const double lz = (a.x[3 * mk + 2] - a.lo[2]) * a.inv_dx - a.off[2] + 1.0;
-  int pl[12];
-  const int np = refresh_planes<L>(a.g, (int)floor(lz), pl);
-  bool ready = true;
-  for (int t = 0; t < np; t++) ready = ready && (ld_acquire_gpu(r.plane_done + pl[t]) == r.blocks_per_plane);
-  // the counters are read by every lane; a lane that saw a plane incomplete
-  // vetoes the warp (the counters only grow, so lanes may disagree)
-  if (!__all_sync(0xffffffffu, ready)) return;
-  prefetch_marker<L, S, true>(a, mk, threadIdx.x & 31, r.epoch);
-  if ((threadIdx.x & 31) == 0) atomicAdd(r.filled, 1);
+  prefetch_marker<L, S>(a, mk, lane, a.cur_epoch);
 }
 
 // Velocity of stencil slot s of marker mk (node (i,j,k) = n).
@@ -439,8 +331,10 @@ __device__ __forceinline__ void node_state(const IbmArgs<S>& a, bool hit, const 
   }
 }
 
-// Weight arithmetic in the storage's compute type: FP64 for the parity form,
-// FP32 for the shifted forms.  Sums are carried in FP64 either way.
+// Weight arithmetic, interpolation sums, their warp reductions and the spread
+// weights in the storage's compute type: FP64 for the parity form, FP32 for
+// the shifted forms (their populations and moments are FP32).  Positions,
+// the penalty force and the total-force accumulators are FP64 in both.
 //
 // LEARNED (D3Q19): the lanes also gather the network input (u0 at the 27
 // nodes round(l)-1..round(l)+1 of each axis, then v / vel_scale) into the
@@ -478,9 +372,9 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
     __syncwarp();
   }
 
-  double ui = 0, vi = 0, wi = 0, ws = 0, wss = 0;
+  R ui = 0, vi = 0, wi = 0, ws = 0, wss = 0;
   long long sn0 = -1, sn1 = -1;   // fluid nodes of this lane (interior index)
-  double sd0 = 0, sd1 = 0;
+  R sd0 = 0, sd1 = 0;
   const StencilKey key = a.skey[mk];
   typename S::A* rec = stencil_record(a, mk);
   // The record entries, the marker's velocity and mass are loaded before the
@@ -498,9 +392,6 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
   const double mass = a.m[mk];
   const double vmk0 = a.v[3 * mk], vmk1 = a.v[3 * mk + 1], vmk2 = a.v[3 * mk + 2];
   const bool hit = key.epoch == a.cur_epoch && key.i0 == i0 && key.j0 == j0 && key.k0 == k0;
-  // a miss of the first sub-step after an LB step whose launch filled the
-  // records computes and stores its record (warp-uniform: one key per warp)
-  fill = fill || (a.fill_miss && !hit && !a.all_valid);
   const LaneNodes<R> ln = lane_nodes<L, DELTA, R>(g, lx, ly, lz, i0, j0, k0, lane);
   bool wall_seen = false;   // a wall node adds to ws but not to wss
 #pragma unroll
@@ -509,7 +400,7 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
     if (s >= NS) break;
     const int t = ln.t[rep];
     if (t == -2) continue;
-    const double dd = double(ln.d[rep]);
+    const R dd = ln.d[rep];
     // slot of this node in the network input, or -1
     int p = -1;
     if (LEARNED) {
@@ -519,16 +410,18 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
     if (t < 0) {
       const size_t src = (size_t)ln.n[rep];
       const int ii = ln.i, jj = ln.j, kk = ln.k[rep];
-      double u0, u1, u2;
+      R u0, u1, u2;
       if (fill) {
         typename S::A v0, v1, v2, vr;
         compute_velocity<L, S>(a, ii, jj, kk, src, v0, v1, v2, vr);
         rec[s] = v0; rec[64 + s] = v1; rec[128 + s] = v2; rec[192 + s] = vr;
-        u0 = double(v0); u1 = double(v1); u2 = double(v2);
+        u0 = R(v0); u1 = R(v1); u2 = R(v2);
       } else if (spec && hit) {
-        u0 = double(pre[rep][0]); u1 = double(pre[rep][1]); u2 = double(pre[rep][2]);
+        u0 = R(pre[rep][0]); u1 = R(pre[rep][1]); u2 = R(pre[rep][2]);
       } else {
-        node_velocity<L, S>(a, hit, rec, s, ii, jj, kk, src, u0, u1, u2);
+        double w0, w1, w2;
+        node_velocity<L, S>(a, hit, rec, s, ii, jj, kk, src, w0, w1, w2);
+        u0 = R(w0); u1 = R(w1); u2 = R(w2);
       }
       ui += u0 * dd;
       vi += u1 * dd;
@@ -542,9 +435,9 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
       ws += dd;
       wall_seen = true;
     } else if (t == 2) {
-      ui += g.uw[0] * dd;
-      vi += g.uw[1] * dd;
-      wi += (L::D == 3 ? g.uw[2] : 0.0) * dd;
+      ui += R(g.uw[0]) * dd;
+      vi += R(g.uw[1]) * dd;
+      wi += R(L::D == 3 ? g.uw[2] : 0.0) * dd;
       ws += dd;
       wall_seen = true;
       if (LEARNED && p >= 0) {
@@ -569,9 +462,9 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
     wss = ws;
   }
   double u0 = 0, u1 = 0, u2 = 0;
-  if (ws > DELTA_TOL) {
-    const double iw = 1.0 / ws;
-    u0 = ui * iw; u1 = vi * iw; u2 = wi * iw;
+  if (ws > R(DELTA_TOL)) {
+    const R iw = R(1) / ws;
+    u0 = double(ui * iw); u1 = double(vi * iw); u2 = double(wi * iw);
   }
   // penalty force (fix_couplb.cpp:777-781)
   double F0 = mass * a.xi_over_dt * (u0 * a.vs - vmk0);
@@ -597,17 +490,18 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
     }
   }
   // spread -F/(N * force_scale) (fix_couplb.cpp:788-792, couplb_ibm.h:124-132)
-  if (wss < DELTA_TOL) return;
-  const double sc = a.dvr / wss;
-  const double fl0 = -F0 * a.inv_N / a.fs, fl1 = -F1 * a.inv_N / a.fs, fl2 = -F2 * a.inv_N / a.fs;
+  if (wss < R(DELTA_TOL)) return;
+  const R sc = R(a.dvr) / wss;
+  const double fl0 = -F0 * a.spread_c, fl1 = -F1 * a.spread_c, fl2 = -F2 * a.spread_c;
+  const R f0 = R(fl0), f1 = R(fl1), f2 = R(fl2);
   if (sn0 >= 0) {
-    const double w = sd0 * sc;   // couplb_ibm.h:128
-    spread_add(a.F + 4 * sn0, fl0 * w, fl1 * w, fl2 * w);
+    const R w = sd0 * sc;   // couplb_ibm.h:128
+    spread_add(a.F + 4 * sn0, f0 * w, f1 * w, f2 * w);
     if (a.seg_force) a.seg_force[sn0 >> 3] = 1;
   }
   if (sn1 >= 0) {
-    const double w = sd1 * sc;
-    spread_add(a.F + 4 * sn1, fl0 * w, fl1 * w, fl2 * w);
+    const R w = sd1 * sc;
+    spread_add(a.F + 4 * sn1, f0 * w, f1 * w, f2 * w);
     if (a.seg_force) a.seg_force[sn1 >> 3] = 1;
   }
   if (lane == 0 && tot3) {

@@ -203,8 +203,8 @@ __device__ __forceinline__ void spread_marker(const IbmArgs<S>& a, int mk, int l
   for (int o = 16; o > 0; o >>= 1) wss += __shfl_xor_sync(0xffffffffu, wss, o);
   if (wss < DELTA_TOL) return;
   const double sc = a.dvr / wss;
-  const double fl0 = -dF[0] * a.inv_N / a.fs, fl1 = -dF[1] * a.inv_N / a.fs;
-  const double fl2 = -dF[2] * a.inv_N / a.fs;
+  const double fl0 = -dF[0] * a.spread_c, fl1 = -dF[1] * a.spread_c;
+  const double fl2 = -dF[2] * a.spread_c;
   if (sn0 >= 0) {
     const double wgt = sd0 * sc;
     spread_add(a.F + 4 * sn0, fl0 * wgt, fl1 * wgt, fl2 * wgt);
@@ -487,9 +487,8 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
   if (have) {
     const MarkerWindow w = marker_window<L, S>(a, mk);
     const StencilKey key = a.skey[mk];
+    const bool fill = P.fill != 0;
     const bool hit = key.epoch == a.cur_epoch && key.i0 == w.i0 && key.j0 == w.j0 && key.k0 == w.k0;
-    // a refresh whose records the LB launch filled: only misses fill
-    const bool fill = P.fill != 0 || (a.fill_miss && !hit && !a.all_valid);
     A* rec = stencil_record(a, mk);
     int ox = 0, oy = 0, oz = 0;
     if (LEARNED) {
@@ -599,7 +598,7 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
   auto spread = [&](double f0, double f1, double f2) {
     double t0 = 0.0, t1 = 0.0, t2 = 0.0;
     if (have && wss >= DELTA_TOL) {
-      const double fl0 = -f0 * a.inv_N / a.fs, fl1 = -f1 * a.inv_N / a.fs, fl2 = -f2 * a.inv_N / a.fs;
+      const double fl0 = -f0 * a.spread_c, fl1 = -f1 * a.spread_c, fl2 = -f2 * a.spread_c;
 #pragma unroll
       for (int rep = 0; rep < 2; rep++) {
         if (nd[rep] < 0) continue;

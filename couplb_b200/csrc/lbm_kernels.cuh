@@ -89,12 +89,11 @@ __device__ __forceinline__ Cf clamp_rho(Cf r, int* status, int slot) {
 // (couplb_streaming.h:86,112-118): rho[n] of the last compute_macroscopic(true),
 // i.e. the clamped density the previous fused launch computed at n, which it
 // stored in the density field; floored at RHO_CLAMP_FRAC * rho0.
-template <class S, bool CG = false>
+template <class S>
 __device__ __forceinline__ typename S::C moving_wall_rho(const typename S::A* rho_field, size_t n,
                                                          double rho0) {
   using C = typename S::C;
-  const C rf = CG ? C(__ldcg(rho_field + n)) : C(rho_field[n]);
-  const C r = S::kShift ? C(rho0) + rf : rf;
+  const C r = S::kShift ? C(rho0) + C(rho_field[n]) : C(rho_field[n]);
   const C fl = C(RHO_CLAMP_FRAC * rho0 < RHO_MIN ? RHO_MIN : RHO_CLAMP_FRAC * rho0);
   return (r < fl) ? fl : r;
 }
@@ -107,20 +106,12 @@ __device__ __forceinline__ bool near_moving_wall(const Geom& g, int i, int j, in
   return m;
 }
 
-// Population load: read-only path, or at L2 (CG) for populations written
-// earlier in the same launch (storage.cuh).
-template <class S, bool CG>
-__device__ __forceinline__ typename S::C ld_pop(const typename S::T* p) {
-  if constexpr (CG) return S::ld_cg(p);
-  else return S::ld(p);
-}
-
 // Pull of all Q populations of node (i,j,k) with the reference's boundary
 // rules (couplb_streaming.h:99-129).  The source x - e_q of an interior node
 // is either interior, or on one or more ghost planes; on a ghost node the wall
 // set last (x, then y, then z: couplb_boundary.h, fix_couplb.cpp:529-531)
 // decides the rule, and a ghost node without wall is a periodic image.
-template <class L, class S, class I, bool CG = false>
+template <class L, class S, class I>
 __device__ __forceinline__ void pull_general(const Geom& g, const typename S::T* __restrict__ fin,
                                              const typename S::A* __restrict__ rho_field, int i,
                                              int j, int k, I n, typename S::C (&f)[L::Q]) {
@@ -128,7 +119,7 @@ __device__ __forceinline__ void pull_general(const Geom& g, const typename S::T*
   const I qs = (I)g.qs;
   const I sx = (I)g.nx, sxy = (I)g.nx * (I)g.ny;
   C rw = C(0);
-  if (near_moving_wall<L>(g, i, j, k)) rw = moving_wall_rho<S, CG>(rho_field, n, g.rho0);
+  if (near_moving_wall<L>(g, i, j, k)) rw = moving_wall_rho<S>(rho_field, n, g.rho0);
 #pragma unroll
   for (int q = 0; q < L::Q; q++) {
     const int ex = L::ex(q), ey = L::ey(q), ez = L::ez(q);
@@ -137,7 +128,7 @@ __device__ __forceinline__ void pull_general(const Geom& g, const typename S::T*
     const bool oy = sj < 0 || sj >= g.ny;
     const bool oz = (L::D == 3) && (sk < 0 || sk >= g.nz);
     if (!(ox || oy || oz)) {
-      f[q] = ld_pop<S, CG>(fin + pidx<L, S, I>(q, (I)(si + (I)sj * sx + (I)sk * sxy), qs));
+      f[q] = S::ld(fin + pidx<L, S, I>(q, (I)(si + (I)sj * sx + (I)sk * sxy), qs));
       continue;
     }
     int t = 0, wd = 0;
@@ -148,24 +139,24 @@ __device__ __forceinline__ void pull_general(const Geom& g, const typename S::T*
       si = si < 0 ? si + g.nx : (si >= g.nx ? si - g.nx : si);
       sj = sj < 0 ? sj + g.ny : (sj >= g.ny ? sj - g.ny : sj);
       if (L::D == 3) sk = sk < 0 ? sk + g.nz : (sk >= g.nz ? sk - g.nz : sk);
-      f[q] = ld_pop<S, CG>(fin + pidx<L, S, I>(q, (I)si + (I)sj * sx + (I)sk * sxy, qs));
+      f[q] = S::ld(fin + pidx<L, S, I>(q, (I)si + (I)sj * sx + (I)sk * sxy, qs));
     } else if (t == 1) {
-      f[q] = ld_pop<S, CG>(fin + pidx<L, S, I>(L::opp(q), n, qs));
+      f[q] = S::ld(fin + pidx<L, S, I>(L::opp(q), n, qs));
     } else if (t == 2) {
       const C eu = C(ex * g.uw[0] + ey * g.uw[1] + ez * g.uw[2]);
-      f[q] = ld_pop<S, CG>(fin + pidx<L, S, I>(L::opp(q), n, qs)) + C(2.0 * L::w(L::opp(q)) * 3.0) * rw * eu;
+      f[q] = S::ld(fin + pidx<L, S, I>(L::opp(q), n, qs)) + C(2.0 * L::w(L::opp(q)) * 3.0) * rw * eu;
     } else if (t == 3) {
       const int qr = wd == 0 ? L::refl(0, q) : (wd == 1 ? L::refl(1, q) : L::refl(2, q));
-      f[q] = ld_pop<S, CG>(fin + pidx<L, S, I>(qr, n, qs));
+      f[q] = S::ld(fin + pidx<L, S, I>(qr, n, qs));
     } else {
-      f[q] = ld_pop<S, CG>(fin + pidx<L, S, I>(q, n, qs));
+      f[q] = S::ld(fin + pidx<L, S, I>(q, n, qs));
     }
   }
 }
 
 // Pull for rows that touch no wall: only x can wrap, handled by selecting the
 // wrapped column; y/z offsets are constants of q.
-template <class L, class S, class I, bool CG = false>
+template <class L, class S, class I>
 __device__ __forceinline__ void pull_interior(const Geom& g, const typename S::T* __restrict__ fin,
                                               int i, int j, int k, typename S::C (&f)[L::Q]) {
   const I qs = (I)g.qs;
@@ -178,7 +169,7 @@ __device__ __forceinline__ void pull_interior(const Geom& g, const typename S::T
     const int ex = L::ex(q), ey = L::ey(q), ez = L::ez(q);
     const I xs = ex == 1 ? im : (ex == -1 ? ip : (I)i);
     const I ro = row - (I)(ey * g.nx) - (I)ez * sxy;   // unsigned wrap-around is exact
-    f[q] = ld_pop<S, CG>(fin + pidx<L, S, I>(q, ro + xs, qs));
+    f[q] = S::ld(fin + pidx<L, S, I>(q, ro + xs, qs));
   }
 }
 
@@ -191,18 +182,18 @@ __device__ __forceinline__ bool row_is_interior(const Geom& g, int j, int k) {
   return yin && zin && g.face[0] == 0 && g.face[1] == 0;
 }
 
-template <class L, class S, class I, bool kPull, bool CG = false>
+template <class L, class S, class I, bool kPull>
 __device__ __forceinline__ void load_node(const Geom& g, const typename S::T* __restrict__ fin,
                                           const typename S::A* __restrict__ rho_field, int i,
                                           int j, int k, I n, typename S::C (&f)[L::Q]) {
   if (!kPull) {
     const I qs = (I)g.qs;
 #pragma unroll
-    for (int q = 0; q < L::Q; q++) f[q] = ld_pop<S, CG>(fin + pidx<L, S, I>(q, n, qs));
+    for (int q = 0; q < L::Q; q++) f[q] = S::ld(fin + pidx<L, S, I>(q, n, qs));
   } else if (row_is_interior<L>(g, j, k)) {
-    pull_interior<L, S, I, CG>(g, fin, i, j, k, f);
+    pull_interior<L, S, I>(g, fin, i, j, k, f);
   } else {
-    pull_general<L, S, I, CG>(g, fin, rho_field, i, j, k, n, f);
+    pull_general<L, S, I>(g, fin, rho_field, i, j, k, n, f);
   }
 }
 

@@ -12,15 +12,7 @@
 //
 // The arithmetic is that of k_stream_collide for the shifted formats (BGK +
 // Guo with the exact mass / momentum correction); nx must be even.
-//
-// REFRESH (D3Q19): the same launch also fills the IBM stencil records of the
-// refresh that follows the LB step (compute_macroscopic(false) at the stencil
-// nodes, fix_couplb.cpp:757-760): blocks are dispatched plane by plane in z,
-// and after storing its nodes a block fills the records of markers whose
-// planes were completed a few planes earlier, while those populations are
-// still in L2 (ibm_kernels.cuh, lb_refresh_tail).
 #pragma once
-#include "ibm_kernels.cuh"
 #include "lbm_kernels.cuh"
 
 namespace couplb {
@@ -53,6 +45,7 @@ struct Pair<StoreF16S> {
     return mul2(v, f2(StoreF16S::kInvScale));
   }
   __device__ __forceinline__ static float ld1(const __half* p) { return StoreF16S::ld(p); }
+
   __device__ __forceinline__ static void st(__half* p, float2 v) {
     *reinterpret_cast<__half2*>(p) = __float22half2_rn(mul2(v, f2(StoreF16S::kScale)));
   }
@@ -204,12 +197,10 @@ __device__ __forceinline__ void x2_node_pair(const LBArgs<S>& a, int i0, int j, 
   }
 }
 
-template <class L, class S, int MINB = 5, bool REFRESH = false>
-__global__ void __launch_bounds__(128, MINB) k_stream_collide_x2(const LBArgs<S> a, const LBRefresh<S> r) {
+template <class L, class S, int MINB = 5>
+__global__ void __launch_bounds__(128, MINB) k_stream_collide_x2(const LBArgs<S> a) {
   const int i0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
-  const int j = blockIdx.y, k = blockIdx.z;
-  if (i0 < a.g.nx) x2_node_pair<L, S>(a, i0, j, k);
-  if constexpr (REFRESH) lb_refresh_tail<L, S>(r, blockIdx.x + gridDim.x * j, k);
+  if (i0 < a.g.nx) x2_node_pair<L, S>(a, i0, blockIdx.y, blockIdx.z);
 }
 
 }  // namespace couplb

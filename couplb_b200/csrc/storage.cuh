@@ -13,10 +13,6 @@
 // free-slip rules commute with the shift because w[q] == w[opp[q]] ==
 // w[refl[d][q]].
 //
-// ld reads through the non-coherent read-only path (populations written by an
-// earlier launch); ld_cg reads at L2 (populations written earlier in the same
-// launch by other blocks, after a release / acquire handshake).
-//
 // Layout in HBM (kTile, read through pidx in lbm_kernels.cuh): 0 = one plane
 // per population, element q * qs + n; kTile > 0 = tiles of kTile consecutive
 // nodes x Q planes, one 32-byte sector per plane and tile.  Every format is
@@ -35,7 +31,6 @@ struct StoreF64 {
   static constexpr bool kShift = false;
   static constexpr int kTile = 0;
   __device__ __forceinline__ static C ld(const T* p) { return __ldg(p); }
-  __device__ __forceinline__ static C ld_cg(const T* p) { return __ldcg(p); }
   __device__ __forceinline__ static C ld_shared(const T* p) { return *p; }
   __device__ __forceinline__ static void st(T* p, C v) { *p = v; }
 };
@@ -47,7 +42,6 @@ struct StoreF32S {
   static constexpr bool kShift = true;
   static constexpr int kTile = 0;
   __device__ __forceinline__ static C ld(const T* p) { return __ldg(p); }
-  __device__ __forceinline__ static C ld_cg(const T* p) { return __ldcg(p); }
   __device__ __forceinline__ static C ld_shared(const T* p) { return *p; }
   __device__ __forceinline__ static void st(T* p, C v) { *p = v; }
 };
@@ -62,9 +56,6 @@ struct StoreF16S {
   static constexpr float kInvScale = 1.0f / 32768.0f;
   __device__ __forceinline__ static C ld(const T* p) {
     return __half2float(__ldg(p)) * kInvScale;
-  }
-  __device__ __forceinline__ static C ld_cg(const T* p) {
-    return __half2float(__ldcg(p)) * kInvScale;
   }
   __device__ __forceinline__ static C ld_shared(const T* p) { return __half2float(*p) * kInvScale; }
   __device__ __forceinline__ static void st(T* p, C v) {

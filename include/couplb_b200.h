@@ -229,10 +229,8 @@ int  couplb_ibm_substep_device(couplb_handle* h, int n, const double* d_x,
  * (fix_couplb.cpp:640-651: do_lbm_step, :659-669, then do_ibm_sub_coupling
  * with the refresh, :730-798), i.e. couplb_lbm_step(h, g_lb) followed by
  * couplb_ibm_substep(h, n, ..., refresh = 1, ncoupled), with the same
- * results.  The atom positions reach the device before the LB launch, so on a
- * D3Q19 lattice in a shifted format the launch itself computes the fluid
- * velocities of the refresh at the markers' stencil nodes while those
- * populations are still in L2 (option "fused_refresh"). */
+ * results.  The host->device copies of the atom arrays run on a copy stream
+ * while the LB kernel runs. */
 int  couplb_lbm_step_ibm(couplb_handle* h, const double* g_lb, int n, const double* x,
                          const double* v, const double* mass, const int* active,
                          double* f_add, int* ncoupled);
@@ -356,14 +354,6 @@ int  couplb_status_last(couplb_handle* h, int* clamps, int* nonfinite);
  *                 A block whose barrier runs out counts a timeout and returns;
  *                 the sub-step's results are then invalid, the next launch
  *                 starts clean.  0 gives up at the first failed poll (tests).
- *   "fused_refresh" 1 (default): couplb_lbm_step_ibm* fill the IBM stencil
- *                 records inside the LB launch where the lattice allows it; 0
- *                 runs the separate refresh kernel (same results).
- *   "refresh_lag" z planes between an LB block and the markers whose records
- *                 it fills (default 8): a marker is filled once every plane
- *                 its refresh reads is complete, else by its first sub-step.
- *   "refresh_filled" read-only: records the last LB launch filled, -1 when it
- *                 did not fill any (synchronises).
  *   "timeouts"    read-only: bounded device waits that gave up (synchronises). */
 int  couplb_set_option(couplb_handle* h, const char* name, long long value);
 int  couplb_get_option(couplb_handle* h, const char* name, long long* value);

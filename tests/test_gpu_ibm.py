@@ -112,64 +112,44 @@ def test_momentum_conservation_per_lb_interval(cuda_lib, prec, tol):
         assert np.abs(tot - expect).max() <= 1e-12 * np.abs(expect).max()
 
 
-def _fused_case_run(prec, lag, fused, wall, n=(64, 48, 40), natoms=600, cycles=3, md_per_lb=2, seed=7):
-    """LB cycles of couplb_lbm_step_ibm (LB step + refresh sub-step in one
-    call) and later sub-steps; returns per-sub-step atom forces, the force
-    field, the populations and the records the last fused launch filled."""
-    rng = np.random.default_rng(seed)
-    hi = np.array(n, float)
-    x0 = rng.uniform(0.0, 1.0, (natoms, 3)) * hi
-    x0[:40, 2] = rng.uniform(0.0, 1.5, 40)                # next to the low z face
-    x0[40:80, 2] = hi[2] - rng.uniform(0.0, 1.5, 40)      # and the high one
-    v = 0.01 * rng.standard_normal((natoms, 3))
-    m = rng.uniform(0.5, 1.5, natoms)
-    L = Lattice(3, *n, tau=0.7, wall=wall, wall_vel=(0.01, 0, 0), body_force=True, precision=prec)
-    L.set_populations(cases.initial_populations(3, n, seed))
-    L.set_ibm_params(delta="peskin4", md_per_lb=md_per_lb, xi_ibm=0.8)
-    L.set_option("fused_refresh", int(fused))
-    L.set_option("refresh_lag", lag)
-    fs, filled = [], []
-    x = x0.copy()
-    g = (1e-5, 0.0, 2e-6)
-    for c in range(cycles):
-        for s in range(md_per_lb):
-            x = np.ascontiguousarray(np.mod(x + 0.3 * v, hi))
-            fa = np.zeros_like(x)
-            if s == 0:
-                L.lbm_step_ibm(x, v, m, fa, g_lb=g)
-                filled.append(L.get_option("refresh_filled"))
-            else:
-                L.ibm_substep(x, v, m, fa, refresh=False)
-            fs.append(fa)
-    out = dict(f=np.stack(fs), F=np.stack(L.get_force_field()), pop=L.get_populations(), filled=filled)
-    L.close()
-    return out
-
-
 @pytest.mark.parametrize("prec", ["fp32", "fp16"])
-@pytest.mark.parametrize("wall", [(0,) * 6, (0, 0, 1, 2, 3, 1)])
-def test_fused_refresh_matches_separate_refresh(cuda_lib, prec, wall):
-    """The LB launch that fills the refresh's stencil records (fused) gives
-    the same forces, force field and populations, bit for bit, as the
-    separate refresh kernel, for any lag (0: no plane is complete when a block
-    looks, so the first sub-step fills every record; 1000: no bucket is
-    served; 6: most records are filled in the launch)."""
-    ref = _fused_case_run(prec, 8, False, wall)
-    assert ref["filled"] == [-1, -1, -1]
-    for lag in (0, 6, 1000):
-        got = _fused_case_run(prec, lag, True, wall)
-        np.testing.assert_array_equal(got["f"], ref["f"])
-        np.testing.assert_array_equal(got["F"], ref["F"])
-        np.testing.assert_array_equal(got["pop"], ref["pop"])
-        if lag == 6:
-            assert min(got["filled"]) > 0.5 * 600, got["filled"]
-        if lag == 1000:
-            assert got["filled"] == [0, 0, 0]
+def test_lbm_step_ibm_matches_separate_calls(cuda_lib, prec):
+    """couplb_lbm_step_ibm (atom copies overlapped with the LB kernel) gives
+    the atom forces of lbm_step + ibm_substep(refresh) bit for bit on the
+    first cycle, then agrees to the rounding of the FP32 atomic sums."""
+    n = (40, 32, 24)
+    rng = np.random.default_rng(7)
+    x0 = rng.uniform(0.0, 1.0, (300, 3)) * np.array(n, float)
+    v = 0.01 * rng.standard_normal((300, 3))
+    m = rng.uniform(0.5, 1.5, 300)
+    out = []
+    for combined in (False, True):
+        L = Lattice(3, *n, tau=0.7, wall=(0, 0, 1, 2, 0, 0), wall_vel=(0.01, 0, 0), body_force=True,
+                    precision=prec)
+        L.set_populations(cases.initial_populations(3, n, 7))
+        L.set_ibm_params(delta="peskin4", md_per_lb=2, xi_ibm=0.8)
+        x = x0.copy()
+        fs = []
+        for c in range(3):
+            for s in range(2):
+                x = np.ascontiguousarray(np.mod(x + 0.3 * v, np.array(n, float)))
+                fa = np.zeros_like(x)
+                if s == 0 and combined:
+                    L.lbm_step_ibm(x, v, m, fa, g_lb=(1e-5, 0.0, 2e-6))
+                else:
+                    if s == 0:
+                        L.lbm_step((1e-5, 0.0, 2e-6))
+                    L.ibm_substep(x, v, m, fa, refresh=(s == 0))
+                fs.append(fa)
+        out.append(np.stack(fs))
+        L.close()
+    np.testing.assert_array_equal(out[1][:2], out[0][:2])
+    assert rel(out[1], out[0]) <= (1e-5 if prec == "fp32" else 1e-3)
 
 
 def test_lbm_step_ibm_fp64_matches_oracle(cuda_lib):
-    """FP64 (no fused refresh): the combined call is the LB step followed by
-    the refresh sub-step of the reference (golden case inputs)."""
+    """FP64: the combined call is the LB step followed by the refresh
+    sub-step of the reference (golden case inputs)."""
     from oracle.bindings import OracleGrid
     case = cases.IBM_CASES["d3_peskin_periodic"]
     n = case["n"]
@@ -182,7 +162,6 @@ def test_lbm_step_ibm_fp64_matches_oracle(cuda_lib):
     ip = cases._ibm_params(case)
     fg, fo = np.zeros_like(x), np.zeros_like(x)
     L.lbm_step_ibm(x, v, m, fg, active=active)
-    assert L.get_option("refresh_filled") == -1
     O.lbm_step()
     O.ibm_substep(ip, x, v, m, fo, active=active, refresh=True, fold=True)
     assert rel(fg, fo) <= 1e-11, rel(fg, fo)

@@ -7,19 +7,25 @@ compiled unmodified, driven by the harness that restates fix_couplb.cpp's
 sequencing) on the full workloads the benchmark times, for a few steps each:
 
 - the D3Q19 channel 256x128x128 (walls y and z, gx 1e-6, seeded noise), 10 LB
-  steps: populations and moments within 1e-12;
+  steps: populations and density within 1e-12, velocities as below;
 - the D3Q19 periodic 256^3 box with 20000 Peskin4 markers, md_per_lb 4, two
   LB cycles: per-atom forces within 1e-11, force field within 1e-12;
 - a 512x256x64 slice of the many-rod geometry (walls on y, 50 rods of 200
   markers, Peskin4, md_per_lb 2), one LB cycle: same tolerances;
 - the D2Q9 Poiseuille channel of the reference quick start (8x32, walls y,
-  gx 5e-6) for all of its 50000 steps: fields within 1e-12 of the reference
-  build, and the profile within 1 % of the analytic parabola
+  gx 5e-6) for all of its 50000 steps: populations and density within 1e-12
+  of the reference build, velocities as below, and the profile within 1 % of
+  the analytic parabola
   (tests/poiseuille2d/validate.py:99,111).
 
-Relative errors are max |a - b| / max |b| per field (velocity components
-against the largest velocity component).  Markers move with prescribed
-velocities between sub-steps, the same on both sides.
+Relative errors are max |a - b| / max |b| per field.  Velocities are
+checked against 1e-12 of the largest velocity component plus a rounding
+floor: u = j / rho, and j is a sum of O(rho0) populations whose FP64 rounding
+(a few ulp of rho0 per step, growing like a random walk) does not shrink with
+|u|.  With |u| ~ 1e-4 (the channel's seeded noise) or after 50000 steps, that
+floor (2e-15 sqrt(steps), absolute) is larger than 1e-12 |u|max; the
+populations and the density are held to 1e-12 relative throughout.  Markers
+move with prescribed velocities between sub-steps, the same on both sides.
 """
 import numpy as np
 import pytest
@@ -36,6 +42,14 @@ KIND = "ref" if B.available("ref") else "port"
 def rel(a, b, scale=None):
     s = np.abs(b).max() if scale is None else scale
     return float(np.abs(a - b).max() / max(s, 1e-300))
+
+
+def velocity_errors(got, ref, steps):
+    """max |du| per component over (1e-12 max|u| + 2e-15 sqrt(steps)): at
+    most 1 when the component passes."""
+    us = max(np.abs(ref[k]).max() for k in ("ux", "uy", "uz"))
+    tol = 1e-12 * us + 2e-15 * np.sqrt(steps)
+    return {k: float(np.abs(got[k] - ref[k]).max() / tol) for k in ("ux", "uy", "uz")}
 
 
 def ibm_params(L, delta, md_per_lb):
@@ -90,17 +104,16 @@ def test_channel_256x128x128_ten_steps_match_reference():
         O.lbm_step(g)
     L.macroscopic()
     O.macroscopic(False)
-    gm = [cases.interior(a, 3) for a in L.get_macroscopic()]
-    om = [cases.interior(a, 3) for a in O.get_macro()]
-    us = max(np.abs(a).max() for a in om[1:])
-    errs = {"rho": rel(gm[0], om[0])}
-    for k, a, b in zip(("ux", "uy", "uz"), gm[1:], om[1:]):
-        errs[k] = rel(a, b, us)
+    gm = dict(zip(("rho", "ux", "uy", "uz"), [cases.interior(a, 3) for a in L.get_macroscopic()]))
+    om = dict(zip(("rho", "ux", "uy", "uz"), [cases.interior(a, 3) for a in O.get_macro()]))
+    errs = {"rho": rel(gm["rho"], om["rho"])}
+    uerr = velocity_errors(gm, om, 10)
     del gm, om
     errs["f"] = rel(cases.interior(L.get_populations(), 3), cases.interior(O.get_f(), 3))
     L.close()
     O.close()
     assert max(errs.values()) <= 1e-12, errs
+    assert max(uerr.values()) <= 1.0, uerr
 
 
 def test_periodic_256cubed_20000_markers_two_cycles_match_reference():
@@ -130,9 +143,10 @@ def test_d2q9_poiseuille_50000_steps_matches_reference_and_analytic():
     case = dict(cases.LB_CASES["d2q9_poiseuille"], steps=50000)
     out = cases.run_lb_case_gpu(case, "fp64")
     ref = cases.run_lb_case_oracle(case, KIND)
-    us = max(np.abs(ref[k]).max() for k in ("ux", "uy", "uz"))
-    errs = {k: rel(out[k], ref[k], us if k in ("ux", "uy", "uz") else None) for k in ref}
+    errs = {k: rel(out[k], ref[k]) for k in ("f", "rho")}
     assert max(errs.values()) <= 1e-12, errs
+    uerr = velocity_errors(out, ref, case["steps"])
+    assert max(uerr.values()) <= 1.0, uerr
     # analytic profile u(y) = g/(2 nu) (y + 1/2)(H - 1/2 - y) for bounce-back
     # walls half a node outside the first and last rows (validate.py:99)
     nu = (case["tau"] - 0.5) / 3.0
