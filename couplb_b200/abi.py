@@ -132,6 +132,7 @@ class FixConfig(C.Structure):
         ("slip_tol", C.c_double),
         ("mlp_model", C.c_char * PATH_MAX),
         ("vtk_solid_attr", (C.c_char * 16) * VTK_MAX_ATTR),
+        ("ibm_window", C.c_int),
     ]
 
 

@@ -92,6 +92,12 @@ int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, co
     a.dvr = dv / cell_vol;
     a.corr = method != COUPLB_IBM_SINGLE ? h->d_corr : nullptr;
     a.mlp = (method == COUPLB_IBM_LEARNED) ? h->mlp->pack : nullptr;
+    a.wrap = 0;
+    if (h->ibm_window) {
+      if (!g.face[0] && !g.face[1]) a.wrap |= 1;
+      if (!g.face[2] && !g.face[3]) a.wrap |= 2;
+      if (h->p.dim == 3 && !g.face[4] && !g.face[5]) a.wrap |= 4;
+    }
     if (method == COUPLB_IBM_SINGLE) {
       if (refresh && !a.all_valid) k_ibm_prefetch<L, S><<<nb, bs, 0, h->stream>>>(a);
       if (ip.delta == COUPLB_DELTA_ROMA) k_ibm_substep<L, S, 0><<<nb, bs, 0, h->stream>>>(a);

@@ -36,7 +36,7 @@ const char* const kKeywords[] = {"md_per_lb", "xi_ibm",      "gravity", "wall_x"
                                  "wall_z",    "wall_vel",    "output",  "check_every", "kernel",
                                  "vtk",       "vtk_region",  "vtk_solid", "checkpoint", "restart",
                                  "precision", "ibm_method", "ibm_passes", "slip_tol", "mlp_model",
-                                 nullptr};
+                                 "ibm_window", nullptr};
 
 // is_couplb_keyword (fix_couplb.cpp:22-36), plus the keywords of this
 // implementation (precision, IBM forcing method).
@@ -609,6 +609,12 @@ int couplb_fix_parse(int narg, const char* const* arg, int dimension, couplb_fix
         if (iarg + 2 > narg) perr("fix couplb mlp_model: need 1 value");
         copy_str(c.mlp_model, arg[iarg + 1]);
         iarg += 2;
+      } else if (!std::strcmp(kw, "ibm_window")) {
+        if (iarg + 2 > narg) perr("fix couplb ibm_window: need 1 value");
+        if (!std::strcmp(arg[iarg + 1], "clip")) c.ibm_window = 0;
+        else if (!std::strcmp(arg[iarg + 1], "wrap")) c.ibm_window = 1;
+        else perr("fix couplb ibm_window: use clip or wrap");
+        iarg += 2;
       }
     }
     c.dimension = dimension;
@@ -806,6 +812,7 @@ int couplb_fix_init(couplb_fix* F, const couplb_domain* dom) {
   ip.force_scale = F->force_scale;
   for (int d = 0; d < 3; d++) { ip.domain_lo[d] = F->domain_lo[d]; ip.offset[d] = F->off[d]; }
   if ((rc = couplb_set_ibm_params(F->h, &ip))) return F->engine_fail(rc);
+  if ((rc = couplb_set_option(F->h, "ibm_window", c.ibm_window))) return F->engine_fail(rc);
   if (c.ibm_method != COUPLB_IBM_SINGLE) {
     couplb_ibm_method m;
     std::memset(&m, 0, sizeof(m));

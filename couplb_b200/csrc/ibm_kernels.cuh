@@ -96,7 +96,20 @@ struct IbmArgs {
   // forcing methods beyond the single pass (null / unused otherwise)
   double* corr;                           // n*3: correction beyond the penalty pass
   const MlpPacked* mlp;                   // learned correction network
+  int wrap;                               // window axes wrapped periodically (bit d: axis d)
 };
+
+// The marker window of the reference is [i0-1, i0+2] per axis clipped to the
+// ghost-inclusive box (couplb_ibm.h:64-73, 110-115): near a high periodic face
+// a marker loses the plane beyond the ghost layer.  With the "ibm_window wrap"
+// option an axis whose two faces are periodic is wrapped instead: the window
+// index maps to its interior image, so every node of the window takes part.
+// Returns the ghost-inclusive index of that image (1..n).
+__device__ __forceinline__ int wrap_ghost_index(int ig, int n) {
+  int i = (ig - 1) % n;
+  if (i < 0) i += n;
+  return i + 1;
+}
 
 // Add a spread force to one node of the interleaved force field: one vector
 // atomic (16 B, sm_90+) for FP32; three FP64 atomics otherwise.
@@ -150,7 +163,7 @@ struct LaneNodes {
 
 template <class L, int DELTA, class R>
 __device__ __forceinline__ LaneNodes<R> lane_nodes(const Geom& g, double lx, double ly, double lz,
-                                                   int i0, int j0, int k0, int lane) {
+                                                   int i0, int j0, int k0, int lane, int wrap) {
   R w1 = R(0);
   {
     const int ax = lane >> 2, o = lane & 3;
@@ -165,7 +178,9 @@ __device__ __forceinline__ LaneNodes<R> lane_nodes(const Geom& g, double lx, dou
   const R wy = __shfl_sync(0xffffffffu, w1, 4 + sy);
   const R wxy = wx * wy;
   const int gx = g.nx + 2, gy = g.ny + 2;
-  const int ig = i0 - 1 + sx, jg = j0 - 1 + sy;
+  int ig = i0 - 1 + sx, jg = j0 - 1 + sy;
+  if (wrap & 1) ig = wrap_ghost_index(ig, g.nx);
+  if (wrap & 2) jg = wrap_ghost_index(jg, g.ny);
   const bool inxy = ig >= 0 && ig < gx && jg >= 0 && jg < gy;
   // classify_node, x then y (a later axis overrides)
   int txy = 0;
@@ -198,7 +213,8 @@ __device__ __forceinline__ LaneNodes<R> lane_nodes(const Geom& g, double lx, dou
   for (int rep = 0; rep < 2; rep++) {
     const int oz = (lane >> 4) + 2 * rep;
     const R wz = __shfl_sync(0xffffffffu, w1, 8 + oz);
-    const int kg = k0 - 1 + oz;
+    int kg = k0 - 1 + oz;
+    if (wrap & 4) kg = wrap_ghost_index(kg, g.nz);
     if (!inxy || kg < 0 || kg >= gz) continue;
     int t = txy;
     if (kg == 0 || kg == gz - 1) { const int ft = kg == 0 ? g.face[4] : g.face[5]; if (ft) t = ft; }
@@ -268,9 +284,12 @@ __device__ __forceinline__ void prefetch_marker(const IbmArgs<S>& a, int mk, int
   for (int rep = 0; rep < 2; rep++) {
     const int s = lane + 32 * rep;
     if (s >= NS) break;
-    const int ig = i0 - 1 + (s & 3);
-    const int jg = j0 - 1 + ((s >> 2) & 3);
-    const int kg = (L::D == 3) ? k0 - 1 + (s >> 4) : 0;
+    int ig = i0 - 1 + (s & 3);
+    int jg = j0 - 1 + ((s >> 2) & 3);
+    int kg = (L::D == 3) ? k0 - 1 + (s >> 4) : 0;
+    if (a.wrap & 1) ig = wrap_ghost_index(ig, g.nx);
+    if (a.wrap & 2) jg = wrap_ghost_index(jg, g.ny);
+    if (a.wrap & 4) kg = wrap_ghost_index(kg, g.nz);
     int ii = 0, jj = 0, kk = 0;
     if (ig >= 0 && ig < gx && jg >= 0 && jg < gy && kg >= 0 && kg < gz &&
         classify_node(g, L::D, ig, jg, kg, ii, jj, kk) < 0) {
@@ -392,7 +411,7 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
   const double mass = a.m[mk];
   const double vmk0 = a.v[3 * mk], vmk1 = a.v[3 * mk + 1], vmk2 = a.v[3 * mk + 2];
   const bool hit = key.epoch == a.cur_epoch && key.i0 == i0 && key.j0 == j0 && key.k0 == k0;
-  const LaneNodes<R> ln = lane_nodes<L, DELTA, R>(g, lx, ly, lz, i0, j0, k0, lane);
+  const LaneNodes<R> ln = lane_nodes<L, DELTA, R>(g, lx, ly, lz, i0, j0, k0, lane, a.wrap);
   bool wall_seen = false;   // a wall node adds to ws but not to wss
 #pragma unroll
   for (int rep = 0; rep < 2; rep++) {

@@ -135,7 +135,7 @@ __device__ __forceinline__ void interp_corr(const PassArgs<S>& P, int mk, int la
   const StencilKey key = a.skey[mk];
   const bool hit = key.epoch == a.cur_epoch && key.i0 == w.i0 && key.j0 == w.j0 && key.k0 == w.k0;
   const typename S::A* rec = stencil_record(a, mk);
-  const LaneNodes<R> ln = lane_nodes<L, DELTA, R>(g, w.lx, w.ly, w.lz, w.i0, w.j0, w.k0, lane);
+  const LaneNodes<R> ln = lane_nodes<L, DELTA, R>(g, w.lx, w.ly, w.lz, w.i0, w.j0, w.k0, lane, a.wrap);
   double ui = 0, vi = 0, wi = 0, ws = 0;
 #pragma unroll
   for (int rep = 0; rep < 2; rep++) {
@@ -188,7 +188,7 @@ __device__ __forceinline__ void spread_marker(const IbmArgs<S>& a, int mk, int l
   long long sn0 = -1, sn1 = -1;
   double sd0 = 0.0, sd1 = 0.0;
   double wss = 0.0;
-  const LaneNodes<R> ln = lane_nodes<L, DELTA, R>(g, w.lx, w.ly, w.lz, w.i0, w.j0, w.k0, lane);
+  const LaneNodes<R> ln = lane_nodes<L, DELTA, R>(g, w.lx, w.ly, w.lz, w.i0, w.j0, w.k0, lane, a.wrap);
 #pragma unroll
   for (int rep = 0; rep < 2; rep++) {
     const int s = lane + 32 * rep;
@@ -343,7 +343,10 @@ __device__ __forceinline__ void record_marker(const PassArgs<S>& P, int mk, int 
   if (lane < 27) {
     const int rx = lane % 3, ry = (lane / 3) % 3, rz = lane / 9;
     const int s = (rx + ox) + 4 * (ry + oy) + 16 * (rz + oz);   // window slot
-    const int ig = w.i0 - 1 + rx + ox, jg = w.j0 - 1 + ry + oy, kg = w.k0 - 1 + rz + oz;
+    int ig = w.i0 - 1 + rx + ox, jg = w.j0 - 1 + ry + oy, kg = w.k0 - 1 + rz + oz;
+    if (a.wrap & 1) ig = wrap_ghost_index(ig, g.nx);
+    if (a.wrap & 2) jg = wrap_ghost_index(jg, g.ny);
+    if (a.wrap & 4) kg = wrap_ghost_index(kg, g.nz);
     if (ig >= 0 && ig < gx && jg >= 0 && jg < gy && kg >= 0 && kg < gz) {
       int ii = 0, jj = 0, kk = 0;
       const int t = classify_node(g, 3, ig, jg, kg, ii, jj, kk);
@@ -499,7 +502,7 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
       __syncwarp();
     }
     double ui = 0, vi = 0, wi = 0;
-    const LaneNodes<R> ln = lane_nodes<L, DELTA, R>(g, w.lx, w.ly, w.lz, w.i0, w.j0, w.k0, lane);
+    const LaneNodes<R> ln = lane_nodes<L, DELTA, R>(g, w.lx, w.ly, w.lz, w.i0, w.j0, w.k0, lane, a.wrap);
 #pragma unroll
     for (int rep = 0; rep < 2; rep++) {
       const int s = lane + 32 * rep;

@@ -349,6 +349,14 @@ int  couplb_status_last(couplb_handle* h, int* clamps, int* nonfinite);
  *                 whose markers each fit a warp of one cooperative launch keep
  *                 each marker's stencil in registers across passes; 0 always
  *                 uses the general form (same results).
+ *   "ibm_window"  0 (default): the IBM window of the reference, [i0-1, i0+2]
+ *                 per axis clipped to the ghost-inclusive box
+ *                 (couplb_ibm.h:64-73, 110-115), so a marker within a cell of a
+ *                 high periodic face loses the plane beyond the ghost layer;
+ *                 1: an axis whose two faces are periodic is wrapped instead
+ *                 (every window node is used, through its interior image) --
+ *                 for physics runs; results then differ from the reference's
+ *                 near those faces.
  *   "barrier_spin" poll limit of each grid-wide barrier of the ITERATIVE /
  *                 LEARNED sub-step kernels (default 2^21 polls of ~100 ns).
  *                 A block whose barrier runs out counts a timeout and returns;
@@ -406,6 +414,10 @@ typedef struct couplb_fix_config {
   double slip_tol;
   char   mlp_model[COUPLB_PATH_MAX];
   char   vtk_solid_attr[COUPLB_VTK_MAX_ATTR][16];  /* vtk_solid attribute names */
+  /* `ibm_window clip|wrap` (no reference counterpart): clip (default) is the
+   * reference's IBM window, clipped to the ghost-inclusive box; wrap wraps it
+   * across periodic axes (handle option "ibm_window"). */
+  int    ibm_window;
 } couplb_fix_config;
 
 /* The MD side of one subdomain (LAMMPS: domain, update). */

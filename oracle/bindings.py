@@ -85,6 +85,7 @@ def load(kind="port"):
                                                   C.c_double, _D, C.c_double, C.c_double, _D, _D,
                                                   _D]),
             "mlp_forward": (None, [_D, C.c_double, C.c_double, C.c_int, _D, C.c_int, _D]),
+            "grid_set_ibm_wrap": (None, [_V, C.c_int]),
             "mlp_loss_grad": (C.c_double, [_D, C.c_double, C.c_double, C.c_int, _D, _D]),
         })
     fns = {}
@@ -179,6 +180,11 @@ class OracleGrid:
         cl = C.c_int(0)
         self.L["grid_diagnostics"](self.h, _d(out), C.byref(cl))
         return out, cl.value
+
+    def set_ibm_wrap(self, mask):
+        """Periodic wrap of the IBM window along the axes of bit mask
+        (port oracle only; the reference clips)."""
+        self.L["grid_set_ibm_wrap"](self.h, int(mask))
 
     def ibm_substep(self, ip, x, v, mass, f_add, active=None, refresh=True, fold=True):
         n = x.shape[0]

@@ -67,6 +67,7 @@ typedef struct orc_grid {
   int rho_clamp_count;
   double tau, omega, rho0;
   int wall_face[3][2];
+  int ibm_wrap;         /* bit d: IBM window wrapped periodically along axis d */
 } orc_grid;
 
 static inline int gidx(const orc_grid* g, int i, int j, int k) {
@@ -508,6 +509,24 @@ static void phys_to_local(const orc_grid* g, const couplb_ibm_params* ip,
   *lz = (g->D == 3) ? ((zp - ip->domain_lo[2]) * inv_dx - ip->offset[2] + 1.0) : 0.0;
 }
 
+/* Window index i along an axis of g ghost-inclusive nodes (n interior):
+ * the reference clips the window to [0, g) (couplb_ibm.h:64-73, 110-115);
+ * with the wrap option (no reference counterpart) an axis whose faces are
+ * both periodic maps i to the interior image 1 + (i - 1 mod n).  Returns 0
+ * when the node is outside. */
+static int window_index(int wrap, int i, int g, int n, int* out) {
+  if (wrap) {
+    int m = (i - 1) % n;
+    if (m < 0) m += n;
+    *out = m + 1;
+    return 1;
+  }
+  *out = i;
+  return i >= 0 && i < g;
+}
+
+void ORC_FN(grid_set_ibm_wrap)(void* gp, int mask) { ((orc_grid*)gp)->ibm_wrap = mask; }
+
 /* IBM::interpolate (couplb_ibm.h:57-90) */
 static void interpolate(const orc_grid* g, const couplb_ibm_params* ip,
                         double inv_dx, double xp, double yp, double zp,
@@ -518,12 +537,15 @@ static void interpolate(const orc_grid* g, const couplb_ibm_params* ip,
   const int k0 = (g->D == 3) ? (int)floor(lz) : 0;
   double ui = 0, vi = 0, wi = 0, ws = 0;
   for (int k = (g->D == 3 ? k0 - 1 : 0); k <= (g->D == 3 ? k0 + 2 : 0); k++) {
-    if (g->D == 3 && (k < 0 || k >= g->gz)) continue;
+    int kw = k;
+    if (g->D == 3 && !window_index(g->ibm_wrap & 4, k, g->gz, g->nz, &kw)) continue;
     for (int j = j0 - 1; j <= j0 + 2; j++) {
-      if (j < 0 || j >= g->gy) continue;
+      int jw;
+      if (!window_index(g->ibm_wrap & 2, j, g->gy, g->ny, &jw)) continue;
       for (int i = i0 - 1; i <= i0 + 2; i++) {
-        if (i < 0 || i >= g->gx) continue;
-        const int n = gidx(g, i, j, k);
+        int iw;
+        if (!window_index(g->ibm_wrap & 1, i, g->gx, g->nx, &iw)) continue;
+        const int n = gidx(g, iw, jw, kw);
         const int nt = g->type[n];
         const double d = delta_product(g, ip->delta, lx - i, ly - j, lz - k);
         if (nt == 0) { ui += g->ux[n]*d; vi += g->uy[n]*d; wi += g->uz[n]*d; ws += d; }
@@ -555,12 +577,15 @@ static void spread(orc_grid* g, const couplb_ibm_params* ip, double inv_dx,
   double ws = 0.0, dcache[64];
   int ncache[64], nc = 0;
   for (int k = (g->D == 3 ? k0 - 1 : 0); k <= (g->D == 3 ? k0 + 2 : 0); k++) {
-    if (g->D == 3 && (k < 0 || k >= g->gz)) continue;
+    int kw = k;
+    if (g->D == 3 && !window_index(g->ibm_wrap & 4, k, g->gz, g->nz, &kw)) continue;
     for (int j = j0 - 1; j <= j0 + 2; j++) {
-      if (j < 0 || j >= g->gy) continue;
+      int jw;
+      if (!window_index(g->ibm_wrap & 2, j, g->gy, g->ny, &jw)) continue;
       for (int i = i0 - 1; i <= i0 + 2; i++) {
-        if (i < 0 || i >= g->gx) continue;
-        const int n = gidx(g, i, j, k);
+        int iw;
+        if (!window_index(g->ibm_wrap & 1, i, g->gx, g->nx, &iw)) continue;
+        const int n = gidx(g, iw, jw, kw);
         if (g->type[n] != 0) continue;
         const double d = delta_product(g, ip->delta, lx - i, ly - j, lz - k);
         dcache[nc] = d; ncache[nc] = n; nc++;

@@ -54,6 +54,9 @@ int    ORC_FN(grid_ibm_substep)(void* g, const couplb_ibm_params* ip, int n,
 
 /* IBM forcing methods and the correction network (project definitions, no
  * reference counterpart; port library only) */
+/* Periodic wrap of the single-pass IBM window (bit d: axis d); 0 = the
+ * reference's clipping. */
+void   ORC_FN(grid_set_ibm_wrap)(void* g, int mask);
 int    ORC_FN(grid_ibm_substep_method)(void* g, const couplb_ibm_params* ip, int n,
                                        const double* x, const double* v,
                                        const double* mass, const int* active,

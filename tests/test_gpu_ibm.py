@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 import cases
+from couplb_b200 import abi
 from couplb_b200.lattice import Lattice
 
 pytestmark = pytest.mark.gpu
@@ -167,3 +168,68 @@ def test_lbm_step_ibm_fp64_matches_oracle(cuda_lib):
     assert rel(fg, fo) <= 1e-11, rel(fg, fo)
     L.close()
     O.close()
+
+
+def _window_case_forces(wrap, xs, prec="fp64", n=(12, 10, 9), wall=(0,) * 6):
+    L = Lattice(3, *n, tau=0.8, wall=wall, precision=prec)
+    L.set_populations(cases.initial_populations(3, n, 31))
+    L.set_ibm_params(delta="peskin4", md_per_lb=1, xi_ibm=0.9)
+    L.set_option("ibm_window", wrap)
+    v = np.tile([0.004, -0.002, 0.003], (xs.shape[0], 1))
+    f = np.zeros_like(xs)
+    L.ibm_substep(np.ascontiguousarray(xs), v, np.ones(xs.shape[0]), f, refresh=True)
+    F = L.get_force_field()
+    L.close()
+    return f, F
+
+
+def test_wrapped_window_is_periodic(cuda_lib):
+    """ibm_window wrap: a marker at x = N - 0.4 takes the same nodes and
+    weights as its periodic image at x = -0.4 (and likewise in y, z), so the
+    forces agree bit for bit; the reference's clipped window (the default)
+    drops a different plane for each of them."""
+    n = (12, 10, 9)
+    base = np.array([[5.3, 4.7, 3.2]])
+    for d in range(3):
+        hi = base.copy()
+        hi[0, d] = n[d] - 0.4
+        lo = base.copy()
+        lo[0, d] = -0.4
+        fw_hi, _ = _window_case_forces(1, hi)
+        fw_lo, _ = _window_case_forces(1, lo)
+        np.testing.assert_array_equal(fw_hi, fw_lo)
+        fc_hi, _ = _window_case_forces(0, hi)
+        fc_lo, _ = _window_case_forces(0, lo)
+        assert np.abs(fc_hi - fc_lo).max() > 1e-6 * np.abs(fc_hi).max()
+
+
+@pytest.mark.parametrize("wall", [(0,) * 6, (0, 0, 1, 1, 0, 0)])
+def test_wrapped_window_matches_oracle(cuda_lib, wall):
+    """FP64 single pass with the wrapped window against the port oracle's
+    restatement of it (no reference counterpart): per-atom forces within
+    1e-11, force field within 1e-12; markers within two cells of every face."""
+    from oracle.bindings import OracleGrid
+    n = (12, 10, 9)
+    rng = np.random.default_rng(41)
+    hi = np.array(n, float)
+    xs = rng.uniform(0.0, 1.0, (60, 3)) * hi
+    for d in range(3):
+        xs[10 * d:10 * d + 5, d] = hi[d] - rng.uniform(0.0, 1.6, 5)
+        xs[10 * d + 5:10 * d + 10, d] = rng.uniform(-0.5, 1.6, 5)
+    fg, Fg = _window_case_forces(1, xs, wall=wall)
+    mask = (0 if wall[0] else 1) | (0 if wall[2] else 2) | (0 if wall[4] else 4)
+    O = OracleGrid(3, *n, tau=0.8, wall=wall)
+    O.set_f(cases.initial_populations(3, n, 31))
+    O.set_ibm_wrap(mask)
+    ip = abi.IbmParams()
+    ip.delta, ip.md_per_lb, ip.xi_ibm = 1, 1, 0.9
+    ip.dt_lbm, ip.dx, ip.vel_scale, ip.force_scale = 1.0, 1.0, 1.0, 1.0
+    v = np.tile([0.004, -0.002, 0.003], (xs.shape[0], 1))
+    fo = np.zeros_like(xs)
+    O.ibm_substep(ip, np.ascontiguousarray(xs), v, np.ones(xs.shape[0]), fo, refresh=True, fold=True)
+    Fo = O.get_force()
+    O.close()
+    assert rel(fg, fo) <= 1e-11, rel(fg, fo)
+    for c in range(3):
+        a, b = cases.interior(Fg[c], 3), cases.interior(Fo[c], 3)
+        assert rel(a, b) <= 1e-12, (c, rel(a, b))

@@ -127,3 +127,12 @@ def test_init_refuses_a_sub_box_smaller_than_the_box(cuda_lib, axis, dim):
     msg = fx.L.couplb_fix_last_error(fx.h).decode()
     assert "sub-box must equal the box" in msg and "xyz"[axis] in msg
     fx.close()
+
+
+def test_ibm_window_keyword(cuda_lib):
+    assert P("f all couplb 8 8 8 0.1 1.0").ibm_window == 0
+    assert P("f all couplb 8 8 8 0.1 1.0 ibm_window wrap").ibm_window == 1
+    assert P("f all couplb 8 8 8 0.1 1.0 ibm_window clip").ibm_window == 0
+    with pytest.raises(CoupLBError) as e:
+        P("f all couplb 8 8 8 0.1 1.0 ibm_window torus")
+    assert e.value.msg == "fix couplb ibm_window: use clip or wrap"
