@@ -364,136 +364,142 @@ __device__ __forceinline__ void node_state(const IbmArgs<S>& a, bool hit, const 
 // to the marker's record (the work of k_ibm_prefetch, fused).
 template <class L, class S, int DELTA, bool LEARNED>
 __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, int lane, bool fill,
-                                                 const MlpPacked* P, float* xs, float* hs,
+                                                 const MlpPacked* P, MlpBlockScratch* blk,
                                                  double* tot3 = nullptr) {
   using R = typename S::C;
-  if (mk >= a.n) return;
-  if (a.active && !a.active[mk]) {
-    if (!a.accumulate && lane < 3) a.fout[3 * mk + lane] = 0.0;
-    return;
-  }
-  const Geom& g = a.g;
-  const double xp = a.x[3 * mk], yp = a.x[3 * mk + 1], zp = a.x[3 * mk + 2];
-  // IBM::phys_to_local (couplb_ibm.h:49-55)
-  const double lx = (xp - a.lo[0]) * a.inv_dx - a.off[0] + 1.0;
-  const double ly = (yp - a.lo[1]) * a.inv_dx - a.off[1] + 1.0;
-  const double lz = (L::D == 3) ? ((zp - a.lo[2]) * a.inv_dx - a.off[2] + 1.0) : 0.0;
-  const int i0 = (int)floor(lx), j0 = (int)floor(ly);
-  const int k0 = (L::D == 3) ? (int)floor(lz) : 0;
-  constexpr int NS = (L::D == 3) ? 64 : 16;
-  // first node of the 27-node network window, in window coordinates
-  int ox = 0, oy = 0, oz = 0;
+  // LEARNED: the 8 warps of the block run the network together (one call of
+  // mlp_block_forward per warp), so a warp without a marker still takes part
+  const bool valid = mk < a.n && !(a.active && !a.active[mk]);
+  if (mk < a.n && !valid && !a.accumulate && lane < 3) a.fout[3 * mk + lane] = 0.0;
+  if (!LEARNED && !valid) return;
+  float* xs = LEARNED ? blk->x + (threadIdx.x >> 5) * kMlpXStride : nullptr;
   if (LEARNED) {
-    ox = (lx - i0) >= 0.5 ? 1 : 0;
-    oy = (ly - j0) >= 0.5 ? 1 : 0;
-    oz = (lz - k0) >= 0.5 ? 1 : 0;
-    for (int t = lane; t < kMlpIn; t += 32) xs[t] = 0.f;
+    for (int t = lane; t < kMlpXStride; t += 32) xs[t] = 0.f;
     __syncwarp();
   }
-
-  R ui = 0, vi = 0, wi = 0, ws = 0, wss = 0;
+  const Geom& g = a.g;
+  constexpr int NS = (L::D == 3) ? 64 : 16;
+  double F0 = 0, F1 = 0, F2 = 0, mass = 0, vmk0 = 0, vmk1 = 0, vmk2 = 0;
   long long sn0 = -1, sn1 = -1;   // fluid nodes of this lane (interior index)
-  R sd0 = 0, sd1 = 0;
-  const StencilKey key = a.skey[mk];
-  typename S::A* rec = stencil_record(a, mk);
-  // The record entries, the marker's velocity and mass are loaded before the
-  // key is compared (their addresses do not depend on it), so that their
-  // latencies overlap; a miss discards the record values.
-  const bool spec = !fill && !a.all_valid;
-  typename S::A pre[2][3] = {{0, 0, 0}, {0, 0, 0}};
-  if (spec) {
+  R sd0 = 0, sd1 = 0, wss = 0;
+  if (valid) {
+    const double xp = a.x[3 * mk], yp = a.x[3 * mk + 1], zp = a.x[3 * mk + 2];
+    // IBM::phys_to_local (couplb_ibm.h:49-55)
+    const double lx = (xp - a.lo[0]) * a.inv_dx - a.off[0] + 1.0;
+    const double ly = (yp - a.lo[1]) * a.inv_dx - a.off[1] + 1.0;
+    const double lz = (L::D == 3) ? ((zp - a.lo[2]) * a.inv_dx - a.off[2] + 1.0) : 0.0;
+    const int i0 = (int)floor(lx), j0 = (int)floor(ly);
+    const int k0 = (L::D == 3) ? (int)floor(lz) : 0;
+    // first node of the 27-node network window, in window coordinates
+    int ox = 0, oy = 0, oz = 0;
+    if (LEARNED) {
+      ox = (lx - i0) >= 0.5 ? 1 : 0;
+      oy = (ly - j0) >= 0.5 ? 1 : 0;
+      oz = (lz - k0) >= 0.5 ? 1 : 0;
+    }
+    R ui = 0, vi = 0, wi = 0, ws = 0;
+    const StencilKey key = a.skey[mk];
+    typename S::A* rec = stencil_record(a, mk);
+    // The record entries, the marker's velocity and mass are loaded before the
+    // key is compared (their addresses do not depend on it), so that their
+    // latencies overlap; a miss discards the record values.
+    const bool spec = !fill && !a.all_valid;
+    typename S::A pre[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    if (spec) {
+#pragma unroll
+      for (int rep = 0; rep < 2; rep++) {
+        const int s = lane + 32 * rep;
+        if (s < NS) { pre[rep][0] = rec[s]; pre[rep][1] = rec[64 + s]; pre[rep][2] = rec[128 + s]; }
+      }
+    }
+    mass = a.m[mk];
+    vmk0 = a.v[3 * mk]; vmk1 = a.v[3 * mk + 1]; vmk2 = a.v[3 * mk + 2];
+    const bool hit = key.epoch == a.cur_epoch && key.i0 == i0 && key.j0 == j0 && key.k0 == k0;
+    const LaneNodes<R> ln = lane_nodes<L, DELTA, R>(g, lx, ly, lz, i0, j0, k0, lane, a.wrap);
+    bool wall_seen = false;   // a wall node adds to ws but not to wss
 #pragma unroll
     for (int rep = 0; rep < 2; rep++) {
       const int s = lane + 32 * rep;
-      if (s < NS) { pre[rep][0] = rec[s]; pre[rep][1] = rec[64 + s]; pre[rep][2] = rec[128 + s]; }
-    }
-  }
-  const double mass = a.m[mk];
-  const double vmk0 = a.v[3 * mk], vmk1 = a.v[3 * mk + 1], vmk2 = a.v[3 * mk + 2];
-  const bool hit = key.epoch == a.cur_epoch && key.i0 == i0 && key.j0 == j0 && key.k0 == k0;
-  const LaneNodes<R> ln = lane_nodes<L, DELTA, R>(g, lx, ly, lz, i0, j0, k0, lane, a.wrap);
-  bool wall_seen = false;   // a wall node adds to ws but not to wss
-#pragma unroll
-  for (int rep = 0; rep < 2; rep++) {
-    const int s = lane + 32 * rep;
-    if (s >= NS) break;
-    const int t = ln.t[rep];
-    if (t == -2) continue;
-    const R dd = ln.d[rep];
-    // slot of this node in the network input, or -1
-    int p = -1;
-    if (LEARNED) {
-      const int rx = (s & 3) - ox, ry = ((s >> 2) & 3) - oy, rz = (s >> 4) - oz;
-      if (rx >= 0 && rx < 3 && ry >= 0 && ry < 3 && rz >= 0 && rz < 3) p = rx + 3 * ry + 9 * rz;
-    }
-    if (t < 0) {
-      const size_t src = (size_t)ln.n[rep];
-      const int ii = ln.i, jj = ln.j, kk = ln.k[rep];
-      R u0, u1, u2;
-      if (fill) {
-        typename S::A v0, v1, v2, vr;
-        compute_velocity<L, S>(a, ii, jj, kk, src, v0, v1, v2, vr);
-        rec[s] = v0; rec[64 + s] = v1; rec[128 + s] = v2; rec[192 + s] = vr;
-        u0 = R(v0); u1 = R(v1); u2 = R(v2);
-      } else if (spec && hit) {
-        u0 = R(pre[rep][0]); u1 = R(pre[rep][1]); u2 = R(pre[rep][2]);
-      } else {
-        double w0, w1, w2;
-        node_velocity<L, S>(a, hit, rec, s, ii, jj, kk, src, w0, w1, w2);
-        u0 = R(w0); u1 = R(w1); u2 = R(w2);
+      if (s >= NS) break;
+      const int t = ln.t[rep];
+      if (t == -2) continue;
+      const R dd = ln.d[rep];
+      // slot of this node in the network input, or -1
+      int p = -1;
+      if (LEARNED) {
+        const int rx = (s & 3) - ox, ry = ((s >> 2) & 3) - oy, rz = (s >> 4) - oz;
+        if (rx >= 0 && rx < 3 && ry >= 0 && ry < 3 && rz >= 0 && rz < 3) p = rx + 3 * ry + 9 * rz;
       }
-      ui += u0 * dd;
-      vi += u1 * dd;
-      wi += u2 * dd;
-      ws += dd;
-      wss += dd;
-      if (rep == 0) { sn0 = (long long)src; sd0 = dd; }
-      else { sn1 = (long long)src; sd1 = dd; }
-      if (LEARNED && p >= 0) { xs[3 * p] = float(u0); xs[3 * p + 1] = float(u1); xs[3 * p + 2] = float(u2); }
-    } else if (t == 1 || t == 3) {
-      ws += dd;
-      wall_seen = true;
-    } else if (t == 2) {
-      ui += R(g.uw[0]) * dd;
-      vi += R(g.uw[1]) * dd;
-      wi += R(L::D == 3 ? g.uw[2] : 0.0) * dd;
-      ws += dd;
-      wall_seen = true;
-      if (LEARNED && p >= 0) {
-        xs[3 * p] = float(g.uw[0]); xs[3 * p + 1] = float(g.uw[1]); xs[3 * p + 2] = float(g.uw[2]);
+      if (t < 0) {
+        const size_t src = (size_t)ln.n[rep];
+        const int ii = ln.i, jj = ln.j, kk = ln.k[rep];
+        R u0, u1, u2;
+        if (fill) {
+          typename S::A v0, v1, v2, vr;
+          compute_velocity<L, S>(a, ii, jj, kk, src, v0, v1, v2, vr);
+          rec[s] = v0; rec[64 + s] = v1; rec[128 + s] = v2; rec[192 + s] = vr;
+          u0 = R(v0); u1 = R(v1); u2 = R(v2);
+        } else if (spec && hit) {
+          u0 = R(pre[rep][0]); u1 = R(pre[rep][1]); u2 = R(pre[rep][2]);
+        } else {
+          double w0, w1, w2;
+          node_velocity<L, S>(a, hit, rec, s, ii, jj, kk, src, w0, w1, w2);
+          u0 = R(w0); u1 = R(w1); u2 = R(w2);
+        }
+        ui += u0 * dd;
+        vi += u1 * dd;
+        wi += u2 * dd;
+        ws += dd;
+        wss += dd;
+        if (rep == 0) { sn0 = (long long)src; sd0 = dd; }
+        else { sn1 = (long long)src; sd1 = dd; }
+        if (LEARNED && p >= 0) { xs[3 * p] = float(u0); xs[3 * p + 1] = float(u1); xs[3 * p + 2] = float(u2); }
+      } else if (t == 1 || t == 3) {
+        ws += dd;
+        wall_seen = true;
+      } else if (t == 2) {
+        ui += R(g.uw[0]) * dd;
+        vi += R(g.uw[1]) * dd;
+        wi += R(L::D == 3 ? g.uw[2] : 0.0) * dd;
+        ws += dd;
+        wall_seen = true;
+        if (LEARNED && p >= 0) {
+          xs[3 * p] = float(g.uw[0]); xs[3 * p + 1] = float(g.uw[1]); xs[3 * p + 2] = float(g.uw[2]);
+        }
       }
     }
-  }
-  if (fill && lane == 0) a.skey[mk] = StencilKey{i0, j0, k0, a.cur_epoch};
-  // without wall nodes in the window ws and wss are the same sums
-  const bool walls = __any_sync(0xffffffffu, wall_seen);
+    if (fill && lane == 0) a.skey[mk] = StencilKey{i0, j0, k0, a.cur_epoch};
+    // without wall nodes in the window ws and wss are the same sums
+    const bool walls = __any_sync(0xffffffffu, wall_seen);
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    ui += __shfl_xor_sync(0xffffffffu, ui, o);
-    vi += __shfl_xor_sync(0xffffffffu, vi, o);
-    wi += __shfl_xor_sync(0xffffffffu, wi, o);
-    ws += __shfl_xor_sync(0xffffffffu, ws, o);
-  }
-  if (walls) {
+    for (int o = 16; o > 0; o >>= 1) {
+      ui += __shfl_xor_sync(0xffffffffu, ui, o);
+      vi += __shfl_xor_sync(0xffffffffu, vi, o);
+      wi += __shfl_xor_sync(0xffffffffu, wi, o);
+      ws += __shfl_xor_sync(0xffffffffu, ws, o);
+    }
+    if (walls) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) wss += __shfl_xor_sync(0xffffffffu, wss, o);
-  } else {
-    wss = ws;
+      for (int o = 16; o > 0; o >>= 1) wss += __shfl_xor_sync(0xffffffffu, wss, o);
+    } else {
+      wss = ws;
+    }
+    double u0 = 0, u1 = 0, u2 = 0;
+    if (ws > R(DELTA_TOL)) {
+      const R iw = R(1) / ws;
+      u0 = double(ui * iw); u1 = double(vi * iw); u2 = double(wi * iw);
+    }
+    // penalty force (fix_couplb.cpp:777-781)
+    F0 = mass * a.xi_over_dt * (u0 * a.vs - vmk0);
+    F1 = mass * a.xi_over_dt * (u1 * a.vs - vmk1);
+    F2 = mass * a.xi_over_dt * (u2 * a.vs - vmk2);
   }
-  double u0 = 0, u1 = 0, u2 = 0;
-  if (ws > R(DELTA_TOL)) {
-    const R iw = R(1) / ws;
-    u0 = double(ui * iw); u1 = double(vi * iw); u2 = double(wi * iw);
-  }
-  // penalty force (fix_couplb.cpp:777-781)
-  double F0 = mass * a.xi_over_dt * (u0 * a.vs - vmk0);
-  double F1 = mass * a.xi_over_dt * (u1 * a.vs - vmk1);
-  double F2 = mass * a.xi_over_dt * (u2 * a.vs - vmk2);
-  if (LEARNED) {
-    if (lane < 3) xs[81 + lane] = float((lane == 0 ? vmk0 : (lane == 1 ? vmk1 : vmk2)) / a.vs);
+  if constexpr (LEARNED) {
+    if (valid && lane < 3) xs[81 + lane] = float((lane == 0 ? vmk0 : (lane == 1 ? vmk1 : vmk2)) / a.vs);
     __syncwarp();
     float y[3];
-    mlp_warp_forward(*P, xs, hs, lane, y);
+    mlp_block_forward(*P, *blk, threadIdx.x >> 5, lane, y);
+    if (!valid) return;
     const double sc = mass * a.xi_over_dt * a.vs;
     const double c0 = sc * double(y[0]), c1 = sc * double(y[1]), c2 = sc * double(y[2]);
     F0 += c0; F1 += c1; F2 += c2;
@@ -549,7 +555,7 @@ __global__ void __launch_bounds__(256) k_ibm_substep(const IbmArgs<S> a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double t3[3] = {0.0, 0.0, 0.0};
   ibm_substep_body<L, S, DELTA, false>(a, (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane, false,
-                                       nullptr, nullptr, nullptr, t3);
+                                       nullptr, nullptr, t3);
   if (!a.ftot) return;
   if (lane == 0) { part[warp][0] = t3[0]; part[warp][1] = t3[1]; part[warp][2] = t3[2]; }
   __syncthreads();
@@ -560,8 +566,8 @@ __global__ void __launch_bounds__(256) k_ibm_substep(const IbmArgs<S> a) {
   }
 }
 
-// Per-warp shared scratch of the learned sub-step: 84 inputs + 64 hidden.
-constexpr int kMlpWarpScratch = kMlpIn + kMlpHid;
-constexpr size_t kLearnedSmem = sizeof(MlpPacked) + 8 * kMlpWarpScratch * sizeof(float);
+// Dynamic shared memory of the learned sub-step kernels (blocks of 8 warps):
+// the packed network, then the block's forward-pass scratch.
+constexpr size_t kLearnedSmem = sizeof(MlpPacked) + sizeof(MlpBlockScratch);
 
 }  // namespace couplb

@@ -378,11 +378,10 @@ __global__ void __launch_bounds__(256) k_ibm_method(const PassArgs<S> P) {
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   MlpPacked* net = reinterpret_cast<MlpPacked*>(smem);
-  float* xs = nullptr;
+  MlpBlockScratch* blk = reinterpret_cast<MlpBlockScratch*>(smem + sizeof(MlpPacked));
   if (LEARNED) {
     mlp_stage(net, a.mlp);
     __syncthreads();
-    xs = reinterpret_cast<float*>(smem + sizeof(MlpPacked)) + (threadIdx.x >> 5) * kMlpWarpScratch;
   }
   if (blockIdx.x == 0) {
     unsigned* z = reinterpret_cast<unsigned*>(P.ps_next);
@@ -390,11 +389,14 @@ __global__ void __launch_bounds__(256) k_ibm_method(const PassArgs<S> P) {
   }
   double ft[3] = {0.0, 0.0, 0.0};
   SlipAcc acc;
-  // first pass: the reference's penalty pass (+ the network correction)
-  for (int mk = gw; mk < a.n; mk += nw) {
+  // first pass: the reference's penalty pass (+ the network correction; the
+  // block's warps step through the markers together, as its network pass
+  // needs all of them)
+  const int wpb = (int)(blockDim.x >> 5);
+  const int mk_end = LEARNED ? (a.n + wpb - 1) / wpb * wpb : a.n;
+  for (int mk = gw; mk < mk_end; mk += nw) {
     double t3[3] = {0.0, 0.0, 0.0};
-    ibm_substep_body<L, S, DELTA, LEARNED>(a, mk, lane, P.fill != 0, net, xs,
-                                           LEARNED ? xs + kMlpIn : nullptr, t3);
+    ibm_substep_body<L, S, DELTA, LEARNED>(a, mk, lane, P.fill != 0, net, blk, t3);
     ft[0] += t3[0]; ft[1] += t3[1]; ft[2] += t3[2];
   }
   block_add_ftot(a.ftot, ft);
@@ -468,11 +470,13 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
   const int lane = threadIdx.x & 31;
   const int mk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   MlpPacked* net = reinterpret_cast<MlpPacked*>(smem);
+  MlpBlockScratch* blk = reinterpret_cast<MlpBlockScratch*>(smem + sizeof(MlpPacked));
   float* xs = nullptr;
   if (LEARNED) {
     mlp_stage(net, a.mlp);
+    xs = blk->x + (threadIdx.x >> 5) * kMlpXStride;
+    for (int t = lane; t < kMlpXStride; t += 32) xs[t] = 0.f;
     __syncthreads();
-    xs = reinterpret_cast<float*>(smem + sizeof(MlpPacked)) + (threadIdx.x >> 5) * kMlpWarpScratch;
   }
   if (blockIdx.x == 0) {
     unsigned* z = reinterpret_cast<unsigned*>(P.ps_next);
@@ -498,8 +502,6 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
       ox = (w.lx - w.i0) >= 0.5 ? 1 : 0;
       oy = (w.ly - w.j0) >= 0.5 ? 1 : 0;
       oz = (w.lz - w.k0) >= 0.5 ? 1 : 0;
-      for (int t = lane; t < kMlpIn; t += 32) xs[t] = 0.f;
-      __syncwarp();
     }
     double ui = 0, vi = 0, wi = 0;
     const LaneNodes<R> ln = lane_nodes<L, DELTA, R>(g, w.lx, w.ly, w.lz, w.i0, w.j0, w.k0, lane, a.wrap);
@@ -572,15 +574,20 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
     F0 = mxi * (U0 * a.vs - vx);
     F1 = mxi * (U1 * a.vs - vy);
     F2 = mxi * (U2 * a.vs - vz);
-    if (LEARNED) {
-      if (lane < 3) xs[81 + lane] = float(a.v[3 * mk + lane] / a.vs);
-      __syncwarp();
-      float y[3];
-      mlp_warp_forward(*net, xs, xs + kMlpIn, lane, y);
+    if (LEARNED && lane < 3) xs[81 + lane] = float(a.v[3 * mk + lane] / a.vs);
+  }
+  if (LEARNED) {
+    // the network for the block's markers (every warp takes part)
+    __syncwarp();
+    float y[3];
+    mlp_block_forward(*net, *blk, threadIdx.x >> 5, lane, y);
+    if (have) {
       const double sc = mxi * a.vs;
       c0 = sc * double(y[0]); c1 = sc * double(y[1]); c2 = sc * double(y[2]);
       F0 += c0; F1 += c1; F2 += c2;
     }
+  }
+  if (have) {
     if (lane == 0) {
       a.corr[3 * mk] = c0; a.corr[3 * mk + 1] = c1; a.corr[3 * mk + 2] = c2;
       if (a.accumulate) {

@@ -228,28 +228,33 @@ __global__ void k_mlp_adam(float* __restrict__ w, float* __restrict__ g, float* 
   w[i] -= lr * (m / c1) / (sqrtf(v / c2) + eps);
 }
 
-// Inference form (BF16 weights, hidden-unit pairs) from the master weights.
+// Inference form (BF16 weights in the padded row-major layout of MlpPacked)
+// from the master weights.
 __global__ void k_mlp_pack(const float* __restrict__ w, float s_in, float s_out, MlpPacked* P) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int nt = gridDim.x * blockDim.x;
-  for (int e = t; e < kMlpIn * 32; e += nt) {
-    const int k = e / 32, l = e % 32;
-    P->w1t[e] = __floats2bfloat162_rn(w[kMlpW1 + l * kMlpIn + k], w[kMlpW1 + (l + 32) * kMlpIn + k]);
+  const __nv_bfloat16 zero = __float2bfloat16_rn(0.f);
+  for (int e = t; e < kMlpHid * kMlpW1Stride; e += nt) {
+    const int n = e / kMlpW1Stride, k = e % kMlpW1Stride;
+    P->w1[e] = k < kMlpIn ? __float2bfloat16_rn(w[kMlpW1 + n * kMlpIn + k]) : zero;
   }
-  for (int e = t; e < kMlpHid * 32; e += nt) {
-    const int k = e / 32, l = e % 32;
-    P->w2t[e] = __floats2bfloat162_rn(w[kMlpW2 + l * kMlpHid + k], w[kMlpW2 + (l + 32) * kMlpHid + k]);
+  for (int e = t; e < kMlpHid * kMlpW2Stride; e += nt) {
+    const int n = e / kMlpW2Stride, k = e % kMlpW2Stride;
+    P->w2[e] = k < kMlpHid ? __float2bfloat16_rn(w[kMlpW2 + n * kMlpHid + k]) : zero;
+  }
+  for (int e = t; e < 8 * kMlpW2Stride; e += nt) {
+    const int n = e / kMlpW2Stride, k = e % kMlpW2Stride;
+    P->w3[e] = (n < kMlpOut && k < kMlpHid) ? __float2bfloat16_rn(w[kMlpW3 + n * kMlpHid + k]) : zero;
   }
   for (int e = t; e < kMlpHid; e += nt) {
     P->b1[e] = w[kMlpB1 + e];
     P->b2[e] = w[kMlpB2 + e];
   }
-  for (int e = t; e < kMlpOut * kMlpHid; e += nt) P->w3[e] = bf16_round(w[kMlpW3 + e]);
-  if (t < kMlpOut) P->b3[t] = w[kMlpB3 + t];
+  if (t < 4) P->b3[t] = t < kMlpOut ? w[kMlpB3 + t] : 0.f;
   if (t == 0) {
     P->s_in = s_in;
     P->s_out = s_out;
-    P->pad[0] = P->pad[1] = P->pad[2] = 0.f;
+    P->pad[0] = P->pad[1] = 0.f;
   }
 }
 

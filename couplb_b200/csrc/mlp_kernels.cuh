@@ -1,6 +1,6 @@
 // mlp_kernels.cuh -- the 84-64-64-3 no-slip correction network: parameter
-// layout, the packed inference form and the warp-level forward pass that the
-// learned IBM sub-step runs per marker.
+// layout, the packed inference form and the tensor-core forward pass that the
+// learned IBM sub-step runs for the markers of a block.
 //
 // Parameters (FP32 master copy, flat): W1[64][84], b1[64], W2[64][64], b2[64],
 // W3[3][64], b3[3].  The network computes in FP32 with weights rounded to
@@ -12,6 +12,7 @@
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <stdint.h>
 
 namespace couplb {
 
@@ -24,18 +25,23 @@ constexpr int kMlpW3 = kMlpB2 + kMlpHid;
 constexpr int kMlpB3 = kMlpW3 + kMlpOut * kMlpHid;
 constexpr int kMlpNParam = kMlpB3 + kMlpOut;   // 9795
 
-// Inference form, copied whole into shared memory by the learned sub-step.
-// Hidden unit pairs (j, j+32) sit in one bf16x2 so lane j reads its two
-// weights of an input column as one conflict-free 4-byte word.
+// Inference form, copied whole into shared memory by the learned sub-step:
+// BF16 weights row-major [output][input] with rows padded so that the
+// tensor-core operand loads of a warp hit 32 distinct banks (stride 104 for
+// the 84 inputs, 72 for the 64 hidden units; padding and W3 rows 3..7 are
+// zero), FP32 biases.
+constexpr int kMlpInPad = 96;     // K of layer 1 rounded up to the MMA k of 16
+constexpr int kMlpW1Stride = 104; // bf16 per W1 row (13 x 8: bank-conflict-free B loads)
+constexpr int kMlpW2Stride = 72;  // bf16 per W2 / W3 row
 struct __align__(16) MlpPacked {
-  __nv_bfloat162 w1t[kMlpIn * 32];    // [k][lane] = (W1[lane][k], W1[lane+32][k])
-  __nv_bfloat162 w2t[kMlpHid * 32];   // [k][lane] = (W2[lane][k], W2[lane+32][k])
+  __nv_bfloat16 w1[kMlpHid * kMlpW1Stride];
+  __nv_bfloat16 w2[kMlpHid * kMlpW2Stride];
+  __nv_bfloat16 w3[8 * kMlpW2Stride];
   float b1[kMlpHid];
   float b2[kMlpHid];
-  float w3[kMlpOut * kMlpHid];        // BF16-rounded values
-  float b3[kMlpOut];
+  float b3[4];
   float s_in, s_out;
-  float pad[3];
+  float pad[2];
 };
 static_assert(sizeof(MlpPacked) % 16 == 0, "MlpPacked is copied in 16-byte words");
 
@@ -50,41 +56,109 @@ __device__ __forceinline__ void mlp_stage(MlpPacked* dst, const MlpPacked* __res
   for (int i = threadIdx.x; i < (int)(sizeof(MlpPacked) / 16); i += blockDim.x) d[i] = __ldg(s + i);
 }
 
-// Forward pass of one sample by one warp.  xs: the warp's 84 inputs in shared
-// memory (raw, lattice velocities), hs: 64 floats of warp scratch.  Every lane
-// returns the three outputs.
-__device__ __forceinline__ void mlp_warp_forward(const MlpPacked& P, const float* xs, float* hs,
-                                                 int lane, float y[3]) {
-  float a0 = P.b1[lane], a1 = P.b1[lane + 32];
-#pragma unroll 4
-  for (int k = 0; k < kMlpIn; k++) {
-    const float xk = xs[k] * P.s_in;
-    const float2 w = __bfloat1622float2(P.w1t[k * 32 + lane]);
-    a0 = fmaf(w.x, xk, a0);
-    a1 = fmaf(w.y, xk, a1);
-  }
-  __syncwarp();
-  hs[lane] = fmaxf(a0, 0.f);
-  hs[lane + 32] = fmaxf(a1, 0.f);
-  __syncwarp();
-  float c0 = P.b2[lane], c1 = P.b2[lane + 32];
-#pragma unroll 4
-  for (int k = 0; k < kMlpHid; k++) {
-    const float hk = hs[k];
-    const float2 w = __bfloat1622float2(P.w2t[k * 32 + lane]);
-    c0 = fmaf(w.x, hk, c0);
-    c1 = fmaf(w.y, hk, c1);
-  }
-  c0 = fmaxf(c0, 0.f);
-  c1 = fmaxf(c1, 0.f);
+// ---- block forward pass on the tensor cores -------------------------------
+// One block of 8 warps evaluates the network for its 8 markers (one row per
+// warp) with mma.sync m16n8k16 (BF16 operands, FP32 accumulation; rows 8-15
+// of the M = 16 tile are zero).  The weights are BF16; the activations are
+// FP32 and enter the MMA split into three BF16 parts, hi + mid + lo, which
+// represent an FP32 value exactly, so every product weight x activation is
+// the exact FP32 product and the network computes the same function as an
+// FP32 evaluation with BF16 weights (up to the order of the FP32 sums).
+constexpr int kMlpXStride = 104;  // floats per input row (84 used, the rest zero)
+constexpr int kMlpHStride = 72;   // floats per hidden row
+struct MlpBlockScratch {
+  float x[8 * kMlpXStride];       // inputs (raw, lattice velocities), one row per warp
+  float h1[8 * kMlpHStride];
+  float h2[8 * kMlpHStride];
+  float y[8 * 4];
+};
+
+__device__ __forceinline__ uint32_t bf16x2_bits(__nv_bfloat162 v) {
+  uint32_t u;
+  memcpy(&u, &v, sizeof u);
+  return u;
+}
+
+// (x0, x1) -> three BF16 pairs with x = hi + mid + lo exactly (FP32 inputs).
+__device__ __forceinline__ void split3(float x0, float x1, uint32_t& hi, uint32_t& mid, uint32_t& lo) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+  const float2 hf = __bfloat1622float2(h);
+  const float r0 = x0 - hf.x, r1 = x1 - hf.y;
+  const __nv_bfloat162 m = __floats2bfloat162_rn(r0, r1);
+  const float2 mf = __bfloat1622float2(m);
+  const __nv_bfloat162 l = __floats2bfloat162_rn(r0 - mf.x, r1 - mf.y);
+  hi = bf16x2_bits(h);
+  mid = bf16x2_bits(m);
+  lo = bf16x2_bits(l);
+}
+
+// D += A B for one m16n8k16 tile; a[1], a[3] (rows 8-15) are zero.
+__device__ __forceinline__ void mma_rows8(float (&d)[4], uint32_t a0, uint32_t a2, uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+      "{%8, %9}, {%0, %1, %2, %3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(0u), "r"(a2), "r"(0u), "r"(b0), "r"(b1));
+}
+
+// acc (8 x 8 tile: rows = the block's markers, columns = 8 outputs starting at
+// row n0 of W) += A[8][K] W^T, A FP32 rows of stride as (scaled by sa), W BF16
+// rows of stride ws.
+template <int K>
+__device__ __forceinline__ void mlp_tile(float (&acc)[4], const float* A, int as, float sa,
+                                         const __nv_bfloat16* W, int ws, int n0, int lane) {
+  const int g = lane >> 2, t = lane & 3;
+  const float* ar = A + g * as + 2 * t;
+  const __nv_bfloat16* wr = W + (n0 + g) * ws + 2 * t;
 #pragma unroll
-  for (int c = 0; c < kMlpOut; c++) {
-    float p = P.w3[c * kMlpHid + lane] * c0 + P.w3[c * kMlpHid + lane + 32] * c1;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
-    y[c] = (p + P.b3[c]) / P.s_out;
+  for (int k0 = 0; k0 < K; k0 += 16) {
+    const float2 x0 = *reinterpret_cast<const float2*>(ar + k0);
+    const float2 x1 = *reinterpret_cast<const float2*>(ar + k0 + 8);
+    uint32_t h0, m0, l0, h1, m1, l1;
+    split3(x0.x * sa, x0.y * sa, h0, m0, l0);
+    split3(x1.x * sa, x1.y * sa, h1, m1, l1);
+    const uint32_t b0 = *reinterpret_cast<const uint32_t*>(wr + k0);
+    const uint32_t b1 = *reinterpret_cast<const uint32_t*>(wr + k0 + 8);
+    mma_rows8(acc, h0, h1, b0, b1);
+    mma_rows8(acc, m0, m1, b0, b1);
+    mma_rows8(acc, l0, l1, b0, b1);
   }
-  __syncwarp();
+}
+
+// Forward pass of the block's 8 rows (all 256 threads call it, after each
+// warp has written its row of S.x); every lane of warp w gets row w's outputs.
+//   h1 = relu(W1 (s_in x) + b1), h2 = relu(W2 h1 + b2), y = (W3 h2 + b3) / s_out.
+__device__ __forceinline__ void mlp_block_forward(const MlpPacked& P, MlpBlockScratch& S, int warp,
+                                                  int lane, float y[3]) {
+  const int g = lane >> 2, t = lane & 3;
+  __syncthreads();
+  {
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    mlp_tile<kMlpInPad>(acc, S.x, kMlpXStride, P.s_in, P.w1, kMlpW1Stride, 8 * warp, lane);
+    const int j = 8 * warp + 2 * t;
+    S.h1[g * kMlpHStride + j] = fmaxf(acc[0] + P.b1[j], 0.f);
+    S.h1[g * kMlpHStride + j + 1] = fmaxf(acc[1] + P.b1[j + 1], 0.f);
+  }
+  __syncthreads();
+  {
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    mlp_tile<kMlpHid>(acc, S.h1, kMlpHStride, 1.f, P.w2, kMlpW2Stride, 8 * warp, lane);
+    const int j = 8 * warp + 2 * t;
+    S.h2[g * kMlpHStride + j] = fmaxf(acc[0] + P.b2[j], 0.f);
+    S.h2[g * kMlpHStride + j + 1] = fmaxf(acc[1] + P.b2[j + 1], 0.f);
+  }
+  __syncthreads();
+  if (warp == 0) {
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    mlp_tile<kMlpHid>(acc, S.h2, kMlpHStride, 1.f, P.w3, kMlpW2Stride, 0, lane);
+    const int c = 2 * t;
+    if (c < kMlpOut) S.y[g * 4 + c] = (acc[0] + P.b3[c]) / P.s_out;
+    if (c + 1 < kMlpOut) S.y[g * 4 + c + 1] = (acc[1] + P.b3[c + 1]) / P.s_out;
+  }
+  __syncthreads();
+  y[0] = S.y[warp * 4];
+  y[1] = S.y[warp * 4 + 1];
+  y[2] = S.y[warp * 4 + 2];
 }
 
 }  // namespace couplb

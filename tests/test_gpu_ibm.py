@@ -184,17 +184,18 @@ def _window_case_forces(wrap, xs, prec="fp64", n=(12, 10, 9), wall=(0,) * 6):
 
 
 def test_wrapped_window_is_periodic(cuda_lib):
-    """ibm_window wrap: a marker at x = N - 0.4 takes the same nodes and
-    weights as its periodic image at x = -0.4 (and likewise in y, z), so the
-    forces agree bit for bit; the reference's clipped window (the default)
-    drops a different plane for each of them."""
+    """ibm_window wrap: a marker at x = N - 0.25 takes the same nodes and
+    weights as its periodic image at x = -0.25 (and likewise in y, z; both
+    positions are exact in binary, so are the weights), and the forces agree
+    bit for bit; the reference's clipped window (the default) drops a
+    different plane for each of them."""
     n = (12, 10, 9)
     base = np.array([[5.3, 4.7, 3.2]])
     for d in range(3):
         hi = base.copy()
-        hi[0, d] = n[d] - 0.4
+        hi[0, d] = n[d] - 0.25
         lo = base.copy()
-        lo[0, d] = -0.4
+        lo[0, d] = -0.25
         fw_hi, _ = _window_case_forces(1, hi)
         fw_lo, _ = _window_case_forces(1, lo)
         np.testing.assert_array_equal(fw_hi, fw_lo)
