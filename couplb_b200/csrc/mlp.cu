@@ -2,14 +2,19 @@
 // correction network, and its C ABI (couplb_mlp_*).
 //
 // Training runs on the GPU with the project's own kernels: one block of 256
-// threads takes a tile of 64 rows, keeps the BF16-rounded weights, the inputs
-// and every activation of the tile in shared memory (113 KB), runs the forward
+// threads takes a tile of 64 rows, keeps the BF16 weights, the inputs and
+// every activation of the tile in shared memory (118 KB), runs the forward
 // pass, the squared-error loss and the backward pass, and adds its partial
 // gradient to an FP32 accumulator with atomics; a second kernel applies Adam
-// to the FP32 master weights.  At these sizes (9795 parameters, 64-wide
-// layers) a step is latency-bound, so the contractions stay on the FP32 pipe.
+// to the FP32 master weights.  The contractions run on the tensor cores
+// (mma.sync m16n8k16, BF16 operands, FP32 accumulation): a BF16 weight times
+// an FP32 activation uses the exact three-part BF16 split of the activation
+// (mlp_kernels.cuh), a product of two FP32 operands (the weight gradients)
+// the six leading products of both splits, so every contraction keeps FP32
+// accuracy.  The tiny layer-3 products (3 outputs) stay on the FP32 pipe.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <stdint.h>
 
 #include <cmath>
 #include <cstdarg>
@@ -25,11 +30,17 @@ namespace {
 
 constexpr int kTile = 64;
 constexpr int kThreads = 256;
-constexpr int kP1 = kMlpIn + 1;    // padded shared-memory row strides
-constexpr int kP2 = kMlpHid + 1;
-constexpr int kTileFloats = kMlpHid * kP1 + kMlpHid * kP2 + kMlpOut * kMlpHid + 2 * kMlpHid + 4 +
-                            kTile * kP1 + 3 * kTile * kP2 + 2 * kTile * kMlpOut + 32;
-constexpr size_t kTileSmem = sizeof(float) * kTileFloats;
+constexpr int kXS = kMlpXStride;   // FP32 row stride of the inputs (84 used, rest zero)
+constexpr int kHS = kMlpHStride;   // FP32 row stride of the hidden activations / deltas
+// shared memory, in bytes: BF16 W1 [64][104], W2 and W2^T [64][72], W3 [8][72];
+// FP32 W3 [3][64], b1, b2, b3; X [64][104]; H1, H2, D2 [64][72]; Y, T [64][3]; scratch
+constexpr size_t kOffW2 = 2 * kMlpHid * kMlpW1Stride;
+constexpr size_t kOffW2T = kOffW2 + 2 * kMlpHid * kMlpW2Stride;
+constexpr size_t kOffW3b = kOffW2T + 2 * kMlpHid * kMlpW2Stride;
+constexpr size_t kOffF = kOffW3b + 2 * 8 * kMlpW2Stride;   // first FP32 array
+constexpr int kTileFloats = kMlpOut * kMlpHid + 2 * kMlpHid + 4 + kTile * kXS + 3 * kTile * kHS +
+                            2 * kTile * kMlpOut + 32;
+constexpr size_t kTileSmem = kOffF + sizeof(float) * kTileFloats;
 constexpr int kAccSlots = 32;
 
 // SplitMix64 (Steele, Lea & Flood, OOPSLA 2014): minibatch row sampling and
@@ -55,28 +66,121 @@ struct TileArgs {
   float* out;                  // null: outputs not stored
 };
 
+// ---- tensor-core tiles of the training kernel ------------------------------
+__device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+      "{%8, %9}, {%0, %1, %2, %3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Fragment element pairs of an m16n8k16 tile for lane (g = lane / 4,
+// t = lane % 4): A rows g and g + 8, columns 2t, 2t + 1 and 2t + 8, 2t + 9;
+// B columns (n) g, rows (k) 2t, 2t + 1 and 2t + 8, 2t + 9.
+// A = M[m0.., k0..] of a row-major FP32 array (stride ms), split in three.
+__device__ __forceinline__ void frag_a_rows(const float* M, int ms, int m0, int k0, int g, int t,
+                                            uint32_t (&h)[4], uint32_t (&m)[4], uint32_t (&l)[4]) {
+  const float* r0 = M + (m0 + g) * ms + k0 + 2 * t;
+  const float* r1 = r0 + 8 * ms;
+  split3(r0[0], r0[1], h[0], m[0], l[0]);
+  split3(r1[0], r1[1], h[1], m[1], l[1]);
+  split3(r0[8], r0[9], h[2], m[2], l[2]);
+  split3(r1[8], r1[9], h[3], m[3], l[3]);
+}
+// A = M^T[m0.., k0..] of a row-major FP32 array M [k][m] (stride ms), split in three.
+__device__ __forceinline__ void frag_a_cols(const float* M, int ms, int m0, int k0, int g, int t,
+                                            uint32_t (&h)[4], uint32_t (&m)[4], uint32_t (&l)[4]) {
+  const float* c = M + (k0 + 2 * t) * ms + m0 + g;
+  split3(c[0], c[ms], h[0], m[0], l[0]);
+  split3(c[8], c[ms + 8], h[1], m[1], l[1]);
+  split3(c[8 * ms], c[9 * ms], h[2], m[2], l[2]);
+  split3(c[8 * ms + 8], c[9 * ms + 8], h[3], m[3], l[3]);
+}
+// B = M[k0.., n0..] of a row-major FP32 array M [k][n] (stride ms), split in three.
+__device__ __forceinline__ void frag_b_rows(const float* M, int ms, int k0, int n0, int g, int t,
+                                            uint32_t (&h)[2], uint32_t (&m)[2], uint32_t (&l)[2]) {
+  const float* c = M + (k0 + 2 * t) * ms + n0 + g;
+  split3(c[0], c[ms], h[0], m[0], l[0]);
+  split3(c[8 * ms], c[9 * ms], h[1], m[1], l[1]);
+}
+// B = W^T[k0.., n0..] of a row-major BF16 array W [n][k] (stride ws): exact.
+__device__ __forceinline__ void frag_b_bf16(const __nv_bfloat16* W, int ws, int k0, int n0, int g, int t,
+                                            uint32_t& b0, uint32_t& b1) {
+  const __nv_bfloat16* r = W + (n0 + g) * ws + k0 + 2 * t;
+  b0 = *reinterpret_cast<const uint32_t*>(r);
+  b1 = *reinterpret_cast<const uint32_t*>(r + 8);
+}
+
+// D[16 x 8] += A (FP32 rows of M, split) * W^T (BF16): three products.
+template <int K>
+__device__ __forceinline__ void tile_act_w(float (&d)[4], const float* M, int ms, int m0,
+                                           const __nv_bfloat16* W, int ws, int n0, int g, int t) {
+#pragma unroll
+  for (int k0 = 0; k0 < K; k0 += 16) {
+    uint32_t h[4], m[4], l[4], b0, b1;
+    frag_a_rows(M, ms, m0, k0, g, t, h, m, l);
+    frag_b_bf16(W, ws, k0, n0, g, t, b0, b1);
+    mma16816(d, h, b0, b1);
+    mma16816(d, m, b0, b1);
+    mma16816(d, l, b0, b1);
+  }
+}
+
+// D[16 x 8] += P^T[m0.., :] Q[:, n0..] over the tile's 64 rows, P and Q FP32
+// row-major [row][.] (strides ps, qs): the six leading products of the
+// three-part splits (the dropped ones are below 2^-24 relative).
+__device__ __forceinline__ void tile_grad(float (&d)[4], const float* Pm, int ps, int m0, const float* Qm,
+                                          int qs, int n0, int g, int t) {
+#pragma unroll
+  for (int k0 = 0; k0 < kTile; k0 += 16) {
+    uint32_t ah[4], am[4], al[4], bh[2], bm[2], bl[2];
+    frag_a_cols(Pm, ps, m0, k0, g, t, ah, am, al);
+    frag_b_rows(Qm, qs, k0, n0, g, t, bh, bm, bl);
+    mma16816(d, ah, bh[0], bh[1]);
+    mma16816(d, ah, bm[0], bm[1]);
+    mma16816(d, am, bh[0], bh[1]);
+    mma16816(d, ah, bl[0], bl[1]);
+    mma16816(d, am, bm[0], bm[1]);
+    mma16816(d, al, bh[0], bh[1]);
+  }
+}
+
 __global__ void __launch_bounds__(kThreads) k_mlp_tile(const TileArgs A) {
-  extern __shared__ float sm[];
-  float* W1 = sm;
-  float* W2 = W1 + kMlpHid * kP1;
-  float* W3 = W2 + kMlpHid * kP2;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __nv_bfloat16* W1b = reinterpret_cast<__nv_bfloat16*>(smraw);
+  __nv_bfloat16* W2b = reinterpret_cast<__nv_bfloat16*>(smraw + kOffW2);
+  __nv_bfloat16* W2Tb = reinterpret_cast<__nv_bfloat16*>(smraw + kOffW2T);
+  __nv_bfloat16* W3b = reinterpret_cast<__nv_bfloat16*>(smraw + kOffW3b);
+  float* W3 = reinterpret_cast<float*>(smraw + kOffF);
   float* B1 = W3 + kMlpOut * kMlpHid;
   float* B2 = B1 + kMlpHid;
   float* B3 = B2 + kMlpHid;
   float* X = B3 + 4;
-  float* H1 = X + kTile * kP1;
-  float* H2 = H1 + kTile * kP2;
-  float* D2 = H2 + kTile * kP2;
-  float* Y = D2 + kTile * kP2;
+  float* H1 = X + kTile * kXS;
+  float* H2 = H1 + kTile * kHS;
+  float* D2 = H2 + kTile * kHS;
+  float* Y = D2 + kTile * kHS;
   float* T = Y + kTile * kMlpOut;
   float* RED = T + kTile * kMlpOut;
   __shared__ long long idx[kTile];
   const int t = threadIdx.x;
+  const int warp = t >> 5, lane = t & 31, g = lane >> 2, q = lane & 3;
+  const __nv_bfloat16 zero = __float2bfloat16_rn(0.f);
 
-  for (int e = t; e < kMlpHid * kMlpIn; e += kThreads)
-    W1[(e / kMlpIn) * kP1 + e % kMlpIn] = bf16_round(A.w[kMlpW1 + e]);
-  for (int e = t; e < kMlpHid * kMlpHid; e += kThreads)
-    W2[(e / kMlpHid) * kP2 + e % kMlpHid] = bf16_round(A.w[kMlpW2 + e]);
+  for (int e = t; e < kMlpHid * kMlpW1Stride; e += kThreads) {
+    const int n = e / kMlpW1Stride, k = e % kMlpW1Stride;
+    W1b[e] = k < kMlpIn ? __float2bfloat16_rn(A.w[kMlpW1 + n * kMlpIn + k]) : zero;
+  }
+  for (int e = t; e < kMlpHid * kMlpW2Stride; e += kThreads) {
+    const int n = e / kMlpW2Stride, k = e % kMlpW2Stride;
+    W2b[e] = k < kMlpHid ? __float2bfloat16_rn(A.w[kMlpW2 + n * kMlpHid + k]) : zero;
+    W2Tb[e] = k < kMlpHid ? __float2bfloat16_rn(A.w[kMlpW2 + k * kMlpHid + n]) : zero;
+  }
+  for (int e = t; e < 8 * kMlpW2Stride; e += kThreads) {
+    const int n = e / kMlpW2Stride, k = e % kMlpW2Stride;
+    W3b[e] = (n < kMlpOut && k < kMlpHid) ? __float2bfloat16_rn(A.w[kMlpW3 + n * kMlpHid + k]) : zero;
+  }
   for (int e = t; e < kMlpOut * kMlpHid; e += kThreads) W3[e] = bf16_round(A.w[kMlpW3 + e]);
   if (t < kMlpHid) { B1[t] = A.w[kMlpB1 + t]; B2[t] = A.w[kMlpB2 + t]; }
   if (t < kMlpOut) B3[t] = A.w[kMlpB3 + t];
@@ -94,45 +198,57 @@ __global__ void __launch_bounds__(kThreads) k_mlp_tile(const TileArgs A) {
     idx[t] = r;
   }
   __syncthreads();
-  for (int e = t; e < kTile * (kMlpIn + kMlpOut); e += kThreads) {
-    const int s = e / (kMlpIn + kMlpOut), k = e % (kMlpIn + kMlpOut);
+  for (int e = t; e < kTile * kXS; e += kThreads) {
+    const int s = e / kXS, k = e % kXS;
     const long long r = idx[s];
-    const float v = r >= 0 ? __ldg(A.rows + r * kMlpRow + k) : 0.f;
-    if (k < kMlpIn) X[s * kP1 + k] = v * A.s_in;
-    else T[s * kMlpOut + k - kMlpIn] = v;
+    float v = 0.f;
+    if (k < kMlpIn && r >= 0) v = __ldg(A.rows + r * kMlpRow + k) * A.s_in;
+    X[e] = v;
+  }
+  for (int e = t; e < kTile * kMlpOut; e += kThreads) {
+    const int s = e / kMlpOut, c = e % kMlpOut;
+    const long long r = idx[s];
+    T[e] = r >= 0 ? __ldg(A.rows + r * kMlpRow + kMlpIn + c) : 0.f;
   }
   __syncthreads();
 
-  // forward
-  for (int e = t; e < kTile * kMlpHid; e += kThreads) {
-    const int s = e / kMlpHid, j = e % kMlpHid;
-    const float* wr = W1 + j * kP1;
-    const float* xr = X + s * kP1;
-    float a = B1[j];
-#pragma unroll 4
-    for (int k = 0; k < kMlpIn; k++) a = fmaf(wr[k], xr[k], a);
-    H1[s * kP2 + j] = fmaxf(a, 0.f);
+  // forward: warp w takes row tile w % 4 and the four column tiles 4 (w / 4) ..
+  const int mt = (warp & 3) * 16;
+  for (int c = 0; c < 4; c++) {
+    const int n0 = ((warp >> 2) * 4 + c) * 8;
+    float d[4] = {0.f, 0.f, 0.f, 0.f};
+    tile_act_w<kMlpInPad>(d, X, kXS, mt, W1b, kMlpW1Stride, n0, g, q);
+    const int j = n0 + 2 * q;
+    H1[(mt + g) * kHS + j] = fmaxf(d[0] + B1[j], 0.f);
+    H1[(mt + g) * kHS + j + 1] = fmaxf(d[1] + B1[j + 1], 0.f);
+    H1[(mt + g + 8) * kHS + j] = fmaxf(d[2] + B1[j], 0.f);
+    H1[(mt + g + 8) * kHS + j + 1] = fmaxf(d[3] + B1[j + 1], 0.f);
   }
   __syncthreads();
-  for (int e = t; e < kTile * kMlpHid; e += kThreads) {
-    const int s = e / kMlpHid, j = e % kMlpHid;
-    const float* wr = W2 + j * kP2;
-    const float* hr = H1 + s * kP2;
-    float a = B2[j];
-#pragma unroll 4
-    for (int k = 0; k < kMlpHid; k++) a = fmaf(wr[k], hr[k], a);
-    H2[s * kP2 + j] = fmaxf(a, 0.f);
+  for (int c = 0; c < 4; c++) {
+    const int n0 = ((warp >> 2) * 4 + c) * 8;
+    float d[4] = {0.f, 0.f, 0.f, 0.f};
+    tile_act_w<kMlpHid>(d, H1, kHS, mt, W2b, kMlpW2Stride, n0, g, q);
+    const int j = n0 + 2 * q;
+    H2[(mt + g) * kHS + j] = fmaxf(d[0] + B2[j], 0.f);
+    H2[(mt + g) * kHS + j + 1] = fmaxf(d[1] + B2[j + 1], 0.f);
+    H2[(mt + g + 8) * kHS + j] = fmaxf(d[2] + B2[j], 0.f);
+    H2[(mt + g + 8) * kHS + j + 1] = fmaxf(d[3] + B2[j + 1], 0.f);
   }
   __syncthreads();
-  if (t < kTile * kMlpOut) {
-    const int s = t / kMlpOut, c = t % kMlpOut;
-    const float* wr = W3 + c * kMlpHid;
-    const float* hr = H2 + s * kP2;
-    float a = B3[c];
-#pragma unroll 4
-    for (int k = 0; k < kMlpHid; k++) a = fmaf(wr[k], hr[k], a);
-    Y[t] = a;
-    if (A.out && idx[s] >= 0) A.out[idx[s] * kMlpOut + c] = a / A.s_out;
+  if (warp < 4) {
+    float d[4] = {0.f, 0.f, 0.f, 0.f};
+    tile_act_w<kMlpHid>(d, H2, kHS, mt, W3b, kMlpW2Stride, 0, g, q);
+    for (int hrow = 0; hrow < 2; hrow++) {
+      const int s = mt + g + 8 * hrow;
+      for (int cc = 0; cc < 2; cc++) {
+        const int c = 2 * q + cc;
+        if (c >= kMlpOut) continue;
+        const float a = d[2 * hrow + cc] + B3[c];
+        Y[s * kMlpOut + c] = a;
+        if (A.out && idx[s] >= 0) A.out[idx[s] * kMlpOut + c] = a / A.s_out;
+      }
+    }
   }
   __syncthreads();
   if (!A.loss) return;
@@ -150,17 +266,18 @@ __global__ void __launch_bounds__(kThreads) k_mlp_tile(const TileArgs A) {
   if ((t & 31) == 0) RED[t >> 5] = lp;
   __syncthreads();
   if (t == 0) {
-    double s = 0.0;
-    for (int i = 0; i < kThreads / 32; i++) s += RED[i];
-    atomicAdd(A.loss + (blockIdx.x & (kAccSlots - 1)), s);
+    double sm = 0.0;
+    for (int i = 0; i < kThreads / 32; i++) sm += RED[i];
+    atomicAdd(A.loss + (blockIdx.x & (kAccSlots - 1)), sm);
   }
   if (!A.grad) return;
 
-  // backward: layer 3, then delta2 = (W3^T dy) * relu'(h2)
+  // backward: layer 3 (three outputs: FP32 pipe), then
+  // delta2 = (W3^T dy) * relu'(h2)
   if (t < kMlpOut * kMlpHid) {
     const int c = t / kMlpHid, k = t % kMlpHid;
     float a = 0.f;
-    for (int s = 0; s < kTile; s++) a = fmaf(Y[s * kMlpOut + c], H2[s * kP2 + k], a);
+    for (int s = 0; s < kTile; s++) a = fmaf(Y[s * kMlpOut + c], H2[s * kHS + k], a);
     atomicAdd(A.grad + kMlpW3 + t, a);
   }
   if (t < kMlpOut) {
@@ -171,44 +288,58 @@ __global__ void __launch_bounds__(kThreads) k_mlp_tile(const TileArgs A) {
   for (int e = t; e < kTile * kMlpHid; e += kThreads) {
     const int s = e / kMlpHid, k = e % kMlpHid;
     float a = 0.f;
-    if (H2[s * kP2 + k] > 0.f)
+    if (H2[s * kHS + k] > 0.f)
       for (int c = 0; c < kMlpOut; c++) a = fmaf(W3[c * kMlpHid + k], Y[s * kMlpOut + c], a);
-    D2[s * kP2 + k] = a;
+    D2[s * kHS + k] = a;
   }
   __syncthreads();
-  // layer 2 gradient, and delta1 = (W2^T delta2) * relu'(h1) into H2
-  for (int e = t; e < kMlpHid * kMlpHid; e += kThreads) {
-    const int j = e / kMlpHid, k = e % kMlpHid;
-    float a = 0.f;
-    for (int s = 0; s < kTile; s++) a = fmaf(D2[s * kP2 + j], H1[s * kP2 + k], a);
-    atomicAdd(A.grad + kMlpW2 + e, a);
+  // layer 2 gradient dW2 = delta2^T h1 (row tile = hidden unit j of layer 2)
+  for (int c = 0; c < 4; c++) {
+    const int n0 = ((warp >> 2) * 4 + c) * 8;
+    float d[4] = {0.f, 0.f, 0.f, 0.f};
+    tile_grad(d, D2, kHS, mt, H1, kHS, n0, g, q);
+    const int j0 = mt + g, k = n0 + 2 * q;
+    atomicAdd(A.grad + kMlpW2 + j0 * kMlpHid + k, d[0]);
+    atomicAdd(A.grad + kMlpW2 + j0 * kMlpHid + k + 1, d[1]);
+    atomicAdd(A.grad + kMlpW2 + (j0 + 8) * kMlpHid + k, d[2]);
+    atomicAdd(A.grad + kMlpW2 + (j0 + 8) * kMlpHid + k + 1, d[3]);
   }
   if (t < kMlpHid) {
     float a = 0.f;
-    for (int s = 0; s < kTile; s++) a += D2[s * kP2 + t];
+    for (int s = 0; s < kTile; s++) a += D2[s * kHS + t];
     atomicAdd(A.grad + kMlpB2 + t, a);
   }
-  for (int e = t; e < kTile * kMlpHid; e += kThreads) {
-    const int s = e / kMlpHid, k = e % kMlpHid;
-    float a = 0.f;
-    if (H1[s * kP2 + k] > 0.f) {
-      const float* dr = D2 + s * kP2;
-#pragma unroll 4
-      for (int j = 0; j < kMlpHid; j++) a = fmaf(W2[j * kP2 + k], dr[j], a);
+  // delta1 = (W2^T delta2) * relu'(h1), into H2 (h2 is no longer read)
+  for (int c = 0; c < 4; c++) {
+    const int n0 = ((warp >> 2) * 4 + c) * 8;
+    float d[4] = {0.f, 0.f, 0.f, 0.f};
+    tile_act_w<kMlpHid>(d, D2, kHS, mt, W2Tb, kMlpW2Stride, n0, g, q);
+    const int k = n0 + 2 * q;
+    for (int hrow = 0; hrow < 2; hrow++) {
+      const int s = mt + g + 8 * hrow;
+      H2[s * kHS + k] = H1[s * kHS + k] > 0.f ? d[2 * hrow] : 0.f;
+      H2[s * kHS + k + 1] = H1[s * kHS + k + 1] > 0.f ? d[2 * hrow + 1] : 0.f;
     }
-    H2[s * kP2 + k] = a;
   }
   __syncthreads();
-  // layer 1 gradient
-  for (int e = t; e < kMlpHid * kMlpIn; e += kThreads) {
-    const int j = e / kMlpIn, k = e % kMlpIn;
-    float a = 0.f;
-    for (int s = 0; s < kTile; s++) a = fmaf(H2[s * kP2 + j], X[s * kP1 + k], a);
-    atomicAdd(A.grad + kMlpW1 + e, a);
+  // layer 1 gradient dW1 = delta1^T x: 4 row tiles (hidden) x 11 column tiles (inputs)
+  for (int tile = warp; tile < 4 * 11; tile += kThreads / 32) {
+    const int m0 = (tile & 3) * 16, n0 = (tile >> 2) * 8;
+    float d[4] = {0.f, 0.f, 0.f, 0.f};
+    tile_grad(d, H2, kHS, m0, X, kXS, n0, g, q);
+    const int j0 = m0 + g, k = n0 + 2 * q;
+    if (k < kMlpIn) {
+      atomicAdd(A.grad + kMlpW1 + j0 * kMlpIn + k, d[0]);
+      atomicAdd(A.grad + kMlpW1 + (j0 + 8) * kMlpIn + k, d[2]);
+    }
+    if (k + 1 < kMlpIn) {
+      atomicAdd(A.grad + kMlpW1 + j0 * kMlpIn + k + 1, d[1]);
+      atomicAdd(A.grad + kMlpW1 + (j0 + 8) * kMlpIn + k + 1, d[3]);
+    }
   }
   if (t < kMlpHid) {
     float a = 0.f;
-    for (int s = 0; s < kTile; s++) a += H2[s * kP2 + t];
+    for (int s = 0; s < kTile; s++) a += H2[s * kHS + t];
     atomicAdd(A.grad + kMlpB1 + t, a);
   }
 }
