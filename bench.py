@@ -601,6 +601,32 @@ def sphere_bench(torch, device, steps, window=500, sample_rows=2_000_000):
     return out
 
 
+def slab_bench(torch, device, steps, warmup, nx, ny, nz, nslab=4):
+    """The FP32 channel as nslab z slabs on one GPU (couplb_b200.slabs: halo
+    planes packed and copied between the slabs after every LB step): MLUPS of
+    the decomposed lattice, to set beside the undecomposed kernel -- the cost
+    of the halo exchange without the interconnect."""
+    from couplb_b200.slabs import SlabLattice
+    S = SlabLattice(nx, ny, nz, nslab, tau=TAU, wall=WALL, body_force=True, precision="fp32",
+                    devices=[device] * nslab)
+    S.set_populations(initial_populations(nx, ny, nz))
+    stream = torch.cuda.current_stream()
+    g = (GX, 0.0, 0.0)
+    for _ in range(warmup):
+        S.lbm_step(g)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        S.lbm_step(g)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    S.close()
+    return {"slabs": nslab, "ms_per_step": ms, "mlups": nx * ny * nz / (ms * 1e-3) / 1e6,
+            "halo_bytes_per_step": 2 * (nslab - 1) * 5 * nx * ny * 4}
+
+
 def cpu_baseline(nx, ny, nz, seconds):
     """The reference's CPU path (its own headers, OpenMP, all host threads)
     on a bounded number of LB steps of the same workload."""
@@ -773,6 +799,7 @@ def main():
         results[prec] = max_over_ranks(torch, ms)
 
     e2e_s = max_over_ranks(torch, e2e_fix(args.steps, args.warmup, nx, ny, nz, local, torch))
+    slab = slab_bench(torch, local, args.steps, args.warmup, nx, ny, nz)
     acc = accuracy_runs(f0, args.accuracy_steps, nx, ny, nz, local) if args.accuracy_steps else {}
     peak, peak_src = load_peak()
 
@@ -815,6 +842,7 @@ def main():
         "e2e": {"value": world * N / e2e_s / 1e6, "unit": "MLUPS", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 8},
         "gpu_launches": args.steps,
+        "slab_decomposition_1gpu": slab,
         "ibm": ibm,
         "ibm_rods": rods,
         "ibm_methods": methods,

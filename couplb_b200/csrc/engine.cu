@@ -398,6 +398,44 @@ int engine_lbm_step(couplb_handle* h, const double* g_lb) {
 
 extern "C" {
 
+int couplb_halo_attach(couplb_handle* h, int side, const void* d_recv) {
+  if (!h) return COUPLB_ERR_ARG;
+  if (side != 0 && side != 1) return fail(h, COUPLB_ERR_ARG, "halo side must be 0 (z low) or 1 (z high)");
+  if (h->p.dim != 3) return fail(h, COUPLB_ERR_UNSUPPORTED, "halo faces are z faces of a D3Q19 lattice");
+  if (d_recv && h->p.wall[4 + side] != COUPLB_WALL_PERIODIC)
+    return fail(h, COUPLB_ERR_ARG, "a halo face must not be a wall (z face %d has type %d)", side,
+                h->p.wall[4 + side]);
+  h->halo[side] = d_recv;
+  return COUPLB_OK;
+}
+
+size_t couplb_halo_bytes(const couplb_handle* h) {
+  if (!h || h->p.dim != 3) return 0;
+  return (size_t)kHaloQ * h->p.nx * h->p.ny * elem_bytes_pop(h->p.precision);
+}
+
+int couplb_halo_pack(couplb_handle* h, int side, void* d_send) {
+  if (!h || !d_send) return fail(h, COUPLB_ERR_ARG, "null argument");
+  if (side != 0 && side != 1) return fail(h, COUPLB_ERR_ARG, "halo side must be 0 (z low) or 1 (z high)");
+  if (h->p.dim != 3) return fail(h, COUPLB_ERR_UNSUPPORTED, "halo faces are z faces of a D3Q19 lattice");
+  if (h->poststream)
+    return fail(h, COUPLB_ERR_STATE, "halo pack needs the post-collision state of an LB step");
+  int rc = set_device(h);
+  if (rc) return rc;
+  const Geom g = make_geom(h);
+  const long long cnt = (long long)kHaloQ * h->p.nx * h->p.ny;
+  with_types(h->p.dim, h->p.precision, [&](auto l, auto s) {
+    using L = decltype(l);
+    using S = decltype(s);
+    using T = typename S::T;
+    if constexpr (L::D == 3)
+      k_halo_pack<L, S><<<flat_blocks(cnt, 256), 256, 0, h->stream>>>(g, (const T*)h->f[h->cur], side,
+                                                                      (T*)d_send);
+  });
+  CK_LAUNCH();
+  return COUPLB_OK;
+}
+
 int couplb_macroscopic(couplb_handle* h) {
   if (!h) return COUPLB_ERR_ARG;
   int rc = set_device(h);

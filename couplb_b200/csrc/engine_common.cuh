@@ -72,6 +72,8 @@ inline Geom make_geom(const couplb_handle* h) {
   for (int d = 0; d < 3; d++) g.uw[d] = h->p.wall_vel[d];
   if (h->p.dim == 2) g.uw[2] = 0.0;
   g.rho0 = h->p.rho0;
+  g.halo[0] = h->halo[0];
+  g.halo[1] = h->halo[1];
   return g;
 }
 

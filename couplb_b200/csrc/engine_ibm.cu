@@ -31,6 +31,9 @@ namespace couplb {
 // the method kernels (launch_method) are compiled in engine_methods_*.cu.
 int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, const double* d_m,
                const int* d_active, double* d_fout, int accumulate, int refresh) {
+  if (h->halo[0] || h->halo[1])
+    return fail(h, COUPLB_ERR_UNSUPPORTED,
+                "IBM coupling on a lattice with halo faces (slab decomposition) is not supported");
   // no coupled atoms: the reference returns before refreshing the moments
   // (fix_couplb.cpp:750-753)
   if (n <= 0) return COUPLB_OK;

@@ -38,7 +38,24 @@ struct Geom {
   int face[6];       // wall type per face: xlo xhi ylo yhi zlo zhi
   double uw[3];      // type-2 wall velocity
   double rho0;       // shift / reference density
+  // z faces that border another subdomain (slab decomposition along z): the
+  // populations that cross the face, taken from the neighbour's boundary
+  // plane after its last LB step (couplb_halo_attach); null = the face wraps
+  // onto this subdomain's other face (or is a wall)
+  const void* halo[2];
 };
+
+// Slot of population q in a z-face halo: the five populations that cross a
+// z face in one direction (ez = +1: 5, 11, 14, 15, 18; ez = -1: 6, 12, 13, 16,
+// 17 in the D3Q19 order), each one plane of nx * ny values.
+template <class L>
+__host__ __device__ constexpr int halo_slot(int q) {
+  int s = 0;
+  for (int p = 0; p < q; p++)
+    if (L::ez(p) == L::ez(q)) s++;
+  return s;
+}
+constexpr int kHaloQ = 5;
 
 // Element index of population q of interior node n (storage.cuh, kTile).
 template <class L, class S, class I>
@@ -138,6 +155,13 @@ __device__ __forceinline__ void pull_general(const Geom& g, const typename S::T*
     if (t == 0) {
       si = si < 0 ? si + g.nx : (si >= g.nx ? si - g.nx : si);
       sj = sj < 0 ? sj + g.ny : (sj >= g.ny ? sj - g.ny : sj);
+      const void* hz = oz ? g.halo[sk < 0 ? 0 : 1] : nullptr;
+      if (L::D == 3 && hz) {
+        // the neighbour subdomain's boundary plane (its exchange face)
+        const typename S::T* hp = static_cast<const typename S::T*>(hz);
+        f[q] = S::ld(hp + (size_t)halo_slot<L>(q) * sxy + (I)si + (I)sj * sx);
+        continue;
+      }
       if (L::D == 3) sk = sk < 0 ? sk + g.nz : (sk >= g.nz ? sk - g.nz : sk);
       f[q] = S::ld(fin + pidx<L, S, I>(q, (I)si + (I)sj * sx + (I)sk * sxy, qs));
     } else if (t == 1) {
@@ -692,6 +716,27 @@ __global__ void __launch_bounds__(256) k_y_profile(Geom g, const typename S::A* 
     out[g.ny + j] = sh[1][0];
     out[2 * g.ny + j] = sh[2][0];
   }
+}
+
+// Halo pack: the populations of the boundary plane of face `side` (0: k = 0,
+// 1: k = nz - 1) that cross it (ez = -1 for side 0, +1 for side 1), from the
+// post-collision store of the last LB step, into kHaloQ planes of nx * ny
+// values in halo_slot order: the neighbour's halo of its facing side.
+template <class L, class S>
+__global__ void k_halo_pack(Geom g, const typename S::T* __restrict__ fin, int side,
+                            typename S::T* __restrict__ out) {
+  const long long sxy = (long long)g.nx * g.ny;
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (e >= kHaloQ * sxy) return;
+  const int slot = (int)(e / sxy);
+  const long long m = e % sxy;
+  const int ez = side ? 1 : -1;
+  int q = -1;
+#pragma unroll
+  for (int p = 0; p < L::Q; p++)
+    if (L::ez(p) == ez && halo_slot<L>(p) == slot) q = p;
+  const long long k = side ? g.nz - 1 : 0;
+  out[e] = fin[pidx<L, S, long long>(q, m + k * sxy, g.qs)];
 }
 
 }  // namespace couplb

@@ -1,0 +1,248 @@
+"""Slab decomposition of a D3Q19 lattice along z.
+
+The reference decomposes the grid over MPI ranks and exchanges the ghost
+planes of the populations every LB step (Streaming::exchange_dim,
+couplb_streaming.h:176-194).  Here each slab is one lattice handle whose
+z faces toward other slabs carry a halo (couplb_halo_attach): before every LB
+step the halo holds the five populations that cross the face, packed by the
+neighbour slab from its boundary plane after its last LB step
+(couplb_halo_pack).  Only those 5 of 19 populations of the interior face
+travel (the reference sends all 19 of the ghost-inclusive face).
+
+- ``partition`` / ``neighbours`` / ``crossing`` are the plan (pure functions,
+  tested on the CPU);
+- ``exchange`` moves the packed planes between ranks with torch.distributed
+  (NCCL for device tensors, gloo for host tensors);
+- ``SlabLattice`` runs all slabs of a lattice in one process (on one device
+  or several), moving the planes with device copies; its results are those
+  of the whole lattice, bit for bit;
+- ``RankSlab`` is the slab of one rank of a process group (one GPU per rank),
+  exchanging with ``exchange``.
+
+The immersed-boundary coupling is not decomposed: a lattice with a halo face
+refuses IBM sub-steps.
+"""
+import numpy as np
+
+from .lattice import Lattice
+
+# D3Q19 velocities in the reference's q order (couplb_lattice.h:44-75)
+EZ = (0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1)
+
+
+def crossing(ez):
+    """Populations that cross a z face moving in direction ez (+1 / -1), in
+    the slot order of a packed halo."""
+    return [q for q in range(19) if EZ[q] == ez]
+
+
+def partition(nz, nslab):
+    """(z0, nz_local) of each slab: nz planes split as evenly as possible."""
+    if nslab < 1 or nslab > nz:
+        raise ValueError(f"cannot split {nz} planes into {nslab} slabs")
+    base, extra = divmod(nz, nslab)
+    out, z0 = [], 0
+    for s in range(nslab):
+        n = base + (1 if s < extra else 0)
+        out.append((z0, n))
+        z0 += n
+    return out
+
+
+def neighbours(slab, nslab, periodic_z):
+    """(below, above): the slab across the low and the high z face, or None
+    at a wall (non-periodic global z) or when one slab wraps onto itself."""
+    if nslab == 1:
+        return None, None
+    below = slab - 1 if slab > 0 else (nslab - 1 if periodic_z else None)
+    above = slab + 1 if slab < nslab - 1 else (0 if periodic_z else None)
+    return below, above
+
+
+def slab_walls(wall, slab, nslab):
+    """Wall types of a slab: the global x and y faces; a z face is the
+    global wall at the ends of a non-periodic z and periodic (a halo or,
+    for a single slab, the self wrap) elsewhere."""
+    w = list(wall)
+    if slab > 0:
+        w[4] = 0
+    if slab < nslab - 1:
+        w[5] = 0
+    return tuple(w)
+
+
+def exchange(dist, rank, world, periodic_z, send_lo, send_hi, recv_lo, recv_hi):
+    """One halo exchange of a rank's slab over torch.distributed: send_hi
+    (the planes leaving through the high face) goes to the slab above, whose
+    recv_lo receives it; send_lo to the slab below, into its recv_hi.  Any
+    argument for a face without a neighbour is ignored.  Every rank calls it
+    at the same point of every step."""
+    below, above = neighbours(rank, world, periodic_z)
+    # upward flow first, then downward, on every rank: with two ranks on a
+    # periodic z the neighbour above is also the one below, and messages of
+    # one pair match in the order they are posted (tags 0 / 1 for backends
+    # that use them)
+    ops = []
+    if above is not None:
+        ops.append(dist.P2POp(dist.isend, send_hi, above, tag=0))
+    if below is not None:
+        ops.append(dist.P2POp(dist.irecv, recv_lo, below, tag=0))
+    if below is not None:
+        ops.append(dist.P2POp(dist.isend, send_lo, below, tag=1))
+    if above is not None:
+        ops.append(dist.P2POp(dist.irecv, recv_hi, above, tag=1))
+    if ops:
+        for r in dist.batch_isend_irecv(ops):
+            r.wait()
+
+
+def _gravity(g_lb):
+    return None if g_lb is None else tuple(g_lb)
+
+
+class SlabLattice:
+    """A D3Q19 lattice of nz planes run as `nslab` z slabs in one process.
+
+    devices: one CUDA device per slab (default: all on device 0); with several
+    devices the planes move by peer copies.  All slabs of one device share
+    that device's current torch stream, so the packs of a step are ordered
+    after every slab's LB step and before the next step."""
+
+    def __init__(self, nx, ny, nz, nslab, tau=0.8, rho0=1.0, wall=(0,) * 6, wall_vel=(0.0, 0.0, 0.0),
+                 body_force=False, precision="fp64", devices=None):
+        import torch
+        self.torch = torch
+        self.n = (nx, ny, nz)
+        self.nslab = nslab
+        self.periodic_z = wall[4] == 0 and wall[5] == 0
+        self.parts = partition(nz, nslab)
+        self.devices = list(devices) if devices is not None else [0] * nslab
+        self.slabs, self.recv = [], []
+        for s, (z0, nzl) in enumerate(self.parts):
+            dev = self.devices[s]
+            L = Lattice(3, nx, ny, nzl, tau=tau, rho0=rho0, wall=slab_walls(wall, s, nslab),
+                        wall_vel=wall_vel, body_force=body_force, precision=precision, device=dev)
+            with torch.cuda.device(dev):
+                L.set_stream(torch.cuda.current_stream().cuda_stream)
+            self.slabs.append(L)
+        nb = int(self.slabs[0].L.couplb_halo_bytes(self.slabs[0].h))
+        for s, L in enumerate(self.slabs):
+            below, above = neighbours(s, nslab, self.periodic_z)
+            bufs = [None, None]
+            for side, nbr in ((0, below), (1, above)):
+                if nbr is None:
+                    continue
+                bufs[side] = torch.zeros(nb, dtype=torch.uint8, device=f"cuda:{self.devices[s]}")
+                L._ck(L.L.couplb_halo_attach(L.h, side, bufs[side].data_ptr()))
+            self.recv.append(bufs)
+        self.stage = [torch.empty(nb, dtype=torch.uint8, device=f"cuda:{d}") for d in self.devices]
+
+    def close(self):
+        for L in self.slabs:
+            L.close()
+        self.slabs = []
+
+    def _exchange(self):
+        """Pack every slab's leaving planes into its neighbours' halos."""
+        torch = self.torch
+        for s, L in enumerate(self.slabs):
+            below, above = neighbours(s, self.nslab, self.periodic_z)
+            for side, nbr in ((1, above), (0, below)):
+                if nbr is None:
+                    continue
+                dst = self.recv[nbr][1 - side]
+                if self.devices[nbr] == self.devices[s]:
+                    L._ck(L.L.couplb_halo_pack(L.h, side, dst.data_ptr()))
+                else:
+                    L._ck(L.L.couplb_halo_pack(L.h, side, self.stage[s].data_ptr()))
+                    torch.cuda.current_stream(self.devices[s]).synchronize()
+                    dst.copy_(self.stage[s])
+        if len(set(self.devices)) > 1:
+            for d in set(self.devices):
+                torch.cuda.current_stream(d).synchronize()
+
+    def lbm_step(self, g_lb=None):
+        for L in self.slabs:
+            L.lbm_step(_gravity(g_lb))
+        self._exchange()
+
+    def set_populations(self, f):
+        """f: global (19, nz+2, ny+2, nx+2) reference layout."""
+        for (z0, nzl), L in zip(self.parts, self.slabs):
+            L.set_populations(np.ascontiguousarray(f[:, z0:z0 + nzl + 2]))
+
+    def init_equilibrium(self, rho=1.0, ux=0.0, uy=0.0, uz=0.0):
+        for L in self.slabs:
+            L.init_equilibrium(rho, ux, uy, uz)
+
+    def get_populations(self):
+        """Interior populations (19, nz, ny, nx) of the whole lattice."""
+        return np.concatenate([L.get_populations()[:, 1:-1, 1:-1, 1:-1] for L in self.slabs], axis=1)
+
+    def get_macroscopic(self):
+        """Interior rho, ux, uy, uz (nz, ny, nx) after a moment pass."""
+        parts = []
+        for L in self.slabs:
+            L.macroscopic()
+            parts.append([a[1:-1, 1:-1, 1:-1] for a in L.get_macroscopic()])
+        return [np.concatenate([p[c] for p in parts], axis=0) for c in range(4)]
+
+    def diagnostics(self):
+        """(umax, mass, momentum[3]) of the whole lattice: FP64 sums of the
+        slabs' FP64 reductions, the largest speed."""
+        ds = []
+        for L in self.slabs:
+            L.macroscopic()
+            ds.append(L.diagnostics())
+        return (max(d.umax for d in ds), sum(d.mass for d in ds),
+                [sum(d.mom[c] for d in ds) for c in range(3)])
+
+
+class RankSlab:
+    """The slab of this rank in a process group (one GPU per rank): a D3Q19
+    lattice of nz global planes, split over the group's ranks along z.  The
+    halos move with ``exchange`` (NCCL device tensors) after every LB step;
+    diagnostics reduce over the group in FP64."""
+
+    def __init__(self, dist, nx, ny, nz, tau=0.8, rho0=1.0, wall=(0,) * 6, wall_vel=(0.0, 0.0, 0.0),
+                 body_force=False, precision="fp64", device=0):
+        import torch
+        self.torch, self.dist = torch, dist
+        self.rank, self.world = dist.get_rank(), dist.get_world_size()
+        self.periodic_z = wall[4] == 0 and wall[5] == 0
+        self.z0, nzl = partition(nz, self.world)[self.rank]
+        self.L = Lattice(3, nx, ny, nzl, tau=tau, rho0=rho0, wall=slab_walls(wall, self.rank, self.world),
+                         wall_vel=wall_vel, body_force=body_force, precision=precision, device=device)
+        torch.cuda.set_device(device)
+        self.L.set_stream(torch.cuda.current_stream().cuda_stream)
+        nb = int(self.L.L.couplb_halo_bytes(self.L.h))
+        mk = lambda: torch.zeros(nb, dtype=torch.uint8, device=f"cuda:{device}")  # noqa: E731
+        self.send = [mk(), mk()]
+        self.recv = [mk(), mk()]
+        below, above = neighbours(self.rank, self.world, self.periodic_z)
+        for side, nbr in ((0, below), (1, above)):
+            if nbr is not None:
+                self.L._ck(self.L.L.couplb_halo_attach(self.L.h, side, self.recv[side].data_ptr()))
+        self.nbrs = (below, above)
+
+    def lbm_step(self, g_lb=None):
+        L = self.L
+        L.lbm_step(_gravity(g_lb))
+        for side in (0, 1):
+            if self.nbrs[side] is not None:
+                L._ck(L.L.couplb_halo_pack(L.h, side, self.send[side].data_ptr()))
+        exchange(self.dist, self.rank, self.world, self.periodic_z, self.send[0], self.send[1],
+                 self.recv[0], self.recv[1])
+
+    def diagnostics(self):
+        torch = self.torch
+        self.L.macroscopic()
+        d = self.L.diagnostics()
+        t = torch.tensor([d.mass, d.mom[0], d.mom[1], d.mom[2]], dtype=torch.float64, device="cuda")
+        self.dist.all_reduce(t)
+        u = torch.tensor([d.umax], dtype=torch.float64, device="cuda")
+        self.dist.all_reduce(u, op=self.dist.ReduceOp.MAX)
+        return float(u.item()), float(t[0].item()), [float(x) for x in t[1:].tolist()]
+
+    def close(self):
+        self.L.close()

@@ -148,6 +148,28 @@ size_t couplb_ghost_nodes(const couplb_handle* h);   /* G */
  * style is set (fix_couplb.cpp:686). */
 int  couplb_lbm_step(couplb_handle* h, const double* g_lb);
 
+/* Slab decomposition along z (the populations part of
+ * Streaming::exchange_dim, couplb_streaming.h:176-194, for d = z): a lattice
+ * that is one z slab of a larger one, with a neighbour subdomain across one
+ * or both z faces.  couplb_halo_attach binds to face `side` (0: z low,
+ * 1: z high; the face must be periodic, COUPLB_WALL_PERIODIC) a device
+ * buffer of couplb_halo_bytes that holds, before every LB step, the
+ * populations that cross that face from the neighbour: the buffer
+ * couplb_halo_pack(neighbour, 1 - side, buf) wrote after the neighbour's last
+ * LB step (5 planes of nx * ny values in the storage format).  The pull of a
+ * source beyond an attached face reads that buffer instead of wrapping onto
+ * this lattice's other face, so the slabs step exactly like the whole
+ * lattice.  NULL detaches.  The caller moves the buffers between slabs (a
+ * device copy, a peer copy or an NCCL send / receive) between LB steps.  The
+ * first LB step after couplb_set_populations or couplb_init_equilibrium reads
+ * the post-stream state in place and needs no halo; pack needs the
+ * post-collision state of an LB step.  Ghost values of attached faces in
+ * couplb_get_populations are not the neighbour's.  IBM sub-steps on a lattice
+ * with an attached face return COUPLB_ERR_UNSUPPORTED. */
+int  couplb_halo_attach(couplb_handle* h, int side, const void* d_recv);
+size_t couplb_halo_bytes(const couplb_handle* h);
+int  couplb_halo_pack(couplb_handle* h, int side, void* d_send);
+
 /* Grid::compute_macroscopic(false) (couplb_lattice.h:155-202) followed by
  * Streaming::exchange_velocity (couplb_streaming.h:140-143). */
 int  couplb_macroscopic(couplb_handle* h);
