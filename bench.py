@@ -57,11 +57,13 @@ def parse():
                     help="LB steps of the 192^3 sphere-drag runs of the IBM methods (0 = skip)")
     ap.add_argument("--kernel", type=int, default=-1,
                     help="fused-kernel variant: -1 auto, 0 plain, 2 packed")
-    ap.add_argument("--only", choices=["fp64", "fp32", "fp16", "ibm", "rods", "methods"], default=None,
+    ap.add_argument("--only", choices=["fp64", "fp32", "fp16", "ibm", "rods", "methods", "train"], default=None,
                     help="time the fused kernel of one precision only, (ibm) the FP32 LBM + "
                          "IBM point-marker cycles only, (rods) the FP32 rod cycles only, or "
                          "(methods) the IBM call of the "
-                         "sphere-drag methods with an untrained network (profiling runs)")
+                         "sphere-drag methods with an untrained network, or (train) network "
+                         "training on --train-rows synthetic rows for --steps epochs (profiling runs)")
+    ap.add_argument("--train-rows", type=int, default=262144, help="rows of --only train")
     ap.add_argument("--rods-box", type=int, nargs=3, default=[512, 256, 256],
                     help="box of --only rods (profiling of smaller cases)")
     ap.add_argument("--rods-count", type=int, default=1000, help="rods of --only rods")
@@ -756,6 +758,26 @@ def main():
             c.close()
         net.close()
         print(json.dumps({"only": "methods", "ms_ibm": out}), flush=True)
+        return
+    if args.only == "train":
+        # the training kernels alone: seeded rows of the network's shape
+        from couplb_b200.mlp import CorrectionNet
+        rng = np.random.default_rng(1)
+        rows = np.zeros((args.train_rows, 88), np.float32)
+        rows[:, :84] = 0.01 * rng.standard_normal((args.train_rows, 84))
+        rows[:, 84:87] = 0.003 * rng.standard_normal((args.train_rows, 3))
+        d = torch.from_numpy(rows).cuda()
+        net = CorrectionNet(local, seed=1)
+        net.fit_scales(d.data_ptr(), args.train_rows)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        tl, vl = net.train(d.data_ptr(), args.train_rows, epochs=args.steps, batch=4096, n_val=4096)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        net.close()
+        print(json.dumps({"only": "train", "rows": args.train_rows, "epochs": args.steps, "s": dt,
+                          "row_updates_per_s": args.train_rows * args.steps / dt, "train_loss": tl,
+                          "val_loss": vl}), flush=True)
         return
     if args.only == "ibm":
         r = ibm_bench(torch, local, "fp32", args.ibm_cycles, args.warmup, load_peak()[0], n=args.ibm_n)
