@@ -676,12 +676,13 @@ def cpu_model():
 
 
 # DRAM bytes (read + write) of one launch of the fused FP32 kernel on the
-# 256x128x128 channel, taken from an ncu capture of a steady-state launch
-# (dram__bytes_read.sum + dram__bytes_write.sum, the launch after 20 warm-up
-# launches, so that the writes of earlier launches still dirty in L2 are
-# counted as they are evicted).  A constant of that capture, not measured by
+# 256x128x128 channel, from an ncu capture of the launch after 25 others
+# (dram__bytes_read.sum 335.6 MB + dram__bytes_write.sum 290.0 MB).  ncu
+# empties L2 before the captured launch, so its own writes still dirty in L2
+# at its end (~46 MB) are missing; in a run they are written during the next
+# launch (steady state ~671 MB).  A constant of that capture, not measured by
 # this run: the line labels it so.
-NCU_TRAFFIC_FP32 = None
+NCU_TRAFFIC_FP32 = 335.6e6 + 290.0e6
 
 
 def run_reference(args):
@@ -838,8 +839,9 @@ def main():
     mlups = world * N / (ms32 * 1e-3) / 1e6
     achieved = BYTES_PER_LU["fp32"] * N / (ms32 * 1e-3) / 1e9
     traffic = NCU_TRAFFIC_FP32 if (nx, ny, nz) == (NX, NY, NZ) else None
-    traffic_src = ("ncu capture of a steady-state launch of this kernel and workload "
-                   "(dram__bytes_read.sum + dram__bytes_write.sum); a constant, not measured by this run"
+    traffic_src = ("ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of the 26th launch of this "
+                   "kernel and workload, L2 emptied before it (its ~46 MB of writes still in L2 at its end "
+                   "are not counted; steady state ~671 MB); a constant, not measured by this run"
                    if traffic else None)
     line = {
         "metric": "D3Q19 MLUPS: FP32-shifted vs plain FP64 on B200 at <=1e-6 L2 velocity error",
