@@ -34,7 +34,7 @@ def _rank(rank, world, port, out):
 
 def test_timed_value_is_the_max_over_ranks():
     world = 2
-    out = mp.Manager().dict()
+    out = mp.get_context("spawn").Manager().dict()
     mp.start_processes(_rank, args=(world, _free_port(), out), nprocs=world, start_method="spawn")
     assert dict(out) == {0: 2.5, 1: 2.5}
 

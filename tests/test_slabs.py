@@ -87,6 +87,6 @@ def _rank(rank, world, port, periodic, out):
 
 @pytest.mark.parametrize("world,periodic", [(2, True), (2, False), (3, True), (3, False)])
 def test_halo_exchange_delivers_the_neighbour_planes(world, periodic):
-    out = mp.Manager().dict()
+    out = mp.get_context("spawn").Manager().dict()
     mp.start_processes(_rank, args=(world, _free_port(), periodic, out), nprocs=world, start_method="spawn")
     assert dict(out) == {r: True for r in range(world)}
