@@ -637,6 +637,11 @@ int couplb_set_option(couplb_handle* h, const char* name, long long value) {
     h->ibm_window = (int)value;
     return COUPLB_OK;
   }
+  if (!std::strcmp(name, "ibm_group")) {
+    if (value != 8 && value != 32) return fail(h, COUPLB_ERR_ARG, "ibm_group must be 8 or 32");
+    h->ibm_group = (int)value;
+    return COUPLB_OK;
+  }
   if (!std::strcmp(name, "barrier_spin")) {
     if (value < 0 || value > (1LL << 40)) return fail(h, COUPLB_ERR_ARG, "barrier_spin must be 0..2^40");
     h->barrier_spin = value;
@@ -652,6 +657,7 @@ int couplb_get_option(couplb_handle* h, const char* name, long long* value) {
   if (!std::strcmp(name, "ibm_resident")) { *value = h->ibm_resident; return COUPLB_OK; }
   if (!std::strcmp(name, "barrier_spin")) { *value = h->barrier_spin; return COUPLB_OK; }
   if (!std::strcmp(name, "ibm_window")) { *value = h->ibm_window; return COUPLB_OK; }
+  if (!std::strcmp(name, "ibm_group")) { *value = h->ibm_group; return COUPLB_OK; }
   if (!std::strcmp(name, "timeouts")) {
     int rc = set_device(h);
     if (rc) return rc;

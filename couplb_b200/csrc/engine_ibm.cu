@@ -103,8 +103,20 @@ int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, co
     }
     if (method == COUPLB_IBM_SINGLE) {
       if (refresh && !a.all_valid) k_ibm_prefetch<L, S><<<nb, bs, 0, h->stream>>>(a);
-      if (ip.delta == COUPLB_DELTA_ROMA) k_ibm_substep<L, S, 0><<<nb, bs, 0, h->stream>>>(a);
-      else k_ibm_substep<L, S, 1><<<nb, bs, 0, h->stream>>>(a);
+      bool grouped = false;
+      if constexpr (L::D == 3) {
+        if (h->ibm_group == 8) {
+          // four markers per warp of 8 lanes each: 32 markers per block
+          const unsigned nb8 = (unsigned)(((long long)n + 31) / 32);
+          if (ip.delta == COUPLB_DELTA_ROMA) k_ibm_substep8<L, S, 0><<<nb8, bs, 0, h->stream>>>(a);
+          else k_ibm_substep8<L, S, 1><<<nb8, bs, 0, h->stream>>>(a);
+          grouped = true;
+        }
+      }
+      if (!grouped) {
+        if (ip.delta == COUPLB_DELTA_ROMA) k_ibm_substep<L, S, 0><<<nb, bs, 0, h->stream>>>(a);
+        else k_ibm_substep<L, S, 1><<<nb, bs, 0, h->stream>>>(a);
+      }
     } else {
       PassState* ps = (PassState*)h->d_pass;
       h->pass_cur ^= 1;

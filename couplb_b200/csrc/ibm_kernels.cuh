@@ -566,6 +566,225 @@ __global__ void __launch_bounds__(256) k_ibm_substep(const IbmArgs<S> a) {
   }
 }
 
+// One row of 4 consecutive record or stencil values (16 B for FP32, 32 B for
+// FP64; record rows are 16-byte aligned).
+__device__ __forceinline__ void load_row4(const float* p, float (&o)[4]) {
+  const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+  o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
+}
+__device__ __forceinline__ void load_row4(const double* p, double (&o)[4]) {
+  const double2 t0 = __ldg(reinterpret_cast<const double2*>(p));
+  const double2 t1 = __ldg(reinterpret_cast<const double2*>(p) + 1);
+  o[0] = t0.x; o[1] = t0.y; o[2] = t1.x; o[3] = t1.y;
+}
+
+// One axis of a window node: ghost-inclusive index b + o (b = i0 - 1), wrapped
+// to its interior image on a wrapped axis.  t: -2 outside the ghost-inclusive
+// box, else the wall type of the ghost plane it lies on (0: none, or a
+// periodic face); i: the interior index of the node or of its periodic image.
+struct AxisNode {
+  int i, t;
+};
+__device__ __forceinline__ AxisNode axis_node(int b, int o, int n, int flo, int fhi, bool wrap) {
+  int ig = b + o;
+  if (wrap) ig = wrap_ghost_index(ig, n);
+  AxisNode r;
+  r.t = (ig < 0 || ig > n + 1) ? -2 : (ig == 0 ? flo : (ig == n + 1 ? fhi : 0));
+  const int i = ig - 1;
+  r.i = i < 0 ? n - 1 : (i >= n ? 0 : i);
+  return r;
+}
+
+// One sub-step of a 3D lattice with eight lanes per marker, four markers per
+// warp.  A marker whose stencil record is valid for this state -- every
+// marker between a refresh and its next move to another cell -- is handled by
+// its group of eight lanes: lane l of the group takes the two window rows
+// (y, z) = (l & 3, l >> 2) and (l & 3, (l >> 2) + 2), four x nodes each, so its
+// record values arrive as six 16-byte loads.  The 1D weights are evaluated
+// once per group (lane l: offset l & 3 of axis x or y, and of axis z) and
+// fetched with shuffles; a node's weight is (wx * wy) * wz.  Window nodes are
+// classified per axis (outside, wall type, periodic image; the type of the
+// last axis whose ghost plane holds a wall wins, as in classify_node), so the
+// clipped and wrapped windows, walls and moving walls follow the warp-per-
+// marker body; the sums are taken over the group's lanes in a fixed order, so
+// results differ from that body only by the order of the sums.  Markers whose
+// record misses (moved to another cell) or that read dense moments run the
+// warp-per-marker body with the whole warp afterwards.  The per-marker work
+// that the 32-lane form repeats in every lane (positions, cell, key, penalty
+// force) is shared by 8 lanes here, and each lane keeps six loads in flight
+// instead of two.
+template <class L, class S, int DELTA>
+__global__ void __launch_bounds__(256) k_ibm_substep8(const IbmArgs<S> a) {
+  static_assert(L::D == 3, "the grouped sub-step is the 3D form");
+  using R = typename S::C;
+  using A = typename S::A;
+  constexpr unsigned kFull = 0xffffffffu;
+  __shared__ double part[8][3];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gl = lane & 7, gb = lane & ~7;
+  const int mk0 = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 4;
+  const int mk = mk0 + (lane >> 3);
+  const Geom& g = a.g;
+  const bool in = mk < a.n;
+  // record rows of this lane, loaded before the key is compared (a miss
+  // discards them)
+  A u[3][2][4];
+  double lx = 0, ly = 0, lz = 0, mass = 0, vm0 = 0, vm1 = 0, vm2 = 0;
+  int i0 = 0, j0 = 0, k0 = 0;
+  bool fast = false, slow = false;
+  const int y = gl & 3, zr = gl >> 2;   // rows (y, zr) and (y, zr + 2)
+  if (in) {
+    const A* rec = stencil_record(a, mk);
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+      for (int r = 0; r < 2; r++) load_row4(rec + 64 * c + 4 * (gl + 8 * r), u[c][r]);
+    const int4 key = __ldg(reinterpret_cast<const int4*>(a.skey + mk));
+    // IBM::phys_to_local (couplb_ibm.h:49-55)
+    lx = (a.x[3 * mk] - a.lo[0]) * a.inv_dx - a.off[0] + 1.0;
+    ly = (a.x[3 * mk + 1] - a.lo[1]) * a.inv_dx - a.off[1] + 1.0;
+    lz = (a.x[3 * mk + 2] - a.lo[2]) * a.inv_dx - a.off[2] + 1.0;
+    mass = a.m[mk];
+    vm0 = a.v[3 * mk]; vm1 = a.v[3 * mk + 1]; vm2 = a.v[3 * mk + 2];
+    const bool valid = !(a.active && !a.active[mk]);
+    i0 = (int)floor(lx); j0 = (int)floor(ly); k0 = (int)floor(lz);
+    const bool hit = (unsigned)key.w == a.cur_epoch && key.x == i0 && key.y == j0 && key.z == k0;
+    fast = valid && hit && !a.all_valid;
+    slow = valid && !fast;
+    // an atom outside the group: zero force unless accumulating
+    if (!valid && !a.accumulate && gl < 3) a.fout[3 * mk + gl] = 0.0;
+  }
+  // 1D weights of the group: lane l holds offset l & 3 of axis x (l < 4) or y
+  // (w1), and of axis z (w2)
+  const R w1 = delta1<DELTA, R>(R((gl < 4 ? lx : ly) - ((gl < 4 ? i0 : j0) - 1 + (gl & 3))));
+  const R w2 = delta1<DELTA, R>(R(lz - (k0 - 1 + (gl & 3))));
+  R wx[4];
+#pragma unroll
+  for (int o = 0; o < 4; o++) wx[o] = __shfl_sync(kFull, w1, gb + o);
+  const R wy = __shfl_sync(kFull, w1, gb + 4 + y);
+  const R wz[2] = {__shfl_sync(kFull, w2, gb + zr), __shfl_sync(kFull, w2, gb + zr + 2)};
+  // classification of the lane's nodes: x offsets (shared by both rows), its
+  // y, its two z
+  AxisNode nx4[4], ny1, nz2[2];
+#pragma unroll
+  for (int o = 0; o < 4; o++) nx4[o] = axis_node(i0 - 1, o, g.nx, g.face[0], g.face[1], a.wrap & 1);
+  ny1 = axis_node(j0 - 1, y, g.ny, g.face[2], g.face[3], a.wrap & 2);
+#pragma unroll
+  for (int r = 0; r < 2; r++) nz2[r] = axis_node(k0 - 1, zr + 2 * r, g.nz, g.face[4], g.face[5], a.wrap & 4);
+  R d[2][4];
+  int t[2][4];   // -2 not in the window sums, -1 fluid, else wall type
+  R ui = 0, vi = 0, wi = 0, ws = 0, wss = 0;
+  bool wall_seen = false;
+#pragma unroll
+  for (int r = 0; r < 2; r++)
+#pragma unroll
+    for (int o = 0; o < 4; o++) {
+      d[r][o] = (wx[o] * wy) * wz[r];
+      const bool outside = nx4[o].t == -2 || ny1.t == -2 || nz2[r].t == -2;
+      const int tw = nz2[r].t ? nz2[r].t : (ny1.t ? ny1.t : nx4[o].t);
+      t[r][o] = outside ? -2 : (tw ? tw : -1);
+      const R dd = d[r][o];
+      if (t[r][o] == -1) {
+        ui += R(u[0][r][o]) * dd;
+        vi += R(u[1][r][o]) * dd;
+        wi += R(u[2][r][o]) * dd;
+        ws += dd;
+        wss += dd;
+      } else if (t[r][o] == 1 || t[r][o] == 3) {
+        ws += dd;
+        wall_seen = true;
+      } else if (t[r][o] == 2) {
+        ui += R(g.uw[0]) * dd;
+        vi += R(g.uw[1]) * dd;
+        wi += R(g.uw[2]) * dd;
+        ws += dd;
+        wall_seen = true;
+      }
+    }
+  // without wall nodes in the window ws and wss are the same sums
+  const bool walls = __any_sync(kFull, wall_seen && fast);
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) {
+    ui += __shfl_xor_sync(kFull, ui, o);
+    vi += __shfl_xor_sync(kFull, vi, o);
+    wi += __shfl_xor_sync(kFull, wi, o);
+    ws += __shfl_xor_sync(kFull, ws, o);
+  }
+  if (walls) {
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) wss += __shfl_xor_sync(kFull, wss, o);
+  } else {
+    wss = ws;
+  }
+  double tot0 = 0, tot1 = 0, tot2 = 0;
+  if (fast) {
+    double u0 = 0, u1 = 0, u2 = 0;
+    if (ws > R(DELTA_TOL)) {
+      const R iw = R(1) / ws;
+      u0 = double(ui * iw); u1 = double(vi * iw); u2 = double(wi * iw);
+    }
+    // penalty force (fix_couplb.cpp:777-781)
+    const double F0 = mass * a.xi_over_dt * (u0 * a.vs - vm0);
+    const double F1 = mass * a.xi_over_dt * (u1 * a.vs - vm1);
+    const double F2 = mass * a.xi_over_dt * (u2 * a.vs - vm2);
+    if (gl == 0) {
+      if (a.accumulate) {
+        a.fout[3 * mk] += F0; a.fout[3 * mk + 1] += F1; a.fout[3 * mk + 2] += F2;
+      } else {
+        a.fout[3 * mk] = F0; a.fout[3 * mk + 1] = F1; a.fout[3 * mk + 2] = F2;
+      }
+      if (a.corr) { a.corr[3 * mk] = 0.0; a.corr[3 * mk + 1] = 0.0; a.corr[3 * mk + 2] = 0.0; }
+    }
+    // spread -F/(N * force_scale) onto the fluid nodes (fix_couplb.cpp:788-792,
+    // couplb_ibm.h:124-132)
+    if (!(wss < R(DELTA_TOL))) {
+      const R sc = R(a.dvr) / wss;
+      const double fl0 = -F0 * a.spread_c, fl1 = -F1 * a.spread_c, fl2 = -F2 * a.spread_c;
+      const R f0 = R(fl0), f1 = R(fl1), f2 = R(fl2);
+      const bool xrow = nx4[0].t == 0 && nx4[3].t == 0 && nx4[3].i == nx4[0].i + 3;
+#pragma unroll
+      for (int r = 0; r < 2; r++) {
+        const long long nyz = (long long)g.nx * ((long long)ny1.i + (long long)g.ny * nz2[r].i);
+#pragma unroll
+        for (int o = 0; o < 4; o++) {
+          if (t[r][o] != -1) continue;
+          const long long nn = nyz + nx4[o].i;
+          const R w = d[r][o] * sc;   // couplb_ibm.h:128
+          spread_add(a.F + 4 * nn, f0 * w, f1 * w, f2 * w);
+          if (a.seg_force && !xrow) a.seg_force[nn >> 3] = 1;
+        }
+        if (a.seg_force && xrow && t[r][0] == -1) {
+          const long long n0 = nyz + nx4[0].i;
+          a.seg_force[n0 >> 3] = 1;
+          a.seg_force[(n0 + 3) >> 3] = 1;
+        }
+      }
+      if (gl == 0) { tot0 = fl0 * a.dvr; tot1 = fl1 * a.dvr; tot2 = fl2 * a.dvr; }
+    }
+  }
+  // markers whose record missed, one at a time with the whole warp
+  unsigned todo = __ballot_sync(kFull, slow && gl == 0);
+  while (todo) {
+    const int b = __ffs(todo) - 1;
+    todo &= todo - 1;
+    double t3[3] = {0.0, 0.0, 0.0};
+    ibm_substep_body<L, S, DELTA, false>(a, mk0 + (b >> 3), lane, false, nullptr, nullptr, t3);
+    if (lane == 0) { tot0 += t3[0]; tot1 += t3[1]; tot2 += t3[2]; }
+  }
+  if (!a.ftot) return;
+  // the warp's total: group leaders (lanes 0, 8, 16, 24), then the block's
+  tot0 += __shfl_xor_sync(kFull, tot0, 8); tot0 += __shfl_xor_sync(kFull, tot0, 16);
+  tot1 += __shfl_xor_sync(kFull, tot1, 8); tot1 += __shfl_xor_sync(kFull, tot1, 16);
+  tot2 += __shfl_xor_sync(kFull, tot2, 8); tot2 += __shfl_xor_sync(kFull, tot2, 16);
+  if (lane == 0) { part[warp][0] = tot0; part[warp][1] = tot1; part[warp][2] = tot2; }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double sum = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) sum += part[w][threadIdx.x];
+    atomicAdd(a.ftot + 4 * (blockIdx.x & (kFtotSlots - 1)) + threadIdx.x, sum);
+  }
+}
+
 // Dynamic shared memory of the learned sub-step kernels (blocks of 8 warps):
 // the packed network, then the block's forward-pass scratch.
 constexpr size_t kLearnedSmem = sizeof(MlpPacked) + sizeof(MlpBlockScratch);

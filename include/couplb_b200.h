@@ -379,6 +379,11 @@ int  couplb_status_last(couplb_handle* h, int* clamps, int* nonfinite);
  *                 (every window node is used, through its interior image) --
  *                 for physics runs; results then differ from the reference's
  *                 near those faces.
+ *   "ibm_group"   lanes per marker of the SINGLE-pass sub-step of a 3D lattice:
+ *                 8 (default; four markers per warp, for markers whose window
+ *                 lies inside the interior and whose stencil is cached, the
+ *                 rest one warp each) or 32 (one warp per marker).  The two
+ *                 differ only in the order of the interpolation sums.
  *   "barrier_spin" poll limit of each grid-wide barrier of the ITERATIVE /
  *                 LEARNED sub-step kernels (default 2^21 polls of ~100 ns).
  *                 A block whose barrier runs out counts a timeout and returns;

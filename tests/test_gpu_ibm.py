@@ -234,3 +234,84 @@ def test_wrapped_window_matches_oracle(cuda_lib, wall):
     for c in range(3):
         a, b = cases.interior(Fg[c], 3), cases.interior(Fo[c], 3)
         assert rel(a, b) <= 1e-12, (c, rel(a, b))
+
+
+def _grouped_case(prec, group, n=(40, 32, 24), cycles=3, md_per_lb=2):
+    """Atom forces per sub-step and the final force field of a walled lattice
+    with 300 markers: most windows inside the interior, some at the faces and
+    walls; every second marker jumps 0.6 cells in x on each later sub-step
+    (a stencil-record miss); one marker in eight is not in the group."""
+    rng = np.random.default_rng(19)
+    x0 = rng.uniform(0.0, 1.0, (300, 3)) * np.array(n, float)
+    x0[:20, 1] = rng.uniform(0.0, 2.5, 20)
+    x0[20:40, 2] = n[2] - rng.uniform(0.0, 2.5, 20)
+    v = 0.01 * rng.standard_normal((300, 3))
+    m = rng.uniform(0.5, 1.5, 300)
+    active = (np.arange(300) % 8 != 3).astype(np.int32)
+    L = Lattice(3, *n, tau=0.7, wall=(0, 0, 1, 2, 0, 0), wall_vel=(0.01, 0, 0), body_force=True, precision=prec)
+    L.set_option("ibm_group", group)
+    L.set_populations(cases.initial_populations(3, n, 7))
+    L.set_ibm_params(delta="peskin4", md_per_lb=md_per_lb, xi_ibm=0.8)
+    x = x0.copy()
+    fs = []
+    for c in range(cycles):
+        L.lbm_step((1e-5, 0.0, 2e-6))
+        for s in range(md_per_lb):
+            if s > 0:
+                x[::2, 0] += 0.6
+            x = np.ascontiguousarray(np.mod(x + 0.3 * v, np.array(n, float)))
+            fa = np.zeros_like(x)
+            L.ibm_substep(x, v, m, fa, active=active, refresh=(s == 0))
+            fs.append(fa)
+    F = [cases.interior(a, 3) for a in L.get_force_field()]
+    L.close()
+    return np.stack(fs), F
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-13), ("fp32", 2e-6)])
+def test_grouped_substep_matches_warp_per_marker(cuda_lib, prec, tol):
+    """ibm_group 8 (four markers per warp, the default) against 32 (one warp
+    per marker): the same forces up to the order of the interpolation sums."""
+    f8, F8 = _grouped_case(prec, 8)
+    f32, F32 = _grouped_case(prec, 32)
+    assert rel(f8, f32) <= tol, rel(f8, f32)
+    for c in range(3):
+        assert rel(F8[c], F32[c]) <= 10 * tol, (c, rel(F8[c], F32[c]))
+
+
+def test_grouped_substep_fp64_matches_oracle(cuda_lib):
+    """The grouped sub-step (interior markers, record hits and misses,
+    inactive atoms, walls) against the oracle: per-atom forces within 1e-11,
+    force field within 1e-12, over two LB cycles."""
+    from oracle.bindings import OracleGrid
+    n = (40, 32, 24)
+    fg, Fg = _grouped_case("fp64", 8, n=n, cycles=2)
+    rng = np.random.default_rng(19)
+    x0 = rng.uniform(0.0, 1.0, (300, 3)) * np.array(n, float)
+    x0[:20, 1] = rng.uniform(0.0, 2.5, 20)
+    x0[20:40, 2] = n[2] - rng.uniform(0.0, 2.5, 20)
+    v = 0.01 * rng.standard_normal((300, 3))
+    m = rng.uniform(0.5, 1.5, 300)
+    active = (np.arange(300) % 8 != 3).astype(np.int32)
+    O = OracleGrid(3, *n, tau=0.7, wall=(0, 0, 1, 2, 0, 0), wall_vel=(0.01, 0, 0))
+    O.set_f(cases.initial_populations(3, n, 7))
+    ip = abi.IbmParams()
+    ip.delta, ip.md_per_lb, ip.xi_ibm = 1, 2, 0.8
+    ip.dt_lbm, ip.dx, ip.vel_scale, ip.force_scale = 1.0, 1.0, 1.0, 1.0
+    x = x0.copy()
+    fo = []
+    for c in range(2):
+        O.lbm_step((1e-5, 0.0, 2e-6))
+        for s in range(2):
+            if s > 0:
+                x[::2, 0] += 0.6
+            x = np.ascontiguousarray(np.mod(x + 0.3 * v, np.array(n, float)))
+            fa = np.zeros_like(x)
+            O.ibm_substep(ip, x, v, m, fa, active=active, refresh=(s == 0), fold=(s == 1))
+            fo.append(fa)
+    Fo = [cases.interior(a, 3) for a in O.get_force()]
+    O.close()
+    fo = np.stack(fo)
+    assert rel(fg, fo) <= 1e-11, rel(fg, fo)
+    for c in range(3):
+        assert rel(Fg[c], Fo[c]) <= 1e-12, (c, rel(Fg[c], Fo[c]))
