@@ -127,8 +127,11 @@ int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, co
       P.ps_next = ps + (h->pass_cur ^ 1);
       P.fill = refresh && !a.all_valid;
       P.status = h->d_status;
-      P.ncorr = h->ibm_passes - 1;
-      P.check_first = method == COUPLB_IBM_LEARNED;
+      // LEARNED with slip_tol >= kNoFallback never falls back: no check, no
+      // corrections
+      P.check_first = method == COUPLB_IBM_LEARNED && h->slip_tol < kNoFallback;
+      P.ncorr = (method == COUPLB_IBM_LEARNED && !P.check_first) ? 0 : h->ibm_passes - 1;
+      P.measure_last = h->ibm_slip;
       P.slip_tol = h->slip_tol;
       for (int d = 0; d < 3; d++) P.g_lb[d] = h->g_lb[d];
       P.rows = record ? h->rec_rows + h->rec_count * kMlpRow : nullptr;

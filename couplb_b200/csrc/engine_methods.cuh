@@ -31,9 +31,23 @@ int coop_resident(couplb_handle* h, K kern, size_t smem, int slot, int* out) {
 }
 }  // namespace eng
 
-// Cooperative launch of one ITERATIVE / LEARNED sub-step (all blocks
-// resident at once, which its grid barriers need).  In 3D, when every marker
-// gets a warp of its own, the register-resident form runs.
+// Launch of one ITERATIVE / LEARNED sub-step: cooperative (all blocks
+// resident at once) when the launch has a grid barrier, a plain launch of the
+// same grid when it has none (one pass, no slip check, no slip statistics).
+// In 3D, when every marker gets a warp of its own, the register-resident form
+// runs.
+template <class K, class A>
+int launch_coop_or_plain(couplb_handle* h, K kern, unsigned grid, size_t smem, bool barrier, A& P) {
+  using namespace eng;
+  if (barrier) {
+    void* args[] = {&P};
+    CK(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(256), args, smem, h->stream));
+  } else {
+    kern<<<grid, 256, smem, h->stream>>>(P);
+  }
+  return COUPLB_OK;
+}
+
 template <class L, class S>
 int launch_method(couplb_handle* h, PassArgs<S>& P, int delta, bool learned, int n) {
   using namespace eng;
@@ -42,18 +56,14 @@ int launch_method(couplb_handle* h, PassArgs<S>& P, int delta, bool learned, int
   const int di = (learned ? 2 : 0) + (roma ? 0 : 1);
   const size_t smem = learned ? kLearnedSmem : 0;
   const long long want = ((long long)n * 32 + 255) / 256;
-  void* args[] = {&P};
+  const bool barrier = P.check_first || P.ncorr > 0 || P.measure_last;
   int rc, resident = 0;
   if constexpr (L::D == 3) {
     if (h->ibm_resident) {
       K kr = learned ? (roma ? k_ibm_method_resident<L, S, 0, true> : k_ibm_method_resident<L, S, 1, true>)
                      : (roma ? k_ibm_method_resident<L, S, 0, false> : k_ibm_method_resident<L, S, 1, false>);
       if ((rc = coop_resident(h, kr, smem, 4 + di, &resident))) return rc;
-      if (want <= resident) {
-        CK(cudaLaunchCooperativeKernel((const void*)kr, dim3((unsigned)want), dim3(256), args, smem,
-                                       h->stream));
-        return COUPLB_OK;
-      }
+      if (want <= resident) return launch_coop_or_plain(h, kr, (unsigned)want, smem, barrier, P);
     }
   }
   K kern = nullptr;
@@ -65,8 +75,7 @@ int launch_method(couplb_handle* h, PassArgs<S>& P, int delta, bool learned, int
   if (!kern) return fail(h, COUPLB_ERR_UNSUPPORTED, "the learned correction is defined for D3Q19");
   if ((rc = coop_resident(h, kern, smem, di, &resident))) return rc;
   const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(want, resident));
-  CK(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(256), args, smem, h->stream));
-  return COUPLB_OK;
+  return launch_coop_or_plain(h, kern, grid, smem, barrier, P);
 }
 
 #endif  // COUPLB_METHODS_IMPL

@@ -31,6 +31,9 @@ enum : int { kStSlipChecks = 4, kStFallbacks = 5 };
 // the handle option "barrier_spin" replaces it (tests drive a barrier to its
 // limit with 0)
 constexpr long long kBarrierSpin = 1LL << 21;
+// slip_tol at or above which the learned method has no fallback (and so no
+// slip check)
+constexpr double kNoFallback = 1e300;
 
 // State of one launch of k_ibm_method.  Two alternate: each launch zeroes the
 // other one for the next launch.
@@ -56,6 +59,7 @@ struct PassArgs {
   int* status;
   int ncorr;            // iterative corrections (passes - 1)
   int check_first;      // learned: slip check first, corrections only above tol
+  int measure_last;     // slip after the last pass into residual 1 (handle option ibm_slip)
   double slip_tol;      // MD velocity units
   double g_lb[3];       // body force of the LB steps, lattice units
   float* rows;          // n x kMlpRow training rows, or null
@@ -379,10 +383,7 @@ __global__ void __launch_bounds__(256) k_ibm_method(const PassArgs<S> P) {
   const int nw = (gridDim.x * blockDim.x) >> 5;
   MlpPacked* net = reinterpret_cast<MlpPacked*>(smem);
   MlpBlockScratch* blk = reinterpret_cast<MlpBlockScratch*>(smem + sizeof(MlpPacked));
-  if (LEARNED) {
-    mlp_stage(net, a.mlp);
-    __syncthreads();
-  }
+  if (LEARNED) mlp_stage_async(net, a.mlp);   // waited for before the first network pass
   if (blockIdx.x == 0) {
     unsigned* z = reinterpret_cast<unsigned*>(P.ps_next);
     for (int i = threadIdx.x; i < (int)(sizeof(PassState) / 4); i += blockDim.x) z[i] = 0u;
@@ -400,7 +401,10 @@ __global__ void __launch_bounds__(256) k_ibm_method(const PassArgs<S> P) {
     ft[0] += t3[0]; ft[1] += t3[1]; ft[2] += t3[2];
   }
   block_add_ftot(a.ftot, ft);
-  if (!grid_barrier(P.ps, P.status, P.spin)) return;
+  // a launch with nothing after the first pass that reads the force field
+  // (no check, no correction, no slip statistics) needs no grid barrier
+  const bool more = P.check_first || P.ncorr > 0 || P.measure_last;
+  if (more && !grid_barrier(P.ps, P.status, P.spin)) return;
   if (P.check_first) {
     for (int mk = gw; mk < a.n; mk += nw)
       if (!a.active || a.active[mk]) measure_marker<L, S, DELTA>(P, mk, lane, 0, &acc);
@@ -448,10 +452,10 @@ __global__ void __launch_bounds__(256) k_ibm_method(const PassArgs<S> P) {
   }
   for (int mk = gw; mk < a.n; mk += nw) {
     if (a.active && !a.active[mk]) continue;
-    measure_marker<L, S, DELTA>(P, mk, lane, 1, &acc);
+    if (P.measure_last) measure_marker<L, S, DELTA>(P, mk, lane, 1, &acc);
     if (P.rows) record_marker<L, S>(P, mk, lane);
   }
-  block_add_slip(P.ps, 1, acc);
+  if (P.measure_last) block_add_slip(P.ps, 1, acc);
 }
 
 // The same sub-step when every marker has a warp of its own (n <= resident
@@ -473,10 +477,12 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
   MlpBlockScratch* blk = reinterpret_cast<MlpBlockScratch*>(smem + sizeof(MlpPacked));
   float* xs = nullptr;
   if (LEARNED) {
-    mlp_stage(net, a.mlp);
+    // the network's copy into shared memory overlaps the stencil fill; the
+    // forward pass waits for it
+    mlp_stage_async(net, a.mlp);
     xs = blk->x + (threadIdx.x >> 5) * kMlpXStride;
     for (int t = lane; t < kMlpXStride; t += 32) xs[t] = 0.f;
-    __syncthreads();
+    __syncwarp();
   }
   if (blockIdx.x == 0) {
     unsigned* z = reinterpret_cast<unsigned*>(P.ps_next);
@@ -683,7 +689,10 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
     __syncthreads();
   };
   spread(F0, F1, F2);
-  if (!grid_barrier(P.ps, P.status, P.spin)) return;
+  // a launch with nothing after the first pass that reads the force field
+  // (no check, no correction, no slip statistics) needs no grid barrier
+  const bool more = P.check_first || P.ncorr > 0 || P.measure_last;
+  if (more && !grid_barrier(P.ps, P.status, P.spin)) return;
   if (P.check_first) {
     measure(0);
     if (!grid_barrier(P.ps, P.status, P.spin)) return;
@@ -719,7 +728,7 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
     if (!grid_barrier(P.ps, P.status, P.spin)) return;
   }
   if (have && lane == 0) { a.corr[3 * mk] = c0; a.corr[3 * mk + 1] = c1; a.corr[3 * mk + 2] = c2; }
-  measure(1);
+  if (P.measure_last) measure(1);
   if (P.rows && have) {
     __syncwarp();
     record_marker<L, S>(P, mk, lane);

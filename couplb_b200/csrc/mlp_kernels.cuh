@@ -49,11 +49,19 @@ __device__ __forceinline__ float bf16_round(float v) {
   return __bfloat162float(__float2bfloat16_rn(v));
 }
 
-// Copy the packed network into shared memory (all threads of the block).
-__device__ __forceinline__ void mlp_stage(MlpPacked* dst, const MlpPacked* __restrict__ src) {
+// Copy the packed network into shared memory (all threads of the block) as
+// asynchronous 16-byte copies (cp.async), so that the kernel's first loads
+// overlap it; mlp_block_forward waits for this thread's
+// copies and its first barrier publishes the block's.  dst and src are
+// 16-byte aligned (MlpPacked is, and so is its slot in dynamic shared memory).
+__device__ __forceinline__ void mlp_stage_async(MlpPacked* dst, const MlpPacked* __restrict__ src) {
   const int4* s = reinterpret_cast<const int4*>(src);
   int4* d = reinterpret_cast<int4*>(dst);
-  for (int i = threadIdx.x; i < (int)(sizeof(MlpPacked) / 16); i += blockDim.x) d[i] = __ldg(s + i);
+  for (int i = threadIdx.x; i < (int)(sizeof(MlpPacked) / 16); i += blockDim.x) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(d + i);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(s + i) : "memory");
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
 // ---- block forward pass on the tensor cores -------------------------------
@@ -110,6 +118,8 @@ __device__ __forceinline__ void mlp_tile(float (&acc)[4], const float* A, int as
   const int g = lane >> 2, t = lane & 3;
   const float* ar = A + g * as + 2 * t;
   const __nv_bfloat16* wr = W + (n0 + g) * ws + 2 * t;
+  // one accumulator per part of the split: three independent MMA chains
+  float ah[4] = {0.f, 0.f, 0.f, 0.f}, am[4] = {0.f, 0.f, 0.f, 0.f}, al[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
   for (int k0 = 0; k0 < K; k0 += 16) {
     const float2 x0 = *reinterpret_cast<const float2*>(ar + k0);
@@ -119,10 +129,12 @@ __device__ __forceinline__ void mlp_tile(float (&acc)[4], const float* A, int as
     split3(x1.x * sa, x1.y * sa, h1, m1, l1);
     const uint32_t b0 = *reinterpret_cast<const uint32_t*>(wr + k0);
     const uint32_t b1 = *reinterpret_cast<const uint32_t*>(wr + k0 + 8);
-    mma_rows8(acc, h0, h1, b0, b1);
-    mma_rows8(acc, m0, m1, b0, b1);
-    mma_rows8(acc, l0, l1, b0, b1);
+    mma_rows8(ah, h0, h1, b0, b1);
+    mma_rows8(am, m0, m1, b0, b1);
+    mma_rows8(al, l0, l1, b0, b1);
   }
+#pragma unroll
+  for (int i = 0; i < 4; i++) acc[i] += ah[i] + (am[i] + al[i]);
 }
 
 // Forward pass of the block's 8 rows (all 256 threads call it, after each
@@ -131,6 +143,9 @@ __device__ __forceinline__ void mlp_tile(float (&acc)[4], const float* A, int as
 __device__ __forceinline__ void mlp_block_forward(const MlpPacked& P, MlpBlockScratch& S, int warp,
                                                   int lane, float y[3]) {
   const int g = lane >> 2, t = lane & 3;
+  // this thread's part of an asynchronous staging of P (mlp_stage_async;
+  // nothing pending otherwise), published to the block by the barrier
+  asm volatile("cp.async.wait_all;" ::: "memory");
   __syncthreads();
   {
     float acc[4] = {0.f, 0.f, 0.f, 0.f};

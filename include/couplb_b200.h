@@ -283,7 +283,9 @@ int  couplb_ibm_total_force(couplb_handle* h, double out[3], int reset);
 #define COUPLB_IBM_ITERATIVE 1  /* passes-1 correction passes, then the slip      */
 #define COUPLB_IBM_LEARNED   2  /* single pass + network correction (D3Q19);
                                    slip check, and the passes-1 corrections run
-                                   when the RMS slip exceeds slip_tol           */
+                                   when the RMS slip exceeds slip_tol; with
+                                   slip_tol >= 1e300 (or +inf) there is no
+                                   fallback and so no check                     */
 
 typedef struct couplb_mlp couplb_mlp;   /* 84-64-64-3 network, BF16 weights */
 
@@ -384,6 +386,10 @@ int  couplb_status_last(couplb_handle* h, int* clamps, int* nonfinite);
  *                 lies inside the interior and whose stencil is cached, the
  *                 rest one warp each) or 32 (one warp per marker).  The two
  *                 differ only in the order of the interpolation sums.
+ *   "ibm_slip"    1 (default): ITERATIVE / LEARNED sub-steps measure the slip
+ *                 after their last pass (couplb_ibm_slip); 0: they do not, which
+ *                 saves an interpolation pass and, for a learned sub-step
+ *                 without fallback, the only grid-wide barrier of the launch.
  *   "barrier_spin" poll limit of each grid-wide barrier of the ITERATIVE /
  *                 LEARNED sub-step kernels (default 2^21 polls of ~100 ns).
  *                 A block whose barrier runs out counts a timeout and returns;

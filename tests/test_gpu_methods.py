@@ -170,6 +170,44 @@ def test_learned_matches_oracle(cuda_lib, tol, fell, resident, delta):
 
 
 @pytest.mark.parametrize("resident", [1, 0])
+def test_learned_without_fallback_runs_no_check(cuda_lib, resident):
+    """slip_tol inf: the learned sub-step cannot fall back, so it runs no
+    slip check (no count, no grid barrier before the statistics); its forces
+    are those of a learned sub-step that never falls back and its slip after
+    the last pass is the oracle's."""
+    L, O, ip = make_pair("fp64", "peskin4")
+    L.set_option("ibm_resident", resident)
+    w = random_net(3)
+    s = (250.0, 400.0)
+    net = CorrectionNet(0, seed=1)
+    net.set_weights(w.astype(np.float32), *s)
+    L.set_ibm_method("learned", passes=4, slip_tol=float("inf"), model=net)
+    for fg, fo, sl, st in run_steps(L, O, ip, 2, 4, 2, slip_tol=1e300, w=w, s=s):
+        assert rel(fg, fo) <= 1e-5, rel(fg, fo)
+        assert sl["fell_back"] == 0 == st[4]
+        assert abs(sl["rms"] - st[2]) <= 1e-4 * st[2]
+    assert L.ibm_slip()["checks"] == 0
+    L.close()
+    net.close()
+
+
+@pytest.mark.parametrize("resident", [1, 0])
+def test_slip_statistics_off_keeps_the_forces(cuda_lib, resident):
+    """Handle option ibm_slip 0: the iterative sub-step skips the slip
+    measurement after its last pass (no markers counted) and its forces still
+    match the oracle."""
+    L, O, ip = make_pair("fp64", "roma")
+    L.set_option("ibm_resident", resident)
+    L.set_ibm_method("iterative", passes=3)
+    L.set_option("ibm_slip", 0)
+    assert L.get_option("ibm_slip") == 0
+    for fg, fo, sl, st in run_steps(L, O, ip, 1, 3, 2):
+        assert rel(fg, fo) <= 1e-10, rel(fg, fo)
+        assert sl["markers"] == 0
+    L.close()
+
+
+@pytest.mark.parametrize("resident", [1, 0])
 def test_record_rows_match_oracle(cuda_lib, resident):
     import torch
     L, O, ip = make_pair("fp64", "roma", wall=(0,) * 6)
