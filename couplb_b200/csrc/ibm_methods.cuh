@@ -559,7 +559,8 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
       if (lane == 0) a.skey[mk] = StencilKey{w.i0, w.j0, w.k0, a.cur_epoch};
     }
     ui += uwx; vi += uwy; wi += uwz;
-#pragma unroll
+    // not unrolled: this launch runs once per SM and waits on instruction fetch
+#pragma unroll 1
     for (int o = 16; o > 0; o >>= 1) {
       ui += __shfl_xor_sync(0xffffffffu, ui, o);
       vi += __shfl_xor_sync(0xffffffffu, vi, o);

@@ -111,16 +111,18 @@ __device__ __forceinline__ void mma_rows8(float (&d)[4], uint32_t a0, uint32_t a
 
 // acc (8 x 8 tile: rows = the block's markers, columns = 8 outputs starting at
 // row n0 of W) += A[8][K] W^T, A FP32 rows of stride as (scaled by sa), W BF16
-// rows of stride ws.
-template <int K>
+// rows of stride ws.  K is a runtime multiple of 16 and the k loop is not
+// unrolled: the sub-step kernels that call this run once per SM per launch,
+// and their time goes to fetching instructions, so one compact loop body
+// serves all three layers.
 __device__ __forceinline__ void mlp_tile(float (&acc)[4], const float* A, int as, float sa,
-                                         const __nv_bfloat16* W, int ws, int n0, int lane) {
+                                         const __nv_bfloat16* W, int ws, int n0, int K, int lane) {
   const int g = lane >> 2, t = lane & 3;
   const float* ar = A + g * as + 2 * t;
   const __nv_bfloat16* wr = W + (n0 + g) * ws + 2 * t;
   // one accumulator per part of the split: three independent MMA chains
   float ah[4] = {0.f, 0.f, 0.f, 0.f}, am[4] = {0.f, 0.f, 0.f, 0.f}, al[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
+#pragma unroll 1
   for (int k0 = 0; k0 < K; k0 += 16) {
     const float2 x0 = *reinterpret_cast<const float2*>(ar + k0);
     const float2 x1 = *reinterpret_cast<const float2*>(ar + k0 + 8);
@@ -140,6 +142,8 @@ __device__ __forceinline__ void mlp_tile(float (&acc)[4], const float* A, int as
 // Forward pass of the block's 8 rows (all 256 threads call it, after each
 // warp has written its row of S.x); every lane of warp w gets row w's outputs.
 //   h1 = relu(W1 (s_in x) + b1), h2 = relu(W2 h1 + b2), y = (W3 h2 + b3) / s_out.
+// Layer l: warp w forms outputs 8w..8w+7 (layers 1, 2) or warp 0 the three
+// outputs (layer 3); one loop over the layers keeps the code compact.
 __device__ __forceinline__ void mlp_block_forward(const MlpPacked& P, MlpBlockScratch& S, int warp,
                                                   int lane, float y[3]) {
   const int g = lane >> 2, t = lane & 3;
@@ -147,30 +151,29 @@ __device__ __forceinline__ void mlp_block_forward(const MlpPacked& P, MlpBlockSc
   // nothing pending otherwise), published to the block by the barrier
   asm volatile("cp.async.wait_all;" ::: "memory");
   __syncthreads();
-  {
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    mlp_tile<kMlpInPad>(acc, S.x, kMlpXStride, P.s_in, P.w1, kMlpW1Stride, 8 * warp, lane);
-    const int j = 8 * warp + 2 * t;
-    S.h1[g * kMlpHStride + j] = fmaxf(acc[0] + P.b1[j], 0.f);
-    S.h1[g * kMlpHStride + j + 1] = fmaxf(acc[1] + P.b1[j + 1], 0.f);
+#pragma unroll 1
+  for (int layer = 0; layer < 3; layer++) {
+    if (layer < 2 || warp == 0) {
+      const bool first = layer == 0;
+      const float* A = first ? S.x : (layer == 1 ? S.h1 : S.h2);
+      const __nv_bfloat16* W = first ? P.w1 : (layer == 1 ? P.w2 : P.w3);
+      const int n0 = layer < 2 ? 8 * warp : 0;
+      float acc[4] = {0.f, 0.f, 0.f, 0.f};
+      mlp_tile(acc, A, first ? kMlpXStride : kMlpHStride, first ? P.s_in : 1.f, W,
+               first ? kMlpW1Stride : kMlpW2Stride, n0, first ? kMlpInPad : kMlpHid, lane);
+      const int j = n0 + 2 * t;
+      if (layer < 2) {
+        const float* b = first ? P.b1 : P.b2;
+        float* H = first ? S.h1 : S.h2;
+        H[g * kMlpHStride + j] = fmaxf(acc[0] + b[j], 0.f);
+        H[g * kMlpHStride + j + 1] = fmaxf(acc[1] + b[j + 1], 0.f);
+      } else {
+        if (j < kMlpOut) S.y[g * 4 + j] = (acc[0] + P.b3[j]) / P.s_out;
+        if (j + 1 < kMlpOut) S.y[g * 4 + j + 1] = (acc[1] + P.b3[j + 1]) / P.s_out;
+      }
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  {
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    mlp_tile<kMlpHid>(acc, S.h1, kMlpHStride, 1.f, P.w2, kMlpW2Stride, 8 * warp, lane);
-    const int j = 8 * warp + 2 * t;
-    S.h2[g * kMlpHStride + j] = fmaxf(acc[0] + P.b2[j], 0.f);
-    S.h2[g * kMlpHStride + j + 1] = fmaxf(acc[1] + P.b2[j + 1], 0.f);
-  }
-  __syncthreads();
-  if (warp == 0) {
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    mlp_tile<kMlpHid>(acc, S.h2, kMlpHStride, 1.f, P.w3, kMlpW2Stride, 0, lane);
-    const int c = 2 * t;
-    if (c < kMlpOut) S.y[g * 4 + c] = (acc[0] + P.b3[c]) / P.s_out;
-    if (c + 1 < kMlpOut) S.y[g * 4 + c + 1] = (acc[1] + P.b3[c + 1]) / P.s_out;
-  }
-  __syncthreads();
   y[0] = S.y[warp * 4];
   y[1] = S.y[warp * 4 + 1];
   y[2] = S.y[warp * 4 + 2];
