@@ -31,9 +31,13 @@ namespace couplb {
 // the method kernels (launch_method) are compiled in engine_methods_*.cu.
 int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, const double* d_m,
                const int* d_active, double* d_fout, int accumulate, int refresh) {
-  if (h->halo[0] || h->halo[1])
+  for (int side = 0; side < 2; side++)
+    if (h->halo[side] && !h->ih_vel[side])
+      return fail(h, COUPLB_ERR_STATE,
+                  "IBM sub-step on a lattice with a halo on z face %d needs couplb_ibm_halo_attach there", side);
+  if ((h->halo[0] || h->halo[1]) && h->ibm_method != COUPLB_IBM_SINGLE)
     return fail(h, COUPLB_ERR_UNSUPPORTED,
-                "IBM coupling on a lattice with halo faces (slab decomposition) is not supported");
+                "the iterative and learned IBM methods are not decomposed into slabs (single pass only)");
   // no coupled atoms: the reference returns before refreshing the moments
   // (fix_couplb.cpp:750-753)
   if (n <= 0) return COUPLB_OK;
@@ -99,7 +103,14 @@ int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, co
     if (h->ibm_window) {
       if (!g.face[0] && !g.face[1]) a.wrap |= 1;
       if (!g.face[2] && !g.face[3]) a.wrap |= 2;
-      if (h->p.dim == 3 && !g.face[4] && !g.face[5]) a.wrap |= 4;
+      // z faces bound to neighbour slabs take the window through their halos
+      if (h->p.dim == 3 && !g.face[4] && !g.face[5] && !h->halo[0] && !h->halo[1]) a.wrap |= 4;
+    }
+    for (int side = 0; side < 2; side++) {
+      const bool bound = h->halo[side] && h->ih_vel[side];
+      a.vh[side] = bound ? (const A*)h->ih_vel[side] : nullptr;
+      a.fh[side] = bound ? (A*)h->ih_force[side] : nullptr;
+      a.zplanes[side] = bound ? h->ih_planes[side] : 0;
     }
     if (method == COUPLB_IBM_SINGLE) {
       if (refresh && !a.all_valid) k_ibm_prefetch<L, S><<<nb, bs, 0, h->stream>>>(a);
@@ -252,6 +263,81 @@ int couplb_ibm_substep_device(couplb_handle* h, int n, const double* d_x, const 
   int rc = set_device(h);
   if (rc) return rc;
   return engine_ibm(h, n, d_x, d_v, d_mass, d_active, d_f_add, 1, refresh);
+}
+
+size_t couplb_ibm_halo_bytes(const couplb_handle* h, int planes) {
+  if (!h || h->p.dim != 3 || planes < 1 || planes > 2) return 0;
+  return (size_t)planes * h->p.nx * h->p.ny * 4 * elem_bytes_aux(h->p.precision);
+}
+
+int couplb_ibm_halo_attach(couplb_handle* h, int side, int planes, const void* d_vel, void* d_force) {
+  if (!h) return COUPLB_ERR_ARG;
+  if (side != 0 && side != 1) return fail(h, COUPLB_ERR_ARG, "halo side must be 0 (z low) or 1 (z high)");
+  if (h->p.dim != 3) return fail(h, COUPLB_ERR_UNSUPPORTED, "halo faces are z faces of a D3Q19 lattice");
+  if (!d_vel) {
+    h->ih_vel[side] = nullptr;
+    h->ih_force[side] = nullptr;
+    h->ih_planes[side] = 0;
+    return COUPLB_OK;
+  }
+  if (!d_force) return fail(h, COUPLB_ERR_ARG, "null force halo");
+  if (planes < 1 || planes > (side ? 2 : 1))
+    return fail(h, COUPLB_ERR_ARG, "an IBM halo holds 1 plane below the low face and 1 or 2 above the high face");
+  if (h->p.nz < 2) return fail(h, COUPLB_ERR_ARG, "IBM across slabs needs slabs of at least 2 planes");
+  if (h->p.wall[4 + side] != COUPLB_WALL_PERIODIC)
+    return fail(h, COUPLB_ERR_ARG, "a halo face must not be a wall (z face %d has type %d)", side,
+                h->p.wall[4 + side]);
+  h->ih_vel[side] = d_vel;
+  h->ih_force[side] = d_force;
+  h->ih_planes[side] = planes;
+  return COUPLB_OK;
+}
+
+int couplb_ibm_halo_moments(couplb_handle* h, int side, int planes, void* d_out) {
+  if (!h || !d_out) return fail(h, COUPLB_ERR_ARG, "null argument");
+  if (side != 0 && side != 1) return fail(h, COUPLB_ERR_ARG, "halo side must be 0 (z low) or 1 (z high)");
+  if (h->p.dim != 3) return fail(h, COUPLB_ERR_UNSUPPORTED, "halo faces are z faces of a D3Q19 lattice");
+  if (planes < 1 || planes > (side ? 1 : 2) || planes > h->p.nz)
+    return fail(h, COUPLB_ERR_ARG, "the neighbour below reads 1 or 2 planes, the one above 1");
+  int rc = set_device(h);
+  if (rc) return rc;
+  const Geom g = make_geom(h);
+  const long long cnt = (long long)planes * h->p.nx * h->p.ny;
+  with_types(h->p.dim, h->p.precision, [&](auto l, auto s) {
+    using L = decltype(l);
+    using S = decltype(s);
+    using A = typename S::A;
+    if constexpr (L::D == 3) {
+      IbmArgs<S> a{};
+      a.g = g;
+      a.fin = (const typename S::T*)h->f[h->cur];
+      a.rho_field = (const A*)h->rho_field;
+      a.pull = h->poststream ? 0 : 1;
+      k_halo_moments<L, S><<<flat_blocks(cnt, 256), 256, 0, h->stream>>>(a, side, planes, (A*)d_out);
+    }
+  });
+  CK_LAUNCH();
+  return COUPLB_OK;
+}
+
+int couplb_ibm_halo_fold(couplb_handle* h, int side, int planes, const void* d_in) {
+  if (!h || !d_in) return fail(h, COUPLB_ERR_ARG, "null argument");
+  if (side != 0 && side != 1) return fail(h, COUPLB_ERR_ARG, "halo side must be 0 (z low) or 1 (z high)");
+  if (h->p.dim != 3) return fail(h, COUPLB_ERR_UNSUPPORTED, "halo faces are z faces of a D3Q19 lattice");
+  if (planes < 1 || planes > (side ? 1 : 2) || planes > h->p.nz)
+    return fail(h, COUPLB_ERR_ARG, "the neighbour below spreads onto 1 or 2 planes, the one above onto 1");
+  int rc = set_device(h);
+  if (rc) return rc;
+  const Geom g = make_geom(h);
+  const long long cnt = (long long)planes * h->p.nx * h->p.ny;
+  with_types(h->p.dim, h->p.precision, [&](auto, auto s) {
+    using A = typename decltype(s)::A;
+    k_halo_fold<A><<<flat_blocks(cnt, 256), 256, 0, h->stream>>>(g, side, planes, (const A*)d_in, (A*)h->F,
+                                                                  h->seg_force);
+  });
+  CK_LAUNCH();
+  h->force_dirty = 1;
+  return COUPLB_OK;
 }
 
 int couplb_set_ibm_method(couplb_handle* h, const couplb_ibm_method* m) {

@@ -79,6 +79,9 @@ struct couplb_handle {
   int ibm_slip = 1;                  // option: ITERATIVE / LEARNED measure the slip after the last pass
   int ibm_group = 8;                 // option: lanes per marker of the single-pass 3D sub-step (8, 32)
   const void* halo[2] = {nullptr, nullptr};   // z-face halos of a slab decomposition
+  const void* ih_vel[2] = {nullptr, nullptr};  // IBM halos of those faces: neighbour moments,
+  void* ih_force[2] = {nullptr, nullptr};      // forces spread beyond the face,
+  int ih_planes[2] = {0, 0};                   // planes of each
   long long barrier_spin = 1LL << 21;   // option: grid-barrier poll limit of the method kernels
   cudaStream_t copy_stream = nullptr;   // host->device atom copies of couplb_lbm_step_ibm
   cudaEvent_t copy_ev[2] = {nullptr, nullptr};   // main stream reached / copies done

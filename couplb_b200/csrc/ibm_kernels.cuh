@@ -97,7 +97,32 @@ struct IbmArgs {
   double* corr;                           // n*3: correction beyond the penalty pass
   const MlpPacked* mlp;                   // learned correction network
   int wrap;                               // window axes wrapped periodically (bit d: axis d)
+  // Slab decomposition along z (couplb_ibm_halo_attach): window planes beyond
+  // a z face bound to a neighbour subdomain, zplanes[side] of them (0: the
+  // face is not bound; side 0: the plane below the low face, side 1: up to
+  // two planes above the high face).  vh: their velocities and densities
+  // {ux, uy, uz, rho} as compute_velocity gives them, computed by the
+  // neighbour (k_halo_moments); fh: the forces this lattice spreads onto them
+  // {fx, fy, fz, 0}, which the neighbour adds to its own field
+  // (k_halo_fold).  4 values per node, plane-major.
+  const typename S::A* vh[2];
+  typename S::A* fh[2];
+  int zplanes[2];
 };
+
+// Halo plane of the ghost-inclusive z index kg (0: the plane below the low
+// face, 1 and 2: the planes above the high face), or -1.
+template <class S>
+__device__ __forceinline__ int z_halo_plane(const IbmArgs<S>& a, int kg) {
+  if (a.zplanes[0] && kg == 0) return 0;
+  if (a.zplanes[1] && kg > a.g.nz && kg <= a.g.nz + a.zplanes[1]) return kg - a.g.nz;
+  return -1;
+}
+
+// Offset (in values) of node (i, j) of halo plane hp in its side's buffer.
+__device__ __forceinline__ size_t z_halo_offset(const Geom& g, int hp, int i, int j) {
+  return 4 * ((size_t)(hp > 0 ? hp - 1 : 0) * g.nx * g.ny + (size_t)i + (size_t)g.nx * j);
+}
 
 // The marker window of the reference is [i0-1, i0+2] per axis clipped to the
 // ghost-inclusive box (couplb_ibm.h:64-73, 110-115): near a high periodic face
@@ -159,11 +184,13 @@ struct LaneNodes {
   long long n[2];    // interior index of a fluid node (or of its periodic image)
   R d[2];            // weight
   int i, j, k[2];    // interior coordinates of a fluid node
+  int h[2];          // z halo plane of a fluid node beyond a bound face (z_halo_plane), or -1
 };
 
 template <class L, int DELTA, class R>
 __device__ __forceinline__ LaneNodes<R> lane_nodes(const Geom& g, double lx, double ly, double lz,
-                                                   int i0, int j0, int k0, int lane, int wrap) {
+                                                   int i0, int j0, int k0, int lane, int wrap,
+                                                   const int* zplanes = nullptr) {
   R w1 = R(0);
   {
     const int ax = lane >> 2, o = lane & 3;
@@ -199,6 +226,7 @@ __device__ __forceinline__ LaneNodes<R> lane_nodes(const Geom& g, double lx, dou
     out.n[rep] = -1;
     out.d[rep] = R(0);
     out.k[rep] = 0;
+    out.h[rep] = -1;
   }
   if (L::D == 2) {
     if (lane < 16 && inxy) {
@@ -215,6 +243,17 @@ __device__ __forceinline__ LaneNodes<R> lane_nodes(const Geom& g, double lx, dou
     const R wz = __shfl_sync(0xffffffffu, w1, 8 + oz);
     int kg = k0 - 1 + oz;
     if (wrap & 4) kg = wrap_ghost_index(kg, g.nz);
+    if (zplanes && inxy) {
+      // a plane of the neighbour beyond a bound face: its x/y walls only
+      const int hp = (zplanes[0] && kg == 0) ? 0
+                   : ((zplanes[1] && kg > g.nz && kg <= g.nz + zplanes[1]) ? kg - g.nz : -1);
+      if (hp >= 0) {
+        out.t[rep] = txy ? txy : -1;
+        out.d[rep] = wxy * wz;
+        out.h[rep] = hp;
+        continue;
+      }
+    }
     if (!inxy || kg < 0 || kg >= gz) continue;
     int t = txy;
     if (kg == 0 || kg == gz - 1) { const int ft = kg == 0 ? g.face[4] : g.face[5]; if (ft) t = ft; }
@@ -291,8 +330,15 @@ __device__ __forceinline__ void prefetch_marker(const IbmArgs<S>& a, int mk, int
     if (a.wrap & 2) jg = wrap_ghost_index(jg, g.ny);
     if (a.wrap & 4) kg = wrap_ghost_index(kg, g.nz);
     int ii = 0, jj = 0, kk = 0;
-    if (ig >= 0 && ig < gx && jg >= 0 && jg < gy && kg >= 0 && kg < gz &&
-        classify_node(g, L::D, ig, jg, kg, ii, jj, kk) < 0) {
+    const int hp = (L::D == 3) ? z_halo_plane(a, kg) : -1;
+    if (hp >= 0) {
+      // the neighbour's node: x/y classification only, moments from the halo
+      if (ig >= 0 && ig < gx && jg >= 0 && jg < gy && classify_node(g, L::D, ig, jg, 1, ii, jj, kk) < 0) {
+        const typename S::A* m = a.vh[hp ? 1 : 0] + z_halo_offset(g, hp, ii, jj);
+        v[rep][0] = m[0]; v[rep][1] = m[1]; v[rep][2] = m[2]; v[rep][3] = m[3];
+      }
+    } else if (ig >= 0 && ig < gx && jg >= 0 && jg < gy && kg >= 0 && kg < gz &&
+               classify_node(g, L::D, ig, jg, kg, ii, jj, kk) < 0) {
       const size_t n = (size_t)ii + (size_t)g.nx * ((size_t)jj + (size_t)g.ny * kk);
       compute_velocity<L, S>(a, ii, jj, kk, n, v[rep][0], v[rep][1], v[rep][2], v[rep][3]);
     }
@@ -380,7 +426,11 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
   const Geom& g = a.g;
   constexpr int NS = (L::D == 3) ? 64 : 16;
   double F0 = 0, F1 = 0, F2 = 0, mass = 0, vmk0 = 0, vmk1 = 0, vmk2 = 0;
-  long long sn0 = -1, sn1 = -1;   // fluid nodes of this lane (interior index)
+  // fluid nodes of this lane: their force entries (interior node or z halo)
+  // and segment (-1 for a halo node)
+  typename S::A* sp0 = nullptr;
+  typename S::A* sp1 = nullptr;
+  long long sg0 = -1, sg1 = -1;
   R sd0 = 0, sd1 = 0, wss = 0;
   if (valid) {
     const double xp = a.x[3 * mk], yp = a.x[3 * mk + 1], zp = a.x[3 * mk + 2];
@@ -415,7 +465,7 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
     mass = a.m[mk];
     vmk0 = a.v[3 * mk]; vmk1 = a.v[3 * mk + 1]; vmk2 = a.v[3 * mk + 2];
     const bool hit = key.epoch == a.cur_epoch && key.i0 == i0 && key.j0 == j0 && key.k0 == k0;
-    const LaneNodes<R> ln = lane_nodes<L, DELTA, R>(g, lx, ly, lz, i0, j0, k0, lane, a.wrap);
+    const LaneNodes<R> ln = lane_nodes<L, DELTA, R>(g, lx, ly, lz, i0, j0, k0, lane, a.wrap, a.zplanes);
     bool wall_seen = false;   // a wall node adds to ws but not to wss
 #pragma unroll
     for (int rep = 0; rep < 2; rep++) {
@@ -431,10 +481,16 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
         if (rx >= 0 && rx < 3 && ry >= 0 && ry < 3 && rz >= 0 && rz < 3) p = rx + 3 * ry + 9 * rz;
       }
       if (t < 0) {
-        const size_t src = (size_t)ln.n[rep];
+        const int hp = ln.h[rep];
+        const size_t src = hp >= 0 ? 0 : (size_t)ln.n[rep];
         const int ii = ln.i, jj = ln.j, kk = ln.k[rep];
         R u0, u1, u2;
-        if (fill) {
+        if (hp >= 0 && !(spec && hit)) {
+          // a node of the neighbour beyond a bound z face: its moments
+          const typename S::A* m = a.vh[hp ? 1 : 0] + z_halo_offset(g, hp, ii, jj);
+          if (fill) { rec[s] = m[0]; rec[64 + s] = m[1]; rec[128 + s] = m[2]; rec[192 + s] = m[3]; }
+          u0 = R(m[0]); u1 = R(m[1]); u2 = R(m[2]);
+        } else if (fill) {
           typename S::A v0, v1, v2, vr;
           compute_velocity<L, S>(a, ii, jj, kk, src, v0, v1, v2, vr);
           rec[s] = v0; rec[64 + s] = v1; rec[128 + s] = v2; rec[192 + s] = vr;
@@ -451,8 +507,10 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
         wi += u2 * dd;
         ws += dd;
         wss += dd;
-        if (rep == 0) { sn0 = (long long)src; sd0 = dd; }
-        else { sn1 = (long long)src; sd1 = dd; }
+        typename S::A* tgt = hp >= 0 ? a.fh[hp ? 1 : 0] + z_halo_offset(g, hp, ii, jj) : a.F + 4 * src;
+        const long long seg = hp >= 0 ? -1 : (long long)(src >> 3);
+        if (rep == 0) { sp0 = tgt; sg0 = seg; sd0 = dd; }
+        else { sp1 = tgt; sg1 = seg; sd1 = dd; }
         if (LEARNED && p >= 0) { xs[3 * p] = float(u0); xs[3 * p + 1] = float(u1); xs[3 * p + 2] = float(u2); }
       } else if (t == 1 || t == 3) {
         ws += dd;
@@ -519,15 +577,15 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
   const R sc = R(a.dvr) / wss;
   const double fl0 = -F0 * a.spread_c, fl1 = -F1 * a.spread_c, fl2 = -F2 * a.spread_c;
   const R f0 = R(fl0), f1 = R(fl1), f2 = R(fl2);
-  if (sn0 >= 0) {
+  if (sp0) {
     const R w = sd0 * sc;   // couplb_ibm.h:128
-    spread_add(a.F + 4 * sn0, f0 * w, f1 * w, f2 * w);
-    if (a.seg_force) a.seg_force[sn0 >> 3] = 1;
+    spread_add(sp0, f0 * w, f1 * w, f2 * w);
+    if (a.seg_force && sg0 >= 0) a.seg_force[sg0] = 1;
   }
-  if (sn1 >= 0) {
+  if (sp1) {
     const R w = sd1 * sc;
-    spread_add(a.F + 4 * sn1, f0 * w, f1 * w, f2 * w);
-    if (a.seg_force) a.seg_force[sn1 >> 3] = 1;
+    spread_add(sp1, f0 * w, f1 * w, f2 * w);
+    if (a.seg_force && sg1 >= 0) a.seg_force[sg1] = 1;
   }
   if (lane == 0 && tot3) {
     // the caller sums the markers of its block before one atomic each
@@ -666,11 +724,16 @@ __global__ void __launch_bounds__(256) k_ibm_substep8(const IbmArgs<S> a) {
   // classification of the lane's nodes: x offsets (shared by both rows), its
   // y, its two z
   AxisNode nx4[4], ny1, nz2[2];
+  int hz[2];   // z halo plane of each row beyond a bound face, or -1
 #pragma unroll
   for (int o = 0; o < 4; o++) nx4[o] = axis_node(i0 - 1, o, g.nx, g.face[0], g.face[1], a.wrap & 1);
   ny1 = axis_node(j0 - 1, y, g.ny, g.face[2], g.face[3], a.wrap & 2);
 #pragma unroll
-  for (int r = 0; r < 2; r++) nz2[r] = axis_node(k0 - 1, zr + 2 * r, g.nz, g.face[4], g.face[5], a.wrap & 4);
+  for (int r = 0; r < 2; r++) {
+    nz2[r] = axis_node(k0 - 1, zr + 2 * r, g.nz, g.face[4], g.face[5], a.wrap & 4);
+    hz[r] = z_halo_plane(a, k0 - 1 + zr + 2 * r);
+    if (hz[r] >= 0) nz2[r].t = 0;   // the neighbour's plane: no z wall
+  }
   R d[2][4];
   int t[2][4];   // -2 not in the window sums, -1 fluid, else wall type
   R ui = 0, vi = 0, wi = 0, ws = 0, wss = 0;
@@ -745,6 +808,17 @@ __global__ void __launch_bounds__(256) k_ibm_substep8(const IbmArgs<S> a) {
 #pragma unroll
       for (int r = 0; r < 2; r++) {
         const long long nyz = (long long)g.nx * ((long long)ny1.i + (long long)g.ny * nz2[r].i);
+        if (hz[r] >= 0) {
+          // onto the neighbour's plane: the halo it adds to its field
+          A* hrow = a.fh[hz[r] ? 1 : 0] + z_halo_offset(g, hz[r], 0, ny1.i);
+#pragma unroll
+          for (int o = 0; o < 4; o++) {
+            if (t[r][o] != -1) continue;
+            const R w = d[r][o] * sc;
+            spread_add(hrow + 4 * nx4[o].i, f0 * w, f1 * w, f2 * w);
+          }
+          continue;
+        }
 #pragma unroll
         for (int o = 0; o < 4; o++) {
           if (t[r][o] != -1) continue;
@@ -783,6 +857,47 @@ __global__ void __launch_bounds__(256) k_ibm_substep8(const IbmArgs<S> a) {
     for (int w = 0; w < (int)(blockDim.x >> 5); w++) sum += part[w][threadIdx.x];
     atomicAdd(a.ftot + 4 * (blockIdx.x & (kFtotSlots - 1)) + threadIdx.x, sum);
   }
+}
+
+// Moments {ux, uy, uz, rho} (compute_velocity) of `planes` boundary planes of
+// this lattice that a neighbour's IBM windows reach across face `side`: side
+// 0, planes 0..planes-1 (the neighbour below reads them above its high face);
+// side 1, plane nz-1 (the neighbour above reads it below its low face).
+template <class L, class S>
+__global__ void k_halo_moments(const IbmArgs<S> a, int side, int planes, typename S::A* __restrict__ out) {
+  const Geom& g = a.g;
+  const long long sxy = (long long)g.nx * g.ny;
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (e >= planes * sxy) return;
+  const int p = (int)(e / sxy);
+  const long long m = e % sxy;
+  const int i = (int)(m % g.nx), j = (int)(m / g.nx);
+  const int k = side ? g.nz - 1 : p;
+  typename S::A v0, v1, v2, vr;
+  compute_velocity<L, S>(a, i, j, k, (size_t)(m + k * sxy), v0, v1, v2, vr);
+  out[4 * e] = v0; out[4 * e + 1] = v1; out[4 * e + 2] = v2; out[4 * e + 3] = vr;
+}
+
+// Forces a neighbour spread onto this lattice's boundary planes (its halo
+// across face `side` of this lattice, layout of IbmArgs::fh) added to the
+// force field: side 0 (from the neighbour below), planes 0..planes-1; side 1
+// (from above), plane nz-1.  The segments that receive a force are flagged
+// for the LB step (the fold of exchange_forces, couplb_streaming.h:217-245).
+template <class A>
+__global__ void k_halo_fold(Geom g, int side, int planes, const A* __restrict__ in, A* __restrict__ F,
+                            unsigned char* __restrict__ seg) {
+  const long long sxy = (long long)g.nx * g.ny;
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (e >= planes * sxy) return;
+  const int p = (int)(e / sxy);
+  const long long m = e % sxy;
+  const long long n = m + (long long)(side ? g.nz - 1 : p) * sxy;
+  const A f0 = in[4 * e], f1 = in[4 * e + 1], f2 = in[4 * e + 2];
+  if (f0 == A(0) && f1 == A(0) && f2 == A(0)) return;
+  F[4 * n] += f0;
+  F[4 * n + 1] += f1;
+  F[4 * n + 2] += f2;
+  if (seg) seg[n >> 3] = 1;
 }
 
 // Dynamic shared memory of the learned sub-step kernels (blocks of 8 warps):

@@ -35,6 +35,10 @@ SIGNATURES = {
     "couplb_halo_attach": (C.c_int, [_H, C.c_int, C.c_void_p]),
     "couplb_halo_bytes": (C.c_size_t, [_H]),
     "couplb_halo_pack": (C.c_int, [_H, C.c_int, C.c_void_p]),
+    "couplb_ibm_halo_bytes": (C.c_size_t, [_H, C.c_int]),
+    "couplb_ibm_halo_attach": (C.c_int, [_H, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+    "couplb_ibm_halo_moments": (C.c_int, [_H, C.c_int, C.c_int, C.c_void_p]),
+    "couplb_ibm_halo_fold": (C.c_int, [_H, C.c_int, C.c_int, C.c_void_p]),
     "couplb_get_macroscopic": (C.c_int, [_H, _D, _D, _D, _D]),
     "couplb_get_force_field": (C.c_int, [_H, _D, _D, _D]),
     "couplb_set_force_field": (C.c_int, [_H, _D, _D, _D]),

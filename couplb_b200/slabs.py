@@ -19,8 +19,13 @@ travel (the reference sends all 19 of the ghost-inclusive face).
 - ``RankSlab`` is the slab of one rank of a process group (one GPU per rank),
   exchanging with ``exchange``.
 
-The immersed-boundary coupling is not decomposed: a lattice with a halo face
-refuses IBM sub-steps.
+The immersed-boundary coupling is decomposed too (``SlabLattice``, single
+pass): a marker belongs to the slab whose planes hold its cell; its window
+reaches one plane below the slab and two above, whose moments the neighbours
+compute after every LB step (couplb_ibm_halo_moments) and whose spread forces
+they add to their own fields before the next one (couplb_ibm_halo_fold) -- the
+velocity exchange and the reverse force exchange of the reference
+(couplb_streaming.h:196-245), with the window the whole lattice uses.
 """
 import numpy as np
 
@@ -142,6 +147,140 @@ class SlabLattice:
             L.close()
         self.slabs = []
 
+    def set_option(self, name, value):
+        for L in self.slabs:
+            L.set_option(name, value)
+        if name == "ibm_window" and getattr(self, "ibm", None):
+            self._attach_ibm()
+
+    # ---- immersed boundary -------------------------------------------------
+    def _high_planes(self, s):
+        """Window planes above slab s: 2, except where the slab's high face
+        wraps the global periodic box and the window is clipped (ibm_window
+        0), where the whole lattice drops the plane beyond its ghost layer."""
+        wraps_box = self.periodic_z and s == self.nslab - 1
+        return 1 if (wraps_box and self.slabs[s].get_option("ibm_window") == 0) else 2
+
+    def _attach_ibm(self):
+        torch = self.torch
+        self.ih = []
+        for s, L in enumerate(self.slabs):
+            below, above = neighbours(s, self.nslab, self.periodic_z)
+            dev = f"cuda:{self.devices[s]}"
+            bufs = {}
+            for side, nbr in ((0, below), (1, above)):
+                if nbr is None:
+                    continue
+                planes = 1 if side == 0 else self._high_planes(s)
+                nb = int(L.L.couplb_ibm_halo_bytes(L.h, planes))
+                vel = torch.zeros(nb, dtype=torch.uint8, device=dev)
+                frc = torch.zeros(nb, dtype=torch.uint8, device=dev)
+                L._ck(L.L.couplb_ibm_halo_attach(L.h, side, planes, vel.data_ptr(), frc.data_ptr()))
+                bufs[side] = (planes, vel, frc)
+            self.ih.append(bufs)
+        self._fold_pending = False
+        self._ibm_moments()
+
+    def set_ibm_params(self, domain_lo=(0.0, 0.0, 0.0), dx=1.0, **kw):
+        """IBM constants of every slab (offset z0: global positions map to the
+        slab's own planes) and the IBM halos of its bound faces."""
+        self.ibm = dict(domain_lo=tuple(domain_lo), dx=float(dx))
+        for (z0, _), L in zip(self.parts, self.slabs):
+            L.set_ibm_params(domain_lo=domain_lo, dx=dx, offset=(0, 0, z0), **kw)
+        self._attach_ibm()
+
+    def _ibm_moments(self):
+        """After the population exchange: every slab's halo moments from its
+        neighbours' boundary planes."""
+        for s, L in enumerate(self.slabs):
+            below, above = neighbours(s, self.nslab, self.periodic_z)
+            for side, nbr in ((0, below), (1, above)):
+                if side not in self.ih[s]:
+                    continue
+                planes, vel, _ = self.ih[s][side]
+                N = self.slabs[nbr]
+                if self.devices[nbr] == self.devices[s]:
+                    N._ck(N.L.couplb_ibm_halo_moments(N.h, 1 - side, planes, vel.data_ptr()))
+                else:
+                    st = self.torch.empty_like(vel, device=f"cuda:{self.devices[nbr]}")
+                    N._ck(N.L.couplb_ibm_halo_moments(N.h, 1 - side, planes, st.data_ptr()))
+                    self.torch.cuda.current_stream(self.devices[nbr]).synchronize()
+                    vel.copy_(st)
+
+    def fold_forces(self):
+        """Add the forces every slab spread beyond its faces to its neighbours'
+        fields and clear them (before the next LB step)."""
+        if not getattr(self, "_fold_pending", False):
+            return
+        for s, L in enumerate(self.slabs):
+            below, above = neighbours(s, self.nslab, self.periodic_z)
+            for side, nbr in ((0, below), (1, above)):
+                if side not in self.ih[s]:
+                    continue
+                planes, _, frc = self.ih[s][side]
+                N = self.slabs[nbr]
+                src = frc
+                if self.devices[nbr] != self.devices[s]:
+                    self.torch.cuda.current_stream(self.devices[s]).synchronize()
+                    src = frc.to(f"cuda:{self.devices[nbr]}")
+                N._ck(N.L.couplb_ibm_halo_fold(N.h, 1 - side, planes, src.data_ptr()))
+                if src is not frc:
+                    self.torch.cuda.current_stream(self.devices[nbr]).synchronize()
+                frc.zero_()
+        self._fold_pending = False
+
+    def owners(self, x):
+        """Slab of every marker: the one whose planes hold its cell (cells
+        below / above the box go to the first / last slab)."""
+        lo, dx = self.ibm["domain_lo"][2], self.ibm["dx"]
+        cell = np.floor((np.asarray(x)[:, 2] - lo) / dx).astype(np.int64)
+        starts = np.array([z0 for z0, _ in self.parts])
+        return np.clip(np.searchsorted(starts, cell, side="right") - 1, 0, self.nslab - 1)
+
+    def _idle_substep(self, s, refresh):
+        """The sub-step of a slab without coupled markers while the group has
+        some elsewhere: the refresh still happens on every subdomain (the
+        group count is global, fix_couplb.cpp:743-760), so the slab runs the
+        sub-step of one marker outside the group."""
+        torch = self.torch
+        L = self.slabs[s]
+        dev = f"cuda:{self.devices[s]}"
+        z = self.ibm["domain_lo"][2] + (self.parts[s][0] + 0.5) * self.ibm["dx"]
+        x = torch.tensor([[0.0, 0.0, z]], dtype=torch.float64, device=dev)
+        zero = torch.zeros((1, 3), dtype=torch.float64, device=dev)
+        one = torch.ones(1, dtype=torch.float64, device=dev)
+        off = torch.zeros(1, dtype=torch.int32, device=dev)
+        L.ibm_substep_device(1, x.data_ptr(), zero.data_ptr(), one.data_ptr(), zero.data_ptr(),
+                             off.data_ptr(), refresh=refresh)
+        torch.cuda.current_stream(self.devices[s]).synchronize()
+
+    def ibm_substep(self, x, v, mass, f_add, active=None, refresh=True):
+        """Single-pass IBM sub-step of host markers (f_add incremented in
+        place), each marker on its slab.  Returns the markers in the group."""
+        own = self.owners(x)
+        coupled = np.ones(x.shape[0], bool) if active is None else np.asarray(active) != 0
+        total = int(coupled.sum())
+        nc = 0
+        for s, L in enumerate(self.slabs):
+            idx = np.nonzero(own == s)[0]
+            if total > 0 and not coupled[idx].any():
+                self._idle_substep(s, refresh)
+                continue
+            xs = np.ascontiguousarray(x[idx])
+            fs = np.zeros_like(xs)
+            act = None if active is None else np.ascontiguousarray(active[idx], dtype=np.int32)
+            nc += L.ibm_substep(xs, np.ascontiguousarray(v[idx]), np.ascontiguousarray(mass[idx]), fs,
+                                active=act, refresh=refresh)
+            f_add[idx] += fs
+        self._fold_pending = True
+        return nc
+
+    def get_force_field(self):
+        """Interior force field (3 arrays nz, ny, nx) after the pending folds."""
+        self.fold_forces()
+        parts = [[a[1:-1, 1:-1, 1:-1] for a in L.get_force_field()] for L in self.slabs]
+        return [np.concatenate([p[c] for p in parts], axis=0) for c in range(3)]
+
     def _exchange(self):
         """Pack every slab's leaving planes into its neighbours' halos."""
         torch = self.torch
@@ -162,18 +301,26 @@ class SlabLattice:
                 torch.cuda.current_stream(d).synchronize()
 
     def lbm_step(self, g_lb=None):
+        if getattr(self, "ibm", None):
+            self.fold_forces()
         for L in self.slabs:
             L.lbm_step(_gravity(g_lb))
         self._exchange()
+        if getattr(self, "ibm", None):
+            self._ibm_moments()
 
     def set_populations(self, f):
         """f: global (19, nz+2, ny+2, nx+2) reference layout."""
         for (z0, nzl), L in zip(self.parts, self.slabs):
             L.set_populations(np.ascontiguousarray(f[:, z0:z0 + nzl + 2]))
+        if getattr(self, "ibm", None):
+            self._ibm_moments()
 
     def init_equilibrium(self, rho=1.0, ux=0.0, uy=0.0, uz=0.0):
         for L in self.slabs:
             L.init_equilibrium(rho, ux, uy, uz)
+        if getattr(self, "ibm", None):
+            self._ibm_moments()
 
     def get_populations(self):
         """Interior populations (19, nz, ny, nx) of the whole lattice."""

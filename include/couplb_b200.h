@@ -165,10 +165,38 @@ int  couplb_lbm_step(couplb_handle* h, const double* g_lb);
  * the post-stream state in place and needs no halo; pack needs the
  * post-collision state of an LB step.  Ghost values of attached faces in
  * couplb_get_populations are not the neighbour's.  IBM sub-steps on a lattice
- * with an attached face return COUPLB_ERR_UNSUPPORTED. */
+ * with an attached face need the IBM halos below on that face. */
 int  couplb_halo_attach(couplb_handle* h, int side, const void* d_recv);
 size_t couplb_halo_bytes(const couplb_handle* h);
 int  couplb_halo_pack(couplb_handle* h, int side, void* d_send);
+
+/* IBM across z slabs (the velocity exchange and the reverse force exchange
+ * of Streaming::exchange_velocity / exchange_forces, couplb_streaming.h:
+ * 196-245, for d = z).  A marker window [k0-1, k0+2] reaches one plane below
+ * a slab's low face and two above its high face; the reference's ghost layer
+ * is one plane wide, so its multi-rank windows lose the second plane above
+ * each internal face.  Here the halo holds what the whole lattice would use:
+ * planes = 1 below; above, 2 at an internal face, and 1 at the face that
+ * wraps the global periodic box in the clipped window mode (ibm_window 0,
+ * where the whole lattice clips the plane beyond its ghost layer), so slab
+ * sub-steps give the forces of the undecomposed lattice.
+ * couplb_ibm_halo_attach binds to z face `side` (which carries a population
+ * halo) d_vel, the neighbour's {ux, uy, uz, rho} of those planes, and
+ * d_force, where sub-steps add the forces spread onto them; both hold
+ * couplb_ibm_halo_bytes(h, planes) in the auxiliary type (4 values per node,
+ * plane-major).  d_vel NULL detaches.  Per LB cycle, after the LB step and the
+ * population exchange: couplb_ibm_halo_moments(neighbour, 1 - side, planes,
+ * buf) writes what this lattice's d_vel of `side` must hold (side 0 of the
+ * neighbour above: its planes 0..planes-1; side 1 of the neighbour below: its
+ * top plane); after the last sub-step of the cycle, before the next LB step,
+ * the caller hands each d_force to the neighbour across that face, which adds
+ * it with couplb_ibm_halo_fold(neighbour, 1 - side, planes, buf), and zeroes
+ * d_force.  Single-pass sub-steps only (the ITERATIVE and LEARNED methods
+ * return COUPLB_ERR_UNSUPPORTED on a slab). */
+size_t couplb_ibm_halo_bytes(const couplb_handle* h, int planes);
+int  couplb_ibm_halo_attach(couplb_handle* h, int side, int planes, const void* d_vel, void* d_force);
+int  couplb_ibm_halo_moments(couplb_handle* h, int side, int planes, void* d_out);
+int  couplb_ibm_halo_fold(couplb_handle* h, int side, int planes, const void* d_in);
 
 /* Grid::compute_macroscopic(false) (couplb_lattice.h:155-202) followed by
  * Streaming::exchange_velocity (couplb_streaming.h:140-143). */

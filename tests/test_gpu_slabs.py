@@ -15,6 +15,10 @@ from couplb_b200.slabs import SlabLattice
 pytestmark = pytest.mark.gpu
 
 
+def rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
 @pytest.mark.parametrize("nslab", [2, 3])
 @pytest.mark.parametrize("wall", [(0, 0, 1, 1, 0, 0), (0, 0, 1, 2, 3, 1), (0,) * 6])
@@ -56,6 +60,83 @@ def test_halo_face_rules(cuda_lib):
     L._ck(L.L.couplb_halo_attach(L.h, 1, buf.data_ptr()))
     L.set_ibm_params(delta="peskin4")
     x = np.array([[4.0, 3.0, 2.5]])
-    with pytest.raises(CoupLBError):     # IBM is not decomposed
+    with pytest.raises(CoupLBError):     # a halo face without its IBM halo
+        L.ibm_substep(x, np.zeros_like(x), np.ones(1), np.zeros_like(x))
+    nb = int(L.L.couplb_ibm_halo_bytes(L.h, 2))
+    assert nb == 2 * 8 * 6 * 4 * 8
+    vel = torch.zeros(nb, dtype=torch.uint8, device="cuda")
+    frc = torch.zeros(nb, dtype=torch.uint8, device="cuda")
+    with pytest.raises(CoupLBError):     # the low face is a wall
+        L._ck(L.L.couplb_ibm_halo_attach(L.h, 0, 1, vel.data_ptr(), frc.data_ptr()))
+    with pytest.raises(CoupLBError):     # at most 2 planes above
+        L._ck(L.L.couplb_ibm_halo_attach(L.h, 1, 3, vel.data_ptr(), frc.data_ptr()))
+    L._ck(L.L.couplb_ibm_halo_attach(L.h, 1, 2, vel.data_ptr(), frc.data_ptr()))
+    L.ibm_substep(x, np.zeros_like(x), np.ones(1), np.zeros_like(x))
+    L.set_ibm_method("iterative", passes=2)
+    with pytest.raises(CoupLBError):     # the correction methods are single-slab
         L.ibm_substep(x, np.zeros_like(x), np.ones(1), np.zeros_like(x))
     L.close()
+
+
+def _slab_markers(n, nslab, seed=23):
+    """Markers across the box, a third of them within two cells of a slab
+    face (internal faces and the global z faces)."""
+    from couplb_b200.slabs import partition
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(0.0, 1.0, (240, 3)) * np.array(n, float)
+    faces = [z0 for z0, _ in partition(n[2], nslab)] + [n[2]]
+    for k in range(80):
+        x[k, 2] = (faces[k % len(faces)] + rng.uniform(-2.0, 2.0)) % n[2]
+    v = 0.01 * rng.standard_normal(x.shape)
+    m = rng.uniform(0.5, 1.5, x.shape[0])
+    return x, v, m
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("fp32", 1e-5)])
+@pytest.mark.parametrize("nslab", [2, 3])
+@pytest.mark.parametrize("window", [0, 1])
+@pytest.mark.parametrize("wall", [(0, 0, 1, 2, 0, 0), (0, 0, 0, 0, 1, 1)])
+@pytest.mark.parametrize("idle", [False, True])
+def test_ibm_on_slabs_matches_the_whole_lattice(cuda_lib, prec, tol, nslab, window, wall, idle):
+    """IBM sub-steps on z slabs (halo moments after every LB step, spread
+    forces folded into the neighbours before the next): the per-atom forces,
+    the force field and the populations of the whole lattice, over three LB
+    cycles of two sub-steps, markers near every slab face, clipped and
+    wrapped windows."""
+    n = (20, 14, 19)
+    f0 = cases.initial_populations(3, n, 5)
+    kw = dict(tau=0.75, wall=wall, wall_vel=(0.01, 0.0, 0.0), body_force=True, precision=prec)
+    ibm = dict(delta="peskin4", md_per_lb=2, xi_ibm=0.8)
+    L = Lattice(3, *n, **kw)
+    L.set_option("ibm_window", window)
+    L.set_populations(f0)
+    L.set_ibm_params(**ibm)
+    S = SlabLattice(*n, nslab, **kw)
+    S.set_option("ibm_window", window)
+    S.set_populations(f0)
+    S.set_ibm_params(**ibm)
+    x0, v, m = _slab_markers(n, nslab)
+    if idle:
+        # markers in the lowest few planes only: the other slabs refresh
+        # without markers of their own
+        x0[:, 2] = np.mod(x0[:, 2], 3.0)
+    g = (1e-5, 0.0, 2e-6)
+    box = np.array(n, float)
+    x = x0.copy()
+    for c in range(3):
+        L.lbm_step(g)
+        S.lbm_step(g)
+        for s in range(2):
+            x = np.ascontiguousarray(np.mod(x + 0.5 * v, box))
+            fl, fs = np.zeros_like(x), np.zeros_like(x)
+            L.ibm_substep(x, v, m, fl, refresh=(s == 0))
+            S.ibm_substep(x, v, m, fs, refresh=(s == 0))
+            assert rel(fs, fl) <= tol, (c, s, rel(fs, fl))
+    FL = [a[1:-1, 1:-1, 1:-1] for a in L.get_force_field()]
+    for c, a in enumerate(S.get_force_field()):
+        assert rel(a, FL[c]) <= tol, (c, rel(a, FL[c]))
+    L.lbm_step(g)
+    S.lbm_step(g)
+    assert rel(S.get_populations(), L.get_populations()[:, 1:-1, 1:-1, 1:-1]) <= tol
+    L.close()
+    S.close()
