@@ -671,8 +671,11 @@ __device__ __forceinline__ AxisNode axis_node(int b, int o, int n, int flo, int 
 // that the 32-lane form repeats in every lane (positions, cell, key, penalty
 // force) is shared by 8 lanes here, and each lane keeps six loads in flight
 // instead of two.
+// FP32 fields: three blocks of 256 per SM (at most 85 registers), measured
+// faster than the unconstrained allocation (94 registers, two blocks); FP64
+// fields keep two (three spill several hundred bytes).
 template <class L, class S, int DELTA>
-__global__ void __launch_bounds__(256) k_ibm_substep8(const IbmArgs<S> a) {
+__global__ void __launch_bounds__(256, sizeof(typename S::A) == 4 ? 3 : 2) k_ibm_substep8(const IbmArgs<S> a) {
   static_assert(L::D == 3, "the grouped sub-step is the 3D form");
   using R = typename S::C;
   using A = typename S::A;

@@ -64,6 +64,18 @@ def neighbours(slab, nslab, periodic_z):
     return below, above
 
 
+def ibm_halo_planes(slab, nslab, periodic_z, window):
+    """(below, above): window planes a slab's markers reach beyond its low and
+    high faces (0 where the face is not bound to a neighbour): 1 below; 2
+    above, except where the high face wraps the global periodic box and the
+    window is clipped (window 0), where the whole lattice drops the plane
+    beyond its ghost layer."""
+    below, above = neighbours(slab, nslab, periodic_z)
+    lo = 0 if below is None else 1
+    hi = 0 if above is None else (1 if (periodic_z and slab == nslab - 1 and window == 0) else 2)
+    return lo, hi
+
+
 def slab_walls(wall, slab, nslab):
     """Wall types of a slab: the global x and y faces; a z face is the
     global wall at the ends of a non-periodic z and periodic (a halo or,
@@ -155,11 +167,7 @@ class SlabLattice:
 
     # ---- immersed boundary -------------------------------------------------
     def _high_planes(self, s):
-        """Window planes above slab s: 2, except where the slab's high face
-        wraps the global periodic box and the window is clipped (ibm_window
-        0), where the whole lattice drops the plane beyond its ghost layer."""
-        wraps_box = self.periodic_z and s == self.nslab - 1
-        return 1 if (wraps_box and self.slabs[s].get_option("ibm_window") == 0) else 2
+        return ibm_halo_planes(s, self.nslab, self.periodic_z, self.slabs[s].get_option("ibm_window"))[1]
 
     def _attach_ibm(self):
         torch = self.torch
@@ -355,6 +363,7 @@ class RankSlab:
                  body_force=False, precision="fp64", device=0):
         import torch
         self.torch, self.dist = torch, dist
+        self.device = device
         self.rank, self.world = dist.get_rank(), dist.get_world_size()
         self.periodic_z = wall[4] == 0 and wall[5] == 0
         self.z0, nzl = partition(nz, self.world)[self.rank]
@@ -374,12 +383,91 @@ class RankSlab:
 
     def lbm_step(self, g_lb=None):
         L = self.L
+        if getattr(self, "ibm", None):
+            self.fold_forces()
         L.lbm_step(_gravity(g_lb))
         for side in (0, 1):
             if self.nbrs[side] is not None:
                 L._ck(L.L.couplb_halo_pack(L.h, side, self.send[side].data_ptr()))
         exchange(self.dist, self.rank, self.world, self.periodic_z, self.send[0], self.send[1],
                  self.recv[0], self.recv[1])
+        if getattr(self, "ibm", None):
+            self._ibm_moments()
+
+    # ---- immersed boundary (single pass; this rank's markers) --------------
+    def set_ibm_params(self, domain_lo=(0.0, 0.0, 0.0), dx=1.0, **kw):
+        """IBM constants (offset z0) and the IBM halos: the moments of the
+        planes beyond each bound face (received after every LB step) and the
+        forces spread onto them (sent before the next)."""
+        torch, L = self.torch, self.L
+        self.ibm = dict(domain_lo=tuple(domain_lo), dx=float(dx))
+        L.set_ibm_params(domain_lo=domain_lo, dx=dx, offset=(0, 0, self.z0), **kw)
+        window = L.get_option("ibm_window")
+        own = ibm_halo_planes(self.rank, self.world, self.periodic_z, window)
+        below, above = self.nbrs
+        # planes of the neighbours' halos that face this slab
+        self.ih_planes = own
+        self.ih_nbr = (0 if below is None else ibm_halo_planes(below, self.world, self.periodic_z, window)[1],
+                       0 if above is None else ibm_halo_planes(above, self.world, self.periodic_z, window)[0])
+        mk = lambda p: torch.zeros(int(L.L.couplb_ibm_halo_bytes(L.h, p)) if p else 1,  # noqa: E731
+                                   dtype=torch.uint8, device=f"cuda:{self.device}")
+        self.vel = [mk(own[0]), mk(own[1])]        # received moments
+        self.frc = [mk(own[0]), mk(own[1])]        # forces spread beyond the faces
+        self.msend = [mk(self.ih_nbr[0]), mk(self.ih_nbr[1])]   # moments for the neighbours
+        self.frecv = [mk(self.ih_nbr[0]), mk(self.ih_nbr[1])]   # their forces on this slab
+        for side in (0, 1):
+            if own[side]:
+                L._ck(L.L.couplb_ibm_halo_attach(L.h, side, own[side], self.vel[side].data_ptr(),
+                                                 self.frc[side].data_ptr()))
+        self._fold_pending = False
+        self._ibm_moments()
+
+    def _ibm_moments(self):
+        L = self.L
+        for side in (0, 1):
+            if self.ih_nbr[side]:
+                L._ck(L.L.couplb_ibm_halo_moments(L.h, side, self.ih_nbr[side], self.msend[side].data_ptr()))
+        # msend[1] (our top plane) goes up into the neighbour's vel[0];
+        # msend[0] (our lowest planes) down into its vel[1]
+        exchange(self.dist, self.rank, self.world, self.periodic_z, self.msend[0], self.msend[1],
+                 self.vel[0], self.vel[1])
+
+    def fold_forces(self):
+        """Send the forces spread beyond each face to the neighbour there, add
+        the neighbours' forces on this slab, clear the halos.  Every rank
+        calls it at the same point (lbm_step does)."""
+        L = self.L
+        exchange(self.dist, self.rank, self.world, self.periodic_z, self.frc[0], self.frc[1],
+                 self.frecv[0], self.frecv[1])
+        for side in (0, 1):
+            if self.ih_nbr[side]:
+                L._ck(L.L.couplb_ibm_halo_fold(L.h, side, self.ih_nbr[side], self.frecv[side].data_ptr()))
+        for b in self.frc:
+            b.zero_()
+        self._fold_pending = False
+
+    def ibm_substep(self, x, v, mass, f_add, active=None, refresh=True):
+        """Single-pass sub-step of this rank's markers (host arrays, global
+        positions within this slab's planes); the group count is global, so a
+        rank without coupled markers still refreshes while others have some."""
+        torch = self.torch
+        mine = x.shape[0] if active is None else int(np.count_nonzero(active))
+        tot = torch.tensor([mine], dtype=torch.int64, device="cuda")
+        self.dist.all_reduce(tot)
+        nc = 0
+        if mine == 0 and int(tot.item()) > 0:
+            z = self.ibm["domain_lo"][2] + (self.z0 + 0.5) * self.ibm["dx"]
+            xd = torch.tensor([[0.0, 0.0, z]], dtype=torch.float64, device="cuda")
+            zero = torch.zeros((1, 3), dtype=torch.float64, device="cuda")
+            one = torch.ones(1, dtype=torch.float64, device="cuda")
+            off = torch.zeros(1, dtype=torch.int32, device="cuda")
+            self.L.ibm_substep_device(1, xd.data_ptr(), zero.data_ptr(), one.data_ptr(), zero.data_ptr(),
+                                      off.data_ptr(), refresh=refresh)
+            torch.cuda.synchronize()
+        elif mine > 0:
+            nc = self.L.ibm_substep(x, v, mass, f_add, active=active, refresh=refresh)
+        self._fold_pending = True
+        return nc
 
     def diagnostics(self):
         torch = self.torch

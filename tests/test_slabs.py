@@ -45,6 +45,27 @@ def test_partition_and_neighbours():
     assert slabs.slab_walls((0, 0, 1, 1, 2, 3), 2, 3) == (0, 0, 1, 1, 0, 3)
 
 
+def test_ibm_halo_planes_match_the_whole_lattice_window():
+    """One plane below a bound face, two above; at the face that wraps the
+    periodic box a clipped window (0) keeps one, as the whole lattice's
+    window stops at its ghost layer; faces at a wall are not bound."""
+    assert [slabs.ibm_halo_planes(s, 3, True, 1) for s in range(3)] == [(1, 2)] * 3
+    assert [slabs.ibm_halo_planes(s, 3, True, 0) for s in range(3)] == [(1, 2), (1, 2), (1, 1)]
+    assert [slabs.ibm_halo_planes(s, 3, False, 0) for s in range(3)] == [(0, 2), (1, 2), (1, 0)]
+    assert slabs.ibm_halo_planes(0, 1, True, 0) == (0, 0)
+    # a bound face has a halo on both sides of it: one plane above the face
+    # for the slab above, one or two below it for the slab below
+    for world in (2, 3, 4):
+        for periodic in (True, False):
+            for window in (0, 1):
+                for s in range(world):
+                    below, above = slabs.neighbours(s, world, periodic)
+                    lo, hi = slabs.ibm_halo_planes(s, world, periodic, window)
+                    assert (lo > 0) == (below is not None) and (hi > 0) == (above is not None)
+                    if above is not None:
+                        assert slabs.ibm_halo_planes(above, world, periodic, window)[0] == 1
+
+
 def test_crossing_populations_are_the_d3q19_z_movers():
     up, down = slabs.crossing(1), slabs.crossing(-1)
     assert up == [5, 11, 14, 15, 18] and down == [6, 12, 13, 16, 17]
