@@ -539,7 +539,7 @@ int couplb_diagnostics(couplb_handle* h, couplb_diag* out) {
                                                  (const A*)h->macro[3], part);
   });
   CK_LAUNCH();
-  k_reduce_final<<<1, 32, 0, h->stream>>>(nb, part, res);
+  k_reduce_final<<<1, kReduceThreads, 0, h->stream>>>(nb, part, res);
   CK_LAUNCH();
   double* hs = (double*)h->h_small;
   CK(cudaMemcpyAsync(hs, res, sizeof(double) * 5, cudaMemcpyDeviceToHost, h->stream));

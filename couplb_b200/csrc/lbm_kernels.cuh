@@ -670,16 +670,31 @@ __global__ void __launch_bounds__(256) k_diag_partial(long long N, double rho0,
   }
 }
 
-static __global__ void k_reduce_final(int nblocks, const double* __restrict__ part,
-                               double* __restrict__ out) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// One block of kReduceThreads: thread t sums blocks t, t + kReduceThreads,
+// ... in order, then a fixed-shape shared-memory tree combines the threads
+// (a single thread walking the partials waited on one load per block).
+constexpr int kReduceThreads = 256;
+static __global__ void __launch_bounds__(kReduceThreads) k_reduce_final(int nblocks, const double* __restrict__ part,
+                                                                        double* __restrict__ out) {
   double o[5] = {0, 0, 0, 0, 0};
-  for (int b = 0; b < nblocks; b++) {
+  for (int b = threadIdx.x; b < nblocks; b += kReduceThreads) {
     o[0] = fmax(o[0], part[b * 5]);
     for (int c = 1; c < 5; c++) o[c] += part[b * 5 + c];
   }
-  out[0] = sqrt(o[0]);
-  for (int c = 1; c < 5; c++) out[c] = o[c];
+  __shared__ double sh[5][kReduceThreads];
+  for (int c = 0; c < 5; c++) sh[c][threadIdx.x] = o[c];
+  __syncthreads();
+  for (int h = kReduceThreads / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) {
+      sh[0][threadIdx.x] = fmax(sh[0][threadIdx.x], sh[0][threadIdx.x + h]);
+      for (int c = 1; c < 5; c++) sh[c][threadIdx.x] += sh[c][threadIdx.x + h];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[0] = sqrt(sh[0][0]);
+    for (int c = 1; c < 5; c++) out[c] = sh[c][0];
+  }
 }
 
 // y-profile sums of FixCoupLB::write_profile (fix_couplb.cpp:906-910): for

@@ -64,6 +64,14 @@ def neighbours(slab, nslab, periodic_z):
     return below, above
 
 
+def owner_slabs(z, parts, lo=0.0, dx=1.0):
+    """Slab of every marker z coordinate: the one whose planes hold its cell
+    (cells below / above the box go to the first / last slab)."""
+    cell = np.floor((np.asarray(z, dtype=np.float64) - lo) / dx).astype(np.int64)
+    starts = np.array([z0 for z0, _ in parts])
+    return np.clip(np.searchsorted(starts, cell, side="right") - 1, 0, len(parts) - 1)
+
+
 def ibm_halo_planes(slab, nslab, periodic_z, window):
     """(below, above): window planes a slab's markers reach beyond its low and
     high faces (0 where the face is not bound to a neighbour): 1 below; 2
@@ -95,22 +103,30 @@ def exchange(dist, rank, world, periodic_z, send_lo, send_hi, recv_lo, recv_hi):
     argument for a face without a neighbour is ignored.  Every rank calls it
     at the same point of every step."""
     below, above = neighbours(rank, world, periodic_z)
+    # gloo moves host tensors: device buffers are staged through the host
+    host = dist.get_backend() == "gloo"
+    stage = (lambda t: t.cpu() if (host and t.is_cuda) else t)   # noqa: E731
+    s_lo, s_hi, r_lo, r_hi = stage(send_lo), stage(send_hi), stage(recv_lo), stage(recv_hi)
     # upward flow first, then downward, on every rank: with two ranks on a
     # periodic z the neighbour above is also the one below, and messages of
     # one pair match in the order they are posted (tags 0 / 1 for backends
     # that use them)
     ops = []
     if above is not None:
-        ops.append(dist.P2POp(dist.isend, send_hi, above, tag=0))
+        ops.append(dist.P2POp(dist.isend, s_hi, above, tag=0))
     if below is not None:
-        ops.append(dist.P2POp(dist.irecv, recv_lo, below, tag=0))
+        ops.append(dist.P2POp(dist.irecv, r_lo, below, tag=0))
     if below is not None:
-        ops.append(dist.P2POp(dist.isend, send_lo, below, tag=1))
+        ops.append(dist.P2POp(dist.isend, s_lo, below, tag=1))
     if above is not None:
-        ops.append(dist.P2POp(dist.irecv, recv_hi, above, tag=1))
+        ops.append(dist.P2POp(dist.irecv, r_hi, above, tag=1))
     if ops:
         for r in dist.batch_isend_irecv(ops):
             r.wait()
+    if below is not None and r_lo is not recv_lo:
+        recv_lo.copy_(r_lo)
+    if above is not None and r_hi is not recv_hi:
+        recv_hi.copy_(r_hi)
 
 
 def _gravity(g_lb):
@@ -240,10 +256,7 @@ class SlabLattice:
     def owners(self, x):
         """Slab of every marker: the one whose planes hold its cell (cells
         below / above the box go to the first / last slab)."""
-        lo, dx = self.ibm["domain_lo"][2], self.ibm["dx"]
-        cell = np.floor((np.asarray(x)[:, 2] - lo) / dx).astype(np.int64)
-        starts = np.array([z0 for z0, _ in self.parts])
-        return np.clip(np.searchsorted(starts, cell, side="right") - 1, 0, self.nslab - 1)
+        return owner_slabs(np.asarray(x)[:, 2], self.parts, self.ibm["domain_lo"][2], self.ibm["dx"])
 
     def _idle_substep(self, s, refresh):
         """The sub-step of a slab without coupled markers while the group has
@@ -452,7 +465,7 @@ class RankSlab:
         rank without coupled markers still refreshes while others have some."""
         torch = self.torch
         mine = x.shape[0] if active is None else int(np.count_nonzero(active))
-        tot = torch.tensor([mine], dtype=torch.int64, device="cuda")
+        tot = torch.tensor([mine], dtype=torch.int64, device=self._rdev())
         self.dist.all_reduce(tot)
         nc = 0
         if mine == 0 and int(tot.item()) > 0:
@@ -469,15 +482,39 @@ class RankSlab:
         self._fold_pending = True
         return nc
 
+    def _rdev(self):
+        """Device of reduction tensors: the host for gloo, this GPU for NCCL."""
+        return "cpu" if self.dist.get_backend() == "gloo" else f"cuda:{self.device}"
+
     def diagnostics(self):
         torch = self.torch
         self.L.macroscopic()
         d = self.L.diagnostics()
-        t = torch.tensor([d.mass, d.mom[0], d.mom[1], d.mom[2]], dtype=torch.float64, device="cuda")
+        t = torch.tensor([d.mass, d.mom[0], d.mom[1], d.mom[2]], dtype=torch.float64, device=self._rdev())
         self.dist.all_reduce(t)
-        u = torch.tensor([d.umax], dtype=torch.float64, device="cuda")
+        u = torch.tensor([d.umax], dtype=torch.float64, device=self._rdev())
         self.dist.all_reduce(u, op=self.dist.ReduceOp.MAX)
         return float(u.item()), float(t[0].item()), [float(x) for x in t[1:].tolist()]
+
+    def set_populations(self, f):
+        """f: the global (19, nz+2, ny+2, nx+2) reference layout; this rank
+        takes its planes."""
+        z0 = self.z0
+        nzl = partition(f.shape[1] - 2, self.world)[self.rank][1]
+        self.L.set_populations(np.ascontiguousarray(f[:, z0:z0 + nzl + 2]))
+        if getattr(self, "ibm", None):
+            self._ibm_moments()
+
+    def get_populations(self):
+        """This rank's interior populations (19, nz_local, ny, nx)."""
+        return self.L.get_populations()[:, 1:-1, 1:-1, 1:-1]
+
+    def get_force_field(self):
+        """This rank's interior force field after the pending folds (a
+        collective: every rank calls it)."""
+        if getattr(self, "ibm", None):
+            self.fold_forces()
+        return [a[1:-1, 1:-1, 1:-1] for a in self.L.get_force_field()]
 
     def close(self):
         self.L.close()

@@ -140,3 +140,90 @@ def test_ibm_on_slabs_matches_the_whole_lattice(cuda_lib, prec, tol, nslab, wind
     assert rel(S.get_populations(), L.get_populations()[:, 1:-1, 1:-1, 1:-1]) <= tol
     L.close()
     S.close()
+
+
+def _rank_ibm(rank, world, port, window, out):
+    """One rank of the gloo test below: a RankSlab on cuda:0, its own
+    markers, the same cycles as the whole lattice."""
+    import datetime
+    import os
+    import torch.distributed as dist
+    from couplb_b200.slabs import RankSlab, owner_slabs, partition
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        n, f0, kw, ibm, x, v, m, g = _rank_case(world)
+        S = RankSlab(dist, *n, device=0, **kw)
+        S.L.set_option("ibm_window", window)
+        S.set_populations(f0)
+        S.set_ibm_params(**ibm)
+        parts = partition(n[2], world)
+        forces = []
+        for c in range(3):
+            S.lbm_step(g)
+            for s in range(2):
+                x = np.ascontiguousarray(np.mod(x + 0.5 * v, np.array(n, float)))
+                mine = np.nonzero(owner_slabs(x[:, 2], parts) == rank)[0]
+                f = np.zeros((mine.size, 3))
+                S.ibm_substep(np.ascontiguousarray(x[mine]), np.ascontiguousarray(v[mine]),
+                              np.ascontiguousarray(m[mine]), f, refresh=(s == 0))
+                forces.append((mine, f))
+        F = S.get_force_field()
+        S.lbm_step(g)
+        out[rank] = (forces, F, S.get_populations())
+        S.close()
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def _rank_case(world):
+    n = (20, 14, 19)
+    f0 = cases.initial_populations(3, n, 5)
+    kw = dict(tau=0.75, wall=(0, 0, 1, 2, 0, 0), wall_vel=(0.01, 0.0, 0.0), body_force=True,
+              precision="fp64")
+    ibm = dict(delta="peskin4", md_per_lb=2, xi_ibm=0.8)
+    x, v, m = _slab_markers(n, world)
+    return n, f0, kw, ibm, x, v, m, (1e-5, 0.0, 2e-6)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("window", [0, 1])
+def test_rank_slabs_over_gloo_match_the_whole_lattice(cuda_lib, world, window):
+    """RankSlab end to end with one process per slab, all on this GPU, the
+    halos (populations, IBM moments, folded forces) moved by gloo through the
+    host (no kernel waits on another process): per-atom forces, force field
+    and populations of the whole lattice, FP64 within 1e-12."""
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    out = mp.get_context("spawn").Manager().dict()
+    mp.start_processes(_rank_ibm, args=(world, port, window, out), nprocs=world, start_method="spawn")
+    n, f0, kw, ibm, x, v, m, g = _rank_case(world)
+    L = Lattice(3, *n, **kw)
+    L.set_option("ibm_window", window)
+    L.set_populations(f0)
+    L.set_ibm_params(**ibm)
+    k = 0
+    for c in range(3):
+        L.lbm_step(g)
+        for s in range(2):
+            x = np.ascontiguousarray(np.mod(x + 0.5 * v, np.array(n, float)))
+            fl = np.zeros_like(x)
+            L.ibm_substep(x, v, m, fl, refresh=(s == 0))
+            fr = np.zeros_like(x)
+            for r in range(world):
+                mine, f = out[r][0][k]
+                fr[mine] = f
+            assert rel(fr, fl) <= 1e-12, (c, s, rel(fr, fl))
+            k += 1
+    FL = [a[1:-1, 1:-1, 1:-1] for a in L.get_force_field()]
+    for c in range(3):
+        got = np.concatenate([out[r][1][c] for r in range(world)], axis=0)
+        assert rel(got, FL[c]) <= 1e-12, (c, rel(got, FL[c]))
+    L.lbm_step(g)
+    pops = np.concatenate([out[r][2] for r in range(world)], axis=1)
+    assert rel(pops, L.get_populations()[:, 1:-1, 1:-1, 1:-1]) <= 1e-12
+    L.close()
