@@ -64,6 +64,44 @@ def neighbours(slab, nslab, periodic_z):
     return below, above
 
 
+CLBK_MAGIC, CLBK_VERSION = 0x434C424B, 1   # "CLBK" (couplb_io.h:21)
+
+
+def write_clbk(path, step, f, offset, glob):
+    """One rank's checkpoint in the .clbk layout (couplb_io.h:669-719):
+    magic, version, step, D, Q, local dims, offset, global dims, then f
+    (Q x ghost-inclusive nodes, FP64)."""
+    import struct
+    Q, gz, gy, gx = f.shape
+    with open(path, "wb") as fp:
+        fp.write(struct.pack("<Iiqii", CLBK_MAGIC, CLBK_VERSION, int(step), 3, Q))
+        fp.write(struct.pack("<3i", gx - 2, gy - 2, gz - 2))
+        fp.write(struct.pack("<3i", *offset))
+        fp.write(struct.pack("<3i", *glob))
+        fp.write(np.ascontiguousarray(f, dtype=np.float64).tobytes())
+
+
+def read_clbk(path, shape, offset, glob):
+    """(step, f) of a .clbk file whose header matches this slab's D, Q, local
+    dims, offset and global dims (ValueError otherwise)."""
+    import struct
+    Q, gz, gy, gx = shape
+    with open(path, "rb") as fp:
+        head = fp.read(24 + 36)
+        if len(head) != 60:
+            raise ValueError(f"{path}: truncated header")
+        magic, version, step, D, q = struct.unpack("<Iiqii", head[:24])
+        dims, offs, gl = (struct.unpack("<3i", head[24 + 12 * i:36 + 12 * i]) for i in range(3))
+        if magic != CLBK_MAGIC or version != CLBK_VERSION:
+            raise ValueError(f"{path}: not a version {CLBK_VERSION} .clbk file")
+        if (D, q) != (3, Q) or dims != (gx - 2, gy - 2, gz - 2) or offs != tuple(offset) or gl != tuple(glob):
+            raise ValueError(f"{path}: written for another lattice or slab")
+        f = np.frombuffer(fp.read(), dtype=np.float64)
+    if f.size != Q * gz * gy * gx:
+        raise ValueError(f"{path}: short read")
+    return step, f.reshape(shape).copy()
+
+
 def owner_slabs(z, parts, lo=0.0, dx=1.0):
     """Slab of every marker z coordinate: the one whose planes hold its cell
     (cells below / above the box go to the first / last slab)."""
@@ -377,6 +415,7 @@ class RankSlab:
         import torch
         self.torch, self.dist = torch, dist
         self.device = device
+        self.L_nx, self.L_ny, self.nz_global = nx, ny, nz
         self.rank, self.world = dist.get_rank(), dist.get_world_size()
         self.periodic_z = wall[4] == 0 and wall[5] == 0
         self.z0, nzl = partition(nz, self.world)[self.rank]
@@ -495,6 +534,35 @@ class RankSlab:
         u = torch.tensor([d.umax], dtype=torch.float64, device=self._rdev())
         self.dist.all_reduce(u, op=self.dist.ReduceOp.MAX)
         return float(u.item()), float(t[0].item()), [float(x) for x in t[1:].tolist()]
+
+    def y_profile(self):
+        """(rho, ux, uy) per j, means over i and k of the whole lattice: the
+        profile of FixCoupLB::write_profile with every rank's sums reduced
+        (fix_couplb.cpp:903-979), lattice units.  A collective."""
+        torch = self.torch
+        self.L.macroscopic()
+        ux, uy, rho = self.L.y_profile()
+        t = torch.tensor(np.concatenate([rho, ux, uy]), dtype=torch.float64, device=self._rdev())
+        self.dist.all_reduce(t)
+        ny = rho.shape[0]
+        a = t.cpu().numpy() / float(self.L_nx * self.nz_global)
+        return a[:ny], a[ny:2 * ny], a[2 * ny:]
+
+    def write_checkpoint(self, prefix, step):
+        """prefix.<rank>.clbk in the layout of IO::write_checkpoint
+        (couplb_io.h:669-719): this rank's planes with their z offset."""
+        write_clbk(f"{prefix}.{self.rank}.clbk", step, self.L.get_populations(),
+                   (0, 0, self.z0), (self.L_nx, self.L_ny, self.nz_global))
+
+    def read_checkpoint(self, prefix):
+        """Restore this rank's planes from prefix.<rank>.clbk (header checked
+        against this slab); returns the step."""
+        step, f = read_clbk(f"{prefix}.{self.rank}.clbk", self.L.get_populations().shape, (0, 0, self.z0),
+                            (self.L_nx, self.L_ny, self.nz_global))
+        self.L.set_populations(f)
+        if getattr(self, "ibm", None):
+            self._ibm_moments()
+        return step
 
     def set_populations(self, f):
         """f: the global (19, nz+2, ny+2, nx+2) reference layout; this rank

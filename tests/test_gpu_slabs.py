@@ -142,7 +142,7 @@ def test_ibm_on_slabs_matches_the_whole_lattice(cuda_lib, prec, tol, nslab, wind
     S.close()
 
 
-def _rank_ibm(rank, world, port, window, out):
+def _rank_ibm(rank, world, port, window, prefix, out):
     """One rank of the gloo test below: a RankSlab on cuda:0, its own
     markers, the same cycles as the whole lattice."""
     import datetime
@@ -170,7 +170,14 @@ def _rank_ibm(rank, world, port, window, out):
                 forces.append((mine, f))
         F = S.get_force_field()
         S.lbm_step(g)
-        out[rank] = (forces, F, S.get_populations())
+        pops = S.get_populations()
+        prof = S.y_profile()
+        # a per-rank checkpoint restores this slab bit for bit
+        S.write_checkpoint(prefix, 7)
+        S2 = RankSlab(dist, *n, device=0, **kw)
+        restored = S2.read_checkpoint(prefix) == 7 and np.array_equal(S2.get_populations(), pops)
+        S2.close()
+        out[rank] = (forces, F, pops, prof, restored)
         S.close()
         dist.barrier()
     finally:
@@ -189,18 +196,20 @@ def _rank_case(world):
 
 @pytest.mark.parametrize("world", [2, 3])
 @pytest.mark.parametrize("window", [0, 1])
-def test_rank_slabs_over_gloo_match_the_whole_lattice(cuda_lib, world, window):
+def test_rank_slabs_over_gloo_match_the_whole_lattice(cuda_lib, tmp_path, world, window):
     """RankSlab end to end with one process per slab, all on this GPU, the
     halos (populations, IBM moments, folded forces) moved by gloo through the
-    host (no kernel waits on another process): per-atom forces, force field
-    and populations of the whole lattice, FP64 within 1e-12."""
+    host (no kernel waits on another process): per-atom forces, force field,
+    populations and y profile of the whole lattice, FP64 within 1e-12, and
+    per-rank checkpoints that restore each slab bit for bit."""
     import socket
     import torch.multiprocessing as mp
     with socket.socket() as sk:
         sk.bind(("127.0.0.1", 0))
         port = sk.getsockname()[1]
     out = mp.get_context("spawn").Manager().dict()
-    mp.start_processes(_rank_ibm, args=(world, port, window, out), nprocs=world, start_method="spawn")
+    prefix = str(tmp_path / "slab")
+    mp.start_processes(_rank_ibm, args=(world, port, window, prefix, out), nprocs=world, start_method="spawn")
     n, f0, kw, ibm, x, v, m, g = _rank_case(world)
     L = Lattice(3, *n, **kw)
     L.set_option("ibm_window", window)
@@ -226,4 +235,13 @@ def test_rank_slabs_over_gloo_match_the_whole_lattice(cuda_lib, world, window):
     L.lbm_step(g)
     pops = np.concatenate([out[r][2] for r in range(world)], axis=1)
     assert rel(pops, L.get_populations()[:, 1:-1, 1:-1, 1:-1]) <= 1e-12
+    # the y profile of the whole lattice (sums over every rank), and the
+    # per-rank checkpoints
+    L.macroscopic()
+    ux, uy, rho = L.y_profile()
+    c = float(n[0] * n[2])
+    for r in range(world):
+        for got, want in zip(out[r][3], (rho / c, ux / c, uy / c)):
+            assert rel(got, want) <= 1e-12
+        assert out[r][4]
     L.close()

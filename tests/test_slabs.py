@@ -111,3 +111,23 @@ def test_halo_exchange_delivers_the_neighbour_planes(world, periodic):
     out = mp.get_context("spawn").Manager().dict()
     mp.start_processes(_rank, args=(world, _free_port(), periodic, out), nprocs=world, start_method="spawn")
     assert dict(out) == {r: True for r in range(world)}
+
+
+def test_clbk_round_trip_and_header_checks(tmp_path):
+    """A slab's checkpoint file: the .clbk header of IO::write_checkpoint
+    (couplb_io.h:669-719) with the slab's dims and z offset, f after it; a
+    reader for another slab refuses it."""
+    import struct
+    f = np.random.default_rng(3).standard_normal((19, 7, 6, 5))
+    path = str(tmp_path / "ck.1.clbk")
+    slabs.write_clbk(path, 42, f, (0, 0, 10), (3, 4, 20))
+    raw = open(path, "rb").read()
+    assert struct.unpack("<Iiqii", raw[:24]) == (0x434C424B, 1, 42, 3, 19)
+    assert struct.unpack("<9i", raw[24:60]) == (3, 4, 5, 0, 0, 10, 3, 4, 20)
+    assert len(raw) == 60 + f.size * 8
+    step, g = slabs.read_clbk(path, f.shape, (0, 0, 10), (3, 4, 20))
+    assert step == 42 and np.array_equal(g, f)
+    with pytest.raises(ValueError):
+        slabs.read_clbk(path, f.shape, (0, 0, 5), (3, 4, 20))
+    with pytest.raises(ValueError):
+        slabs.read_clbk(path, (19, 8, 6, 5), (0, 0, 10), (3, 4, 20))
