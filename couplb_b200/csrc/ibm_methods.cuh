@@ -492,10 +492,14 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
   if (mk < a.n && !have && !a.accumulate && lane < 3) a.fout[3 * mk + lane] = 0.0;
 
   // ---- first pass: window, stencil state, penalty (+ network) force, spread
+  // Node state, weights and the interpolation sums in the storage's compute
+  // type R (FP32 for the shifted formats, as in the single-pass sub-step);
+  // marker velocities and forces in FP64.
   long long nd[2] = {-1, -1};      // interior index of a fluid node, else -1
-  double dw[2] = {0.0, 0.0};       // delta weight
-  double uu[2][3] = {{0, 0, 0}, {0, 0, 0}}, ir[2] = {0.0, 0.0};
-  double ws = 0.0, wss = 0.0, uwx = 0.0, uwy = 0.0, uwz = 0.0;   // wall velocity sums
+  R dw[2] = {R(0), R(0)};          // delta weight
+  R uu[2][3] = {{0, 0, 0}, {0, 0, 0}}, ir[2] = {R(0), R(0)};
+  A rh[2] = {A(0), A(0)};          // density of a filled node, for its record
+  R ws = 0, wss = 0, uwx = 0, uwy = 0, uwz = 0;   // wall velocity sums
   double F0 = 0, F1 = 0, F2 = 0, c0 = 0, c1 = 0, c2 = 0, mxi = 0, vx = 0, vy = 0, vz = 0;
   if (have) {
     const MarkerWindow w = marker_window<L, S>(a, mk);
@@ -509,14 +513,14 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
       oy = (w.ly - w.j0) >= 0.5 ? 1 : 0;
       oz = (w.lz - w.k0) >= 0.5 ? 1 : 0;
     }
-    double ui = 0, vi = 0, wi = 0;
+    R ui = 0, vi = 0, wi = 0;
     const LaneNodes<R> ln = lane_nodes<L, DELTA, R>(g, w.lx, w.ly, w.lz, w.i0, w.j0, w.k0, lane, a.wrap);
 #pragma unroll
     for (int rep = 0; rep < 2; rep++) {
       const int s = lane + 32 * rep;
       const int t = ln.t[rep];
       if (t == -2) continue;
-      const double dd = double(ln.d[rep]);
+      const R dd = ln.d[rep];
       const int ii = ln.i, jj = ln.j, kk = ln.k[rep];
       int p = -1;
       if (LEARNED) {
@@ -525,24 +529,27 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
       }
       if (t < 0) {
         const size_t n = (size_t)ln.n[rep];
-        double u0, u1, u2, rho;
+        R u0, u1, u2, rho;
         if (fill) {
           // the record is written after the loop, so that the loads of both
           // nodes can be in flight together
           A v0, v1, v2, vr;
           compute_velocity<L, S>(a, ii, jj, kk, n, v0, v1, v2, vr);
-          u0 = double(v0); u1 = double(v1); u2 = double(v2); rho = double(vr);
+          u0 = R(v0); u1 = R(v1); u2 = R(v2); rho = R(vr);
+          rh[rep] = vr;
         } else {
-          node_state<L, S>(a, hit, rec, s, ii, jj, kk, n, u0, u1, u2, rho);
+          double w0, w1, w2, wr;
+          node_state<L, S>(a, hit, rec, s, ii, jj, kk, n, w0, w1, w2, wr);
+          u0 = R(w0); u1 = R(w1); u2 = R(w2); rho = R(wr);
         }
         nd[rep] = (long long)n; dw[rep] = dd;
-        uu[rep][0] = u0; uu[rep][1] = u1; uu[rep][2] = u2; ir[rep] = 1.0 / rho;
+        uu[rep][0] = u0; uu[rep][1] = u1; uu[rep][2] = u2; ir[rep] = R(1) / rho;
         ui += u0 * dd; vi += u1 * dd; wi += u2 * dd; ws += dd; wss += dd;
         if (LEARNED && p >= 0) { xs[3 * p] = float(u0); xs[3 * p + 1] = float(u1); xs[3 * p + 2] = float(u2); }
       } else if (t == 1 || t == 3) {
         ws += dd;
       } else if (t == 2) {
-        uwx += g.uw[0] * dd; uwy += g.uw[1] * dd; uwz += g.uw[2] * dd; ws += dd;
+        uwx += R(g.uw[0]) * dd; uwy += R(g.uw[1]) * dd; uwz += R(g.uw[2]) * dd; ws += dd;
         if (LEARNED && p >= 0) {
           xs[3 * p] = float(g.uw[0]); xs[3 * p + 1] = float(g.uw[1]); xs[3 * p + 2] = float(g.uw[2]);
         }
@@ -554,7 +561,7 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
         if (nd[rep] < 0) continue;
         const int s = lane + 32 * rep;
         rec[s] = A(uu[rep][0]); rec[64 + s] = A(uu[rep][1]); rec[128 + s] = A(uu[rep][2]);
-        rec[192 + s] = A(1.0 / ir[rep]);
+        rec[192 + s] = rh[rep];
       }
       if (lane == 0) a.skey[mk] = StencilKey{w.i0, w.j0, w.k0, a.cur_epoch};
     }
@@ -572,9 +579,9 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
       uwz += __shfl_xor_sync(0xffffffffu, uwz, o);
     }
     double U0 = 0, U1 = 0, U2 = 0;
-    if (ws > DELTA_TOL) {
-      const double iw = 1.0 / ws;
-      U0 = ui * iw; U1 = vi * iw; U2 = wi * iw;
+    if (ws > R(DELTA_TOL)) {
+      const R iw = R(1) / ws;
+      U0 = double(ui * iw); U1 = double(vi * iw); U2 = double(wi * iw);
     }
     mxi = a.m[mk] * a.xi_over_dt;
     vx = a.v[3 * mk]; vy = a.v[3 * mk + 1]; vz = a.v[3 * mk + 2];
@@ -605,7 +612,8 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
     }
   }
   // spread -F/(N fs) with w = d dvr / wss (couplb_ibm.h:124-132)
-  const double ssc = (have && wss >= DELTA_TOL) ? a.dvr / wss : 0.0;
+  const bool spreads = have && wss >= R(DELTA_TOL);
+  const R ssc = spreads ? R(a.dvr) / wss : R(0);
   // Per-block sums before the FP64 slot atomics (total force, slip): one
   // atomic per block and quantity instead of one per marker.  Every thread of
   // the block calls spread and measure at the same points.
@@ -614,13 +622,14 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
   const int nwarp = (int)(blockDim.x >> 5);
   auto spread = [&](double f0, double f1, double f2) {
     double t0 = 0.0, t1 = 0.0, t2 = 0.0;
-    if (have && wss >= DELTA_TOL) {
+    if (spreads) {
       const double fl0 = -f0 * a.spread_c, fl1 = -f1 * a.spread_c, fl2 = -f2 * a.spread_c;
+      const R r0 = R(fl0), r1 = R(fl1), r2 = R(fl2);
 #pragma unroll
       for (int rep = 0; rep < 2; rep++) {
         if (nd[rep] < 0) continue;
-        const double wgt = dw[rep] * ssc;
-        spread_add(a.F + 4 * nd[rep], fl0 * wgt, fl1 * wgt, fl2 * wgt);
+        const R wgt = dw[rep] * ssc;
+        spread_add(a.F + 4 * nd[rep], r0 * wgt, r1 * wgt, r2 * wgt);
         if (a.seg_force) a.seg_force[nd[rep] >> 3] = 1;
       }
       t0 = fl0 * a.dvr; t1 = fl1 * a.dvr; t2 = fl2 * a.dvr;
@@ -637,26 +646,27 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
   };
   // interpolated u_corr from the registers and the current force field
   auto interp_corr_reg = [&](double U[3]) {
-    double ui = 0, vi = 0, wi = 0;
+    R ui = 0, vi = 0, wi = 0;
+    const R half = R(0.5), g0 = R(P.g_lb[0]), g1 = R(P.g_lb[1]), g2 = R(P.g_lb[2]);
 #pragma unroll
     for (int rep = 0; rep < 2; rep++) {
       if (nd[rep] < 0) continue;
       double G[3];
       load_force(a.F, (size_t)nd[rep], G);
-      const double c0 = uu[rep][0] + 0.5 * (G[0] * ir[rep] + P.g_lb[0]);
-      const double c1 = uu[rep][1] + 0.5 * (G[1] * ir[rep] + P.g_lb[1]);
-      const double c2 = uu[rep][2] + 0.5 * (G[2] * ir[rep] + P.g_lb[2]);
+      const R c0 = uu[rep][0] + half * (R(G[0]) * ir[rep] + g0);
+      const R c1 = uu[rep][1] + half * (R(G[1]) * ir[rep] + g1);
+      const R c2 = uu[rep][2] + half * (R(G[2]) * ir[rep] + g2);
       ui += c0 * dw[rep]; vi += c1 * dw[rep]; wi += c2 * dw[rep];
     }
-#pragma unroll
+#pragma unroll 1
     for (int o = 16; o > 0; o >>= 1) {
       ui += __shfl_xor_sync(0xffffffffu, ui, o);
       vi += __shfl_xor_sync(0xffffffffu, vi, o);
       wi += __shfl_xor_sync(0xffffffffu, wi, o);
     }
-    if (ws > DELTA_TOL) {
-      const double iw = 1.0 / ws;
-      U[0] = (ui + uwx) * iw; U[1] = (vi + uwy) * iw; U[2] = (wi + uwz) * iw;
+    if (ws > R(DELTA_TOL)) {
+      const R iw = R(1) / ws;
+      U[0] = double((ui + uwx) * iw); U[1] = double((vi + uwy) * iw); U[2] = double((wi + uwz) * iw);
     } else {
       U[0] = U[1] = U[2] = 0.0;
     }
