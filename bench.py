@@ -73,8 +73,6 @@ def parse():
                     help="edge of the periodic box of the point-marker workload")
     ap.add_argument("--ibm-group", type=int, default=8, choices=[8, 32],
                     help="lanes per marker of the single-pass IBM sub-step (handle option ibm_group)")
-    ap.add_argument("--ibm-refresh", type=int, default=-1, choices=[-1, 0, 1],
-                    help="IBM refresh form (handle option ibm_refresh): -1 auto, 0 per marker, 1 per node segment")
     ap.add_argument("--nx", type=int, default=NX)
     ap.add_argument("--ny", type=int, default=NY)
     ap.add_argument("--nz", type=int, default=NZ)
@@ -166,7 +164,6 @@ class Clocks:
 # --------------------------------------------------------------------------
 KERNEL = -1
 IBM_GROUP = 8   # lanes per marker of the single-pass IBM sub-step
-IBM_REFRESH = -1   # IBM refresh form: -1 auto, 0 per marker, 1 per node segment
 
 
 def make_lattice(prec, nx, ny, nz, device):
@@ -283,7 +280,6 @@ def marker_bench(torch, device, prec, cycles, warmup, box, wall, tau, x0, v0, md
     # reference clips it at the ghost layer, option value 0)
     L.set_option("ibm_window", 1)
     L.set_option("ibm_group", IBM_GROUP)
-    L.set_option("ibm_refresh", IBM_REFRESH)
     stream = torch.cuda.current_stream()
     L.set_stream(stream.cuda_stream)
     L.init_equilibrium(1.0)
@@ -345,7 +341,6 @@ def marker_bench(torch, device, prec, cycles, warmup, box, wall, tau, x0, v0, md
     L.set_option("ibm_slip", 1)
     ms = sum(a.elapsed_time(b) for a, b in evs) / cycles
     out = {"workload": workload, "precision": prec, "cycles": cycles, "ms_per_lb_cycle": ms,
-           "refresh": "node segments" if L.get_option("last_refresh") else "per marker",
            "ibm_window": "wrap (periodic axes)"}
     if combined:
         # the refresh sub-step shares its call with the LB step
@@ -742,11 +737,10 @@ def load_peak():
 
 
 def main():
-    global KERNEL, IBM_GROUP, IBM_REFRESH
+    global KERNEL, IBM_GROUP
     args = parse()
     KERNEL = args.kernel
     IBM_GROUP = args.ibm_group
-    IBM_REFRESH = args.ibm_refresh
     if args.impl == "reference":
         return run_reference(args)
     import torch

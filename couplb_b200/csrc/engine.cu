@@ -195,12 +195,6 @@ int couplb_destroy(couplb_handle* h) {
   p = h->seg_force; dfree(p);
   p = h->skey; dfree(p);
   dfree(h->sbuf);
-  dfree(h->nmom);
-  p = h->seg_need; dfree(p);
-  p = h->seg_list; dfree(p);
-  p = h->seg_count; dfree(p);
-  if (h->h_seg_count) cudaFreeHost(h->h_seg_count);
-  if (h->seg_ev) cudaEventDestroy(h->seg_ev);
   p = h->d_ftot; dfree(p);
   p = h->d_corr; dfree(p);
   p = h->d_dF; dfree(p);
@@ -643,13 +637,6 @@ int couplb_set_option(couplb_handle* h, const char* name, long long value) {
     h->ibm_window = (int)value;
     return COUPLB_OK;
   }
-  if (!std::strcmp(name, "ibm_refresh")) {
-    if (value < -1 || value > 1) return fail(h, COUPLB_ERR_ARG, "ibm_refresh must be -1 (auto), 0 or 1");
-    h->ibm_refresh = (int)value;
-    h->refresh_node = 1;
-    h->refresh_calls = 0;
-    return COUPLB_OK;
-  }
   if (!std::strcmp(name, "ibm_slip")) {
     if (value != 0 && value != 1) return fail(h, COUPLB_ERR_ARG, "ibm_slip must be 0 or 1");
     h->ibm_slip = (int)value;
@@ -677,8 +664,6 @@ int couplb_get_option(couplb_handle* h, const char* name, long long* value) {
   if (!std::strcmp(name, "ibm_window")) { *value = h->ibm_window; return COUPLB_OK; }
   if (!std::strcmp(name, "ibm_group")) { *value = h->ibm_group; return COUPLB_OK; }
   if (!std::strcmp(name, "ibm_slip")) { *value = h->ibm_slip; return COUPLB_OK; }
-  if (!std::strcmp(name, "ibm_refresh")) { *value = h->ibm_refresh; return COUPLB_OK; }
-  if (!std::strcmp(name, "last_refresh")) { *value = h->last_refresh_node; return COUPLB_OK; }
   if (!std::strcmp(name, "timeouts")) {
     int rc = set_device(h);
     if (rc) return rc;

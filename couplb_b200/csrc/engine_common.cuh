@@ -146,28 +146,7 @@ inline void bump_epoch(couplb_handle* h) {
   if (++h->cur_epoch == 0xffffffffu) {
     h->cur_epoch = 0;
     if (h->skey) cudaMemsetAsync(h->skey, 0xff, sizeof(couplb::StencilKey) * (size_t)h->stencil_cap, h->stream);
-    if (h->seg_need) cudaMemsetAsync(h->seg_need, 0xff, sizeof(unsigned) * ((h->N + 7) / 8), h->stream);
   }
-}
-
-// Segment list of the node-centric refresh (seg_need starts at 0xffffffff,
-// an epoch never current; one list entry per segment at most, so N/8
-// entries never overflow) and, with moments, the dense moment array.
-inline int ensure_refresh_buffers(couplb_handle* h, bool moments) {
-  const size_t nseg = (h->N + 7) / 8;
-  int rc;
-  if (!h->seg_need) {
-    if ((rc = dalloc(h, (void**)&h->seg_need, sizeof(unsigned) * nseg))) return rc;
-    if ((rc = dalloc(h, (void**)&h->seg_list, sizeof(unsigned) * nseg))) return rc;
-    if ((rc = dalloc(h, (void**)&h->seg_count, sizeof(unsigned)))) return rc;
-    CK(cudaMemsetAsync(h->seg_need, 0xff, sizeof(unsigned) * nseg, h->stream));
-    CK(cudaMallocHost((void**)&h->h_seg_count, sizeof(unsigned)));
-    CK(cudaEventCreateWithFlags(&h->seg_ev, cudaEventDisableTiming));
-  }
-  if (moments && !h->nmom) {
-    if ((rc = dalloc(h, &h->nmom, 4 * elem_bytes_aux(h->p.precision) * h->N))) return rc;
-  }
-  return COUPLB_OK;
 }
 
 // Per-marker buffers of the correction passes and their state block.

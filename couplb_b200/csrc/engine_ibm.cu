@@ -27,16 +27,6 @@ int couplb_set_ibm_params(couplb_handle* h, const couplb_ibm_params* ip) {
 
 namespace couplb {
 
-// CK inside the launch lambda of engine_ibm: the status goes to lrc.
-#define CK_VOID(call)                                                                      \
-  do {                                                                                     \
-    cudaError_t e_ = (call);                                                               \
-    if (e_ != cudaSuccess) {                                                               \
-      lrc = fail(h, COUPLB_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));      \
-      return;                                                                              \
-    }                                                                                      \
-  } while (0)
-
 // Shared body of the host- and device-array IBM sub-step.  The launches of
 // the method kernels (launch_method) are compiled in engine_methods_*.cu.
 int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, const double* d_m,
@@ -109,7 +99,6 @@ int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, co
     a.dvr = dv / cell_vol;
     a.corr = method != COUPLB_IBM_SINGLE ? h->d_corr : nullptr;
     a.mlp = (method == COUPLB_IBM_LEARNED) ? h->mlp->pack : nullptr;
-    a.mom = nullptr;
     a.wrap = 0;
     if (h->ibm_window) {
       if (!g.face[0] && !g.face[1]) a.wrap |= 1;
@@ -124,46 +113,7 @@ int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, co
       a.zplanes[side] = bound ? h->ih_planes[side] : 0;
     }
     if (method == COUPLB_IBM_SINGLE) {
-      if (refresh && !a.all_valid) {
-        // per-marker or node-centric refresh (k_refresh_mark); auto: the
-        // node-centric one while the markers' windows list fewer nodes than
-        // the per-marker one visits, re-measured every 16th refresh
-        bool node = h->ibm_refresh == 1, measure = node;
-        if (h->ibm_refresh < 0) {
-          if (h->seg_pending && cudaEventQuery(h->seg_ev) == cudaSuccess) {
-            h->seg_pending = 0;
-            const unsigned long long visits = (unsigned long long)h->seg_markers * (L::D == 3 ? 64 : 16);
-            h->refresh_node = 8ull * *h->h_seg_count <= visits;
-            h->refresh_calls = 0;
-          }
-          node = h->refresh_node != 0;
-          measure = node || (++h->refresh_calls % 16 == 0);
-        }
-        if (measure) {
-          if ((lrc = ensure_refresh_buffers(h, node))) return;
-          CK_VOID(cudaMemsetAsync(h->seg_count, 0, sizeof(unsigned), h->stream));
-          constexpr int kRows = (L::D == 3) ? 16 : 4;
-          k_refresh_mark<L, S><<<flat_blocks((long long)n * kRows, bs), bs, 0, h->stream>>>(a, h->seg_need,
-                                                                                           h->seg_list, h->seg_count);
-          if (h->ibm_refresh < 0 && !h->seg_pending) {
-            CK_VOID(cudaMemcpyAsync(h->h_seg_count, h->seg_count, sizeof(unsigned), cudaMemcpyDeviceToHost,
-                                    h->stream));
-            CK_VOID(cudaEventRecord(h->seg_ev, h->stream));
-            h->seg_pending = 1;
-            h->seg_markers = n;
-          }
-        }
-        if (node) {
-          int sms = 0;
-          CK_VOID(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->p.device));
-          k_refresh_moments<L, S><<<(unsigned)(4 * sms), bs, 0, h->stream>>>(a, h->seg_list, h->seg_count,
-                                                                              (A*)h->nmom);
-          a.mom = (const A*)h->nmom;
-        }
-        h->last_refresh_node = node;
-        k_ibm_prefetch<L, S><<<nb, bs, 0, h->stream>>>(a);
-        a.mom = nullptr;
-      }
+      if (refresh && !a.all_valid) k_ibm_prefetch<L, S><<<nb, bs, 0, h->stream>>>(a);
       bool grouped = false;
       if constexpr (L::D == 3) {
         if (h->ibm_group == 8) {

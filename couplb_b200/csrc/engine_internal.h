@@ -76,19 +76,6 @@ struct couplb_handle {
   int pass_cur = 0;                  // the one of the last sub-step
   int ibm_resident = 1;              // option: register-resident form when markers fit
   int ibm_window = 0;                // option: 0 clip the IBM window like the reference, 1 wrap
-  // node-centric IBM refresh (option ibm_refresh; k_refresh_mark / _moments)
-  int ibm_refresh = -1;              // option: -1 auto, 0 per marker, 1 per needed node segment
-  void* nmom = nullptr;              // moments of the needed segments' nodes, 4 values per node
-  unsigned* seg_need = nullptr;      // per 8-node segment: epoch of the last refresh that listed it
-  unsigned* seg_list = nullptr;      // segments listed by the current refresh
-  unsigned* seg_count = nullptr;     // their number (device)
-  unsigned* h_seg_count = nullptr;   // pinned copy of the last measured count
-  cudaEvent_t seg_ev = nullptr;      // that copy is complete
-  int seg_pending = 0;               // a measured count awaits reading
-  long long seg_markers = 0;         // markers of the measured refresh
-  int refresh_node = 1;              // auto: the form of the next refresh
-  int last_refresh_node = 0;         // the form the last refresh ran (1: node-centric)
-  long long refresh_calls = 0;       // refreshes since the form was last measured
   int ibm_slip = 1;                  // option: ITERATIVE / LEARNED measure the slip after the last pass
   int ibm_group = 8;                 // option: lanes per marker of the single-pass 3D sub-step (8, 32)
   const void* halo[2] = {nullptr, nullptr};   // z-face halos of a slab decomposition

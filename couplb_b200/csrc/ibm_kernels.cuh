@@ -108,10 +108,6 @@ struct IbmArgs {
   const typename S::A* vh[2];
   typename S::A* fh[2];
   int zplanes[2];
-  // node-centric refresh: moments {ux, uy, uz, rho} (compute_velocity) of
-  // every node of the 8-node segments the markers' windows need, 4 values
-  // per node, or null (the refresh computes each marker's nodes itself)
-  const typename S::A* mom;
 };
 
 // Halo plane of the ghost-inclusive z index kg (0: the plane below the low
@@ -344,12 +340,7 @@ __device__ __forceinline__ void prefetch_marker(const IbmArgs<S>& a, int mk, int
     } else if (ig >= 0 && ig < gx && jg >= 0 && jg < gy && kg >= 0 && kg < gz &&
                classify_node(g, L::D, ig, jg, kg, ii, jj, kk) < 0) {
       const size_t n = (size_t)ii + (size_t)g.nx * ((size_t)jj + (size_t)g.ny * kk);
-      if (a.mom) {
-        const typename S::A* m = a.mom + 4 * n;
-        v[rep][0] = m[0]; v[rep][1] = m[1]; v[rep][2] = m[2]; v[rep][3] = m[3];
-      } else {
-        compute_velocity<L, S>(a, ii, jj, kk, n, v[rep][0], v[rep][1], v[rep][2], v[rep][3]);
-      }
+      compute_velocity<L, S>(a, ii, jj, kk, n, v[rep][0], v[rep][1], v[rep][2], v[rep][3]);
     }
   }
 #pragma unroll
@@ -359,79 +350,6 @@ __device__ __forceinline__ void prefetch_marker(const IbmArgs<S>& a, int mk, int
     rec[s] = v[rep][0]; rec[64 + s] = v[rep][1]; rec[128 + s] = v[rep][2]; rec[192 + s] = v[rep][3];
   }
   if (lane == 0) a.skey[mk] = StencilKey{i0, j0, k0, epoch};
-}
-
-// Node-centric refresh, for markers whose windows overlap (rods, surfaces
-// with markers closer than a cell): instead of every marker pulling its 4^D
-// nodes, (1) k_refresh_mark lists the 8-node segments of fluid nodes that
-// some window needs, each once (the epoch stamp of a segment makes the first
-// marker to reach it the one that appends it), (2) k_refresh_moments computes
-// the moments of every node of the listed segments, eight consecutive nodes
-// per segment so that the pulls of a plane are contiguous, and (3)
-// k_ibm_prefetch copies each marker's nodes from there into its record.  The
-// moments come from the same compute_velocity call as in the per-marker
-// refresh, so the records are the same bit for bit.
-//
-// (1): one thread per marker and window row (4^(D-1) rows of 4 x nodes); the
-// node classification is prefetch_marker's.  Planes beyond a bound slab face
-// come from the halo and are not listed.
-template <class L, class S>
-__global__ void __launch_bounds__(256) k_refresh_mark(const IbmArgs<S> a, unsigned* __restrict__ seg_need,
-                                                      unsigned* __restrict__ seg_list,
-                                                      unsigned* __restrict__ count) {
-  constexpr int kRows = (L::D == 3) ? 16 : 4;
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const int mk = (int)(t / kRows), row = (int)(t % kRows);
-  if (mk >= a.n) return;
-  if (a.active && !a.active[mk]) return;
-  const Geom& g = a.g;
-  const double lx = (a.x[3 * mk] - a.lo[0]) * a.inv_dx - a.off[0] + 1.0;
-  const double ly = (a.x[3 * mk + 1] - a.lo[1]) * a.inv_dx - a.off[1] + 1.0;
-  const double lz = (L::D == 3) ? ((a.x[3 * mk + 2] - a.lo[2]) * a.inv_dx - a.off[2] + 1.0) : 0.0;
-  const int i0 = (int)floor(lx), j0 = (int)floor(ly);
-  const int k0 = (L::D == 3) ? (int)floor(lz) : 0;
-  const int gx = g.nx + 2, gy = g.ny + 2, gz = (L::D == 3) ? g.nz + 2 : 1;
-  int jg = j0 - 1 + (row & 3);
-  int kg = (L::D == 3) ? k0 - 1 + (row >> 2) : 0;
-  if (a.wrap & 2) jg = wrap_ghost_index(jg, g.ny);
-  if (a.wrap & 4) kg = wrap_ghost_index(kg, g.nz);
-  if (L::D == 3 && z_halo_plane(a, kg) >= 0) return;
-  if (jg < 0 || jg >= gy || kg < 0 || kg >= gz) return;
-  long long last = -1;
-#pragma unroll
-  for (int o = 0; o < 4; o++) {
-    int ig = i0 - 1 + o;
-    if (a.wrap & 1) ig = wrap_ghost_index(ig, g.nx);
-    int ii = 0, jj = 0, kk = 0;
-    if (ig < 0 || ig >= gx || classify_node(g, L::D, ig, jg, kg, ii, jj, kk) >= 0) continue;
-    const long long seg = ((long long)ii + (long long)g.nx * ((long long)jj + (long long)g.ny * kk)) >> 3;
-    if (seg == last) continue;
-    last = seg;
-    if (atomicExch(seg_need + seg, a.cur_epoch) != a.cur_epoch) seg_list[atomicAdd(count, 1u)] = (unsigned)seg;
-  }
-}
-
-// (2): grid-stride over the listed segments' nodes (the count is read on the
-// device, so the host launches a fixed grid without waiting for it).
-template <class L, class S>
-__global__ void __launch_bounds__(256) k_refresh_moments(const IbmArgs<S> a, const unsigned* __restrict__ seg_list,
-                                                         const unsigned* __restrict__ count,
-                                                         typename S::A* __restrict__ mom) {
-  const Geom& g = a.g;
-  const long long total = 8LL * (long long)*count;
-  const long long N = (long long)g.nx * g.ny * ((L::D == 3) ? g.nz : 1);
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const long long n = 8LL * seg_list[t >> 3] + (t & 7);
-    if (n >= N) continue;
-    const int i = (int)(n % g.nx);
-    const long long r = n / g.nx;
-    const int j = (int)(r % g.ny), k = (int)(r / g.ny);
-    typename S::A v0, v1, v2, vr;
-    compute_velocity<L, S>(a, i, j, k, (size_t)n, v0, v1, v2, vr);
-    typename S::A* m = mom + 4 * n;
-    m[0] = v0; m[1] = v1; m[2] = v2; m[3] = vr;
-  }
 }
 
 // Refresh prefetch: one warp per active marker fills its slot's record.

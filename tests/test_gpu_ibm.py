@@ -315,75 +315,3 @@ def test_grouped_substep_fp64_matches_oracle(cuda_lib):
     assert rel(fg, fo) <= 1e-11, rel(fg, fo)
     for c in range(3):
         assert rel(Fg[c], Fo[c]) <= 1e-12, (c, rel(Fg[c], Fo[c]))
-
-
-def _refresh_case(prec, mode, markers, n=(36, 30, 28), wall=(0, 0, 1, 2, 0, 0), window=1, cycles=3):
-    """Forces per sub-step and the final force field with refresh form
-    `mode` (handle option ibm_refresh)."""
-    x0, v, m = markers
-    L = Lattice(3, *n, tau=0.7, wall=wall, wall_vel=(0.01, 0, 0), body_force=True, precision=prec)
-    L.set_option("ibm_refresh", mode)
-    L.set_option("ibm_window", window)
-    L.set_populations(cases.initial_populations(3, n, 9))
-    L.set_ibm_params(delta="peskin4", md_per_lb=2, xi_ibm=0.8)
-    x = x0.copy()
-    fs, forms = [], []
-    for c in range(cycles):
-        L.lbm_step((1e-5, 0.0, 2e-6))
-        for s in range(2):
-            x = np.ascontiguousarray(np.mod(x + 0.3 * v, np.array(n, float)))
-            fa = np.zeros_like(x)
-            L.ibm_substep(x, v, m, fa, refresh=(s == 0))
-            if s == 0:
-                forms.append(L.get_option("last_refresh"))
-            fs.append(fa)
-    F = [cases.interior(a, 3) for a in L.get_force_field()]
-    L.close()
-    return np.stack(fs), F, forms
-
-
-def _rod_markers(n, rods=6, per=40, seed=4):
-    from couplb_b200.markers import random_rods
-    x = random_rods(rods, per, n, seed, wall_margin=3.0)
-    rng = np.random.default_rng(seed)
-    v = np.repeat(0.01 * rng.standard_normal((rods, 3)), per, axis=0)
-    return x, v, np.ones(x.shape[0])
-
-
-def _sparse_markers(n, k=60, seed=5):
-    rng = np.random.default_rng(seed)
-    x = rng.uniform(0.0, 1.0, (k, 3)) * np.array(n, float)
-    return x, 0.01 * rng.standard_normal(x.shape), rng.uniform(0.5, 1.5, k)
-
-
-@pytest.mark.parametrize("prec", ["fp64", "fp32"])
-@pytest.mark.parametrize("window", [0, 1])
-@pytest.mark.parametrize("wall", [(0, 0, 1, 2, 0, 0), (0,) * 6])
-def test_node_centric_refresh_is_bit_identical(cuda_lib, prec, window, wall):
-    """ibm_refresh 1 (moments of the listed node segments, then copied into
-    the records) against 0 (every marker pulls its own nodes): the records
-    come from the same arithmetic, so forces and force field agree bit for
-    bit; rods of markers at unit spacing and sparse markers, walls, clipped
-    and wrapped windows."""
-    n = (36, 30, 28)
-    for markers in (_rod_markers(n), _sparse_markers(n)):
-        f0, F0, _ = _refresh_case(prec, 0, markers, n, wall, window)
-        f1, F1, forms = _refresh_case(prec, 1, markers, n, wall, window)
-        assert forms == [1, 1, 1]
-        np.testing.assert_array_equal(f1, f0)
-        for a, b in zip(F1, F0):
-            np.testing.assert_array_equal(a, b)
-
-
-def test_auto_refresh_picks_the_form_by_overlap(cuda_lib):
-    """ibm_refresh -1 (default): after its first (node-centric, measuring)
-    refresh, markers whose windows overlap (rods) stay node-centric and
-    sparse markers switch to the per-marker form; the forces are those of
-    either form."""
-    n = (36, 30, 28)
-    fr, _, forms_r = _refresh_case("fp64", -1, _rod_markers(n), n, cycles=4)
-    assert forms_r[0] == 1 and forms_r[-1] == 1
-    fs, _, forms_s = _refresh_case("fp64", -1, _sparse_markers(n), n, cycles=4)
-    assert forms_s[0] == 1 and forms_s[-1] == 0
-    f0, _, _ = _refresh_case("fp64", 0, _sparse_markers(n), n, cycles=4)
-    np.testing.assert_array_equal(fs, f0)
