@@ -73,8 +73,6 @@ def parse():
                     help="edge of the periodic box of the point-marker workload")
     ap.add_argument("--ibm-group", type=int, default=8, choices=[8, 32],
                     help="lanes per marker of the single-pass IBM sub-step (handle option ibm_group)")
-    ap.add_argument("--ibm-fill", type=int, default=0, choices=[0, 1],
-                    help="refresh sub-step fills its stencils in the same launch (handle option ibm_fill)")
     ap.add_argument("--nx", type=int, default=NX)
     ap.add_argument("--ny", type=int, default=NY)
     ap.add_argument("--nz", type=int, default=NZ)
@@ -166,7 +164,6 @@ class Clocks:
 # --------------------------------------------------------------------------
 KERNEL = -1
 IBM_GROUP = 8   # lanes per marker of the single-pass IBM sub-step
-IBM_FILL = 0    # 1: the refresh sub-step fills its stencils in the same launch
 
 
 def make_lattice(prec, nx, ny, nz, device):
@@ -283,7 +280,6 @@ def marker_bench(torch, device, prec, cycles, warmup, box, wall, tau, x0, v0, md
     # reference clips it at the ghost layer, option value 0)
     L.set_option("ibm_window", 1)
     L.set_option("ibm_group", IBM_GROUP)
-    L.set_option("ibm_fill", IBM_FILL)
     stream = torch.cuda.current_stream()
     L.set_stream(stream.cuda_stream)
     L.init_equilibrium(1.0)
@@ -741,11 +737,10 @@ def load_peak():
 
 
 def main():
-    global KERNEL, IBM_GROUP, IBM_FILL
+    global KERNEL, IBM_GROUP
     args = parse()
     KERNEL = args.kernel
     IBM_GROUP = args.ibm_group
-    IBM_FILL = args.ibm_fill
     if args.impl == "reference":
         return run_reference(args)
     import torch

@@ -637,11 +637,6 @@ int couplb_set_option(couplb_handle* h, const char* name, long long value) {
     h->ibm_window = (int)value;
     return COUPLB_OK;
   }
-  if (!std::strcmp(name, "ibm_fill")) {
-    if (value != 0 && value != 1) return fail(h, COUPLB_ERR_ARG, "ibm_fill must be 0 or 1");
-    h->ibm_fill = (int)value;
-    return COUPLB_OK;
-  }
   if (!std::strcmp(name, "ibm_slip")) {
     if (value != 0 && value != 1) return fail(h, COUPLB_ERR_ARG, "ibm_slip must be 0 or 1");
     h->ibm_slip = (int)value;
@@ -669,7 +664,6 @@ int couplb_get_option(couplb_handle* h, const char* name, long long* value) {
   if (!std::strcmp(name, "ibm_window")) { *value = h->ibm_window; return COUPLB_OK; }
   if (!std::strcmp(name, "ibm_group")) { *value = h->ibm_group; return COUPLB_OK; }
   if (!std::strcmp(name, "ibm_slip")) { *value = h->ibm_slip; return COUPLB_OK; }
-  if (!std::strcmp(name, "ibm_fill")) { *value = h->ibm_fill; return COUPLB_OK; }
   if (!std::strcmp(name, "timeouts")) {
     int rc = set_device(h);
     if (rc) return rc;

@@ -113,14 +113,7 @@ int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, co
       a.zplanes[side] = bound ? h->ih_planes[side] : 0;
     }
     if (method == COUPLB_IBM_SINGLE) {
-      const bool fill = refresh && !a.all_valid;
-      if (fill && h->ibm_fill) {
-        // the refresh sub-step as one launch that fills and steps
-        if (ip.delta == COUPLB_DELTA_ROMA) k_ibm_substep<L, S, 0, true><<<nb, bs, 0, h->stream>>>(a);
-        else k_ibm_substep<L, S, 1, true><<<nb, bs, 0, h->stream>>>(a);
-        return;
-      }
-      if (fill) k_ibm_prefetch<L, S><<<nb, bs, 0, h->stream>>>(a);
+      if (refresh && !a.all_valid) k_ibm_prefetch<L, S><<<nb, bs, 0, h->stream>>>(a);
       bool grouped = false;
       if constexpr (L::D == 3) {
         if (h->ibm_group == 8) {

@@ -76,7 +76,6 @@ struct couplb_handle {
   int pass_cur = 0;                  // the one of the last sub-step
   int ibm_resident = 1;              // option: register-resident form when markers fit
   int ibm_window = 0;                // option: 0 clip the IBM window like the reference, 1 wrap
-  int ibm_fill = 0;                  // option: the refresh sub-step fills its stencils in the same launch
   int ibm_slip = 1;                  // option: ITERATIVE / LEARNED measure the slip after the last pass
   int ibm_group = 8;                 // option: lanes per marker of the single-pass 3D sub-step (8, 32)
   const void* halo[2] = {nullptr, nullptr};   // z-face halos of a slab decomposition

@@ -607,15 +607,12 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
 // blockIdx % kFtotSlots with three FP64 atomics per block: with a few
 // thousand blocks per launch, per-marker atomics on the 64 slots queued in
 // L2 and took about as long as the rest of the sub-step (2e5 markers).
-// FILL: the refresh sub-step in one launch -- each warp computes its
-// marker's stencil from the populations (the work of k_ibm_prefetch), writes
-// the record for the later sub-steps and uses the values directly.
-template <class L, class S, int DELTA, bool FILL = false>
+template <class L, class S, int DELTA>
 __global__ void __launch_bounds__(256) k_ibm_substep(const IbmArgs<S> a) {
   __shared__ double part[8][3];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double t3[3] = {0.0, 0.0, 0.0};
-  ibm_substep_body<L, S, DELTA, false>(a, (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane, FILL,
+  ibm_substep_body<L, S, DELTA, false>(a, (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane, false,
                                        nullptr, nullptr, t3);
   if (!a.ftot) return;
   if (lane == 0) { part[warp][0] = t3[0]; part[warp][1] = t3[1]; part[warp][2] = t3[2]; }

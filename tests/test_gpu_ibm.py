@@ -236,7 +236,7 @@ def test_wrapped_window_matches_oracle(cuda_lib, wall):
         assert rel(a, b) <= 1e-12, (c, rel(a, b))
 
 
-def _grouped_case(prec, group, n=(40, 32, 24), cycles=3, md_per_lb=2, fill=0):
+def _grouped_case(prec, group, n=(40, 32, 24), cycles=3, md_per_lb=2):
     """Atom forces per sub-step and the final force field of a walled lattice
     with 300 markers: most windows inside the interior, some at the faces and
     walls; every second marker jumps 0.6 cells in x on each later sub-step
@@ -250,7 +250,6 @@ def _grouped_case(prec, group, n=(40, 32, 24), cycles=3, md_per_lb=2, fill=0):
     active = (np.arange(300) % 8 != 3).astype(np.int32)
     L = Lattice(3, *n, tau=0.7, wall=(0, 0, 1, 2, 0, 0), wall_vel=(0.01, 0, 0), body_force=True, precision=prec)
     L.set_option("ibm_group", group)
-    L.set_option("ibm_fill", fill)
     L.set_populations(cases.initial_populations(3, n, 7))
     L.set_ibm_params(delta="peskin4", md_per_lb=md_per_lb, xi_ibm=0.8)
     x = x0.copy()
@@ -316,15 +315,3 @@ def test_grouped_substep_fp64_matches_oracle(cuda_lib):
     assert rel(fg, fo) <= 1e-11, rel(fg, fo)
     for c in range(3):
         assert rel(Fg[c], Fo[c]) <= 1e-12, (c, rel(Fg[c], Fo[c]))
-
-
-@pytest.mark.parametrize("prec,tol", [("fp64", 1e-13), ("fp32", 2e-6)])
-def test_refresh_in_the_sub_step_launch(cuda_lib, prec, tol):
-    """ibm_fill 1: the refresh sub-step fills the stencils and steps in one
-    launch (warp per marker); the later sub-steps read the records it wrote.
-    Same forces as prefetch + grouped sub-steps up to the order of the sums."""
-    f1, F1 = _grouped_case(prec, 8, fill=1)
-    f0, F0 = _grouped_case(prec, 8, fill=0)
-    assert rel(f1, f0) <= tol, rel(f1, f0)
-    for c in range(3):
-        assert rel(F1[c], F0[c]) <= 10 * tol, (c, rel(F1[c], F0[c]))
