@@ -683,7 +683,7 @@ __global__ void __launch_bounds__(256, sizeof(typename S::A) == 4 ? 3 : 2) k_ibm
   __shared__ double part[8][3];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gl = lane & 7, gb = lane & ~7;
-  const int mk0 = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 4;
+  const int mk0 = (int)((((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 4);
   const int mk = mk0 + (lane >> 3);
   const Geom& g = a.g;
   const bool in = mk < a.n;
