@@ -52,6 +52,12 @@ int engine_atom_host_buffers(couplb_handle* h, int n, double** mass, int** activ
   return COUPLB_OK;
 }
 
+void engine_atom_host_hint(couplb_handle* h, int n, int count, int unchanged) {
+  h->hint_n = n;
+  h->hint_count = count;
+  h->hint_unchanged = unchanged;
+}
+
 int engine_macro(couplb_handle* h) {
   int rc = ensure_macro(h);
   if (rc) return rc;

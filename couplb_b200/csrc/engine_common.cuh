@@ -186,6 +186,7 @@ inline int ensure_atoms(couplb_handle* h, int n) {
   CK(cudaMallocHost(&h->h_mass, sizeof(double) * cap));
   CK(cudaMallocHost(&h->h_active, sizeof(int) * cap));
   h->atom_cap = cap;
+  h->statics_n = -1;
   return COUPLB_OK;
 }
 

@@ -172,14 +172,26 @@ int stage_host_atoms(couplb_handle* h, cudaStream_t s, int n, const double* x, c
   if (n < 0 || (n > 0 && (!x || !v || !mass))) return fail(h, COUPLB_ERR_ARG, "bad atom arrays");
   int rc = ensure_atoms(h, n);
   if (rc) return rc;
+  // the fix core's pinned mass / group buffers come with their count and
+  // whether they changed since their last device copy
+  const bool pinned = mass == h->h_mass && active == h->h_active && h->hint_n == n;
   int c = 0;
-  for (int a = 0; a < n; a++) c += active ? (active[a] != 0) : 1;
+  if (pinned) {
+    c = h->hint_count;
+  } else {
+    for (int a = 0; a < n; a++) c += active ? (active[a] != 0) : 1;
+  }
+  const bool statics_current = pinned && h->hint_unchanged && h->statics_n == n;
+  h->hint_n = -1;
   *nc = c;
   if (n > 0) {
     CK(cudaMemcpyAsync(h->d_x, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(h->d_v, v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(h->d_m, mass, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-    if (active) CK(cudaMemcpyAsync(h->d_active, active, sizeof(int) * n, cudaMemcpyHostToDevice, s));
+    if (!statics_current) {
+      CK(cudaMemcpyAsync(h->d_m, mass, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+      if (active) CK(cudaMemcpyAsync(h->d_active, active, sizeof(int) * n, cudaMemcpyHostToDevice, s));
+    }
+    h->statics_n = (pinned && active) ? n : -1;
   }
   return COUPLB_OK;
 }

@@ -63,6 +63,11 @@ struct couplb_handle {
   double* h_mass = nullptr;          // pinned host staging of the per-atom masses
   int* h_active = nullptr;           // pinned host staging of the group flags
   int atom_cap = 0;
+  // staging hint of the fix core (engine_atom_host_hint): for the next
+  // host-array sub-step of hint_n atoms from h_mass / h_active, their group
+  // count and whether they are unchanged since their last device copy
+  int hint_n = -1, hint_count = 0, hint_unchanged = 0;
+  int statics_n = -1;                // d_m / d_active hold the pinned buffers' n atoms
 
   // IBM forcing method (couplb_set_ibm_method)
   int ibm_method = 0;                // COUPLB_IBM_*
@@ -105,6 +110,10 @@ int engine_lbm_step(couplb_handle* h, const double* g_lb);
 // arrays before couplb_ibm_substep, so that every host->device copy of a
 // sub-step starts from pinned memory.
 int engine_atom_host_buffers(couplb_handle* h, int n, double** mass, int** active);
+// After filling those buffers: the group count and whether the values are
+// the ones of the previous fill, so the next sub-step neither recounts nor
+// copies them again.
+void engine_atom_host_hint(couplb_handle* h, int n, int count, int unchanged);
 int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, const double* d_m,
                const int* d_active, double* d_fout, int accumulate, int refresh);
 }  // namespace couplb

@@ -429,12 +429,18 @@ int ibm_sub_coupling(couplb_fix* F, const couplb_atoms* at, bool lbm = false,
   int rc0 = couplb::engine_atom_host_buffers(F->h, nl, &mass_buf, &active_buf);
   if (rc0) return F->engine_fail(rc0);
   int ng = 0;
+  bool changed = false;
   for (int i = 0; i < nl; i++) {
     const int act = at->mask ? ((at->mask[i] & at->groupbit) != 0) : 1;
-    active_buf[i] = act;
+    const double m = at->rmass ? at->rmass[i] : (at->mass ? at->mass[at->type[i]] : 1.0);
+    if (active_buf[i] != act || !(mass_buf[i] == m)) {
+      changed = true;
+      active_buf[i] = act;
+      mass_buf[i] = m;
+    }
     ng += act;
-    mass_buf[i] = at->rmass ? at->rmass[i] : (at->mass ? at->mass[at->type[i]] : 1.0);
   }
+  couplb::engine_atom_host_hint(F->h, nl, ng, changed ? 0 : 1);
   if (ng == 0) {
     F->ibm_has_particles = false;
     if (lbm) {
