@@ -463,7 +463,9 @@ def e2e_ibm_fix(torch, device, cycles, warmup, peak, n=256, natoms=20000, md_per
             "precision": "fp32", "cycles": cycles, "ms_per_lb_cycle": ms,
             "mlups": nodes / (ms * 1e-3) / 1e6, "marker_updates_per_s": natoms * md_per_lb / (ms * 1e-3),
             "roofline_frac": (nodes * b_lu + natoms * md_per_lb * b_mk) / (ms * 1e-3) / 1e9 / peak,
-            "h2d_bytes_per_lb_cycle": md_per_lb * natoms * (3 * 8 + 3 * 8 + 8 + 4),
+            # x and v every sub-step; masses and group flags are unchanged
+            # here, so the fix path copies them once, not per sub-step
+            "h2d_bytes_per_lb_cycle": md_per_lb * natoms * (3 * 8 + 3 * 8),
             "d2h_bytes_per_lb_cycle": md_per_lb * natoms * 3 * 8,
             "path": "couplb_fix_post_force + couplb_fix_end_of_step, pinned host atom arrays",
             "ibm_window": "wrap (periodic axes)",
