@@ -28,7 +28,7 @@ int materialize(couplb_handle* h) {
     using S = decltype(s);
     using T = typename S::T;
     k_materialize<L, S><<<grid, block, 0, h->stream>>>(g, (const T*)h->f[h->cur],
-                                                       (const typename S::D*)h->rho_field,
+                                                       (const typename S::A*)h->rho_field,
                                                        (T*)h->f[1 - h->cur]);
   });
   CK_LAUNCH();
@@ -74,7 +74,7 @@ int engine_macro(couplb_handle* h) {
     MacroArgs<S> a;
     a.g = g;
     a.fin = (const T*)h->f[h->cur];
-    a.rho_field = (const typename S::D*)h->rho_field;
+    a.rho_field = (const A*)h->rho_field;
     a.rho = (A*)h->macro[0]; a.ux = (A*)h->macro[1]; a.uy = (A*)h->macro[2]; a.uz = (A*)h->macro[3];
     a.status = h->d_status;
     if (pull) k_macro<L, S, true><<<grid, block, 0, h->stream>>>(a);
@@ -152,8 +152,7 @@ int couplb_create(const couplb_lattice_params* p, couplb_handle** out) {
   if (!rc) rc = dalloc(h, &h->F, 4 * ab * h->qs);
   h->moving_walls = false;
   for (int f = 0; f < (p->dim == 3 ? 6 : 4); f++) h->moving_walls |= (p->wall[f] == 2);
-  if (!rc && (p->body_force || h->moving_walls))
-    rc = dalloc(h, &h->rho_field, (p->precision == COUPLB_FP64 ? 8 : 2) * h->qs);
+  if (!rc && (p->body_force || h->moving_walls)) rc = dalloc(h, &h->rho_field, ab * h->qs);
   h->idx32 = ((unsigned long long)Q * h->qs < (1ULL << 32));
   if (!rc) rc = dalloc(h, (void**)&h->d_status, sizeof(int) * 8);
   if (!rc) rc = dalloc(h, (void**)&h->d_ftot, sizeof(double) * 4 * kFtotSlots);
@@ -259,7 +258,7 @@ int couplb_init_equilibrium(couplb_handle* h, double rho, double ux, double uy, 
     using S = decltype(s);
     k_init_eq<L, S><<<flat_blocks(N, 256), 256, 0, h->stream>>>(
         g, (typename S::T*)h->f[0], rho, ux, uy, h->p.dim == 3 ? uz : 0.0,
-        (typename S::D*)h->rho_field);
+        (typename S::A*)h->rho_field);
   });
   CK_LAUNCH();
   h->cur = 0;
@@ -354,7 +353,7 @@ int engine_lbm_step(couplb_handle* h, const double* g_lb) {
     a.fout = (T*)h->f[1 - h->cur];
     a.F = h->force_dirty ? (A*)h->F : nullptr;
     a.seg_force = h->force_rows_all ? nullptr : h->seg_force;
-    a.rho_field = (typename S::D*)h->rho_field;
+    a.rho_field = (A*)h->rho_field;
     a.rho_mode = rho_mode;
     a.write_rho = h->p.body_force ? 2 : (h->moving_walls ? 1 : 0);
     for (int d = 0; d < 3; d++) a.grav[d] = g_active ? g_lb[d] : 0.0;

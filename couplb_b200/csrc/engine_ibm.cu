@@ -73,7 +73,7 @@ int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, co
     IbmArgs<S> a;
     a.g = g;
     a.fin = (const typename S::T*)h->f[h->cur];
-    a.rho_field = (const typename S::D*)h->rho_field;
+    a.rho_field = (const A*)h->rho_field;
     a.pull = h->poststream ? 0 : 1;
     a.cux = (const A*)h->macro[1]; a.cuy = (const A*)h->macro[2]; a.cuz = (const A*)h->macro[3];
     a.all_valid = h->macro_valid;
@@ -323,7 +323,7 @@ int couplb_ibm_halo_moments(couplb_handle* h, int side, int planes, void* d_out)
       IbmArgs<S> a{};
       a.g = g;
       a.fin = (const typename S::T*)h->f[h->cur];
-      a.rho_field = (const typename S::D*)h->rho_field;
+      a.rho_field = (const A*)h->rho_field;
       a.pull = h->poststream ? 0 : 1;
       k_halo_moments<L, S><<<flat_blocks(cnt, 256), 256, 0, h->stream>>>(a, side, planes, (A*)d_out);
     }

@@ -67,7 +67,7 @@ struct IbmArgs {
   Geom g;
   // populations of the current state and how to read them
   const typename S::T* __restrict__ fin;
-  const typename S::D* __restrict__ rho_field;
+  const typename S::A* __restrict__ rho_field;
   int pull;                               // 1: post-collision store (pull), 0: post-stream
   // dense moment arrays, used when they hold this state everywhere
   const typename S::A* cux;

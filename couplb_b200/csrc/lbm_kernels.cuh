@@ -77,7 +77,7 @@ struct LBArgs {
   // zeroing the nonzero entries
   typename S::A* __restrict__ F;
   const unsigned char* __restrict__ seg_force;  // per 8 nodes (n >> 3): force present, or null = all
-  typename S::D* __restrict__ rho_field;  // stale density (see RhoMode)
+  typename S::A* __restrict__ rho_field;  // stale density (see RhoMode)
   int rho_mode;
   int write_rho;
   double grav[3];
@@ -107,10 +107,10 @@ __device__ __forceinline__ Cf clamp_rho(Cf r, int* status, int slot) {
 // i.e. the clamped density the previous fused launch computed at n, which it
 // stored in the density field; floored at RHO_CLAMP_FRAC * rho0.
 template <class S>
-__device__ __forceinline__ typename S::C moving_wall_rho(const typename S::D* rho_field, size_t n,
+__device__ __forceinline__ typename S::C moving_wall_rho(const typename S::A* rho_field, size_t n,
                                                          double rho0) {
   using C = typename S::C;
-  const C r = S::kShift ? C(rho0) + S::rd(rho_field + n) : S::rd(rho_field + n);
+  const C r = S::kShift ? C(rho0) + C(rho_field[n]) : C(rho_field[n]);
   const C fl = C(RHO_CLAMP_FRAC * rho0 < RHO_MIN ? RHO_MIN : RHO_CLAMP_FRAC * rho0);
   return (r < fl) ? fl : r;
 }
@@ -130,7 +130,7 @@ __device__ __forceinline__ bool near_moving_wall(const Geom& g, int i, int j, in
 // decides the rule, and a ghost node without wall is a periodic image.
 template <class L, class S, class I>
 __device__ __forceinline__ void pull_general(const Geom& g, const typename S::T* __restrict__ fin,
-                                             const typename S::D* __restrict__ rho_field, int i,
+                                             const typename S::A* __restrict__ rho_field, int i,
                                              int j, int k, I n, typename S::C (&f)[L::Q]) {
   using C = typename S::C;
   const I qs = (I)g.qs;
@@ -208,7 +208,7 @@ __device__ __forceinline__ bool row_is_interior(const Geom& g, int j, int k) {
 
 template <class L, class S, class I, bool kPull>
 __device__ __forceinline__ void load_node(const Geom& g, const typename S::T* __restrict__ fin,
-                                          const typename S::D* __restrict__ rho_field, int i,
+                                          const typename S::A* __restrict__ rho_field, int i,
                                           int j, int k, I n, typename S::C (&f)[L::Q]) {
   if (!kPull) {
     const I qs = (I)g.qs;
@@ -375,14 +375,14 @@ __device__ __forceinline__ void node_update(const LBArgs<S>& a, typename S::C (&
 
   if (a.rho_mode != kRhoNone) {
     C rp;
-    if (a.rho_mode == kRhoField) rp = S::kShift ? C(g.rho0) + S::rd(a.rho_field + n) : S::rd(a.rho_field + n);
+    if (a.rho_mode == kRhoField) rp = S::kShift ? C(g.rho0) + C(a.rho_field[n]) : C(a.rho_field[n]);
     else rp = rho;
     Fx += C(a.grav[0]) * rp;
     Fy += C(a.grav[1]) * rp;
     Fz += C(a.grav[2]) * rp;
   }
   if (a.write_rho == 2 || (a.write_rho == 1 && near_moving_wall<L>(g, i, j, k)))
-    S::wr(a.rho_field + n, S::kShift ? r : rho);
+    a.rho_field[n] = typename S::A(S::kShift ? r : rho);
 
   // compute_macroscopic(true): u = (sum e f + F/2) / rho
   const C inv_r = C(1) / rho;
@@ -426,7 +426,7 @@ template <class S>
 struct MacroArgs {
   Geom g;
   const typename S::T* __restrict__ fin;
-  const typename S::D* __restrict__ rho_field;
+  const typename S::A* __restrict__ rho_field;
   typename S::A* __restrict__ rho;
   typename S::A* __restrict__ ux;
   typename S::A* __restrict__ uy;
@@ -461,7 +461,7 @@ __global__ void __launch_bounds__(256) k_macro(const MacroArgs<S> a) {
 // (streaming alone), so it can be exported or restarted from.
 template <class L, class S>
 __global__ void __launch_bounds__(256) k_materialize(Geom g, const typename S::T* __restrict__ fin,
-                                                     const typename S::D* __restrict__ rho_field,
+                                                     const typename S::A* __restrict__ rho_field,
                                                      typename S::T* __restrict__ fout) {
   using C = typename S::C;
   using I = size_t;
@@ -478,7 +478,7 @@ __global__ void __launch_bounds__(256) k_materialize(Geom g, const typename S::T
 // Equilibrium initial state (Grid::init_equilibrium, couplb_lattice.h:137-154).
 template <class L, class S>
 __global__ void k_init_eq(Geom g, typename S::T* __restrict__ f, double rho, double ux, double uy,
-                          double uz, typename S::D* __restrict__ rho_field) {
+                          double uz, typename S::A* __restrict__ rho_field) {
   const long long N = (long long)g.nx * g.ny * g.nz;
   const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
@@ -490,7 +490,7 @@ __global__ void k_init_eq(Geom g, typename S::T* __restrict__ f, double rho, dou
     const double fe = L::w(q) * rho * (1.0 + eu / cs2 + 0.5 * eu * eu / cs4 - 0.5 * uu / cs2);
     S::st(f + pidx<L, S, long long>(q, n, g.qs), typename S::C(S::kShift ? fe - L::w(q) * g.rho0 : fe));
   }
-  if (rho_field) S::wr(rho_field + n, typename S::C(S::kShift ? rho - g.rho0 : rho));
+  if (rho_field) rho_field[n] = typename S::A(S::kShift ? rho - g.rho0 : rho);
 }
 
 // Import of reference-layout populations (double, ghost-inclusive G nodes):

@@ -123,21 +123,16 @@ __device__ __forceinline__ void x2_node_pair(const LBArgs<S>& a, int i0, int j, 
 
   if (a.rho_mode != kRhoNone) {
     float2 rp = rho;
-    if (a.rho_mode == kRhoField) {
-      // two half deviations of the density field (n0 even: 4-byte aligned)
-      const float2 d = __half22float2(*reinterpret_cast<const __half2*>(a.rho_field + n0));
-      rp = add2(f2(rho0), make_float2(d.x * S::kRhoInvScale, d.y * S::kRhoInvScale));
-    }
+    if (a.rho_mode == kRhoField) rp = add2(f2(rho0), *reinterpret_cast<const float2*>(a.rho_field + n0));
     Fx = fma2(f2(float(a.grav[0])), rp, Fx);
     Fy = fma2(f2(float(a.grav[1])), rp, Fy);
     Fz = fma2(f2(float(a.grav[2])), rp, Fz);
   }
   if (a.write_rho == 2) {
-    *reinterpret_cast<__half2*>(a.rho_field + n0) =
-        __floats2half2_rn(r.x * S::kRhoScale, r.y * S::kRhoScale);
+    *reinterpret_cast<float2*>(a.rho_field + n0) = r;
   } else if (a.write_rho == 1) {
-    if (near_moving_wall<L>(g, i0, j, k)) S::wr(a.rho_field + n0, r.x);
-    if (near_moving_wall<L>(g, i0 + 1, j, k)) S::wr(a.rho_field + n0 + 1, r.y);
+    if (near_moving_wall<L>(g, i0, j, k)) a.rho_field[n0] = r.x;
+    if (near_moving_wall<L>(g, i0 + 1, j, k)) a.rho_field[n0 + 1] = r.y;
   }
 
   // u = (j + F/2) / rho

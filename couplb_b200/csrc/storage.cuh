@@ -24,39 +24,21 @@
 
 namespace couplb {
 
-// D: the density field (the density of the last fused launch, which the
-// body force and the moving-wall rule read; the deviation from rho0 for the
-// shifted formats), rd / wr its access.  The shifted formats keep it as IEEE
-// half of the deviation scaled by 2^10 (|rho - rho0| < 64; absolute error
-// below 3e-8 for deviations under 1e-4): the field is read and written every
-// step, and 2 B instead of 4 B per node is 2.5 % of the fused kernel's
-// traffic.
 struct StoreF64 {
   using T = double;  // stored population
   using C = double;  // arithmetic
-  using A = double;  // auxiliary fields (force, moments)
-  using D = double;  // density field
+  using A = double;  // auxiliary fields (force, density, moments)
   static constexpr bool kShift = false;
   static constexpr int kTile = 0;
   __device__ __forceinline__ static C ld(const T* p) { return __ldg(p); }
   __device__ __forceinline__ static C ld_shared(const T* p) { return *p; }
   __device__ __forceinline__ static void st(T* p, C v) { *p = v; }
-  __device__ __forceinline__ static C rd(const D* p) { return *p; }
-  __device__ __forceinline__ static void wr(D* p, C v) { *p = v; }
 };
 
-struct DensityHalf {
-  static constexpr float kRhoScale = 1024.0f;
-  static constexpr float kRhoInvScale = 1.0f / 1024.0f;
-  __device__ __forceinline__ static float rd(const __half* p) { return __half2float(*p) * kRhoInvScale; }
-  __device__ __forceinline__ static void wr(__half* p, float v) { *p = __float2half_rn(v * kRhoScale); }
-};
-
-struct StoreF32S : DensityHalf {
+struct StoreF32S {
   using T = float;
   using C = float;
   using A = float;
-  using D = __half;
   static constexpr bool kShift = true;
   static constexpr int kTile = 0;
   __device__ __forceinline__ static C ld(const T* p) { return __ldg(p); }
@@ -64,11 +46,10 @@ struct StoreF32S : DensityHalf {
   __device__ __forceinline__ static void st(T* p, C v) { *p = v; }
 };
 
-struct StoreF16S : DensityHalf {
+struct StoreF16S {
   using T = __half;
   using C = float;
   using A = float;
-  using D = __half;
   static constexpr bool kShift = true;
   static constexpr int kTile = 0;
   static constexpr float kScale = 32768.0f;
