@@ -15,10 +15,14 @@
 //
 // Layout in HBM (kTile, read through pidx in lbm_kernels.cuh): 0 = one plane
 // per population, element q * qs + n; kTile > 0 = tiles of kTile consecutive
-// nodes x Q planes, one 32-byte sector per plane and tile.  Every format is
-// plane-major: measured on the D3Q19 workloads, tiles (FP32, kTile 8) cut the
-// IBM refresh of 20000 markers in 256^3 from ~165 to ~113 us but slowed the
-// fused LB kernel by 7 % (37.2 -> 34.6 GLUPS on 256x128x128).
+// nodes x Q planes.  FP32-shifted uses tiles of 64 nodes (256 B per plane and
+// tile, the span of one warp of the packed kernel): the IBM refresh, which
+// reads 19 short rows around each stencil node, then finds them within one
+// 4.9 KB tile instead of 19 planes 64 MB apart.  Measured on the D3Q19
+// workloads against plane-major: fused LB kernel unchanged (36.6 vs 36.7
+// GLUPS on 256x128x128), LBM + IBM cycle 0.729 -> 0.710 ms (256^3, 20000
+// markers) and 1.560 -> 1.511 ms (rods); tiles of 8 nodes cut the refresh
+// more but slowed the LB kernel by 7 %, tiles of 32 by 2 %.
 #pragma once
 #include <cuda_fp16.h>
 
@@ -40,7 +44,7 @@ struct StoreF32S {
   using C = float;
   using A = float;
   static constexpr bool kShift = true;
-  static constexpr int kTile = 0;
+  static constexpr int kTile = 64;
   __device__ __forceinline__ static C ld(const T* p) { return __ldg(p); }
   __device__ __forceinline__ static C ld_shared(const T* p) { return *p; }
   __device__ __forceinline__ static void st(T* p, C v) { *p = v; }
