@@ -556,7 +556,7 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
     if (valid && lane < 3) xs[81 + lane] = float((lane == 0 ? vmk0 : (lane == 1 ? vmk1 : vmk2)) / a.vs);
     __syncwarp();
     float y[3];
-    mlp_block_forward(*P, *blk, threadIdx.x >> 5, lane, y);
+    mlp_block_forward<false>(*P, *blk, threadIdx.x >> 5, lane, y);
     if (!valid) return;
     const double sc = mass * a.xi_over_dt * a.vs;
     const double c0 = sc * double(y[0]), c1 = sc * double(y[1]), c2 = sc * double(y[2]);

@@ -594,7 +594,7 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
     // the network for the block's markers (every warp takes part)
     __syncwarp();
     float y[3];
-    mlp_block_forward(*net, *blk, threadIdx.x >> 5, lane, y);
+    mlp_block_forward<true>(*net, *blk, threadIdx.x >> 5, lane, y);
     if (have) {
       const double sc = mxi * a.vs;
       c0 = sc * double(y[0]); c1 = sc * double(y[1]); c2 = sc * double(y[2]);

@@ -109,70 +109,96 @@ __device__ __forceinline__ void mma_rows8(float (&d)[4], uint32_t a0, uint32_t a
       : "r"(a0), "r"(0u), "r"(a2), "r"(0u), "r"(b0), "r"(b1));
 }
 
+// One k-step of 16 of a tile: the FP32 activations split into three BF16
+// parts, each into its own accumulator (three independent MMA chains).
+__device__ __forceinline__ void mlp_kstep(float (&ah)[4], float (&am)[4], float (&al)[4], const float* ar,
+                                          const __nv_bfloat16* wr, int k0, float sa) {
+  const float2 x0 = *reinterpret_cast<const float2*>(ar + k0);
+  const float2 x1 = *reinterpret_cast<const float2*>(ar + k0 + 8);
+  uint32_t h0, m0, l0, h1, m1, l1;
+  split3(x0.x * sa, x0.y * sa, h0, m0, l0);
+  split3(x1.x * sa, x1.y * sa, h1, m1, l1);
+  const uint32_t b0 = *reinterpret_cast<const uint32_t*>(wr + k0);
+  const uint32_t b1 = *reinterpret_cast<const uint32_t*>(wr + k0 + 8);
+  mma_rows8(ah, h0, h1, b0, b1);
+  mma_rows8(am, m0, m1, b0, b1);
+  mma_rows8(al, l0, l1, b0, b1);
+}
+
 // acc (8 x 8 tile: rows = the block's markers, columns = 8 outputs starting at
 // row n0 of W) += A[8][K] W^T, A FP32 rows of stride as (scaled by sa), W BF16
-// rows of stride ws.  K is a runtime multiple of 16 and the k loop is not
-// unrolled: the sub-step kernels that call this run once per SM per launch,
-// and their time goes to fetching instructions, so one compact loop body
-// serves all three layers.
+// rows of stride ws.  COMPACT: K at run time and the k loop not unrolled --
+// for launches that run once per SM (few markers), whose time goes to
+// fetching instructions; otherwise K at compile time, unrolled, for launches
+// that loop over many markers.  Same sums in the same order either way.
+template <bool COMPACT, int KC = 0>
 __device__ __forceinline__ void mlp_tile(float (&acc)[4], const float* A, int as, float sa,
                                          const __nv_bfloat16* W, int ws, int n0, int K, int lane) {
   const int g = lane >> 2, t = lane & 3;
   const float* ar = A + g * as + 2 * t;
   const __nv_bfloat16* wr = W + (n0 + g) * ws + 2 * t;
-  // one accumulator per part of the split: three independent MMA chains
   float ah[4] = {0.f, 0.f, 0.f, 0.f}, am[4] = {0.f, 0.f, 0.f, 0.f}, al[4] = {0.f, 0.f, 0.f, 0.f};
+  if constexpr (COMPACT) {
 #pragma unroll 1
-  for (int k0 = 0; k0 < K; k0 += 16) {
-    const float2 x0 = *reinterpret_cast<const float2*>(ar + k0);
-    const float2 x1 = *reinterpret_cast<const float2*>(ar + k0 + 8);
-    uint32_t h0, m0, l0, h1, m1, l1;
-    split3(x0.x * sa, x0.y * sa, h0, m0, l0);
-    split3(x1.x * sa, x1.y * sa, h1, m1, l1);
-    const uint32_t b0 = *reinterpret_cast<const uint32_t*>(wr + k0);
-    const uint32_t b1 = *reinterpret_cast<const uint32_t*>(wr + k0 + 8);
-    mma_rows8(ah, h0, h1, b0, b1);
-    mma_rows8(am, m0, m1, b0, b1);
-    mma_rows8(al, l0, l1, b0, b1);
+    for (int k0 = 0; k0 < K; k0 += 16) mlp_kstep(ah, am, al, ar, wr, k0, sa);
+  } else {
+#pragma unroll
+    for (int k0 = 0; k0 < KC; k0 += 16) mlp_kstep(ah, am, al, ar, wr, k0, sa);
   }
 #pragma unroll
   for (int i = 0; i < 4; i++) acc[i] += ah[i] + (am[i] + al[i]);
 }
 
+// Output tile of layer `layer` (0, 1, 2) for warp `warp`: warp w forms
+// outputs 8w..8w+7 of layers 1 and 2, warp 0 the three of layer 3.
+template <bool COMPACT>
+__device__ __forceinline__ void mlp_layer(const MlpPacked& P, MlpBlockScratch& S, int layer, int warp, int lane) {
+  const int g = lane >> 2, t = lane & 3;
+  const bool first = layer == 0;
+  const float* A = first ? S.x : (layer == 1 ? S.h1 : S.h2);
+  const __nv_bfloat16* W = first ? P.w1 : (layer == 1 ? P.w2 : P.w3);
+  const int n0 = layer < 2 ? 8 * warp : 0;
+  float acc[4] = {0.f, 0.f, 0.f, 0.f};
+  if (COMPACT || !first)
+    mlp_tile<COMPACT, kMlpHid>(acc, A, first ? kMlpXStride : kMlpHStride, first ? P.s_in : 1.f, W,
+                               first ? kMlpW1Stride : kMlpW2Stride, n0, first ? kMlpInPad : kMlpHid, lane);
+  else
+    mlp_tile<false, kMlpInPad>(acc, A, kMlpXStride, P.s_in, W, kMlpW1Stride, n0, kMlpInPad, lane);
+  const int j = n0 + 2 * t;
+  if (layer < 2) {
+    const float* b = first ? P.b1 : P.b2;
+    float* H = first ? S.h1 : S.h2;
+    H[g * kMlpHStride + j] = fmaxf(acc[0] + b[j], 0.f);
+    H[g * kMlpHStride + j + 1] = fmaxf(acc[1] + b[j + 1], 0.f);
+  } else {
+    if (j < kMlpOut) S.y[g * 4 + j] = (acc[0] + P.b3[j]) / P.s_out;
+    if (j + 1 < kMlpOut) S.y[g * 4 + j + 1] = (acc[1] + P.b3[j + 1]) / P.s_out;
+  }
+}
+
 // Forward pass of the block's 8 rows (all 256 threads call it, after each
 // warp has written its row of S.x); every lane of warp w gets row w's outputs.
 //   h1 = relu(W1 (s_in x) + b1), h2 = relu(W2 h1 + b2), y = (W3 h2 + b3) / s_out.
-// Layer l: warp w forms outputs 8w..8w+7 (layers 1, 2) or warp 0 the three
-// outputs (layer 3); one loop over the layers keeps the code compact.
+// COMPACT (see mlp_tile): one loop over the layers; otherwise unrolled.
+template <bool COMPACT>
 __device__ __forceinline__ void mlp_block_forward(const MlpPacked& P, MlpBlockScratch& S, int warp,
                                                   int lane, float y[3]) {
-  const int g = lane >> 2, t = lane & 3;
   // this thread's part of an asynchronous staging of P (mlp_stage_async;
   // nothing pending otherwise), published to the block by the barrier
   asm volatile("cp.async.wait_all;" ::: "memory");
   __syncthreads();
+  if constexpr (COMPACT) {
 #pragma unroll 1
-  for (int layer = 0; layer < 3; layer++) {
-    if (layer < 2 || warp == 0) {
-      const bool first = layer == 0;
-      const float* A = first ? S.x : (layer == 1 ? S.h1 : S.h2);
-      const __nv_bfloat16* W = first ? P.w1 : (layer == 1 ? P.w2 : P.w3);
-      const int n0 = layer < 2 ? 8 * warp : 0;
-      float acc[4] = {0.f, 0.f, 0.f, 0.f};
-      mlp_tile(acc, A, first ? kMlpXStride : kMlpHStride, first ? P.s_in : 1.f, W,
-               first ? kMlpW1Stride : kMlpW2Stride, n0, first ? kMlpInPad : kMlpHid, lane);
-      const int j = n0 + 2 * t;
-      if (layer < 2) {
-        const float* b = first ? P.b1 : P.b2;
-        float* H = first ? S.h1 : S.h2;
-        H[g * kMlpHStride + j] = fmaxf(acc[0] + b[j], 0.f);
-        H[g * kMlpHStride + j + 1] = fmaxf(acc[1] + b[j + 1], 0.f);
-      } else {
-        if (j < kMlpOut) S.y[g * 4 + j] = (acc[0] + P.b3[j]) / P.s_out;
-        if (j + 1 < kMlpOut) S.y[g * 4 + j + 1] = (acc[1] + P.b3[j + 1]) / P.s_out;
-      }
+    for (int layer = 0; layer < 3; layer++) {
+      if (layer < 2 || warp == 0) mlp_layer<true>(P, S, layer, warp, lane);
+      __syncthreads();
     }
-    __syncthreads();
+  } else {
+#pragma unroll
+    for (int layer = 0; layer < 3; layer++) {
+      if (layer < 2 || warp == 0) mlp_layer<false>(P, S, layer, warp, lane);
+      __syncthreads();
+    }
   }
   y[0] = S.y[warp * 4];
   y[1] = S.y[warp * 4 + 1];
