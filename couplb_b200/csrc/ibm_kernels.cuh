@@ -408,7 +408,9 @@ __device__ __forceinline__ void node_state(const IbmArgs<S>& a, bool hit, const 
 //
 // FILL: the stencil velocities are computed from the populations and written
 // to the marker's record (the work of k_ibm_prefetch, fused).
-template <class L, class S, int DELTA, bool LEARNED>
+// HALO: the lattice may have z faces bound to neighbour slabs (false for the
+// method kernels, which refuse them: the halo branches compile out).
+template <class L, class S, int DELTA, bool LEARNED, bool HALO = true>
 __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, int lane, bool fill,
                                                  const MlpPacked* P, MlpBlockScratch* blk,
                                                  double* tot3 = nullptr) {
@@ -465,7 +467,8 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
     mass = a.m[mk];
     vmk0 = a.v[3 * mk]; vmk1 = a.v[3 * mk + 1]; vmk2 = a.v[3 * mk + 2];
     const bool hit = key.epoch == a.cur_epoch && key.i0 == i0 && key.j0 == j0 && key.k0 == k0;
-    const LaneNodes<R> ln = lane_nodes<L, DELTA, R>(g, lx, ly, lz, i0, j0, k0, lane, a.wrap, a.zplanes);
+    const LaneNodes<R> ln = lane_nodes<L, DELTA, R>(g, lx, ly, lz, i0, j0, k0, lane, a.wrap,
+                                                    HALO ? a.zplanes : nullptr);
     bool wall_seen = false;   // a wall node adds to ws but not to wss
 #pragma unroll
     for (int rep = 0; rep < 2; rep++) {
@@ -481,7 +484,7 @@ __device__ __forceinline__ void ibm_substep_body(const IbmArgs<S>& a, int mk, in
         if (rx >= 0 && rx < 3 && ry >= 0 && ry < 3 && rz >= 0 && rz < 3) p = rx + 3 * ry + 9 * rz;
       }
       if (t < 0) {
-        const int hp = ln.h[rep];
+        const int hp = HALO ? ln.h[rep] : -1;
         const size_t src = hp >= 0 ? 0 : (size_t)ln.n[rep];
         const int ii = ln.i, jj = ln.j, kk = ln.k[rep];
         R u0, u1, u2;

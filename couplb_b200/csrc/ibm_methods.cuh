@@ -397,7 +397,7 @@ __global__ void __launch_bounds__(256) k_ibm_method(const PassArgs<S> P) {
   const int mk_end = LEARNED ? (a.n + wpb - 1) / wpb * wpb : a.n;
   for (int mk = gw; mk < mk_end; mk += nw) {
     double t3[3] = {0.0, 0.0, 0.0};
-    ibm_substep_body<L, S, DELTA, LEARNED>(a, mk, lane, P.fill != 0, net, blk, t3);
+    ibm_substep_body<L, S, DELTA, LEARNED, false>(a, mk, lane, P.fill != 0, net, blk, t3);
     ft[0] += t3[0]; ft[1] += t3[1]; ft[2] += t3[2];
   }
   block_add_ftot(a.ftot, ft);
