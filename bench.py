@@ -692,12 +692,12 @@ def cpu_model():
 
 # DRAM bytes (read + write) of one launch of the fused FP32 kernel on the
 # 256x128x128 channel, from an ncu capture of the launch after 25 others
-# (dram__bytes_read.sum 335.6 MB + dram__bytes_write.sum 290.0 MB).  ncu
-# empties L2 before the captured launch, so its own writes still dirty in L2
-# at its end (~46 MB) are missing; in a run they are written during the next
-# launch (steady state ~671 MB).  A constant of that capture, not measured by
-# this run: the line labels it so.
-NCU_TRAFFIC_FP32 = 335.6e6 + 290.0e6
+# (dram__bytes_read.sum 335.6 MB + dram__bytes_write.sum 285.9 MB, populations
+# in 64-node tiles).  ncu empties L2 before the captured launch, so its own
+# writes still dirty in L2 at its end (~50 MB) are missing; in a run they are
+# written during the next launch (steady state ~671 MB).  A constant of that
+# capture, not measured by this run: the line labels it so.
+NCU_TRAFFIC_FP32 = 335.6e6 + 285.9e6
 
 
 def run_reference(args):
@@ -858,7 +858,7 @@ def main():
     achieved = BYTES_PER_LU["fp32"] * N / (ms32 * 1e-3) / 1e9
     traffic = NCU_TRAFFIC_FP32 if (nx, ny, nz) == (NX, NY, NZ) else None
     traffic_src = ("ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of the 26th launch of this "
-                   "kernel and workload, L2 emptied before it (its ~46 MB of writes still in L2 at its end "
+                   "kernel and workload, L2 emptied before it (its ~50 MB of writes still in L2 at its end "
                    "are not counted; steady state ~671 MB); a constant, not measured by this run"
                    if traffic else None)
     line = {
