@@ -677,7 +677,9 @@ __device__ __forceinline__ AxisNode axis_node(int b, int o, int n, int flo, int 
 // FP32 fields: three blocks of 256 per SM (at most 85 registers), measured
 // faster than the unconstrained allocation (94 registers, two blocks); FP64
 // fields keep two (three spill several hundred bytes).
-template <class L, class S, int DELTA>
+// HALO: the lattice has a z face bound to a neighbour slab (the instance
+// without it drops the halo branches).
+template <class L, class S, int DELTA, bool HALO>
 __global__ void __launch_bounds__(256, sizeof(typename S::A) == 4 ? 3 : 2) k_ibm_substep8(const IbmArgs<S> a) {
   static_assert(L::D == 3, "the grouped sub-step is the 3D form");
   using R = typename S::C;
@@ -737,7 +739,7 @@ __global__ void __launch_bounds__(256, sizeof(typename S::A) == 4 ? 3 : 2) k_ibm
 #pragma unroll
   for (int r = 0; r < 2; r++) {
     nz2[r] = axis_node(k0 - 1, zr + 2 * r, g.nz, g.face[4], g.face[5], a.wrap & 4);
-    hz[r] = z_halo_plane(a, k0 - 1 + zr + 2 * r);
+    hz[r] = HALO ? z_halo_plane(a, k0 - 1 + zr + 2 * r) : -1;
     if (hz[r] >= 0) nz2[r].t = 0;   // the neighbour's plane: no z wall
   }
   R d[2][4];
@@ -848,7 +850,7 @@ __global__ void __launch_bounds__(256, sizeof(typename S::A) == 4 ? 3 : 2) k_ibm
     const int b = __ffs(todo) - 1;
     todo &= todo - 1;
     double t3[3] = {0.0, 0.0, 0.0};
-    ibm_substep_body<L, S, DELTA, false>(a, mk0 + (b >> 3), lane, false, nullptr, nullptr, t3);
+    ibm_substep_body<L, S, DELTA, false, HALO>(a, mk0 + (b >> 3), lane, false, nullptr, nullptr, t3);
     if (lane == 0) { tot0 += t3[0]; tot1 += t3[1]; tot2 += t3[2]; }
   }
   if (!a.ftot) return;
