@@ -18,7 +18,8 @@
 // nodes x Q planes.  FP32-shifted uses tiles of 64 nodes (256 B per plane and
 // tile, the span of one warp of the packed kernel): the IBM refresh, which
 // reads 19 short rows around each stencil node, then finds them within one
-// 4.9 KB tile instead of 19 planes 64 MB apart.  Measured on the D3Q19
+// 4.9 KB tile instead of 19 planes 64 MB apart (the same DRAM bytes, better
+// DRAM row locality).  Measured on the D3Q19
 // workloads against plane-major: fused LB kernel unchanged (36.6 vs 36.7
 // GLUPS on 256x128x128), LBM + IBM cycle 0.729 -> 0.710 ms (256^3, 20000
 // markers) and 1.560 -> 1.511 ms (rods); tiles of 8 nodes cut the refresh
