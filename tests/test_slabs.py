@@ -131,3 +131,13 @@ def test_clbk_round_trip_and_header_checks(tmp_path):
         slabs.read_clbk(path, f.shape, (0, 0, 5), (3, 4, 20))
     with pytest.raises(ValueError):
         slabs.read_clbk(path, (19, 8, 6, 5), (0, 0, 10), (3, 4, 20))
+
+
+def test_owner_slabs_by_cell():
+    """A marker belongs to the slab whose planes hold its cell; cells below
+    or above the box go to the first or last slab."""
+    parts = slabs.partition(10, 3)          # (0,4) (4,3) (7,3)
+    z = np.array([0.0, 3.999, 4.0, 6.5, 7.0, 9.99, -0.5, 10.2])
+    assert slabs.owner_slabs(z, parts).tolist() == [0, 0, 1, 1, 2, 2, 0, 2]
+    # lattice units from MD units: z = lo + dx * cell
+    assert slabs.owner_slabs(z * 0.5 - 1.0, parts, lo=-1.0, dx=0.5).tolist() == [0, 0, 1, 1, 2, 2, 0, 2]
