@@ -196,15 +196,25 @@ def make_atoms(x, v, f, mask=None, groupbit=1, rmass=None, mass=None, type_=None
     return at
 
 
-def make_domain(dimension, boxlo, boxhi, dt, periodicity=(1, 1, 1), ntimestep=0):
+def make_domain(dimension, boxlo, boxhi, dt, periodicity=(1, 1, 1), ntimestep=0, sublo=None, subhi=None):
     d = Domain()
     d.dimension = dimension
     for k in range(3):
         d.boxlo[k] = boxlo[k]
         d.boxhi[k] = boxhi[k]
-        d.sublo[k] = boxlo[k]
-        d.subhi[k] = boxhi[k]
+        d.sublo[k] = boxlo[k] if sublo is None else sublo[k]
+        d.subhi[k] = boxhi[k] if subhi is None else subhi[k]
         d.periodicity[k] = periodicity[k]
     d.dt = dt
     d.ntimestep = ntimestep
     return d
+
+
+# couplb_fix_comm (several ranks along z)
+SENDRECV_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t)
+ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_double), C.c_int, C.c_int)
+
+
+class FixComm(C.Structure):
+    _fields_ = [("nprocs", C.c_int), ("rank", C.c_int), ("sendrecv", SENDRECV_FN),
+                ("allreduce", ALLREDUCE_FN), ("ctx", C.c_void_p)]

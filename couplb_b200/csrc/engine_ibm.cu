@@ -27,6 +27,10 @@ int couplb_set_ibm_params(couplb_handle* h, const couplb_ibm_params* ip) {
 
 namespace couplb {
 
+void engine_note_refresh(couplb_handle* h) {
+  if (h->p.body_force) h->rho_state = kRhoCurrent;
+}
+
 // Shared body of the host- and device-array IBM sub-step.  The launches of
 // the method kernels (launch_method) are compiled in engine_methods_*.cu.
 int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, const double* d_m,

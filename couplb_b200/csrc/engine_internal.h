@@ -114,6 +114,9 @@ int engine_atom_host_buffers(couplb_handle* h, int n, double** mass, int** activ
 // the ones of the previous fill, so the next sub-step neither recounts nor
 // copies them again.
 void engine_atom_host_hint(couplb_handle* h, int n, int count, int unchanged);
+// A refresh sub-step with no coupled atoms on this lattice (other slabs have
+// some): only its effect on the density the next LB step reads.
+void engine_note_refresh(couplb_handle* h);
 int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, const double* d_m,
                const int* d_active, double* d_fout, int accumulate, int refresh);
 }  // namespace couplb

@@ -111,6 +111,19 @@ struct couplb_fix {
   double vtk_rlo[3] = {0, 0, 0}, vtk_rhi[3] = {0, 0, 0};   // clamped region, MD units
   std::vector<long long> vtk_steps;   // steps with field output (the .pvd series)
   long long vtk_last = -1;            // step of the last field output
+  // several ranks along z (couplb_fix_set_comm): this rank's slab and its halos
+  couplb_fix_comm comm{};
+  bool decomposed = false;
+  int nbr[2] = {0, 0};                // a neighbour across z face side
+  int ih_own[2] = {0, 0};             // IBM halo planes beyond each face of this slab
+  int ih_nbr[2] = {0, 0};             // planes of the neighbours' halos that face this slab
+  void* pop_send[2] = {nullptr, nullptr};
+  void* pop_recv[2] = {nullptr, nullptr};
+  void* vel[2] = {nullptr, nullptr};  // neighbour moments beyond each face
+  void* frc[2] = {nullptr, nullptr};  // forces spread beyond each face
+  void* msend[2] = {nullptr, nullptr};   // this slab's moments for the neighbours
+  void* frecv[2] = {nullptr, nullptr};   // the neighbours' forces on this slab
+  bool fold_pending = false;
 
   int fail(int code, const char* fmt, ...) {
     char buf[512];
@@ -138,15 +151,99 @@ struct couplb_fix {
 
 namespace {
 
+// ---- several ranks along z: the slab halos through the host communicator --
+void free_slab_buffers(couplb_fix* F) {
+  void** bufs[] = {F->pop_send, F->pop_recv, F->vel, F->frc, F->msend, F->frecv};
+  for (void** b : bufs)
+    for (int s = 0; s < 2; s++)
+      if (b[s]) { cudaFree(b[s]); b[s] = nullptr; }
+}
+
+int slab_alloc(couplb_fix* F, void** p, size_t bytes) {
+  if (!bytes) return COUPLB_OK;
+  if (cudaSetDevice(F->device) != cudaSuccess || cudaMalloc(p, bytes) != cudaSuccess ||
+      cudaMemsetAsync(*p, 0, bytes, F->h->stream) != cudaSuccess)
+    return F->fail(COUPLB_ERR_CUDA, "fix couplb: cannot allocate %zu bytes of slab halo", bytes);
+  return COUPLB_OK;
+}
+
+// One sendrecv of the communicator after the lattice's stream has finished
+// what the buffers depend on.
+int slab_sendrecv(couplb_fix* F, int side, const void* send, size_t sb, void* recv, size_t rb) {
+  int rc = couplb_synchronize(F->h);
+  if (rc) return F->engine_fail(rc);
+  if (F->comm.sendrecv(F->comm.ctx, side, send, send ? sb : 0, recv, recv ? rb : 0) != 0)
+    return F->fail(COUPLB_ERR_CUDA, "fix couplb: halo exchange across z face %d failed", side);
+  return COUPLB_OK;
+}
+
+int slab_allreduce(couplb_fix* F, double* buf, int n, int op) {
+  if (!F->decomposed) return COUPLB_OK;
+  if (F->comm.allreduce(F->comm.ctx, buf, n, op) != 0)
+    return F->fail(COUPLB_ERR_CUDA, "fix couplb: allreduce over the ranks failed");
+  return COUPLB_OK;
+}
+
+// After an LB step: the populations that cross each bound face (5 planes),
+// then the moments of the planes the neighbours' marker windows reach.
+int slab_exchange_state(couplb_fix* F, bool populations) {
+  if (!F->decomposed) return COUPLB_OK;
+  int rc;
+  if (populations) {
+    const size_t pb = couplb_halo_bytes(F->h);
+    for (int s = 0; s < 2; s++)
+      if (F->nbr[s] && (rc = couplb_halo_pack(F->h, s, F->pop_send[s]))) return F->engine_fail(rc);
+    // up: my top planes into the slab above, the slab below's into my low halo
+    if ((rc = slab_sendrecv(F, 1, F->nbr[1] ? F->pop_send[1] : nullptr, pb, F->nbr[0] ? F->pop_recv[0] : nullptr,
+                            pb)))
+      return rc;
+    if ((rc = slab_sendrecv(F, 0, F->nbr[0] ? F->pop_send[0] : nullptr, pb, F->nbr[1] ? F->pop_recv[1] : nullptr,
+                            pb)))
+      return rc;
+  }
+  for (int s = 0; s < 2; s++)
+    if (F->nbr[s] && (rc = couplb_ibm_halo_moments(F->h, s, F->ih_nbr[s], F->msend[s]))) return F->engine_fail(rc);
+  const size_t m1 = couplb_ibm_halo_bytes(F->h, F->ih_nbr[1]), v0 = couplb_ibm_halo_bytes(F->h, F->ih_own[0]);
+  const size_t m0 = couplb_ibm_halo_bytes(F->h, F->ih_nbr[0]), v1 = couplb_ibm_halo_bytes(F->h, F->ih_own[1]);
+  if ((rc = slab_sendrecv(F, 1, F->nbr[1] ? F->msend[1] : nullptr, m1, F->nbr[0] ? F->vel[0] : nullptr, v0)))
+    return rc;
+  return slab_sendrecv(F, 0, F->nbr[0] ? F->msend[0] : nullptr, m0, F->nbr[1] ? F->vel[1] : nullptr, v1);
+}
+
+// Before an LB step: the forces this slab spread beyond its faces go to the
+// neighbours, theirs on this slab are added to its field.
+int slab_fold(couplb_fix* F) {
+  if (!F->decomposed) return COUPLB_OK;   // a collective: every rank, every LB step
+  const size_t f0 = couplb_ibm_halo_bytes(F->h, F->ih_own[0]), r1 = couplb_ibm_halo_bytes(F->h, F->ih_nbr[1]);
+  const size_t f1 = couplb_ibm_halo_bytes(F->h, F->ih_own[1]), r0 = couplb_ibm_halo_bytes(F->h, F->ih_nbr[0]);
+  int rc;
+  if ((rc = slab_sendrecv(F, 0, F->nbr[0] ? F->frc[0] : nullptr, f0, F->nbr[1] ? F->frecv[1] : nullptr, r1)))
+    return rc;
+  if ((rc = slab_sendrecv(F, 1, F->nbr[1] ? F->frc[1] : nullptr, f1, F->nbr[0] ? F->frecv[0] : nullptr, r0)))
+    return rc;
+  for (int s = 0; s < 2; s++) {
+    if (!F->nbr[s]) continue;
+    if ((rc = couplb_ibm_halo_fold(F->h, s, F->ih_nbr[s], F->frecv[s]))) return F->engine_fail(rc);
+    if (cudaMemsetAsync(F->frc[s], 0, couplb_ibm_halo_bytes(F->h, F->ih_own[s]), F->h->stream) != cudaSuccess)
+      return F->fail(COUPLB_ERR_CUDA, "fix couplb: cannot clear a force halo");
+  }
+  F->fold_pending = false;
+  return COUPLB_OK;
+}
+
 // FixCoupLB::write_profile (fix_couplb.cpp:903-979) for one rank.
 int write_profile(couplb_fix* F, long long step) {
   const int ny = F->nl[1];
   std::vector<double> su(ny), sv(ny), sr(ny);
   int rc = couplb_y_profile(F->h, su.data(), sv.data(), sr.data());
   if (rc) return F->engine_fail(rc);
+  // sums over the ranks' slabs (fix_couplb.cpp:955-958)
+  if ((rc = slab_allreduce(F, su.data(), ny, 0)) || (rc = slab_allreduce(F, sv.data(), ny, 0)) ||
+      (rc = slab_allreduce(F, sr.data(), ny, 0)))
+    return rc;
   if (F->rank != 0) return COUPLB_OK;
   const int Ny = F->cfg.Ny;
-  const int cxz = F->nl[0] * (F->is3d ? F->nl[2] : 1);
+  const int cxz = F->nl[0] * (F->is3d ? (F->decomposed ? F->cfg.Nz : F->nl[2]) : 1);
   std::vector<double> ux(Ny, 0.0), uy(Ny, 0.0), rr(Ny, 0.0);
   std::vector<int> cnt(Ny, 0);
   for (int j = 0; j < ny; j++) {
@@ -441,7 +538,13 @@ int ibm_sub_coupling(couplb_fix* F, const couplb_atoms* at, bool lbm = false,
     ng += act;
   }
   couplb::engine_atom_host_hint(F->h, nl, ng, changed ? 0 : 1);
-  if (ng == 0) {
+  // the group count is global (fix_couplb.cpp:743-747)
+  double ng_all = ng;
+  if (F->decomposed) {
+    int rca = slab_allreduce(F, &ng_all, 1, 0);
+    if (rca) return rca;
+  }
+  if (ng_all == 0) {
     F->ibm_has_particles = false;
     if (lbm) {
       const int rc = couplb_lbm_step(F->h, g_lb);
@@ -451,6 +554,12 @@ int ibm_sub_coupling(couplb_fix* F, const couplb_atoms* at, bool lbm = false,
   }
   const int refresh = (first || !F->ibm_has_particles) ? 1 : 0;
   F->ibm_has_particles = true;
+  if (ng == 0) {
+    // a slab without coupled atoms while other slabs have some: the refresh
+    // still happens here (its density state), nothing is spread
+    if (refresh) couplb::engine_note_refresh(F->h);
+    return COUPLB_OK;
+  }
   int nc = 0;
   const int rc = lbm ? couplb_lbm_step_ibm(F->h, g_lb, nl, at->x, at->v, mass_buf, active_buf, at->f, &nc)
                      : couplb_ibm_substep(F->h, nl, at->x, at->v, mass_buf, active_buf, at->f, refresh, &nc);
@@ -646,6 +755,7 @@ int couplb_fix_create(const couplb_fix_config* cfg, couplb_fix** out) {
 
 int couplb_fix_destroy(couplb_fix* F) {
   if (!F) return COUPLB_OK;
+  free_slab_buffers(F);
   if (F->h) couplb_destroy(F->h);
   if (F->mlp) couplb_mlp_destroy(F->mlp);
   delete F;
@@ -678,6 +788,18 @@ int couplb_fix_set_device(couplb_fix* F, int device) {
   if (!F) return COUPLB_ERR_ARG;
   if (F->h) return F->fail(COUPLB_ERR_STATE, "couplb_fix_set_device must precede couplb_fix_init");
   F->device = device;
+  return COUPLB_OK;
+}
+
+int couplb_fix_set_comm(couplb_fix* F, const couplb_fix_comm* comm) {
+  if (!F || !comm) return COUPLB_ERR_ARG;
+  if (F->h) return F->fail(COUPLB_ERR_STATE, "couplb_fix_set_comm must precede couplb_fix_init");
+  if (comm->nprocs < 1 || comm->rank < 0 || comm->rank >= comm->nprocs)
+    return F->fail(COUPLB_ERR_ARG, "fix couplb: bad communicator (rank %d of %d)", comm->rank, comm->nprocs);
+  if (comm->nprocs > 1 && (!comm->sendrecv || !comm->allreduce))
+    return F->fail(COUPLB_ERR_ARG, "fix couplb: a communicator of several ranks needs sendrecv and allreduce");
+  F->comm = *comm;
+  F->rank = comm->rank;
   return COUPLB_OK;
 }
 
@@ -775,20 +897,40 @@ int couplb_fix_init(couplb_fix* F, const couplb_domain* dom) {
   if (!F->is3d) { F->nl[2] = 1; F->off[2] = 0; }
   if (F->nl[0] <= 0 || F->nl[1] <= 0 || (F->is3d && F->nl[2] <= 0))
     return F->fail(COUPLB_ERR_ARG, "fix couplb: local grid empty");
-  // One lattice per fix: the kernels wrap every non-wall face of the local
-  // grid onto itself (the self-exchange of a one-rank run), so a sub-box that
-  // is only part of the box would silently simulate a periodic slab of its
-  // own.  The reference splits the grid over ranks with ghost exchanges
-  // (fix_couplb.cpp:494-500, couplb_streaming.h:176-245); that is refused.
+  // Without a communicator the fix runs one lattice: the kernels wrap every
+  // non-wall face of the local grid onto itself (the self-exchange of a
+  // one-rank run), so a sub-box that is only part of the box would silently
+  // simulate a periodic piece of its own; that is refused.  With one
+  // (couplb_fix_set_comm) the sub-boxes may split z: this rank runs its slab
+  // and exchanges the halos (fix_couplb.cpp:494-500, couplb_streaming.h:176-245).
+  F->decomposed = F->is3d && F->comm.nprocs > 1;
   {
     const int full[3] = {c.Nx, c.Ny, F->is3d ? c.Nz : 1};
     for (int d = 0; d < (F->is3d ? 3 : 2); d++)
-      if (F->off[d] != 0 || F->nl[d] != full[d])
+      if ((F->off[d] != 0 || F->nl[d] != full[d]) && !(F->decomposed && d == 2))
         return F->fail(COUPLB_ERR_UNSUPPORTED,
                        "fix couplb: the MD sub-box covers nodes %d..%d of %d along %c, but this build "
-                       "runs the whole lattice on one rank (sub-box must equal the box; no domain "
-                       "decomposition across ranks)",
+                       "runs the whole lattice on one rank, or z slabs with a communicator "
+                       "(couplb_fix_set_comm; sub-boxes split along z only)",
                        F->off[d], F->off[d] + F->nl[d] - 1, full[d], "xyz"[d]);
+  }
+  if (F->decomposed) {
+    if (F->nl[2] < 2) return F->fail(COUPLB_ERR_UNSUPPORTED, "fix couplb: a z slab needs at least 2 planes");
+    if (c.vtk_every > 0) return F->fail(COUPLB_ERR_UNSUPPORTED, "fix couplb: vtk output with several ranks");
+    const bool periodic = c.wall[4] == 0 && c.wall[5] == 0;
+    const bool glo = F->off[2] == 0, ghi = F->off[2] + F->nl[2] == c.Nz;
+    // a face is bound to a neighbour unless it is a wall of the box
+    F->nbr[0] = !glo || periodic;
+    F->nbr[1] = !ghi || periodic;
+    // window planes beyond each face: 1 below, 2 above, 1 above the face
+    // that wraps the periodic box with the clipped window (where the whole
+    // lattice stops at its ghost layer); and those of the neighbours' halos
+    // facing this slab
+    const bool clip = c.ibm_window == 0;
+    F->ih_own[0] = F->nbr[0] ? 1 : 0;
+    F->ih_own[1] = F->nbr[1] ? ((ghi && periodic && clip) ? 1 : 2) : 0;
+    F->ih_nbr[0] = F->nbr[0] ? ((glo && periodic && clip) ? 1 : 2) : 0;
+    F->ih_nbr[1] = F->nbr[1] ? 1 : 0;
   }
   if (F->h) { couplb_destroy(F->h); F->h = nullptr; }
   couplb_lattice_params lp;
@@ -797,8 +939,12 @@ int couplb_fix_init(couplb_fix* F, const couplb_domain* dom) {
   lp.nx = F->nl[0]; lp.ny = F->nl[1]; lp.nz = F->nl[2];
   lp.tau = F->tau;
   lp.rho0 = kRhoLb;
-  // setup_boundaries (fix_couplb.cpp:522-539): in 2D only x and y walls
+  // setup_boundaries (fix_couplb.cpp:522-539): in 2D only x and y walls; a
+  // z face bound to a neighbour slab is an open (periodic-type) face
   for (int f = 0; f < (F->is3d ? 6 : 4); f++) lp.wall[f] = c.wall[f];
+  if (F->decomposed)
+    for (int s = 0; s < 2; s++)
+      if (F->nbr[s]) lp.wall[4 + s] = COUPLB_WALL_PERIODIC;
   for (int d = 0; d < 3; d++) lp.wall_vel[d] = wv_lb[d];
   if (!F->is3d) lp.wall_vel[2] = 0.0;
   lp.body_force = (c.gstyle[0] != COUPLB_G_NONE || c.gstyle[1] != COUPLB_G_NONE ||
@@ -819,6 +965,22 @@ int couplb_fix_init(couplb_fix* F, const couplb_domain* dom) {
   for (int d = 0; d < 3; d++) { ip.domain_lo[d] = F->domain_lo[d]; ip.offset[d] = F->off[d]; }
   if ((rc = couplb_set_ibm_params(F->h, &ip))) return F->engine_fail(rc);
   if ((rc = couplb_set_option(F->h, "ibm_window", c.ibm_window))) return F->engine_fail(rc);
+  if (F->decomposed) {
+    free_slab_buffers(F);
+    const size_t pb = couplb_halo_bytes(F->h);
+    for (int s = 0; s < 2; s++) {
+      if (!F->nbr[s]) continue;
+      if ((rc = slab_alloc(F, &F->pop_send[s], pb)) || (rc = slab_alloc(F, &F->pop_recv[s], pb))) return rc;
+      const size_t own = couplb_ibm_halo_bytes(F->h, F->ih_own[s]);
+      const size_t nb = couplb_ibm_halo_bytes(F->h, F->ih_nbr[s]);
+      if ((rc = slab_alloc(F, &F->vel[s], own)) || (rc = slab_alloc(F, &F->frc[s], own)) ||
+          (rc = slab_alloc(F, &F->msend[s], nb)) || (rc = slab_alloc(F, &F->frecv[s], nb)))
+        return rc;
+      if ((rc = couplb_halo_attach(F->h, s, F->pop_recv[s]))) return F->engine_fail(rc);
+      if ((rc = couplb_ibm_halo_attach(F->h, s, F->ih_own[s], F->vel[s], F->frc[s]))) return F->engine_fail(rc);
+    }
+    F->fold_pending = false;
+  }
   if (c.ibm_method != COUPLB_IBM_SINGLE) {
     couplb_ibm_method m;
     std::memset(&m, 0, sizeof(m));
@@ -901,8 +1063,9 @@ int couplb_fix_init(couplb_fix* F, const couplb_domain* dom) {
 int couplb_fix_setup(couplb_fix* F, const couplb_atoms* at, long long ntimestep) {
   if (!F || !F->inited) return F ? F->fail(COUPLB_ERR_STATE, "couplb_fix_init not called") : COUPLB_ERR_ARG;
   F->md_sub_count = 0;
-  int rc = ibm_sub_coupling(F, at);
+  int rc = slab_exchange_state(F, false);
   if (rc) return rc;
+  if ((rc = ibm_sub_coupling(F, at))) return rc;
   F->md_sub_count = 0;
   const couplb_fix_config& c = F->cfg;
   const bool need_macro = (c.output_every > 0 || c.vtk_every > 0);
@@ -955,7 +1118,16 @@ int couplb_fix_post_force(couplb_fix* F, const couplb_atoms* at, long long ntime
       const double ac = F->dt_LBM * F->dt_LBM / F->dx;
       for (int d = 0; d < 3; d++) gl[d] = gv[d] * ac;
     }
-    rc = ibm_sub_coupling(F, at, true, none ? nullptr : gl);
+    if (F->decomposed) {
+      // fold last cycle's halo forces, the LB step, the halos of the new
+      // state, then the refresh sub-step
+      if ((rc = slab_fold(F))) return rc;
+      if ((rc = couplb_lbm_step(F->h, none ? nullptr : gl))) return F->engine_fail(rc);
+      if ((rc = slab_exchange_state(F, true))) return rc;
+      rc = ibm_sub_coupling(F, at);
+    } else {
+      rc = ibm_sub_coupling(F, at, true, none ? nullptr : gl);
+    }
     if (rc) return rc;
     F->lbm_step_count++;
   } else {
@@ -984,6 +1156,15 @@ int couplb_fix_end_of_step(couplb_fix* F, long long step) {
   if (chk) {
     couplb_diag d;
     if ((rc = couplb_diagnostics(F->h, &d))) return F->engine_fail(rc);
+    if (F->decomposed) {
+      // check_stability_precomputed reduces over the ranks (fix_couplb.cpp:818-844)
+      double sums[5] = {d.mass, d.mom[0], d.mom[1], d.mom[2], (double)d.clamps};
+      double mx = d.umax;
+      if ((rc = slab_allreduce(F, sums, 5, 0)) || (rc = slab_allreduce(F, &mx, 1, 1))) return rc;
+      d.mass = sums[0]; d.mom[0] = sums[1]; d.mom[1] = sums[2]; d.mom[2] = sums[3];
+      d.clamps = (int)sums[4];
+      d.umax = mx;
+    }
     F->last_diag = d;
     const double ma = d.umax / std::sqrt(1.0 / 3.0);
     if (ma > kMaError) return F->fail(COUPLB_ERR_NUMERIC, "fix couplb: Ma>0.5, simulation invalid");

@@ -104,11 +104,37 @@ class FixCoupLB:
         self._ck(self.L.couplb_fix_set_gravity_values(self.h, abi.dptr(arr)))
 
     # -- hooks (fix_couplb.h:26-30) ------------------------------------------
-    def init(self, boxlo, boxhi, dt, ntimestep=0, periodicity=(1, 1, 1)):
-        self.domain = abi.make_domain(self.dimension, boxlo, boxhi, dt, periodicity, ntimestep)
+    def set_comm(self, nprocs, rank, sendrecv, allreduce):
+        """Several ranks along z (couplb_fix_set_comm): sendrecv(side, d_send,
+        send_bytes, d_recv, recv_bytes) and allreduce(numpy array, op) (op 0
+        sum, 1 max, in place) move this rank's slab halos and reductions; the
+        pointers are raw device addresses (0 where there is no neighbour)."""
+        def sr(_ctx, side, d_send, sb, d_recv, rb):
+            try:
+                sendrecv(side, d_send or 0, sb, d_recv or 0, rb)
+                return 0
+            except Exception:
+                return 1
+
+        def ar(_ctx, buf, n, op):
+            try:
+                a = np.ctypeslib.as_array(buf, shape=(n,))
+                allreduce(a, op)
+                return 0
+            except Exception:
+                return 1
+        self._comm_cbs = (abi.SENDRECV_FN(sr), abi.ALLREDUCE_FN(ar))
+        self._comm = abi.FixComm(nprocs, rank, self._comm_cbs[0], self._comm_cbs[1], None)
+        self._ck(self.L.couplb_fix_set_comm(self.h, C.byref(self._comm)))
+
+    def init(self, boxlo, boxhi, dt, ntimestep=0, periodicity=(1, 1, 1), sublo=None, subhi=None):
+        self.domain = abi.make_domain(self.dimension, boxlo, boxhi, dt, periodicity, ntimestep, sublo, subhi)
         self._ck(self.L.couplb_fix_init(self.h, C.byref(self.domain)))
         c = self.cfg
-        self.lattice = _LatticeView(self.L.couplb_fix_handle(self.h), self.dimension, c.Nx, c.Ny, c.Nz)
+        nz = c.Nz
+        if sublo is not None and self.dimension == 3:
+            nz = int(round((subhi[2] - sublo[2]) / self.scales()["dx"]))
+        self.lattice = _LatticeView(self.L.couplb_fix_handle(self.h), self.dimension, c.Nx, c.Ny, nz)
         return self
 
     def setup(self, atoms, ntimestep=0):

@@ -87,6 +87,7 @@ SIGNATURES = {
     "couplb_fix_set_log_callback": (C.c_int, [_H, C.c_void_p, C.c_void_p]),
     "couplb_fix_set_gravity_values": (C.c_int, [_H, _D]),
     "couplb_fix_set_device": (C.c_int, [_H, C.c_int]),
+    "couplb_fix_set_comm": (C.c_int, [_H, C.c_void_p]),
     "couplb_fix_setmask": (C.c_int, []),
     "couplb_fix_init": (C.c_int, [_H, C.POINTER(abi.Domain)]),
     "couplb_fix_setup": (C.c_int, [_H, C.POINTER(abi.Atoms), C.c_longlong]),

@@ -534,6 +534,32 @@ int  couplb_fix_set_log_callback(couplb_fix* fx, couplb_log_fn fn, void* ctx);
 int  couplb_fix_set_gravity_values(couplb_fix* fx, const double g[3]);
 int  couplb_fix_set_device(couplb_fix* fx, int device);
 
+/* Several ranks, the MD domain split along z only (every sub-box spans the
+ * box in x and y, and its z range is whole lattice planes, at least 2): the
+ * fix runs this rank's slab of the lattice and moves the slab halos through
+ * the host code's communicator (the exchanges of Streaming::exchange_dim /
+ * exchange_velocity / exchange_forces for d = z, couplb_streaming.h:176-245,
+ * with the windows of the undecomposed lattice, see couplb_ibm_halo_attach).
+ *   sendrecv: send send_bytes of device memory d_send to the rank across z
+ *     face `side` of this sub-box (0 low, 1 high) and receive recv_bytes into
+ *     d_recv from the rank across the other face (MPI_Sendrecv with
+ *     procneigh[2]); a pointer is NULL where that neighbour does not exist
+ *     (MPI_PROC_NULL).  The fix synchronises its stream first; every rank
+ *     makes the same calls in the same order.
+ *   allreduce: n doubles in place over all ranks, op 0 sum, op 1 max.
+ * Both return 0 on success.  Diagnostics and the profile are reduced over
+ * the ranks (rank 0 writes), checkpoints are one file per rank; VTK output is
+ * refused.  Call before couplb_fix_init; nprocs 1 is the one-rank run. */
+typedef struct couplb_fix_comm {
+  int   nprocs;
+  int   rank;
+  int (*sendrecv)(void* ctx, int side, const void* d_send, size_t send_bytes, void* d_recv,
+                  size_t recv_bytes);
+  int (*allreduce)(void* ctx, double* buf, int n, int op);
+  void* ctx;
+} couplb_fix_comm;
+int  couplb_fix_set_comm(couplb_fix* fx, const couplb_fix_comm* comm);
+
 /* FixCoupLB::setmask: POST_FORCE | END_OF_STEP (fix_couplb.cpp:248-254). */
 #define COUPLB_MASK_POST_FORCE  1
 #define COUPLB_MASK_END_OF_STEP 2

@@ -125,7 +125,50 @@ def test_init_refuses_a_sub_box_smaller_than_the_box(cuda_lib, axis, dim):
     rc = fx.L.couplb_fix_init(fx.h, C.byref(d))
     assert rc == abi.ERR_UNSUPPORTED
     msg = fx.L.couplb_fix_last_error(fx.h).decode()
-    assert "sub-box must equal the box" in msg and "xyz"[axis] in msg
+    assert "one rank" in msg and "xyz"[axis] in msg
+    fx.close()
+
+
+def _comm_fix(words, rank=0, nprocs=2):
+    from couplb_b200.fix import FixCoupLB
+    fx = FixCoupLB(words.split(), dimension=3)
+    fx.set_comm(nprocs, rank, lambda *a: None, lambda a, op: None)
+    return fx
+
+
+@pytest.mark.parametrize("axis,why", [(0, "split along z only"), (1, "split along z only")])
+def test_comm_refuses_x_and_y_splits(cuda_lib, axis, why):
+    """With a communicator the sub-boxes may split z only."""
+    import ctypes as C
+    fx = _comm_fix("f all couplb 16 8 8 0.1 1.0")
+    d = abi.make_domain(3, (0.0, 0.0, 0.0), (16.0, 8.0, 8.0), 0.1)
+    d.subhi[axis] /= 2
+    assert fx.L.couplb_fix_init(fx.h, C.byref(d)) == abi.ERR_UNSUPPORTED
+    assert why in fx.L.couplb_fix_last_error(fx.h).decode()
+    fx.close()
+
+
+def test_comm_slab_rules(cuda_lib):
+    """A z slab has at least 2 planes; VTK output is refused with several
+    ranks; a communicator of several ranks needs both callbacks."""
+    import ctypes as C
+    fx = _comm_fix("f all couplb 8 8 8 0.1 1.0")
+    d = abi.make_domain(3, (0.0, 0.0, 0.0), (8.0, 8.0, 8.0), 0.1)
+    d.subhi[2] = 1.0
+    assert fx.L.couplb_fix_init(fx.h, C.byref(d)) == abi.ERR_UNSUPPORTED
+    assert "at least 2 planes" in fx.L.couplb_fix_last_error(fx.h).decode()
+    fx.close()
+    fx = _comm_fix("f all couplb 8 8 8 0.1 1.0 vtk 10 out")
+    d.subhi[2] = 4.0
+    assert fx.L.couplb_fix_init(fx.h, C.byref(d)) == abi.ERR_UNSUPPORTED
+    assert "vtk" in fx.L.couplb_fix_last_error(fx.h).decode()
+    fx.close()
+    from couplb_b200.fix import FixCoupLB
+    fx = FixCoupLB("f all couplb 8 8 8 0.1 1.0".split(), dimension=3)
+    comm = abi.FixComm(2, 0, abi.SENDRECV_FN(), abi.ALLREDUCE_FN(), None)
+    assert fx.L.couplb_fix_set_comm(fx.h, C.byref(comm)) == abi.ERR_ARG
+    comm = abi.FixComm(2, 2, abi.SENDRECV_FN(), abi.ALLREDUCE_FN(), None)
+    assert fx.L.couplb_fix_set_comm(fx.h, C.byref(comm)) == abi.ERR_ARG
     fx.close()
 
 
