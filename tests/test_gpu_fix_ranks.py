@@ -4,7 +4,7 @@ code's communicator -- here threads of this process on one GPU, exchanging
 through host memory (each rank synchronises its own stream and copies; no
 kernel waits on another rank).  The run matches one fix over the whole box:
 atom forces at every step, populations and the reduced diagnostics, FP64
-within 1e-12."""
+within 1e-12, and rank 0's profile file."""
 import ctypes as C
 import threading
 
@@ -62,9 +62,15 @@ class ThreadComm:
         a[:] = r
 
 
-def _cfg(wall):
+def _cfg(wall, profile=""):
     return cases.make_cfg(Nx=N[0], Ny=N[1], Nz=N[2], nu=0.1, rho=1.0, md_per_lb=2, delta=1,
-                          gravity=(3e-5, 0, 0), wall=wall, check_every=5, dimension=3)
+                          gravity=(3e-5, 0, 0), wall=wall, check_every=5, dimension=3,
+                          output_every=6 if profile else 0, output_file=profile)
+
+
+def _profile(path):
+    return np.array([[float(w) for w in line.split()] for line in open(path)
+                     if line.strip() and not line.startswith("#")])
 
 
 def _markers():
@@ -91,10 +97,10 @@ def _run(fix, x, v, steps=12):
 
 @pytest.mark.parametrize("nprocs", [2, 3])
 @pytest.mark.parametrize("wall", [(0, 0, 1, 1, 0, 0), (0, 0, 1, 1, 1, 1)])
-def test_z_slab_ranks_match_one_rank(cuda_lib, nprocs, wall):
+def test_z_slab_ranks_match_one_rank(cuda_lib, tmp_path, nprocs, wall):
     from couplb_b200.slabs import owner_slabs, partition
     x, v = _markers()
-    one = FixCoupLB(_cfg(wall), dimension=3)
+    one = FixCoupLB(_cfg(wall, str(tmp_path / "one.dat")), dimension=3)
     one.init(*BOX, 0.5)
     f1, d1 = _run(one, x, v)
     p1 = cases.interior(one.lattice.get_populations(), 3)
@@ -108,7 +114,7 @@ def test_z_slab_ranks_match_one_rank(cuda_lib, nprocs, wall):
 
     def rank_main(r):
         try:
-            fx = FixCoupLB(_cfg(wall), dimension=3)
+            fx = FixCoupLB(_cfg(wall, str(tmp_path / f"ranks{r}.dat")), dimension=3)
             fx.set_comm(nprocs, r, lambda *a: comm.sendrecv(r, *a), lambda a, op: comm.allreduce(r, a, op))
             z0, nzl = parts[r]
             fx.init(*BOX, 0.5, sublo=(0.0, 0.0, float(z0)), subhi=(16.0, 14.0, float(z0 + nzl)))
@@ -135,3 +141,7 @@ def test_z_slab_ranks_match_one_rank(cuda_lib, nprocs, wall):
     assert rel(pr, p1) <= 1e-12, rel(pr, p1)
     for o in out:   # every rank holds the reduced diagnostics
         assert np.abs(o[2] - d1).max() <= 1e-12 * np.abs(d1).max()
+    # rank 0 writes the profile of the whole lattice (sums over the ranks)
+    a, b = _profile(tmp_path / "ranks0.dat"), _profile(tmp_path / "one.dat")
+    assert a.shape == b.shape and np.abs(a - b).max() <= 1e-9 * np.abs(b).max()
+    assert not any((tmp_path / f"ranks{r}.dat").exists() for r in range(1, nprocs))
