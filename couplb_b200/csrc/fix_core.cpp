@@ -917,6 +917,10 @@ int couplb_fix_init(couplb_fix* F, const couplb_domain* dom) {
   if (F->decomposed) {
     if (F->nl[2] < 2) return F->fail(COUPLB_ERR_UNSUPPORTED, "fix couplb: a z slab needs at least 2 planes");
     if (c.vtk_every > 0) return F->fail(COUPLB_ERR_UNSUPPORTED, "fix couplb: vtk output with several ranks");
+    // every correction pass would need its own halo exchange
+    if (c.ibm_method != COUPLB_IBM_SINGLE)
+      return F->fail(COUPLB_ERR_UNSUPPORTED, "fix couplb: ibm_method %s with several ranks",
+                     c.ibm_method == COUPLB_IBM_LEARNED ? "learned" : "iterative");
     const bool periodic = c.wall[4] == 0 && c.wall[5] == 0;
     const bool glo = F->off[2] == 0, ghi = F->off[2] + F->nl[2] == c.Nz;
     // a face is bound to a neighbour unless it is a wall of the box

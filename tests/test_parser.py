@@ -149,8 +149,9 @@ def test_comm_refuses_x_and_y_splits(cuda_lib, axis, why):
 
 
 def test_comm_slab_rules(cuda_lib):
-    """A z slab has at least 2 planes; VTK output is refused with several
-    ranks; a communicator of several ranks needs both callbacks."""
+    """A z slab has at least 2 planes; VTK output and the correction methods
+    are refused with several ranks; a communicator of several ranks needs
+    both callbacks."""
     import ctypes as C
     fx = _comm_fix("f all couplb 8 8 8 0.1 1.0")
     d = abi.make_domain(3, (0.0, 0.0, 0.0), (8.0, 8.0, 8.0), 0.1)
@@ -162,6 +163,10 @@ def test_comm_slab_rules(cuda_lib):
     d.subhi[2] = 4.0
     assert fx.L.couplb_fix_init(fx.h, C.byref(d)) == abi.ERR_UNSUPPORTED
     assert "vtk" in fx.L.couplb_fix_last_error(fx.h).decode()
+    fx.close()
+    fx = _comm_fix("f all couplb 8 8 8 0.1 1.0 ibm_method iterative")
+    assert fx.L.couplb_fix_init(fx.h, C.byref(d)) == abi.ERR_UNSUPPORTED
+    assert "iterative with several ranks" in fx.L.couplb_fix_last_error(fx.h).decode()
     fx.close()
     from couplb_b200.fix import FixCoupLB
     fx = FixCoupLB("f all couplb 8 8 8 0.1 1.0".split(), dimension=3)
