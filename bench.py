@@ -71,6 +71,8 @@ def parse():
                     help="with --only ibm: also time the workload through the fix hooks (1) or not (0)")
     ap.add_argument("--ibm-n", type=int, default=256,
                     help="edge of the periodic box of the point-marker workload")
+    ap.add_argument("--ibm-block", type=int, default=128, choices=[64, 128, 256],
+                    help="threads per block of the grouped IBM sub-step (handle option ibm_block)")
     ap.add_argument("--ibm-group", type=int, default=8, choices=[8, 32],
                     help="lanes per marker of the single-pass IBM sub-step (handle option ibm_group)")
     ap.add_argument("--nx", type=int, default=NX)
@@ -164,6 +166,7 @@ class Clocks:
 # --------------------------------------------------------------------------
 KERNEL = -1
 IBM_GROUP = 8   # lanes per marker of the single-pass IBM sub-step
+IBM_BLOCK = 128  # threads per block of the grouped sub-step
 
 
 def make_lattice(prec, nx, ny, nz, device):
@@ -280,6 +283,7 @@ def marker_bench(torch, device, prec, cycles, warmup, box, wall, tau, x0, v0, md
     # reference clips it at the ghost layer, option value 0)
     L.set_option("ibm_window", 1)
     L.set_option("ibm_group", IBM_GROUP)
+    L.set_option("ibm_block", IBM_BLOCK)
     stream = torch.cuda.current_stream()
     L.set_stream(stream.cuda_stream)
     L.init_equilibrium(1.0)
@@ -739,10 +743,11 @@ def load_peak():
 
 
 def main():
-    global KERNEL, IBM_GROUP
+    global KERNEL, IBM_GROUP, IBM_BLOCK
     args = parse()
     KERNEL = args.kernel
     IBM_GROUP = args.ibm_group
+    IBM_BLOCK = args.ibm_block
     if args.impl == "reference":
         return run_reference(args)
     import torch

@@ -653,6 +653,12 @@ int couplb_set_option(couplb_handle* h, const char* name, long long value) {
     h->ibm_group = (int)value;
     return COUPLB_OK;
   }
+  if (!std::strcmp(name, "ibm_block")) {
+    if (value != 64 && value != 128 && value != 256)
+      return fail(h, COUPLB_ERR_ARG, "ibm_block must be 64, 128 or 256");
+    h->ibm_block = (int)value;
+    return COUPLB_OK;
+  }
   if (!std::strcmp(name, "barrier_spin")) {
     if (value < 0 || value > (1LL << 40)) return fail(h, COUPLB_ERR_ARG, "barrier_spin must be 0..2^40");
     h->barrier_spin = value;
@@ -669,6 +675,7 @@ int couplb_get_option(couplb_handle* h, const char* name, long long* value) {
   if (!std::strcmp(name, "barrier_spin")) { *value = h->barrier_spin; return COUPLB_OK; }
   if (!std::strcmp(name, "ibm_window")) { *value = h->ibm_window; return COUPLB_OK; }
   if (!std::strcmp(name, "ibm_group")) { *value = h->ibm_group; return COUPLB_OK; }
+  if (!std::strcmp(name, "ibm_block")) { *value = h->ibm_block; return COUPLB_OK; }
   if (!std::strcmp(name, "ibm_slip")) { *value = h->ibm_slip; return COUPLB_OK; }
   if (!std::strcmp(name, "timeouts")) {
     int rc = set_device(h);

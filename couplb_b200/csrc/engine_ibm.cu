@@ -121,15 +121,16 @@ int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, co
       bool grouped = false;
       if constexpr (L::D == 3) {
         if (h->ibm_group == 8) {
-          // four markers per warp of 8 lanes each: 32 markers per block
-          const unsigned nb8 = (unsigned)(((long long)n + 31) / 32);
+          // four markers per warp of 8 lanes each: ibm_block / 8 markers per block
+          const int bs8 = h->ibm_block;
+          const unsigned nb8 = (unsigned)(((long long)n * 8 + bs8 - 1) / bs8);
           const bool halo = a.zplanes[0] || a.zplanes[1];
           if (ip.delta == COUPLB_DELTA_ROMA) {
-            if (halo) k_ibm_substep8<L, S, 0, true><<<nb8, bs, 0, h->stream>>>(a);
-            else k_ibm_substep8<L, S, 0, false><<<nb8, bs, 0, h->stream>>>(a);
+            if (halo) k_ibm_substep8<L, S, 0, true><<<nb8, bs8, 0, h->stream>>>(a);
+            else k_ibm_substep8<L, S, 0, false><<<nb8, bs8, 0, h->stream>>>(a);
           } else {
-            if (halo) k_ibm_substep8<L, S, 1, true><<<nb8, bs, 0, h->stream>>>(a);
-            else k_ibm_substep8<L, S, 1, false><<<nb8, bs, 0, h->stream>>>(a);
+            if (halo) k_ibm_substep8<L, S, 1, true><<<nb8, bs8, 0, h->stream>>>(a);
+            else k_ibm_substep8<L, S, 1, false><<<nb8, bs8, 0, h->stream>>>(a);
           }
           grouped = true;
         }

@@ -83,6 +83,7 @@ struct couplb_handle {
   int ibm_window = 0;                // option: 0 clip the IBM window like the reference, 1 wrap
   int ibm_slip = 1;                  // option: ITERATIVE / LEARNED measure the slip after the last pass
   int ibm_group = 8;                 // option: lanes per marker of the single-pass 3D sub-step (8, 32)
+  int ibm_block = 128;               // option: threads per block of the grouped sub-step (64, 128, 256)
   const void* halo[2] = {nullptr, nullptr};   // z-face halos of a slab decomposition
   const void* ih_vel[2] = {nullptr, nullptr};  // IBM halos of those faces: neighbour moments,
   void* ih_force[2] = {nullptr, nullptr};      // forces spread beyond the face,

@@ -414,6 +414,9 @@ int  couplb_status_last(couplb_handle* h, int* clamps, int* nonfinite);
  *                 lies inside the interior and whose stencil is cached, the
  *                 rest one warp each) or 32 (one warp per marker).  The two
  *                 differ only in the order of the interpolation sums.
+ *   "ibm_block"   threads per block of the grouped (ibm_group 8) sub-step: 64,
+ *                 128 (default) or 256; a launch shape, results unchanged up
+ *                 to the order of the FP64 total-force sums.
  *   "ibm_slip"    1 (default): ITERATIVE / LEARNED sub-steps measure the slip
  *                 after their last pass (couplb_ibm_slip); 0: they do not, which
  *                 saves an interpolation pass and, for a learned sub-step

@@ -11,6 +11,7 @@ import pytest
 import cases
 from couplb_b200 import abi
 from couplb_b200.lattice import Lattice
+from couplb_b200.lib import CoupLBError
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
@@ -236,7 +237,7 @@ def test_wrapped_window_matches_oracle(cuda_lib, wall):
         assert rel(a, b) <= 1e-12, (c, rel(a, b))
 
 
-def _grouped_case(prec, group, n=(40, 32, 24), cycles=3, md_per_lb=2):
+def _grouped_case(prec, group, n=(40, 32, 24), cycles=3, md_per_lb=2, block=None):
     """Atom forces per sub-step and the final force field of a walled lattice
     with 300 markers: most windows inside the interior, some at the faces and
     walls; every second marker jumps 0.6 cells in x on each later sub-step
@@ -250,6 +251,8 @@ def _grouped_case(prec, group, n=(40, 32, 24), cycles=3, md_per_lb=2):
     active = (np.arange(300) % 8 != 3).astype(np.int32)
     L = Lattice(3, *n, tau=0.7, wall=(0, 0, 1, 2, 0, 0), wall_vel=(0.01, 0, 0), body_force=True, precision=prec)
     L.set_option("ibm_group", group)
+    if block:
+        L.set_option("ibm_block", block)
     L.set_populations(cases.initial_populations(3, n, 7))
     L.set_ibm_params(delta="peskin4", md_per_lb=md_per_lb, xi_ibm=0.8)
     x = x0.copy()
@@ -277,6 +280,25 @@ def test_grouped_substep_matches_warp_per_marker(cuda_lib, prec, tol):
     assert rel(f8, f32) <= tol, rel(f8, f32)
     for c in range(3):
         assert rel(F8[c], F32[c]) <= 10 * tol, (c, rel(F8[c], F32[c]))
+
+
+@pytest.mark.parametrize("block", [64, 256])
+def test_grouped_substep_block_size(cuda_lib, block):
+    """The launch shape of the grouped sub-step (option ibm_block, default
+    128) leaves each marker's arithmetic alone: FP64 atom forces of the first
+    sub-step equal bit for bit; later ones and the force field differ only by
+    the order of the spread atomics."""
+    f, F = _grouped_case("fp64", 8, block=block)
+    fd, Fd = _grouped_case("fp64", 8)
+    assert np.array_equal(f[0], fd[0])
+    assert rel(f, fd) <= 1e-13, rel(f, fd)
+    for c in range(3):
+        assert rel(F[c], Fd[c]) <= 1e-13, (c, rel(F[c], Fd[c]))
+    L = Lattice(3, 8, 8, 8)
+    with pytest.raises(CoupLBError):
+        L.set_option("ibm_block", 96)
+    assert L.get_option("ibm_block") == 128
+    L.close()
 
 
 def test_grouped_substep_fp64_matches_oracle(cuda_lib):
