@@ -4,9 +4,11 @@ code's communicator -- here threads of this process on one GPU, exchanging
 through host memory (each rank synchronises its own stream and copies; no
 kernel waits on another rank).  The run matches one fix over the whole box:
 atom forces at every step, populations and the reduced diagnostics, FP64
-within 1e-12, and rank 0's profile file."""
+within 1e-12, and rank 0's profile file; checkpoints are written per rank
+and a restart from them continues bit for bit."""
 import ctypes as C
 import threading
+import struct
 
 import numpy as np
 import pytest
@@ -145,3 +147,76 @@ def test_z_slab_ranks_match_one_rank(cuda_lib, tmp_path, nprocs, wall):
     a, b = _profile(tmp_path / "ranks0.dat"), _profile(tmp_path / "one.dat")
     assert a.shape == b.shape and np.abs(a - b).max() <= 1e-9 * np.abs(b).max()
     assert not any((tmp_path / f"ranks{r}.dat").exists() for r in range(1, nprocs))
+
+
+def _in_threads(nprocs, body):
+    """body(rank, comm) on `nprocs` threads; their results in rank order."""
+    comm = ThreadComm(nprocs)
+    out, errors = [None] * nprocs, []
+
+    def main(r):
+        try:
+            out[r] = body(r, comm)
+        except Exception as e:      # noqa: BLE001 -- reported by the main thread
+            errors.append(repr(e))
+            comm.bar.abort()
+
+    threads = [threading.Thread(target=main, args=(r,)) for r in range(nprocs)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join(120)
+    assert not errors, errors
+    return out
+
+
+@pytest.mark.parametrize("nprocs", [2, 3])
+def test_z_slab_checkpoint_restart(cuda_lib, tmp_path, nprocs):
+    """A channel on z slabs writes prefix.<rank>.clbk with the slab's local
+    grid and offset (couplb_io.h:669-719); fixes restarted from those files
+    continue bit for bit, and the slabs match one fix over the whole box."""
+    from couplb_b200.slabs import partition
+    n = (6, 5, 9)
+    box = ((0.0, 0.0, 0.0), (6.0, 5.0, 9.0))
+    args = "f all couplb 6 5 9 0.1 1.0 wall_y 1 2 wall_vel 0.01 0 0 gravity 1e-5 0 2e-6".split()
+    one = FixCoupLB(args, dimension=3)
+    one.init(*box, 1.0)
+    md.run(one, md.empty_atoms(), 17, 1.0)
+    f17 = cases.interior(one.lattice.get_populations(), 3)
+    one.close()
+    parts = partition(n[2], nprocs)
+    pre = str(tmp_path / "ck")
+
+    def sub(r):
+        z0, nzl = parts[r]
+        return dict(sublo=(0.0, 0.0, float(z0)), subhi=(6.0, 5.0, float(z0 + nzl)))
+
+    def first(r, comm):
+        fx = FixCoupLB(args + ["checkpoint", "10", pre], dimension=3)
+        fx.set_comm(nprocs, r, lambda *a: comm.sendrecv(r, *a), lambda a, op: comm.allreduce(r, a, op))
+        fx.init(*box, 1.0, **sub(r))
+        md.run(fx, md.empty_atoms(), 17, 1.0)
+        f = cases.interior(fx.lattice.get_populations(), 3)
+        fx.close()
+        return f
+
+    def again(r, comm):
+        fx = FixCoupLB(args + ["restart", pre], dimension=3)
+        fx.set_comm(nprocs, r, lambda *a: comm.sendrecv(r, *a), lambda a, op: comm.allreduce(r, a, op))
+        fx.init(*box, 1.0, ntimestep=10, **sub(r))
+        md.run(fx, md.empty_atoms(), 7, 1.0, start_step=10)
+        f = cases.interior(fx.lattice.get_populations(), 3)
+        fx.close()
+        return f
+
+    cont = _in_threads(nprocs, first)
+    np.testing.assert_array_equal(np.concatenate(cont, axis=1), f17)
+    for r in range(nprocs):
+        raw = open(f"{pre}.{r}.clbk", "rb").read()
+        step = struct.unpack_from("<q", raw, 8)[0]
+        dims = struct.unpack_from("<9i", raw, 24)
+        z0, nzl = parts[r]
+        assert step == 10 and dims == (6, 5, nzl, 0, 0, z0, 6, 5, 9)
+    rest = _in_threads(nprocs, again)
+    for a, b in zip(rest, cont):
+        np.testing.assert_array_equal(a, b)
