@@ -210,6 +210,8 @@ int couplb_destroy(couplb_handle* h) {
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   for (int e = 0; e < 2; e++)
     if (h->copy_ev[e]) cudaEventDestroy(h->copy_ev[e]);
+  for (cudaEvent_t e : h->fout_ev)
+    if (e) cudaEventDestroy(e);
   dfree(h->d_x); dfree(h->d_v); dfree(h->d_m); dfree(h->d_fout); dfree(h->d_active);
   if (h->h_fout) cudaFreeHost(h->h_fout);
   if (h->h_mass) cudaFreeHost(h->h_mass);

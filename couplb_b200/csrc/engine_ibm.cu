@@ -170,19 +170,80 @@ int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, co
 
 }  // namespace couplb
 
-extern "C" {
-
-}  // extern "C"
-
 namespace {
 
-// Host atom arrays of one sub-step copied to the handle's device buffers,
-// queued on stream s; *nc = atoms in the group.
-int stage_host_atoms(couplb_handle* h, cudaStream_t s, int n, const double* x, const double* v,
-                     const double* mass, const int* active, int* nc) {
-  if (n < 0 || (n > 0 && (!x || !v || !mass))) return fail(h, COUPLB_ERR_ARG, "bad atom arrays");
-  int rc = ensure_atoms(h, n);
+constexpr int kForceChunks = 4;
+
+int ensure_copy_stream(couplb_handle* h) {
+  if (h->copy_stream) return COUPLB_OK;
+  CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+  for (int e = 0; e < 2; e++) CK(cudaEventCreateWithFlags(&h->copy_ev[e], cudaEventDisableTiming));
+  for (int e = 0; e < kForceChunks; e++) CK(cudaEventCreateWithFlags(&h->fout_ev[e], cudaEventDisableTiming));
+  return COUPLB_OK;
+}
+
+// The sub-step of the staged atoms, then the forces back to the host: the
+// copy comes back in kForceChunks pieces and each is added to f_add while the
+// next one travels.
+int substep_staged(couplb_handle* h, int n, const int* active, int nc, double* f_add, int refresh) {
+  int rc = engine_ibm(h, nc > 0 ? n : 0, (const double*)h->d_x, (const double*)h->d_v,
+                      (const double*)h->d_m, active ? (const int*)h->d_active : nullptr,
+                      (double*)h->d_fout, 0, refresh);
   if (rc) return rc;
+  if (nc > 0) {
+    const long long tot = 3LL * n;
+    const double* d = (const double*)h->d_fout;
+    for (int k = 0; k < kForceChunks; k++) {
+      const long long lo = tot * k / kForceChunks, hi = tot * (k + 1) / kForceChunks;
+      if (hi > lo)
+        CK(cudaMemcpyAsync(h->h_fout + lo, d + lo, sizeof(double) * (hi - lo), cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaEventRecord(h->fout_ev[k], h->stream));
+    }
+    for (int k = 0; k < kForceChunks; k++) {
+      const long long lo = tot * k / kForceChunks, hi = tot * (k + 1) / kForceChunks;
+      CK(cudaEventSynchronize(h->fout_ev[k]));
+      for (long long a = lo; a < hi; a++) f_add[a] += h->h_fout[a];
+    }
+  }
+  return COUPLB_OK;
+}
+
+int check_host_args(couplb_handle* h, int n, const double* f_add) {
+  if (!h) return COUPLB_ERR_ARG;
+  if (!h->ip_set) return fail(h, COUPLB_ERR_STATE, "couplb_set_ibm_params not called");
+  if (n > 0 && !f_add) return fail(h, COUPLB_ERR_ARG, "bad atom arrays");
+  return set_device(h);
+}
+
+}  // namespace
+
+namespace couplb {
+
+int engine_host_begin(couplb_handle* h, bool lbm, const double* g_lb, int n, const double* x, const double* v) {
+  if (!h->ip_set) return fail(h, COUPLB_ERR_STATE, "couplb_set_ibm_params not called");
+  if (n < 0 || (n > 0 && (!x || !v))) return fail(h, COUPLB_ERR_ARG, "bad atom arrays");
+  int rc = set_device(h);
+  if (rc) return rc;
+  if ((rc = ensure_atoms(h, n))) return rc;
+  if ((rc = ensure_copy_stream(h))) return rc;
+  // the copies wait for the lattice's stream to reach this point (the
+  // previous sub-step read the same device buffers), then run beside the LB
+  // kernel
+  CK(cudaEventRecord(h->copy_ev[0], h->stream));
+  CK(cudaStreamWaitEvent(h->copy_stream, h->copy_ev[0], 0));
+  if (n > 0) {
+    CK(cudaMemcpyAsync(h->d_x, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->copy_stream));
+    CK(cudaMemcpyAsync(h->d_v, v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->copy_stream));
+  }
+  h->staged_n = n;
+  return lbm ? engine_lbm_step(h, g_lb) : COUPLB_OK;
+}
+
+int engine_host_finish(couplb_handle* h, bool lbm, int n, const double* mass, const int* active, double* f_add,
+                       int refresh, int* ncoupled) {
+  if (h->staged_n != n) return fail(h, COUPLB_ERR_STATE, "sub-step of %d atoms without their positions", n);
+  h->staged_n = -1;
+  if (n > 0 && !mass) return fail(h, COUPLB_ERR_ARG, "bad atom arrays");
   // the fix core's pinned mass / group buffers come with their count and
   // whether they changed since their last device copy
   const bool pinned = mass == h->h_mass && active == h->h_active && h->hint_n == n;
@@ -194,75 +255,36 @@ int stage_host_atoms(couplb_handle* h, cudaStream_t s, int n, const double* x, c
   }
   const bool statics_current = pinned && h->hint_unchanged && h->statics_n == n;
   h->hint_n = -1;
-  *nc = c;
-  if (n > 0) {
-    CK(cudaMemcpyAsync(h->d_x, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(h->d_v, v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
-    if (!statics_current) {
-      CK(cudaMemcpyAsync(h->d_m, mass, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-      if (active) CK(cudaMemcpyAsync(h->d_active, active, sizeof(int) * n, cudaMemcpyHostToDevice, s));
-    }
-    h->statics_n = (pinned && active) ? n : -1;
+  if (ncoupled) *ncoupled = c;
+  if (n > 0 && !statics_current) {
+    CK(cudaMemcpyAsync(h->d_m, mass, sizeof(double) * n, cudaMemcpyHostToDevice, h->copy_stream));
+    if (active) CK(cudaMemcpyAsync(h->d_active, active, sizeof(int) * n, cudaMemcpyHostToDevice, h->copy_stream));
   }
-  return COUPLB_OK;
+  if (n > 0) h->statics_n = (pinned && active) ? n : -1;
+  CK(cudaEventRecord(h->copy_ev[1], h->copy_stream));
+  CK(cudaStreamWaitEvent(h->stream, h->copy_ev[1], 0));
+  return substep_staged(h, n, active, c, f_add, lbm ? 1 : refresh);
 }
 
-// The sub-step of staged host atoms, then the forces back to the host.
-int substep_staged(couplb_handle* h, int n, const int* active, int nc, double* f_add, int refresh) {
-  int rc = engine_ibm(h, nc > 0 ? n : 0, (const double*)h->d_x, (const double*)h->d_v,
-                      (const double*)h->d_m, active ? (const int*)h->d_active : nullptr,
-                      (double*)h->d_fout, 0, refresh);
-  if (rc) return rc;
-  if (nc > 0) {
-    CK(cudaMemcpyAsync(h->h_fout, h->d_fout, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    for (int a = 0; a < 3 * n; a++) f_add[a] += h->h_fout[a];
-  }
-  return COUPLB_OK;
-}
-
-}  // namespace
+}  // namespace couplb
 
 extern "C" {
 
 int couplb_ibm_substep(couplb_handle* h, int n, const double* x, const double* v,
                        const double* mass, const int* active, double* f_add, int refresh,
                        int* ncoupled) {
-  if (!h) return COUPLB_ERR_ARG;
-  if (!h->ip_set) return fail(h, COUPLB_ERR_STATE, "couplb_set_ibm_params not called");
-  if (n > 0 && !f_add) return fail(h, COUPLB_ERR_ARG, "bad atom arrays");
-  int rc = set_device(h);
+  int rc = check_host_args(h, n, f_add);
   if (rc) return rc;
-  int nc = 0;
-  if ((rc = stage_host_atoms(h, h->stream, n, x, v, mass, active, &nc))) return rc;
-  if (ncoupled) *ncoupled = nc;
-  return substep_staged(h, n, active, nc, f_add, refresh);
+  if ((rc = engine_host_begin(h, false, nullptr, n, x, v))) return rc;
+  return engine_host_finish(h, false, n, mass, active, f_add, refresh, ncoupled);
 }
 
 int couplb_lbm_step_ibm(couplb_handle* h, const double* g_lb, int n, const double* x, const double* v,
                         const double* mass, const int* active, double* f_add, int* ncoupled) {
-  if (!h) return COUPLB_ERR_ARG;
-  if (!h->ip_set) return fail(h, COUPLB_ERR_STATE, "couplb_set_ibm_params not called");
-  if (n > 0 && !f_add) return fail(h, COUPLB_ERR_ARG, "bad atom arrays");
-  int rc = set_device(h);
+  int rc = check_host_args(h, n, f_add);
   if (rc) return rc;
-  // the atom copies run on a copy stream while the LB kernel runs (the
-  // previous sub-step, which read the same buffers, is complete: the host
-  // path synchronises at its end; the copy stream still waits for the main
-  // stream to reach this point)
-  if (!h->copy_stream) {
-    CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
-    for (int e = 0; e < 2; e++) CK(cudaEventCreateWithFlags(&h->copy_ev[e], cudaEventDisableTiming));
-  }
-  CK(cudaEventRecord(h->copy_ev[0], h->stream));
-  CK(cudaStreamWaitEvent(h->copy_stream, h->copy_ev[0], 0));
-  int nc = 0;
-  if ((rc = stage_host_atoms(h, h->copy_stream, n, x, v, mass, active, &nc))) return rc;
-  CK(cudaEventRecord(h->copy_ev[1], h->copy_stream));
-  if (ncoupled) *ncoupled = nc;
-  if ((rc = engine_lbm_step(h, g_lb))) return rc;
-  CK(cudaStreamWaitEvent(h->stream, h->copy_ev[1], 0));
-  return substep_staged(h, n, active, nc, f_add, 1);
+  if ((rc = engine_host_begin(h, true, g_lb, n, x, v))) return rc;
+  return engine_host_finish(h, true, n, mass, active, f_add, 1, ncoupled);
 }
 
 int couplb_lbm_step_ibm_device(couplb_handle* h, const double* g_lb, int n, const double* d_x,

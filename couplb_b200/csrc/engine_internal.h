@@ -91,6 +91,8 @@ struct couplb_handle {
   long long barrier_spin = 1LL << 21;   // option: grid-barrier poll limit of the method kernels
   cudaStream_t copy_stream = nullptr;   // host->device atom copies of couplb_lbm_step_ibm
   cudaEvent_t copy_ev[2] = {nullptr, nullptr};   // main stream reached / copies done
+  cudaEvent_t fout_ev[4] = {nullptr, nullptr, nullptr, nullptr};   // force chunks back on the host
+  int staged_n = -1;                    // atoms whose x, v engine_host_begin queued
   int coop_blocks[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // resident blocks of k_ibm_method (Roma,
                                                    // Peskin4, learned Roma, learned Peskin4),
                                                    // then of its register-resident form
@@ -118,6 +120,15 @@ void engine_atom_host_hint(couplb_handle* h, int n, int count, int unchanged);
 // A refresh sub-step with no coupled atoms on this lattice (other slabs have
 // some): only its effect on the density the next LB step reads.
 void engine_note_refresh(couplb_handle* h);
+// A sub-step of host atom arrays in two calls, so that the caller can fill
+// the masses and group flags while the positions travel (and the LB kernel
+// runs): engine_host_begin queues the x, v copies on the copy stream and, with
+// lbm, the LB step on the lattice's stream; engine_host_finish copies the
+// masses and flags unless the hint says they are unchanged, runs the
+// sub-step (the refresh one with lbm) and adds the forces to f_add.
+int engine_host_begin(couplb_handle* h, bool lbm, const double* g_lb, int n, const double* x, const double* v);
+int engine_host_finish(couplb_handle* h, bool lbm, int n, const double* mass, const int* active, double* f_add,
+                       int refresh, int* ncoupled);
 int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, const double* d_m,
                const int* d_active, double* d_fout, int accumulate, int refresh);
 }  // namespace couplb

@@ -513,29 +513,41 @@ int read_checkpoint(couplb_fix* F, long long* step_out) {
 
 // FixCoupLB::do_ibm_sub_coupling (fix_couplb.cpp:730-798).  With lbm, the
 // LB step of the cycle (do_lbm_step with body force g_lb, or none when
-// g_lb is null) runs first, in the same engine call when there are atoms
-// (couplb_lbm_step_ibm: the LB launch fills the refresh's stencil records).
+// g_lb is null) is queued first, the position copies beside it, and the host
+// loop over the atoms runs while both are in flight.
 int ibm_sub_coupling(couplb_fix* F, const couplb_atoms* at, bool lbm = false,
                      const double* g_lb = nullptr) {
   const bool first = (F->md_sub_count == 0);
   const int nl = at ? at->nlocal : 0;
+  // the position copies (and the cycle's LB step) start before the loop over
+  // the atoms below
+  int rc0 = couplb::engine_host_begin(F->h, lbm, g_lb, nl, nl ? at->x : nullptr, nl ? at->v : nullptr);
+  if (rc0) return F->engine_fail(rc0);
   // masses and group flags go to pinned buffers of the lattice handle, so the
   // engine's host->device copies of a sub-step start from pinned memory
   double* mass_buf = nullptr;
   int* active_buf = nullptr;
-  int rc0 = couplb::engine_atom_host_buffers(F->h, nl, &mass_buf, &active_buf);
-  if (rc0) return F->engine_fail(rc0);
+  if ((rc0 = couplb::engine_atom_host_buffers(F->h, nl, &mass_buf, &active_buf))) return F->engine_fail(rc0);
   int ng = 0;
-  bool changed = false;
-  for (int i = 0; i < nl; i++) {
-    const int act = at->mask ? ((at->mask[i] & at->groupbit) != 0) : 1;
-    const double m = at->rmass ? at->rmass[i] : (at->mass ? at->mass[at->type[i]] : 1.0);
-    if (active_buf[i] != act || !(mass_buf[i] == m)) {
-      changed = true;
+  int changed = 0;
+  // every value is written and compared without a branch (m != old is also
+  // true for NaN), so the loop vectorises
+  auto fill = [&](auto mass_of) {
+    const int* mask = at->mask;
+    const int gb = at->groupbit;
+    for (int i = 0; i < nl; i++) {
+      const int act = mask ? ((mask[i] & gb) != 0) : 1;
+      const double m = mass_of(i);
+      changed |= (active_buf[i] != act) | (mass_buf[i] != m);
       active_buf[i] = act;
       mass_buf[i] = m;
+      ng += act;
     }
-    ng += act;
+  };
+  if (nl > 0) {
+    if (at->rmass) fill([r = at->rmass](int i) { return r[i]; });
+    else if (at->mass) fill([m = at->mass, t = at->type](int i) { return m[t[i]]; });
+    else fill([](int) { return 1.0; });
   }
   couplb::engine_atom_host_hint(F->h, nl, ng, changed ? 0 : 1);
   // the group count is global (fix_couplb.cpp:743-747)
@@ -545,11 +557,8 @@ int ibm_sub_coupling(couplb_fix* F, const couplb_atoms* at, bool lbm = false,
     if (rca) return rca;
   }
   if (ng_all == 0) {
+    // the cycle's LB step is queued already
     F->ibm_has_particles = false;
-    if (lbm) {
-      const int rc = couplb_lbm_step(F->h, g_lb);
-      if (rc) return F->engine_fail(rc);
-    }
     return COUPLB_OK;
   }
   const int refresh = (first || !F->ibm_has_particles) ? 1 : 0;
@@ -561,8 +570,7 @@ int ibm_sub_coupling(couplb_fix* F, const couplb_atoms* at, bool lbm = false,
     return COUPLB_OK;
   }
   int nc = 0;
-  const int rc = lbm ? couplb_lbm_step_ibm(F->h, g_lb, nl, at->x, at->v, mass_buf, active_buf, at->f, &nc)
-                     : couplb_ibm_substep(F->h, nl, at->x, at->v, mass_buf, active_buf, at->f, refresh, &nc);
+  const int rc = couplb::engine_host_finish(F->h, lbm, nl, mass_buf, active_buf, at->f, refresh, &nc);
   if (rc) return F->engine_fail(rc);
   return COUPLB_OK;
 }
