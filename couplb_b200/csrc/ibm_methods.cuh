@@ -503,6 +503,10 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
   double F0 = 0, F1 = 0, F2 = 0, c0 = 0, c1 = 0, c2 = 0, mxi = 0, vx = 0, vy = 0, vz = 0;
   if (have) {
     const MarkerWindow w = marker_window<L, S>(a, mk);
+    // the marker's mass and velocity load beside its position, off the chain
+    // of the stencil fill
+    mxi = a.m[mk] * a.xi_over_dt;
+    vx = a.v[3 * mk]; vy = a.v[3 * mk + 1]; vz = a.v[3 * mk + 2];
     const StencilKey key = a.skey[mk];
     const bool fill = P.fill != 0;
     const bool hit = key.epoch == a.cur_epoch && key.i0 == w.i0 && key.j0 == w.j0 && key.k0 == w.k0;
@@ -583,12 +587,10 @@ __global__ void __launch_bounds__(256) k_ibm_method_resident(const PassArgs<S> P
       const R iw = R(1) / ws;
       U0 = double(ui * iw); U1 = double(vi * iw); U2 = double(wi * iw);
     }
-    mxi = a.m[mk] * a.xi_over_dt;
-    vx = a.v[3 * mk]; vy = a.v[3 * mk + 1]; vz = a.v[3 * mk + 2];
     F0 = mxi * (U0 * a.vs - vx);
     F1 = mxi * (U1 * a.vs - vy);
     F2 = mxi * (U2 * a.vs - vz);
-    if (LEARNED && lane < 3) xs[81 + lane] = float(a.v[3 * mk + lane] / a.vs);
+    if (LEARNED && lane < 3) xs[81 + lane] = float((lane == 0 ? vx : (lane == 1 ? vy : vz)) / a.vs);
   }
   if (LEARNED) {
     // the network for the block's markers (every warp takes part)
