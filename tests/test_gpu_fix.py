@@ -63,6 +63,27 @@ def test_quickstart_poiseuille_profile(cuda_lib, tmp_path, precision):
     assert any("CoupLB step 50000: Ma=" in m for m in fix.messages)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_poiseuille3d_profile(cuda_lib, tmp_path, precision):
+    """tests/poiseuille3d/in.poiseuille3d (D3Q19 8x32x8, nu 0.1, g 5e-6,
+    wall_y 1 1, x and z periodic, 50000 steps, profile every 5000) with the
+    criterion of tests/poiseuille2d/validate.py:99,111 on the z-averaged
+    profile (fix_couplb.cpp:903-979)."""
+    out = tmp_path / "p3d.dat"
+    fix = FixCoupLB(f"flow noatoms couplb 8 32 8 0.1 1.0 wall_y 1 1 gravity 5e-6 0.0 0.0 "
+                    f"output 5000 {out} check_every 2000 precision {precision}".split(), dimension=3)
+    fix.init(boxlo=(0, 0, 0), boxhi=(8, 32, 8), dt=1.0, periodicity=(1, 0, 1))
+    md.run(fix, md.empty_atoms(), 50000, 1.0)
+    header, blocks = read_profile(out)
+    assert header.startswith("# H=Ny=32 tau=0.800000")
+    assert sorted(blocks) == list(range(0, 50001, 5000))
+    d = blocks[50000]
+    y, ux, uy = d[:, 2], d[:, 4], d[:, 5]
+    exact = 5e-6 / (2 * 0.1) * (y + 0.5) * (32 - 0.5 - y)
+    assert np.abs(ux - exact).max() / exact.max() < 0.01
+    assert np.abs(uy).max() < 1e-6 * exact.max()
+
+
 def test_profile_matches_oracle_moments(cuda_lib, tmp_path):
     """Profile lines (fix_couplb.cpp:960-970) from the oracle's moments."""
     from oracle.bindings import OracleGrid
