@@ -71,6 +71,8 @@ def parse():
                     help="with --only ibm: also time the workload through the fix hooks (1) or not (0)")
     ap.add_argument("--ibm-n", type=int, default=256,
                     help="edge of the periodic box of the point-marker workload")
+    ap.add_argument("--ibm-order", default="drawn", choices=["drawn", "cell"],
+                    help="marker order of --only ibm: as drawn, or sorted by cell")
     ap.add_argument("--ibm-block", type=int, default=128, choices=[64, 128, 256],
                     help="threads per block of the grouped IBM sub-step (handle option ibm_block)")
     ap.add_argument("--ibm-group", type=int, default=8, choices=[8, 32],
@@ -476,10 +478,23 @@ def e2e_ibm_fix(torch, device, cycles, warmup, peak, n=256, natoms=20000, md_per
             "nonfinite": nonfinite}
 
 
-def ibm_bench(torch, device, prec, cycles, warmup, peak, n=256, natoms=20000, md_per_lb=4, seed=3):
+def cell_order(x):
+    """Permutation that orders markers by their cell (z, then y, then x), as
+    LAMMPS' periodic spatial sort of the atom arrays (atom_modify sort) leaves
+    them; the positions themselves are unchanged."""
+    c = np.floor(x).astype(np.int64)
+    return np.lexsort((c[:, 0], c[:, 1], c[:, 2]))
+
+
+def ibm_bench(torch, device, prec, cycles, warmup, peak, n=256, natoms=20000, md_per_lb=4, seed=3,
+              order="drawn"):
     """D3Q19 256^3 periodic box, nu 0.1, 20000 point markers at uniform random
-    positions with v ~ N(0, 0.01^2), Peskin4, md_per_lb 4."""
+    positions with v ~ N(0, 0.01^2), Peskin4, md_per_lb 4; order "cell" runs
+    the same markers sorted by cell."""
     x0, v0 = ibm_markers(torch, n, natoms, seed)
+    if order == "cell":
+        p = cell_order(x0)
+        x0, v0 = np.ascontiguousarray(x0[p]), np.ascontiguousarray(v0[p])
     return marker_bench(torch, device, prec, cycles, warmup, (n, n, n), (0,) * 6, 3 * 0.1 + 0.5, x0, v0,
                         md_per_lb, f"d3q19_periodic_{n}^3_{natoms}_markers_peskin4_md_per_lb{md_per_lb}",
                         peak, momentum_check=True)
@@ -804,7 +819,8 @@ def main():
                           "val_loss": vl}), flush=True)
         return
     if args.only == "ibm":
-        r = ibm_bench(torch, local, "fp32", args.ibm_cycles, args.warmup, load_peak()[0], n=args.ibm_n)
+        r = ibm_bench(torch, local, "fp32", args.ibm_cycles, args.warmup, load_peak()[0], n=args.ibm_n,
+                      order=args.ibm_order)
         if args.ibm_e2e:
             r["e2e"] = e2e_ibm_fix(torch, local, args.ibm_cycles, args.warmup, load_peak()[0], n=args.ibm_n)
         print(json.dumps(r), flush=True)

@@ -212,6 +212,11 @@ int couplb_destroy(couplb_handle* h) {
     if (h->copy_ev[e]) cudaEventDestroy(h->copy_ev[e]);
   for (cudaEvent_t e : h->fout_ev)
     if (e) cudaEventDestroy(e);
+  {
+    void* p2 = h->d_order; dfree(p2);
+    p2 = h->d_order_rank; dfree(p2);
+    p2 = h->d_order_count; dfree(p2);
+  }
   dfree(h->d_x); dfree(h->d_v); dfree(h->d_m); dfree(h->d_fout); dfree(h->d_active);
   if (h->h_fout) cudaFreeHost(h->h_fout);
   if (h->h_mass) cudaFreeHost(h->h_mass);
@@ -655,6 +660,12 @@ int couplb_set_option(couplb_handle* h, const char* name, long long value) {
     h->ibm_group = (int)value;
     return COUPLB_OK;
   }
+  if (!std::strcmp(name, "ibm_sort")) {
+    if (value < 0 || value > (1 << 30)) return fail(h, COUPLB_ERR_ARG, "ibm_sort must be 0..2^30");
+    h->ibm_sort = (int)value;
+    h->order_n = -1;
+    return COUPLB_OK;
+  }
   if (!std::strcmp(name, "ibm_block")) {
     if (value != 64 && value != 128 && value != 256)
       return fail(h, COUPLB_ERR_ARG, "ibm_block must be 64, 128 or 256");
@@ -678,6 +689,7 @@ int couplb_get_option(couplb_handle* h, const char* name, long long* value) {
   if (!std::strcmp(name, "ibm_window")) { *value = h->ibm_window; return COUPLB_OK; }
   if (!std::strcmp(name, "ibm_group")) { *value = h->ibm_group; return COUPLB_OK; }
   if (!std::strcmp(name, "ibm_block")) { *value = h->ibm_block; return COUPLB_OK; }
+  if (!std::strcmp(name, "ibm_sort")) { *value = h->ibm_sort; return COUPLB_OK; }
   if (!std::strcmp(name, "ibm_slip")) { *value = h->ibm_slip; return COUPLB_OK; }
   if (!std::strcmp(name, "timeouts")) {
     int rc = set_device(h);

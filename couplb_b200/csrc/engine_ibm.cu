@@ -31,6 +31,39 @@ void engine_note_refresh(couplb_handle* h) {
   if (h->p.body_force) h->rho_state = kRhoCurrent;
 }
 
+// The processing order of the markers' refresh and grouped sub-step
+// (k_order_count / k_order_scan / k_order_scatter on the lattice's stream).
+template <class L, class S>
+int make_order(couplb_handle* h, const IbmArgs<S>& a, int n) {
+  const int nb = ((L::D == 3 ? h->p.nz : h->p.ny) + kOrderPlanes - 1) / kOrderPlanes;
+  if (h->order_cap < n) {
+    void* p = h->d_order; dfree(p); h->d_order = nullptr;
+    p = h->d_order_rank; dfree(p); h->d_order_rank = nullptr;
+    h->order_cap = 0;
+    const int cap = std::max(n, 1024);
+    int rc;
+    if ((rc = dalloc(h, (void**)&h->d_order, sizeof(int) * (size_t)cap))) return rc;
+    if ((rc = dalloc(h, (void**)&h->d_order_rank, sizeof(int) * (size_t)cap))) return rc;
+    h->order_cap = cap;
+  }
+  if (h->order_nb < nb) {
+    void* p = h->d_order_count; dfree(p); h->d_order_count = nullptr;
+    h->order_nb = 0;
+    int rc = dalloc(h, (void**)&h->d_order_count, sizeof(int) * (size_t)nb);
+    if (rc) return rc;
+    h->order_nb = nb;
+  }
+  CK(cudaMemsetAsync(h->d_order_count, 0, sizeof(int) * (size_t)nb, h->stream));
+  const unsigned g = (unsigned)((n + 255) / 256);
+  k_order_count<L, S><<<g, 256, 0, h->stream>>>(a, nb, h->d_order_count, h->d_order_rank);
+  k_order_scan<<<1, 256, 0, h->stream>>>(nb, h->d_order_count);
+  k_order_scatter<L, S><<<g, 256, 0, h->stream>>>(a, nb, h->d_order_count, h->d_order_rank, h->d_order);
+  CK_LAUNCH();
+  h->order_n = n;
+  h->order_age = 0;
+  return COUPLB_OK;
+}
+
 // Shared body of the host- and device-array IBM sub-step.  The launches of
 // the method kernels (launch_method) are compiled in engine_methods_*.cu.
 int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, const double* d_m,
@@ -117,7 +150,20 @@ int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, co
       a.zplanes[side] = bound ? h->ih_planes[side] : 0;
     }
     if (method == COUPLB_IBM_SINGLE) {
-      if (refresh && !a.all_valid) k_ibm_prefetch<L, S><<<nb, bs, 0, h->stream>>>(a);
+      if (refresh && !a.all_valid) {
+        // the marker order is remade every ibm_sort refreshes (and for a new
+        // marker count); in between it only gets less local as markers move
+        if (h->ibm_sort > 0 && (h->order_n != n || ++h->order_age >= h->ibm_sort)) {
+          lrc = make_order<L, S>(h, a, n);
+          if (lrc) return;
+        }
+        a.order = (h->ibm_sort > 0 && h->order_n == n) ? h->d_order : nullptr;
+        k_ibm_prefetch<L, S><<<nb, bs, 0, h->stream>>>(a);
+        // the sub-steps keep the index order: markers that the caller keeps
+        // in chain order (rods, filaments) spread onto shared nodes from one
+        // warp there, which the cell order would scatter
+        a.order = nullptr;
+      }
       bool grouped = false;
       if constexpr (L::D == 3) {
         if (h->ibm_group == 8) {

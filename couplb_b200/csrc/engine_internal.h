@@ -84,6 +84,12 @@ struct couplb_handle {
   int ibm_slip = 1;                  // option: ITERATIVE / LEARNED measure the slip after the last pass
   int ibm_group = 8;                 // option: lanes per marker of the single-pass 3D sub-step (8, 32)
   int ibm_block = 128;               // option: threads per block of the grouped sub-step (64, 128, 256)
+  int ibm_sort = 16;                 // option: refreshes between re-sorts of the marker order (0: off)
+  int* d_order = nullptr;            // marker processing order (k_order_*), its ranks and buckets
+  int* d_order_rank = nullptr;
+  int* d_order_count = nullptr;
+  int order_cap = 0, order_nb = 0;   // capacity of the two per-marker arrays, buckets
+  int order_n = -1, order_age = 0;   // markers the order is for, refreshes since it was made
   const void* halo[2] = {nullptr, nullptr};   // z-face halos of a slab decomposition
   const void* ih_vel[2] = {nullptr, nullptr};  // IBM halos of those faces: neighbour moments,
   void* ih_force[2] = {nullptr, nullptr};      // forces spread beyond the face,

@@ -108,6 +108,9 @@ struct IbmArgs {
   const typename S::A* vh[2];
   typename S::A* fh[2];
   int zplanes[2];
+  // processing order of k_ibm_prefetch and k_ibm_substep8 (a permutation of
+  // 0..n-1, k_order_*), or null for the index order
+  const int* order = nullptr;
 };
 
 // Halo plane of the ghost-inclusive z index kg (0: the plane below the low
@@ -355,11 +358,74 @@ __device__ __forceinline__ void prefetch_marker(const IbmArgs<S>& a, int mk, int
 // Refresh prefetch: one warp per active marker fills its slot's record.
 template <class L, class S>
 __global__ void __launch_bounds__(256) k_ibm_prefetch(const IbmArgs<S> a) {
-  const int mk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (mk >= a.n) return;
+  if (w >= a.n) return;
+  const int mk = a.order ? a.order[w] : w;
   if (a.active && !a.active[mk]) return;
   prefetch_marker<L, S>(a, mk, lane, a.cur_epoch);
+}
+
+// Processing order of the refresh: the markers grouped by bands of
+// kOrderPlanes z planes of their cell (y rows in 2D), so that markers whose
+// windows share population lines run close together in time and find them
+// in L2.  Bands rather than single planes keep runs of markers that the
+// caller holds in chain order (rods) together, as far as the atomic ranks
+// below follow the index order within a warp.  Every marker is still
+// handled once by its own lanes, so the records do not depend on the order.
+// A counting sort in three launches: band sizes with each marker's rank in
+// its band, the band offsets, the scatter.
+constexpr int kOrderPlanes = 8;
+
+template <class L, class S>
+__device__ __forceinline__ int order_bucket(const IbmArgs<S>& a, int mk, int nb) {
+  constexpr int d = (L::D == 3) ? 2 : 1;
+  const double l = ((a.x[3 * mk + d] - a.lo[d]) * a.inv_dx - a.off[d]) * (1.0 / kOrderPlanes);
+  int b = 0;   // below the lattice, and NaN: band 0
+  if (l >= 0.0) b = l < (double)nb ? (int)l : nb - 1;
+  return b;
+}
+
+template <class L, class S>
+__global__ void k_order_count(const IbmArgs<S> a, int nb, int* __restrict__ count, int* __restrict__ rank) {
+  const int mk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (mk >= a.n) return;
+  rank[mk] = atomicAdd(count + order_bucket<L, S>(a, mk, nb), 1);
+}
+
+// Exclusive prefix sum of the nb bucket sizes, in place; one block of 256.
+static __global__ void __launch_bounds__(256) k_order_scan(int nb, int* __restrict__ count) {
+  __shared__ int part[256];
+  const int t = threadIdx.x;
+  const int per = (nb + 255) / 256;
+  const int lo = min(nb, t * per), hi = min(nb, lo + per);
+  int sum = 0;
+  for (int b = lo; b < hi; b++) sum += count[b];
+  part[t] = sum;
+  __syncthreads();
+  if (t == 0) {
+    int run = 0;
+    for (int i = 0; i < 256; i++) {
+      const int c = part[i];
+      part[i] = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+  int run = part[t];
+  for (int b = lo; b < hi; b++) {
+    const int c = count[b];
+    count[b] = run;
+    run += c;
+  }
+}
+
+template <class L, class S>
+__global__ void k_order_scatter(const IbmArgs<S> a, int nb, const int* __restrict__ start,
+                                const int* __restrict__ rank, int* __restrict__ order) {
+  const int mk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (mk >= a.n) return;
+  order[start[order_bucket<L, S>(a, mk, nb)] + rank[mk]] = mk;
 }
 
 // Velocity of stencil slot s of marker mk (node (i,j,k) = n).
@@ -691,10 +757,11 @@ __global__ void __launch_bounds__(256, sizeof(typename S::A) == 4 ? 3 : 2) k_ibm
   __shared__ double part[8][3];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gl = lane & 7, gb = lane & ~7;
-  const int mk0 = (int)((((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 4);
-  const int mk = mk0 + (lane >> 3);
+  const int w0 = (int)((((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 4);
+  const int w = w0 + (lane >> 3);
   const Geom& g = a.g;
-  const bool in = mk < a.n;
+  const bool in = w < a.n;
+  const int mk = (in && a.order) ? a.order[w] : w;
   // record rows of this lane, loaded before the key is compared (a miss
   // discards them)
   A u[3][2][4];
@@ -853,7 +920,7 @@ __global__ void __launch_bounds__(256, sizeof(typename S::A) == 4 ? 3 : 2) k_ibm
     const int b = __ffs(todo) - 1;
     todo &= todo - 1;
     double t3[3] = {0.0, 0.0, 0.0};
-    ibm_substep_body<L, S, DELTA, false, HALO>(a, mk0 + (b >> 3), lane, false, nullptr, nullptr, t3);
+    ibm_substep_body<L, S, DELTA, false, HALO>(a, __shfl_sync(kFull, mk, b), lane, false, nullptr, nullptr, t3);
     if (lane == 0) { tot0 += t3[0]; tot1 += t3[1]; tot2 += t3[2]; }
   }
   if (!a.ftot) return;

@@ -414,6 +414,13 @@ int  couplb_status_last(couplb_handle* h, int* clamps, int* nonfinite);
  *                 lies inside the interior and whose stencil is cached, the
  *                 rest one warp each) or 32 (one warp per marker).  The two
  *                 differ only in the order of the interpolation sums.
+ *   "ibm_sort"    refreshes between re-sorts of the order in which the
+ *                 single-pass refresh visits the markers: by bands of 8 z
+ *                 planes of their cell (y rows in 2D), so that markers whose
+ *                 windows share population lines meet them in L2.  Default
+ *                 16; 0 visits them in index order (markers the caller
+ *                 keeps in chain order refresh as fast that way).  Results
+ *                 do not depend on it.
  *   "ibm_block"   threads per block of the grouped (ibm_group 8) sub-step: 64,
  *                 128 (default) or 256; a launch shape, results unchanged up
  *                 to the order of the FP64 total-force sums.

@@ -237,7 +237,7 @@ def test_wrapped_window_matches_oracle(cuda_lib, wall):
         assert rel(a, b) <= 1e-12, (c, rel(a, b))
 
 
-def _grouped_case(prec, group, n=(40, 32, 24), cycles=3, md_per_lb=2, block=None):
+def _grouped_case(prec, group, n=(40, 32, 24), cycles=3, md_per_lb=2, block=None, sort=None):
     """Atom forces per sub-step and the final force field of a walled lattice
     with 300 markers: most windows inside the interior, some at the faces and
     walls; every second marker jumps 0.6 cells in x on each later sub-step
@@ -253,6 +253,8 @@ def _grouped_case(prec, group, n=(40, 32, 24), cycles=3, md_per_lb=2, block=None
     L.set_option("ibm_group", group)
     if block:
         L.set_option("ibm_block", block)
+    if sort is not None:
+        L.set_option("ibm_sort", sort)
     L.set_populations(cases.initial_populations(3, n, 7))
     L.set_ibm_params(delta="peskin4", md_per_lb=md_per_lb, xi_ibm=0.8)
     x = x0.copy()
@@ -299,6 +301,21 @@ def test_grouped_substep_block_size(cuda_lib, block):
         L.set_option("ibm_block", 96)
     assert L.get_option("ibm_block") == 128
     L.close()
+
+
+@pytest.mark.parametrize("sort", [0, 1])
+def test_marker_order(cuda_lib, sort):
+    """Option ibm_sort: the refresh and the grouped sub-step take the markers
+    in cell order, remade every ibm_sort refreshes (default 16; 1: every
+    refresh; 0: index order).  Each marker is still handled once by its own
+    lanes: FP64 atom forces of the first sub-step equal bit for bit, later
+    ones and the force field differ only by the order of the spread sums."""
+    f, F = _grouped_case("fp64", 8, sort=sort)
+    fd, Fd = _grouped_case("fp64", 8)
+    assert np.array_equal(f[0], fd[0])
+    assert rel(f, fd) <= 1e-13, rel(f, fd)
+    for c in range(3):
+        assert rel(F[c], Fd[c]) <= 1e-13, (c, rel(F[c], Fd[c]))
 
 
 def test_grouped_substep_fp64_matches_oracle(cuda_lib):
