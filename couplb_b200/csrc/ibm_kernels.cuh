@@ -108,8 +108,9 @@ struct IbmArgs {
   const typename S::A* vh[2];
   typename S::A* fh[2];
   int zplanes[2];
-  // processing order of k_ibm_prefetch and k_ibm_substep8 (a permutation of
-  // 0..n-1, k_order_*), or null for the index order
+  // order in which k_ibm_prefetch (and k_ibm_substep8, when given one) visit
+  // the markers: a permutation of 0..n-1 (k_order_*), or null for the index
+  // order.  The engine passes it to the refresh only.
   const int* order = nullptr;
 };
 

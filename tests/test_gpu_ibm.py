@@ -305,11 +305,12 @@ def test_grouped_substep_block_size(cuda_lib, block):
 
 @pytest.mark.parametrize("sort", [0, 1])
 def test_marker_order(cuda_lib, sort):
-    """Option ibm_sort: the refresh and the grouped sub-step take the markers
-    in cell order, remade every ibm_sort refreshes (default 16; 1: every
-    refresh; 0: index order).  Each marker is still handled once by its own
-    lanes: FP64 atom forces of the first sub-step equal bit for bit, later
-    ones and the force field differ only by the order of the spread sums."""
+    """Option ibm_sort: the refresh visits the markers by z bands of their
+    cells, the order remade every ibm_sort refreshes (default 16; 1: every
+    refresh; 0: index order).  Each record is still filled once by its
+    marker's own lanes: FP64 atom forces of the first sub-step equal bit for
+    bit, later ones and the force field differ only by the order of the
+    spread sums."""
     f, F = _grouped_case("fp64", 8, sort=sort)
     fd, Fd = _grouped_case("fp64", 8)
     assert np.array_equal(f[0], fd[0])
