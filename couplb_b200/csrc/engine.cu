@@ -212,6 +212,7 @@ int couplb_destroy(couplb_handle* h) {
     if (h->copy_ev[e]) cudaEventDestroy(h->copy_ev[e]);
   for (cudaEvent_t e : h->fout_ev)
     if (e) cudaEventDestroy(e);
+  if (h->h_order_near) cudaFreeHost(h->h_order_near);
   {
     void* p2 = h->d_order; dfree(p2);
     p2 = h->d_order_rank; dfree(p2);

@@ -49,19 +49,34 @@ int make_order(couplb_handle* h, const IbmArgs<S>& a, int n) {
   if (h->order_nb < nb) {
     void* p = h->d_order_count; dfree(p); h->d_order_count = nullptr;
     h->order_nb = 0;
-    int rc = dalloc(h, (void**)&h->d_order_count, sizeof(int) * (size_t)nb);
+    // the band sizes, then the count of markers next to their successor
+    int rc = dalloc(h, (void**)&h->d_order_count, sizeof(int) * ((size_t)nb + 1));
     if (rc) return rc;
     h->order_nb = nb;
   }
-  CK(cudaMemsetAsync(h->d_order_count, 0, sizeof(int) * (size_t)nb, h->stream));
+  if (!h->h_order_near) CK(cudaMallocHost(&h->h_order_near, sizeof(int)));
+  CK(cudaMemsetAsync(h->d_order_count, 0, sizeof(int) * ((size_t)nb + 1), h->stream));
   const unsigned g = (unsigned)((n + 255) / 256);
   k_order_count<L, S><<<g, 256, 0, h->stream>>>(a, nb, h->d_order_count, h->d_order_rank);
   k_order_scan<<<1, 256, 0, h->stream>>>(nb, h->d_order_count);
   k_order_scatter<L, S><<<g, 256, 0, h->stream>>>(a, nb, h->d_order_count, h->d_order_rank, h->d_order);
   CK_LAUNCH();
+  // the scatter's choice, read back now (one wait per sort, every ibm_sort
+  // refreshes): when it kept the index order the refresh is launched
+  // without the order, whose lookup would only lengthen each warp's chain
+  CK(cudaMemcpyAsync(h->h_order_near, h->d_order_count + nb, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->order_identity = 2LL * *h->h_order_near > n ? 1 : 0;
   h->order_n = n;
   h->order_age = 0;
   return COUPLB_OK;
+}
+
+// The order to pass to the refresh: null while none is made, or when the
+// last sort kept the index order.
+inline const int* refresh_order(couplb_handle* h, int n) {
+  if (h->ibm_sort <= 0 || h->order_n != n || h->order_identity != 0) return nullptr;
+  return h->d_order;
 }
 
 // Shared body of the host- and device-array IBM sub-step.  The launches of
@@ -157,7 +172,7 @@ int engine_ibm(couplb_handle* h, int n, const double* d_x, const double* d_v, co
           lrc = make_order<L, S>(h, a, n);
           if (lrc) return;
         }
-        a.order = (h->ibm_sort > 0 && h->order_n == n) ? h->d_order : nullptr;
+        a.order = refresh_order(h, n);
         k_ibm_prefetch<L, S><<<nb, bs, 0, h->stream>>>(a);
         // the sub-steps keep the index order: markers that the caller keeps
         // in chain order (rods, filaments) spread onto shared nodes from one

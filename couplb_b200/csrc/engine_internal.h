@@ -90,6 +90,8 @@ struct couplb_handle {
   int* d_order_count = nullptr;
   int order_cap = 0, order_nb = 0;   // capacity of the two per-marker arrays, buckets
   int order_n = -1, order_age = 0;   // markers the order is for, refreshes since it was made
+  int* h_order_near = nullptr;       // pinned copy of the near-successor count of the last sort
+  int order_identity = -1;           // the last sort kept the index order: 1, else 0
   const void* halo[2] = {nullptr, nullptr};   // z-face halos of a slab decomposition
   const void* ih_vel[2] = {nullptr, nullptr};  // IBM halos of those faces: neighbour moments,
   void* ih_force[2] = {nullptr, nullptr};      // forces spread beyond the face,

@@ -387,11 +387,33 @@ __device__ __forceinline__ int order_bucket(const IbmArgs<S>& a, int mk, int nb)
   return b;
 }
 
+// count[nb] collects the markers whose successor lies within 2 cells on
+// every axis: when that is most of them, the caller already keeps the
+// markers in a spatial or chain order and the scatter keeps the index order.
 template <class L, class S>
 __global__ void k_order_count(const IbmArgs<S> a, int nb, int* __restrict__ count, int* __restrict__ rank) {
   const int mk = blockIdx.x * blockDim.x + threadIdx.x;
-  if (mk >= a.n) return;
-  rank[mk] = atomicAdd(count + order_bucket<L, S>(a, mk, nb), 1);
+  const int lane = threadIdx.x & 31;
+  const bool in = mk < a.n;
+  const int b = in ? order_bucket<L, S>(a, mk, nb) : -1;
+  // one atomic per band and warp (markers in chain order share a few bands,
+  // and same-address atomics queue in L2); ranks follow the lane order
+  const unsigned peers = __match_any_sync(0xffffffffu, b);
+  const int leader = __ffs(peers) - 1;
+  int base = 0;
+  if (in && lane == leader) base = atomicAdd(count + b, __popc(peers));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  bool near = false;
+  if (in) {
+    rank[mk] = base + __popc(peers & ((1u << lane) - 1u));
+    if (mk + 1 < a.n) {
+      near = true;
+#pragma unroll
+      for (int d = 0; d < L::D; d++) near = near && fabs(a.x[3 * (mk + 1) + d] - a.x[3 * mk + d]) * a.inv_dx < 2.0;
+    }
+  }
+  const unsigned nn = __ballot_sync(0xffffffffu, near);
+  if ((threadIdx.x & 31) == 0 && nn) atomicAdd(count + nb, __popc(nn));
 }
 
 // Exclusive prefix sum of the nb bucket sizes, in place; one block of 256.
@@ -426,7 +448,8 @@ __global__ void k_order_scatter(const IbmArgs<S> a, int nb, const int* __restric
                                 const int* __restrict__ rank, int* __restrict__ order) {
   const int mk = blockIdx.x * blockDim.x + threadIdx.x;
   if (mk >= a.n) return;
-  order[start[order_bucket<L, S>(a, mk, nb)] + rank[mk]] = mk;
+  if (2LL * start[nb] > a.n) order[mk] = mk;   // mostly near neighbours: index order
+  else order[start[order_bucket<L, S>(a, mk, nb)] + rank[mk]] = mk;
 }
 
 // Velocity of stencil slot s of marker mk (node (i,j,k) = n).

@@ -417,10 +417,12 @@ int  couplb_status_last(couplb_handle* h, int* clamps, int* nonfinite);
  *   "ibm_sort"    refreshes between re-sorts of the order in which the
  *                 single-pass refresh visits the markers: by bands of 8 z
  *                 planes of their cell (y rows in 2D), so that markers whose
- *                 windows share population lines meet them in L2.  Default
- *                 16; 0 visits them in index order (markers the caller
- *                 keeps in chain order refresh as fast that way).  Results
- *                 do not depend on it.
+ *                 windows share population lines meet them in L2; when most
+ *                 markers lie within 2 cells of their successor (chain or
+ *                 spatially sorted arrays) the index order is kept.  A
+ *                 sort waits for the lattice's stream once to read that
+ *                 choice back.  Default 16; 0 always visits them in index
+ *                 order.  Results do not depend on it.
  *   "ibm_block"   threads per block of the grouped (ibm_group 8) sub-step: 64,
  *                 128 (default) or 256; a launch shape, results unchanged up
  *                 to the order of the FP64 total-force sums.
