@@ -319,6 +319,40 @@ def test_marker_order(cuda_lib, sort):
         assert rel(F[c], Fd[c]) <= 1e-13, (c, rel(F[c], Fd[c]))
 
 
+def _chain_case(sort, n=(40, 32, 24), cycles=3):
+    """200 markers in chain order (0.21 cells apart along a tilted line)."""
+    i = np.arange(200, dtype=np.float64)
+    x0 = np.stack([5.0 + 0.15 * i, 4.0 + 0.12 * i, 3.0 + 0.08 * i], axis=1)
+    v = np.zeros_like(x0)
+    m = np.ones(200)
+    L = Lattice(3, *n, tau=0.7, wall=(0, 0, 1, 1, 0, 0), body_force=True)
+    L.set_option("ibm_sort", sort)
+    L.set_populations(cases.initial_populations(3, n, 5))
+    L.set_ibm_params(delta="peskin4", md_per_lb=2, xi_ibm=0.8)
+    fs = []
+    for c in range(cycles):
+        L.lbm_step((1e-5, 0.0, 0.0))
+        for s in range(2):
+            fa = np.zeros_like(x0)
+            L.ibm_substep(x0, v, m, fa, refresh=(s == 0))
+            fs.append(fa)
+    F = [cases.interior(a, 3) for a in L.get_force_field()]
+    L.close()
+    return np.stack(fs), F
+
+
+def test_marker_order_keeps_chains(cuda_lib):
+    """Markers within 2 cells of their successor (a chain): the sort keeps
+    the index order and the refresh runs without it, so the results match
+    ibm_sort 0."""
+    f, F = _chain_case(1)
+    f0, F0 = _chain_case(0)
+    assert np.array_equal(f[0], f0[0])
+    assert rel(f, f0) <= 1e-13, rel(f, f0)
+    for c in range(3):
+        assert rel(F[c], F0[c]) <= 1e-13
+
+
 def test_grouped_substep_fp64_matches_oracle(cuda_lib):
     """The grouped sub-step (interior markers, record hits and misses,
     inactive atoms, walls) against the oracle: per-atom forces within 1e-11,
